@@ -1,0 +1,412 @@
+"""ctypes bindings for the oracle (TEST INFRASTRUCTURE ONLY).
+
+Loads ``liboracle.so`` (the C restatement of frame-aligner's warper path, fa_oracle.c) and, when
+present, ``_ref/libfa_ref.so`` (the reference's own FrameWarper.cpp, Sobel3d.cpp,
+VolumePhaseCorrelator.cpp and OptimisationModel.cpp compiled unchanged against container
+stand-ins). Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg may import
+this module; it is the checker, never the product path.
+
+Phase correlation (FrameAligner/VolumePhaseCorrelator.cpp:57-166) is restated here with numpy's
+FP64 FFT (pocketfft); window, normalisation, first-maximum argmax and wrap follow the reference
+lines cited in ``phase_shift``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_u16p = np.ctypeslib.ndpointer(np.uint16, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+
+
+class OrScan(C.Structure):
+    _fields_ = [
+        ("line_duration", C.c_double),
+        ("interline_duration", C.c_double),
+        ("pixel_duration", C.c_double),
+        ("frame_duration", C.c_double),
+        ("interframe_duration", C.c_double),
+        ("stack_duration", C.c_double),
+        ("n_x", C.c_int),
+        ("n_y", C.c_int),
+        ("n_z", C.c_int),
+        ("bidirectional", C.c_int),
+    ]
+
+
+class OrStats(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int),
+        ("evaluations", C.c_int),
+        ("accepted", C.c_int),
+        ("f_final", C.c_double),
+        ("radius_final", C.c_double),
+    ]
+
+
+_lib = None
+_ref = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"oracle not built: {path} (run make -C oracle)")
+        L = C.CDLL(path)
+        L.or_scan_init.argtypes = [C.POINTER(OrScan), C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
+                                   C.c_int, C.c_int]
+        L.or_process_scan.argtypes = [C.POINTER(OrScan), C.c_int, C.c_int, C.POINTER(OrScan)]
+        L.or_warper_create.restype = C.c_void_p
+        L.or_warper_create.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(OrScan), C.c_char_p]
+        L.or_warper_destroy.argtypes = [C.c_void_p]
+        L.or_warper_n_dim.argtypes = [C.c_void_p]
+        L.or_warper_precomp.argtypes = [C.c_void_p, _u16p, _f32p, _i32p]
+        L.or_warper_hessian.argtypes = [C.c_void_p, _f64p]
+        L.or_warper_gradient.argtypes = [C.c_void_p, _f32p, _f32p, _f32p]
+        L.or_warp_interpolated.argtypes = [C.c_void_p, _f32p, _f64p, C.c_float, _f32p]
+        L.or_get_error.restype = C.c_double
+        L.or_get_error.argtypes = [C.c_void_p, _f32p, _f64p, _f32p]
+        L.or_get_jacobian.argtypes = [C.c_void_p, _f32p, _f64p]
+        L.or_warp_image.argtypes = [C.c_void_p, _f32p, _f64p, _f32p, _f32p]
+        L.or_warp_point.argtypes = [C.c_void_p, _f64p, C.c_int, C.c_int, C.c_int, C.c_int, _f64p]
+        L.or_sobel3d.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, _f32p, _f32p, _f32p]
+        L.or_downsample.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, _f32p]
+        L.or_correlation.restype = C.c_double
+        L.or_correlation.argtypes = [_f32p, _f32p, _u8p, C.c_long]
+        L.or_tr_subproblem.argtypes = [C.c_int, _f64p, _f64p, C.c_double, C.c_double, C.c_int, _f64p]
+        L.or_align_frame.argtypes = [C.c_void_p, _f32p, _f64p, C.c_int, _f64p, C.POINTER(OrStats)]
+        L.or_align_frames_mt.argtypes = [C.c_void_p, _f32p, C.c_int, _f64p, C.c_int, C.c_int, _f64p, _i32p]
+        _lib = L
+    return _lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "libfa_ref.so"))
+
+
+def reflib():
+    global _ref
+    if _ref is None:
+        path = os.path.join(HERE, "_ref", "libfa_ref.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"reference build missing: {path}")
+        R = C.CDLL(path)
+        R.fr_warper_create.restype = C.c_void_p
+        R.fr_warper_create.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                       C.c_double, C.c_int, C.c_char_p]
+        R.fr_warper_destroy.argtypes = [C.c_void_p]
+        R.fr_n_dim.argtypes = [C.c_void_p]
+        R.fr_set_frame.argtypes = [C.c_void_p, _f32p]
+        R.fr_get_error.restype = C.c_double
+        R.fr_get_error.argtypes = [C.c_void_p, _f64p]
+        R.fr_get_jacobian.argtypes = [C.c_void_p, _f64p, _f64p]
+        R.fr_hessian.argtypes = [C.c_void_p, _f64p]
+        R.fr_model_f.restype = C.c_double
+        R.fr_model_f.argtypes = [C.c_void_p, _f64p]
+        R.fr_precomp.argtypes = [C.c_void_p, _u16p, _f32p, _i32p]
+        R.fr_warp_interpolated.argtypes = [C.c_void_p, _f64p, C.c_int, _f32p]
+        R.fr_warp_image.argtypes = [C.c_void_p, _f64p, _f32p, _f32p]
+        R.fr_warp_point.argtypes = [C.c_void_p, _f64p, C.c_int, C.c_int, C.c_int, C.c_int, _f64p]
+        R.fr_sobel3d.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, _f32p, _f32p, _f32p]
+        R.fr_phase_shift.argtypes = [_f32p, _f32p, C.c_int, C.c_int, C.c_int, _f64p]
+        R.fr_align_frame.argtypes = [C.c_void_p, _f32p, _f64p, C.c_int, _f64p, _i32p]
+        R.fr_mt_create.restype = C.c_void_p
+        R.fr_mt_create.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                   C.c_int, C.c_int, C.c_char_p]
+        R.fr_mt_destroy.argtypes = [C.c_void_p]
+        R.fr_mt_align.argtypes = [C.c_void_p, _f32p, C.c_int, _f64p, C.c_int, _f64p, _i32p]
+        _ref = R
+    return _ref
+
+
+def scan_init(line, interline, interframe, nx, ny, nz, bidirectional=False) -> OrScan:
+    s = OrScan()
+    lib().or_scan_init(C.byref(s), line, interline, interframe, nx, ny, nz, int(bidirectional))
+    return s
+
+
+def _c32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _c64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class OracleWarper:
+    """The restated AbstractFrameWarper/CpuFrameWarper (FrameAligner/FrameWarper.h:95-160)."""
+
+    def __init__(self, reference, nD, scan: OrScan):
+        ref = _c32(reference)
+        assert ref.ndim == 3
+        self.dims = ref.shape
+        self.nD = int(nD)
+        err = C.create_string_buffer(256)
+        self._h = lib().or_warper_create(ref, ref.shape[0], ref.shape[1], ref.shape[2], self.nD, C.byref(scan), err)
+        if not self._h:
+            raise RuntimeError(err.value.decode())
+        self.n_dim = lib().or_warper_n_dim(self._h)
+        self.N = int(np.prod(self.dims))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().or_warper_destroy(self._h)
+            self._h = None
+
+    @property
+    def P(self):
+        return self.nD * self.n_dim
+
+    def precomp(self):
+        Di = np.empty(self.N, np.uint16)
+        Df = np.empty(self.N, np.float32)
+        r = np.empty(2 * self.nD, np.int32)
+        lib().or_warper_precomp(self._h, Di, Df, r)
+        return Di.reshape(self.dims), Df.reshape(self.dims), r.reshape(self.nD, 2)
+
+    def hessian(self):
+        H = np.empty((self.P, self.P), np.float64)
+        lib().or_warper_hessian(self._h, H)
+        return H
+
+    def gradient(self):
+        g = [np.empty(self.N, np.float32) for _ in range(3)]
+        lib().or_warper_gradient(self._h, *g)
+        return [x.reshape(self.dims) for x in g]
+
+    def warp_interpolated(self, frame, D, invalid_value=0.0):
+        out = np.empty(self.N, np.float32)
+        lib().or_warp_interpolated(self._h, _c32(frame).ravel(), _c64(D).ravel(), float(invalid_value), out)
+        return out.reshape(self.dims)
+
+    def get_error(self, frame, D, want_image=False):
+        err = np.empty(self.N, np.float32)
+        f = lib().or_get_error(self._h, _c32(frame).ravel(), _c64(D).ravel(), err)
+        return (f, err.reshape(self.dims)) if want_image else f
+
+    def get_jacobian_from_error(self, err):
+        jac = np.empty(self.P, np.float64)
+        lib().or_get_jacobian(self._h, _c32(err).ravel(), jac)
+        return jac
+
+    def get_jacobian(self, frame, D):
+        _, e = self.get_error(frame, D, want_image=True)
+        return self.get_jacobian_from_error(e)
+
+    def warp_image(self, frame, D):
+        w = np.empty(self.N, np.float32)
+        c = np.empty(self.N, np.float32)
+        lib().or_warp_image(self._h, _c32(frame).ravel(), _c64(D).ravel(), w, c)
+        return w.reshape(self.dims), c.reshape(self.dims)
+
+    def warp_point(self, D, x, y, z, spatial_binning=1):
+        out = np.empty(3, np.float64)
+        lib().or_warp_point(self._h, _c64(D).ravel(), x, y, z, spatial_binning, out)
+        return out
+
+    def align_frame(self, frame, rigid_shift=(0.0, 0.0, 0.0), max_iter=100):
+        D = np.empty((self.nD, 3), np.float64)
+        st = OrStats()
+        lib().or_align_frame(self._h, _c32(frame).ravel(), _c64(rigid_shift), max_iter, D, C.byref(st))
+        return D, st
+
+    def align_frames_mt(self, frames, rigid_shifts, n_threads, max_iter=100):
+        frames = _c32(frames)
+        n = frames.shape[0]
+        D = np.empty((n, self.nD, 3), np.float64)
+        iters = np.empty(n, np.int32)
+        lib().or_align_frames_mt(self._h, frames.ravel(), n, _c64(rigid_shifts).ravel(), max_iter, n_threads, D,
+                                 iters)
+        return D, iters
+
+
+class RefWarper:
+    """The reference's own CpuFrameWarper, built from its sources (oracle/_ref/libfa_ref.so)."""
+
+    def __init__(self, reference, nD, line, interline, interframe, bidirectional=False):
+        ref = _c32(reference)
+        self.dims = ref.shape
+        self.nD = int(nD)
+        err = C.create_string_buffer(256)
+        R = reflib()
+        self._h = R.fr_warper_create(ref, ref.shape[0], ref.shape[1], ref.shape[2], self.nD, line, interline,
+                                     interframe, int(bidirectional), err)
+        if not self._h:
+            raise RuntimeError(err.value.decode())
+        self.n_dim = R.fr_n_dim(self._h)
+        self.N = int(np.prod(self.dims))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            reflib().fr_warper_destroy(self._h)
+            self._h = None
+
+    @property
+    def P(self):
+        return self.nD * self.n_dim
+
+    def set_frame(self, frame):
+        reflib().fr_set_frame(self._h, _c32(frame).ravel())
+
+    def get_error(self, D):
+        return reflib().fr_get_error(self._h, _c64(D).ravel())
+
+    def get_jacobian(self, D):
+        j = np.empty(self.P, np.float64)
+        reflib().fr_get_jacobian(self._h, _c64(D).ravel(), j)
+        return j
+
+    def hessian(self):
+        H = np.empty((self.P, self.P), np.float64)
+        reflib().fr_hessian(self._h, H)
+        return H
+
+    def precomp(self):
+        Di = np.empty(self.N, np.uint16)
+        Df = np.empty(self.N, np.float32)
+        r = np.empty(2 * self.nD, np.int32)
+        reflib().fr_precomp(self._h, Di, Df, r)
+        return Di.reshape(self.dims), Df.reshape(self.dims), r.reshape(self.nD, 2)
+
+    def warp_interpolated(self, D, invalid_value=0):
+        out = np.empty(self.N, np.float32)
+        reflib().fr_warp_interpolated(self._h, _c64(D).ravel(), int(invalid_value), out)
+        return out.reshape(self.dims)
+
+    def warp_image(self, D):
+        w = np.empty(self.N, np.float32)
+        c = np.empty(self.N, np.float32)
+        reflib().fr_warp_image(self._h, _c64(D).ravel(), w, c)
+        return w.reshape(self.dims), c.reshape(self.dims)
+
+    def warp_point(self, D, x, y, z, spatial_binning=1):
+        out = np.empty(3, np.float64)
+        reflib().fr_warp_point(self._h, _c64(D).ravel(), x, y, z, spatial_binning, out)
+        return out
+
+    def align_frame(self, frame, rigid_shift=(0.0, 0.0, 0.0), max_iter=100):
+        D = np.empty((self.nD, 3), np.float64)
+        it = np.zeros(1, np.int32)
+        reflib().fr_align_frame(self._h, _c32(frame).ravel(), _c64(rigid_shift), max_iter, D, it)
+        return D, int(it[0])
+
+
+class RefPool:
+    """One reference warper per worker thread (fr_mt_create / fr_mt_align)."""
+
+    def __init__(self, reference, nD, line, interline, interframe, n_threads, bidirectional=False):
+        ref = _c32(reference)
+        self.dims = ref.shape
+        self.nD = nD
+        err = C.create_string_buffer(256)
+        self._h = reflib().fr_mt_create(ref, ref.shape[0], ref.shape[1], ref.shape[2], nD, line, interline,
+                                        interframe, int(bidirectional), n_threads, err)
+        if not self._h:
+            raise RuntimeError(err.value.decode())
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            reflib().fr_mt_destroy(self._h)
+            self._h = None
+
+    def align(self, frames, rigid_shifts, max_iter=100):
+        frames = _c32(frames)
+        n = frames.shape[0]
+        D = np.empty((n, self.nD, 3), np.float64)
+        iters = np.empty(n, np.int32)
+        reflib().fr_mt_align(self._h, frames.ravel(), n, _c64(rigid_shifts).ravel(), max_iter, D, iters)
+        return D, iters
+
+
+def ref_sobel3d(m):
+    m = _c32(m)
+    out = [np.empty(m.size, np.float32) for _ in range(3)]
+    reflib().fr_sobel3d(m.ravel(), m.shape[0], m.shape[1], m.shape[2], *out)
+    return [o.reshape(m.shape) for o in out]
+
+
+def ref_phase_shift(ref, vol):
+    ref = _c32(ref)
+    s = np.empty(3, np.float64)
+    reflib().fr_phase_shift(ref.ravel(), _c32(vol).ravel(), ref.shape[0], ref.shape[1], ref.shape[2], s)
+    return s
+
+
+def sobel3d(m):
+    m = _c32(m)
+    out = [np.empty(m.size, np.float32) for _ in range(3)]
+    lib().or_sobel3d(m.ravel(), m.shape[0], m.shape[1], m.shape[2], *out)
+    return [o.reshape(m.shape) for o in out]
+
+
+def downsample(vol, factor):
+    v = _c32(vol)
+    nz, ny, nx = v.shape
+    nh = -(-ny // factor)
+    nw = -(-nx // factor)
+    out = np.empty(nz * nh * nw, np.float32)
+    lib().or_downsample(v.ravel(), nz, ny, nx, factor, out)
+    return out.reshape(nz, nh, nw)
+
+
+def correlation(a, b, mask):
+    a = _c32(a).ravel()
+    return lib().or_correlation(a, _c32(b).ravel(), np.ascontiguousarray(mask, np.uint8).ravel(), a.size)
+
+
+def tr_subproblem(H, g, radius, eps=0.1, max_iter=20):
+    H = _c64(H)
+    p = np.empty(H.shape[0], np.float64)
+    b = lib().or_tr_subproblem(H.shape[0], H, _c64(g), radius, eps, max_iter, p)
+    return p, bool(b)
+
+
+def hann(n):
+    """VolumePhaseCorrelator::hann, VolumePhaseCorrelator.cpp:155-166 (square-root Hann)."""
+    w = np.ones(n, np.float64)
+    if n > 1:
+        f = 2.0 * 3.14159265358979323846 / (n - 1)
+        w = np.sqrt(0.5 * (1 - np.cos(f * np.arange(n))))
+    return w
+
+
+def phase_window(nz, ny, nx):
+    """VolumePhaseCorrelator::computeWindow, VolumePhaseCorrelator.cpp:141-153 (1 along z)."""
+    return (np.ones(nz)[:, None, None] * hann(ny)[None, :, None] * hann(nx)[None, None, :])
+
+
+def phase_correlation_surface(ref, vol):
+    """Steps 1-4 of VolumePhaseCorrelator::computeShift (VolumePhaseCorrelator.cpp:57-78)."""
+    ref = np.asarray(ref, np.float32).astype(np.float64)
+    vol = np.asarray(vol, np.float32).astype(np.float64)
+    w = phase_window(*ref.shape)
+    R = np.conj(np.fft.rfftn(ref * w))
+    X = np.fft.rfftn(vol * w)
+    prod = X * R
+    prod = prod / (np.abs(prod) + np.finfo(np.float64).tiny)
+    return np.fft.irfftn(prod, s=ref.shape, axes=(0, 1, 2)) * ref.size  # unnormalised like FFTW c2r
+
+
+def phase_shift(ref, vol):
+    """Integer shift (x, y, z): first maximum, wrapped at > n/2 (VolumePhaseCorrelator.cpp:81-103)."""
+    surf = phase_correlation_surface(ref, vol)
+    nz, ny, nx = surf.shape
+    idx = int(np.argmax(surf.ravel()))  # numpy returns the first maximum
+    x = idx % nx
+    y = (idx // nx) % ny
+    z = idx // (nx * ny)
+    if x > nx // 2:
+        x -= nx
+    if y > ny // 2:
+        y -= ny
+    if z > nz // 2:
+        z -= nz
+    return np.array([x, y, z], np.float64)

@@ -1,0 +1,124 @@
+"""Pins the CPU oracle (oracle/fa_oracle.c) to the reference.
+
+Against the committed golden fixtures (outputs of the reference's own FrameWarper.cpp, Sobel3d.cpp,
+VolumePhaseCorrelator.cpp and OptimisationModel.cpp, see tests/golden/make_golden.py) every
+quantity must be bit-identical. When oracle/_ref/libfa_ref.so is present the same comparison also
+runs live on further seeded cases.
+"""
+import numpy as np
+import pytest
+
+import fa_synth as S
+import oracle_py as O
+from conftest import load_golden
+
+
+def _warper(g):
+    ref = g["reference"]
+    nz, ny, nx = ref.shape
+    line, interline, interframe = g["scan"]
+    sc = O.scan_init(line, interline, interframe, nx, ny, nz, bool(g["bidirectional"]))
+    return O.OracleWarper(ref, int(g["nD"]), sc)
+
+
+def test_precompute_tables(golden):
+    name, g = golden
+    Di, Df, ranges = _warper(g).precomp()
+    assert np.array_equal(Di, g["Di"])
+    assert np.array_equal(Df, g["Df"])
+    # The last D_range entry is never set by the reference (value-initialised to {0, 0}).
+    assert np.array_equal(ranges, g["ranges"])
+
+
+def test_sobel_gradient(golden):
+    _, g = golden
+    gx, gy, gz = O.sobel3d(g["reference"])
+    assert np.array_equal(gx, g["gx"]) and np.array_equal(gy, g["gy"]) and np.array_equal(gz, g["gz"])
+    wx, wy, wz = _warper(g).gradient()
+    assert np.array_equal(wx, g["gx"]) and np.array_equal(wy, g["gy"])
+
+
+def test_hessian(golden):
+    _, g = golden
+    H = _warper(g).hessian()
+    assert np.array_equal(H, g["H"])
+    assert np.array_equal(H, H.T)
+
+
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_error_jacobian_and_warps(golden, tag):
+    _, g = golden
+    w = _warper(g)
+    D = g[f"D_{tag}"]
+    f, err = w.get_error(g["frame"], D, want_image=True)
+    assert f == g[f"f_{tag}"]
+    assert np.array_equal(w.get_jacobian_from_error(err), g[f"jac_{tag}"])
+    assert np.array_equal(w.warp_interpolated(g["frame"], D, 0), g[f"warp0_{tag}"])
+    assert np.array_equal(w.warp_interpolated(g["frame"], D, -1), g[f"warpm1_{tag}"])
+    wimg, cov = w.warp_image(g["frame"], D)
+    assert np.array_equal(wimg, g[f"splat_{tag}"]) and np.array_equal(cov, g[f"coverage_{tag}"])
+
+
+def test_warp_point(golden):
+    _, g = golden
+    w = _warper(g)
+    for p, want in zip(g["warp_point_xyz"], g["warp_point"]):
+        assert np.array_equal(w.warp_point(g["D_b"], *[int(v) for v in p]), want)
+
+
+def test_phase_shift(golden):
+    _, g = golden
+    assert np.array_equal(O.phase_shift(g["raw_reference"], g["raw_frame"]), g["phase_shift"])
+
+
+def test_phase_shift_known_cases():
+    d = load_golden("phase_shifts")
+    keys = [k[len("shift_"):] for k in d if k.startswith("shift_")]
+    assert len(keys) >= 12
+    for k in keys:
+        assert np.array_equal(O.phase_shift(d[f"ref_{k}"], d[f"vol_{k}"]), d[f"shift_{k}"]), k
+
+
+def test_full_solve(golden):
+    _, g = golden
+    D, st = _warper(g).align_frame(g["frame"], g["phase_shift"], max_iter=100)
+    assert np.array_equal(D, g["D_solve"])
+    assert st.iterations == int(g["solve_iterations"])
+
+
+def test_scan_init_matches_reference_constructor():
+    s = O.scan_init(100.0, 50.0, 102.0, 0, 7, 3)  # interline < line -> 1.01 * line; n_x clamped to 1
+    assert s.interline_duration == 1.01 * 100.0
+    assert s.n_x == 1 and s.pixel_duration == 100.0
+    assert s.frame_duration == 7 * 101.0
+    assert s.stack_duration == 2 * 102.0 + 7 * 101.0
+
+
+def test_last_interval_check_throws():
+    # More control intervals than the scan can reach: the last voxel falls short of interval nD-2
+    # and the reference throws "Something went wrong" (FrameWarper.cpp:280-281).
+    ref = np.ones((3, 8, 8), np.float32)
+    sc = O.scan_init(1.0, 1.01, 8 * 1.01, 8, 8, 3)
+    with pytest.raises(RuntimeError, match="Something went wrong"):
+        O.OracleWarper(ref, 500, sc)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference build not present")
+@pytest.mark.parametrize("seed", [101, 202, 303])
+def test_live_against_reference_build(seed):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    nz = int(rng.integers(1, 4))
+    ny, nx = int(rng.integers(10, 40)), int(rng.integers(10, 40))
+    nD = int(rng.integers(2, 5)) * nz + 1
+    acq = S.make_acquisition((nz, ny, nx), nD, 1, S.BlobSpec(8, (1.5, 4.0), (1.0, 2.0)),
+                             S.WalkSpec(0.8, 2.0, 0.2, 0.6), seed=seed)
+    line, il, ifr = acq.scan
+    ref, fr = acq.reference + 1, acq.frames[0] + 1
+    ow = O.OracleWarper(ref, nD, O.scan_init(line, il, ifr, nx, ny, nz))
+    rw = O.RefWarper(ref, nD, line, il, ifr)
+    rw.set_frame(fr)
+    D = acq.D_true[0] + rng.normal(0, 0.5, acq.D_true[0].shape) * (np.array([1, 1, 1 if nz > 1 else 0]))
+    assert ow.get_error(fr, D) == rw.get_error(D)
+    assert np.array_equal(ow.get_jacobian(fr, D), rw.get_jacobian(D))
+    assert np.array_equal(ow.hessian(), rw.hessian())
+    assert np.array_equal(ow.warp_interpolated(fr, D, 0), rw.warp_interpolated(D, 0))
