@@ -1,0 +1,337 @@
+#!/usr/bin/env python3
+"""Benchmark of the frame-aligner non-rigid registration path on B200.
+
+Workload: the 512x512x16 z-stack with nD = 32 control points and three displacement components,
+50 frames per step (seeded synthetic acquisition: blob reference, random-walk displacement,
+Poisson noise; see frame-aligner_b200/fa_synth.py). One step = FrameWarpAligner::addFrame for all
+50 frames: +1 offset, phase-correlation rigid start (cuFFT FP64 + hand-written normalise / argmax),
+starting-point choice and the trust-region solve, batched (one fused warp + error + J^T e pass and
+one solve launch per iteration, captured in a CUDA graph).
+
+  value  frames aligned per second with the frames already in HBM (device timing: CUDA events
+         on the library's streams, summed over the K timed steps; max over ranks)
+  e2e    the same through fa_aligner_add_frames with raw uint16 frames in pinned host memory,
+         host->device copies and the D readback inside the timed region (wall clock)
+
+Extra keys: `plain_fp32` (the FP32 single-frame path, host-driven iterations, one frame at a time),
+`roofline` (the fused evaluation kernel against the measured HBM copy bandwidth), `cpu_baseline`
+(the reference's CPU warper, compiled from its own sources, on a bounded sample), `clocks`.
+
+--impl reference times the reference CPU path on this host's cores (rank 0 only).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "frame-aligner_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import fa_synth as S  # noqa: E402
+
+METRIC = "aligned frames/s (512x512x16, nD=32)"
+UNIT = "frames/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--frames", type=int, default=50)
+    ap.add_argument("--plain-frames", type=int, default=8)
+    ap.add_argument("--cpu-frames", type=int, default=0, help="CPU baseline sample size (0 = one per thread)")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def config_dict(n_frames, world):
+    return {"workload": "z-stack 512x512x16, nD=32, 3 displacement components, %d frames per GPU per step" % n_frames,
+            "volume": [16, 512, 512], "nD": 32, "frames_per_step": n_frames, "precision": "bf16 ref/grad, fp16 frames, fp32 sums, fp64 solve",
+            "parallelism": "frames sharded over %d GPU(s), no collective on the data path" % world,
+            "l2": "inputs exceed L2: %d frames x 8.4 MB fp16 + 33.6 MB reference/gradient per step" % n_frames}
+
+
+def make_data(n_frames, rank):
+    cfg = dict(S.CONFIG1)
+    cfg["seed"] = S.CONFIG1["seed"] + 7919 * rank
+    return S.make_config(cfg, n_frames=n_frames)
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for i, n in enumerate(names):
+                if len(r) > 5 + i and r[5 + i].lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def cpu_baseline(acq, n_threads, n_frames):
+    """The reference CPU warper (oracle/_ref, compiled from the reference's FrameWarper.cpp et al.)
+    driving the trust-region solve, one frame per worker thread (FrameAlignerMex.cpp:24-25,120);
+    falls back to the C restatement if the reference build is absent. Rigid shifts are computed
+    before the timed region (numpy FP64 FFT), so the sample times the non-rigid solve only."""
+    import oracle_py as O
+
+    nz, ny, nx = acq.reference.shape
+    line, il, ifr = acq.scan
+    frames = acq.frames[:n_frames] + 1
+    shifts = np.array([O.phase_shift(acq.reference, acq.frames[k]) for k in range(n_frames)])
+    if O.ref_available():
+        pool = O.RefPool(acq.reference + 1, acq.nD, line, il, ifr, n_threads)
+        t0 = time.perf_counter()
+        D, iters = pool.align(frames, shifts, 100)
+        dt = time.perf_counter() - t0
+        kind = "reference"
+    else:
+        ow = O.OracleWarper(acq.reference + 1, acq.nD, O.scan_init(line, il, ifr, nx, ny, nz))
+        t0 = time.perf_counter()
+        D, iters = ow.align_frames_mt(frames, shifts, n_threads, 100)
+        dt = time.perf_counter() - t0
+        kind = "port"
+    return {"value": n_frames / dt, "unit": UNIT, "cores": n_threads, "kind": kind,
+            "sample": "%d frames of the 512x512x16 nD=32 workload, non-rigid solve only (rigid shifts "
+                      "precomputed), %.1f s, %d threads" % (n_frames, dt, n_threads)}, D, shifts
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    n_threads = os.cpu_count() or 1
+    n = args.cpu_frames or n_threads
+    acq = make_data(n, 0)
+    times = []
+    for step in range(args.warmup + args.steps):
+        cb, _, _ = cpu_baseline(acq, n_threads, n)
+        if step >= args.warmup:
+            times.append(n / cb["value"])
+    total = sum(times)
+    value = n * args.steps / total
+    cb["value"] = value
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic (seeded blob acquisition)",
+            "config": config_dict(n, 1), "impl": "reference", "cpu_baseline": cb,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args, rank, world, local):
+    import fa_b200 as fa
+
+    pg = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        pg = dist
+    n = args.frames
+    acq = make_data(n, rank)
+    nz, ny, nx = acq.reference.shape
+    line, il, ifr = acq.scan
+    scan = fa.scan_params(line, il, ifr, nx, ny, nz)
+    ctx = fa.Context(device=local)
+    al = fa.Aligner(ctx, nD=acq.nD, precision=fa.PREC_MIXED, max_iterations=100)
+    al.set_reference(acq.reference, scan)
+    raw_u16 = np.ascontiguousarray(acq.frames.astype(np.uint16))
+    N = nz * ny * nx
+
+    import torch
+
+    dev_frames = torch.from_numpy(raw_u16.view(np.int16)).to(f"cuda:{local}")  # raw counts, resident in HBM
+    ptrs = [dev_frames[i].data_ptr() for i in range(n)]
+    pinned = torch.from_numpy(raw_u16.view(np.int16)).pin_memory()
+    host_ptrs = [pinned[i].data_ptr() for i in range(n)]
+
+    def barrier():
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+
+    def max_over_ranks(x):
+        if not pg:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up (untimed)
+    for _ in range(args.warmup):
+        D, stats = al.add_frames_device(ptrs, fa.U16, n)
+    barrier()
+    launches0 = fa.kernel_launches()
+    dev_ms = 0.0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            D, stats = al.add_frames_device(ptrs, fa.U16, n)
+            dev_ms += al.last_device_ms()
+        barrier()
+    launches = fa.kernel_launches() - launches0
+    dev_ms = max_over_ranks(dev_ms)
+    value = n * world * args.steps / (dev_ms / 1000.0)
+    iters = [s["iterations"] for s in stats]
+
+    # end to end: raw uint16 frames from pinned host memory through the public API
+    class HostFrames:
+        pass
+
+    import ctypes as C
+
+    arr = (C.c_void_p * n)(*host_ptrs)
+    Dh = np.empty((n, acq.nD, 3), np.float64)
+    st = (fa.AlignStats * n)()
+    for _ in range(max(1, args.warmup // 2)):
+        fa.check(fa.lib().fa_aligner_add_frames(al._h, C.cast(arr, C.c_void_p), fa.U16, n, Dh, C.cast(st, C.c_void_p)))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        fa.check(fa.lib().fa_aligner_add_frames(al._h, C.cast(arr, C.c_void_p), fa.U16, n, Dh, C.cast(st, C.c_void_p)))
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e = {"value": n * world * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(n * N * 2),
+           "d2h_bytes_per_step": int(n * acq.nD * 3 * 8 + n * C.sizeof(fa.AlignStats))}
+
+    out = None
+    if rank == 0:
+        # roofline of the fused evaluation kernel: algorithmic bytes per launch / event-timed duration
+        ref_m = fa.Reference(ctx, acq.reference + 1, acq.nD, scan, fa.PREC_MIXED)
+        frs = [fa.Frame(ref_m, (acq.frames[k] + 1).astype(np.float16)) for k in range(n)]
+        ms = fa.profile_eval(frs, acq.D_true[0], 20)
+        bytes_per_voxel = 2 + 2 + 3 * 2  # fp16 frame + bf16 reference + 3 bf16 gradient planes
+        algo_bytes = n * N * bytes_per_voxel
+        achieved = algo_bytes / (ms / 1000.0) / 1e9
+        peak, peak_kind = load_peaks()
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "eval_traffic.json")
+        if os.path.exists(tp):
+            t = json.load(open(tp))
+            traffic = t.get("dram_bytes_per_frame_eval", 0) * n or None
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": traffic, "kernel": "eval_kernel<3, half, bf16> (fused warp+error+J^T e)",
+                    "algorithmic_bytes_per_launch": algo_bytes, "ms_per_launch": ms,
+                    "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind if peak_kind == "measured" else "fallback 6.65 TB/s"}
+        for f in frs:
+            f.close()
+        ref_m.close()
+        # plain FP32 single-frame path: one frame at a time, host-driven iterations
+        ref32 = fa.Reference(ctx, acq.reference + 1, acq.nD, scan, fa.PREC_F32)
+        corr = fa.Correlator(ctx, acq.reference)
+        pf = min(args.plain_frames, n)
+        fr32 = fa.Frame(ref32, acq.frames[0] + 1)
+        fr32.align(corr.compute_shift(acq.frames[0]), 100)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for k in range(pf):
+            fr32.update(acq.frames[k] + 1)
+            fr32.align(corr.compute_shift(acq.frames[k]), 100)
+        plain_fps = pf / (time.perf_counter() - t0)
+        fr32.close()
+        corr.close()
+        ref32.close()
+        cb = None
+        D_cpu = None
+        if not args.no_cpu:
+            try:
+                nt = os.cpu_count() or 1
+                cb, D_cpu, _ = cpu_baseline(acq, nt, args.cpu_frames or min(nt, n))
+            except Exception as ex:  # the baseline is reported, never required
+                cb = {"value": None, "unit": UNIT, "cores": 0, "kind": "unavailable", "sample": str(ex)[:200]}
+        rms_vs_cpu = None
+        if D_cpu is not None:
+            k = D_cpu.shape[0]
+            rms_vs_cpu = float(np.sqrt(((D[:k] - D_cpu) ** 2).sum(-1).mean()))
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "bf16/fp16 storage, f32 accumulate, f64 solve",
+               "data": "synthetic (seeded blob acquisition, Poisson noise)", "config": config_dict(n, world),
+               "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cb,
+               "clocks": clk.summary(),
+               "plain_fp32": {"value": plain_fps, "unit": UNIT, "frames": pf,
+                              "note": "FP32 single-frame path, host-driven trust-region iterations"},
+               "batched_over_plain": value / world / plain_fps,
+               "displacement_rms_vs_cpu_px": rms_vs_cpu,
+               "iterations": {"mean": float(np.mean(iters)), "max": int(np.max(iters))}}
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    if out:
+        print(json.dumps(out))
+    return 0
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    return run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

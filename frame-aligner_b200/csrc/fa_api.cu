@@ -1,0 +1,1403 @@
+// fa_api.cu -- host runtime behind the C ABI (include/fa_b200.h): device memory under a budget,
+// reference set-up (exact scan geometry, Sobel, Hessian), frame slots, fused evaluations, the
+// single-frame and batched trust-region drivers, and the phase correlator.
+#include <cufft.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "fa_kernels.cuh"
+
+using fa::Job;
+using fa::RefDev;
+using fa::RowDesc;
+
+namespace {
+
+thread_local std::string g_err;
+std::atomic<long long> g_launches{0};
+
+fa_status fail(fa_status s, const std::string& msg) {
+  g_err = msg;
+  return s;
+}
+
+#define FA_CU(call)                                                                             \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess) return fail(FA_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define FA_TRY(call)                  \
+  do {                                \
+    fa_status s_ = (call);            \
+    if (s_ != FA_OK) return s_;       \
+  } while (0)
+
+struct Alloc {
+  void* p;
+  size_t n;
+};
+
+}  // namespace
+
+struct fa_context {
+  int device = 0;
+  size_t budget = 0;
+  std::atomic<size_t> used{0};
+  std::mutex mu;
+};
+
+namespace {
+
+fa_status dalloc(fa_context* ctx, size_t bytes, void** out, std::vector<Alloc>& owner) {
+  if (bytes == 0) bytes = 16;
+  size_t prev = ctx->used.fetch_add(bytes);
+  if (ctx->budget && prev + bytes > ctx->budget) {
+    ctx->used.fetch_sub(bytes);
+    return fail(FA_ERR_OOM, "memory budget exhausted (" + std::to_string(prev + bytes) + " > " +
+                                std::to_string(ctx->budget) + " bytes)");
+  }
+  cudaError_t e = cudaMalloc(out, bytes);
+  if (e != cudaSuccess) {
+    ctx->used.fetch_sub(bytes);
+    cudaGetLastError();
+    return fail(e == cudaErrorMemoryAllocation ? FA_ERR_OOM : FA_ERR_CUDA,
+                std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  owner.push_back({*out, bytes});
+  return FA_OK;
+}
+
+template <typename T>
+fa_status dalloc_t(fa_context* ctx, size_t count, T** out, std::vector<Alloc>& owner) {
+  void* p = nullptr;
+  FA_TRY(dalloc(ctx, count * sizeof(T), &p, owner));
+  *out = static_cast<T*>(p);
+  return FA_OK;
+}
+
+void dfree_all(fa_context* ctx, std::vector<Alloc>& owner) {
+  for (auto& a : owner) {
+    cudaFree(a.p);
+    ctx->used.fetch_sub(a.n);
+  }
+  owner.clear();
+}
+
+// ImageScanParameters fields after AbstractFrameWarper::processScanParameters
+// (FrameWarper.cpp:223-236).
+fa_scan_params process_scan(const fa_scan_params& in, int nz, int nD) {
+  fa_scan_params out = in;
+  double frame_interval_max = nz * in.frame_duration / (nD - nz);
+  if ((in.interframe_duration - in.frame_duration) > frame_interval_max) {
+    out.interframe_duration = out.frame_duration + frame_interval_max;
+    out.stack_duration = (nz - 1) * out.interframe_duration + out.frame_duration;
+  }
+  return out;
+}
+
+// Exact scan geometry, computed on the host in double with the reference's expressions
+// (FrameWarper.cpp:252-283), without per-voxel tables.
+struct Geometry {
+  int nz, ny, nx, nD, n_rows;
+  long long N;
+  std::vector<long long> scan_begin;  // first scan index of interval k (k = 0..nD-2)
+  std::vector<int> begin, end;        // storage D_range
+  std::vector<RowDesc> rows;
+  float dq;
+  int tile_rows, n_tiles;
+  std::vector<int> tile_c0;
+  std::vector<int2> ctrl_tiles;
+};
+
+struct ScanEval {
+  fa_scan_params p;
+  int ny, nx, nD;
+  double q(long long s) const {
+    const long long plane = (long long)ny * nx;
+    int z = (int)(s / plane);
+    int y = (int)((s / nx) % ny);
+    int x = (int)(s % nx);
+    double t = z * p.interframe_duration + y * p.interline_duration + x * p.pixel_duration;
+    return t / p.stack_duration * (nD - 1);
+  }
+  int i(long long s) const {
+    double ip;
+    modf(q(s), &ip);
+    return (int)ip;
+  }
+};
+
+fa_status build_geometry(const fa_scan_params& scan, int nz, int ny, int nx, int nD, int target_tile_voxels,
+                         Geometry& G) {
+  if (nx < 2 || ny < 2 || nz < 1 || nD < 2)
+    return fail(FA_ERR_BAD_ARG, "need nx >= 2, ny >= 2, nz >= 1 and nD >= 2 (the Sobel edge filters read two "
+                                "samples per axis)");
+  const long long N = (long long)nz * ny * nx;
+  if (N >= (1LL << 31)) return fail(FA_ERR_UNSUPPORTED, "volume larger than 2^31 voxels");
+  const fa_scan_params p = process_scan(scan, nz, nD);
+  if (!(p.pixel_duration > 0) || !(p.stack_duration > 0) || !std::isfinite(p.stack_duration) ||
+      !std::isfinite(p.interframe_duration) || !std::isfinite(p.interline_duration))
+    return fail(FA_ERR_BAD_ARG, "scan durations must be finite and positive");
+  ScanEval S{p, ny, nx, nD};
+  G.nz = nz;
+  G.ny = ny;
+  G.nx = nx;
+  G.nD = nD;
+  G.N = N;
+  G.n_rows = nz * ny;
+  // The scan time must increase along the scan so that interval boundaries are single points.
+  for (int r = 0; r + 1 < G.n_rows; r++)
+    if (S.q((long long)r * nx + nx - 1) > S.q((long long)(r + 1) * nx))
+      return fail(FA_ERR_UNSUPPORTED, "scan time decreases between lines or planes (interframe or interline "
+                                      "duration shorter than the line/frame it follows)");
+  if ((long long)S.i(N - 1) != (long long)nD - 2) return fail(FA_ERR_BAD_ARG, "Something went wrong");
+  G.scan_begin.assign(nD - 1, 0);
+  for (int k = 1; k <= nD - 2; k++) {
+    long long lo = G.scan_begin[k - 1], hi = N - 1;
+    while (lo < hi) {
+      long long mid = lo + (hi - lo) / 2;
+      if (S.i(mid) >= k)
+        hi = mid;
+      else
+        lo = mid + 1;
+    }
+    if (S.i(lo) != k) return fail(FA_ERR_UNSUPPORTED, "a control interval is skipped by the scan");
+    G.scan_begin[k] = lo;
+  }
+  auto storage_of = [&](long long s) {
+    long long row = s / nx;
+    int xs = (int)(s % nx);
+    int y = (int)(row % ny);
+    int xt = (scan.bidirectional && (y % 2 == 1)) ? nx - 1 - xs : xs;
+    return row * nx + xt;
+  };
+  G.begin.assign(nD, 0);
+  G.end.assign(nD, 0);
+  for (int k = 0; k <= nD - 2; k++) G.begin[k] = (int)storage_of(G.scan_begin[k]);
+  for (int k = 1; k <= nD - 2; k++)
+    if (G.begin[k] <= G.begin[k - 1])
+      return fail(FA_ERR_UNSUPPORTED, "bidirectional ranges are not increasing in storage order");
+  for (int k = 0; k < nD - 2; k++) G.end[k] = G.begin[k + 1] - 1;
+  G.end[nD - 2] = (int)(N - 1);
+  long long lmin = N;
+  for (int k = 0; k <= nD - 2; k++) {
+    lmin = std::min<long long>(lmin, (long long)G.end[k] - G.begin[k] + 1);
+    long long send = (k < nD - 2) ? G.scan_begin[k + 1] : N;
+    lmin = std::min<long long>(lmin, send - G.scan_begin[k]);
+  }
+  if (lmin < nx)
+    return fail(FA_ERR_UNSUPPORTED, "a control interval is shorter than one image row (" + std::to_string(lmin) +
+                                        " < " + std::to_string(nx) + " voxels)");
+  G.dq = (float)(p.pixel_duration / p.stack_duration * (nD - 1));
+  G.rows.resize(G.n_rows);
+  int r0 = 0;
+  for (int row = 0; row < G.n_rows; row++) {
+    RowDesc d{};
+    const long long s0 = (long long)row * nx;
+    d.di0 = S.i(s0);
+    d.qbase = (float)(S.q(s0) - d.di0);
+    d.xdi = nx;
+    if (d.di0 + 1 <= nD - 2 && G.scan_begin[d.di0 + 1] < s0 + nx) d.xdi = (int)(G.scan_begin[d.di0 + 1] - s0);
+    while (r0 + 1 <= nD - 2 && G.begin[r0 + 1] <= s0) r0++;
+    d.r0 = r0;
+    d.xr = nx;
+    if (r0 + 1 <= nD - 2 && G.begin[r0 + 1] < s0 + nx) d.xr = (int)(G.begin[r0 + 1] - s0);
+    d.xlast = -1;
+    const long long e = G.end[r0];
+    if (e >= s0 && e < s0 + nx) d.xlast = (int)(e - s0);
+    G.rows[row] = d;
+  }
+  int tr = std::max(1, target_tile_voxels / nx);
+  tr = (int)std::min<long long>(tr, std::max<long long>(1, lmin / nx));
+  G.tile_rows = tr;
+  G.n_tiles = (G.n_rows + tr - 1) / tr;
+  G.tile_c0.resize(G.n_tiles);
+  for (int t = 0; t < G.n_tiles; t++) G.tile_c0[t] = G.rows[(size_t)t * tr].r0;
+  G.ctrl_tiles.resize(nD);
+  for (int c = 0; c < nD; c++) {
+    int a = (int)(std::lower_bound(G.tile_c0.begin(), G.tile_c0.end(), c - 2) - G.tile_c0.begin());
+    int b = (int)(std::upper_bound(G.tile_c0.begin(), G.tile_c0.end(), c) - G.tile_c0.begin());
+    G.ctrl_tiles[c] = make_int2(a, b);
+  }
+  return FA_OK;
+}
+
+// Control-point parameters of the fused pass from a host displacement set (see kDParamF4).
+void make_dparams(const double* D, int nD, int n_dim, float4* out) {
+  for (int k = 0; k < nD; k++) {
+    double d[3], dn[3];
+    for (int c = 0; c < 3; c++) {
+      d[c] = c < n_dim ? D[3 * k + c] : 0.0;
+      dn[c] = (c < n_dim && k + 1 < nD) ? D[3 * (k + 1) + c] : d[c];
+    }
+    const double f0 = std::floor(d[0]), f1 = std::floor(d[1]), f2 = std::floor(d[2]);
+    out[3 * k + 0] = make_float4((float)f0, (float)f1, (float)f2, 0.f);
+    out[3 * k + 1] = make_float4((float)(d[0] - f0), (float)(d[1] - f1), (float)(d[2] - f2), 0.f);
+    out[3 * k + 2] = make_float4((float)(dn[0] - d[0]), (float)(dn[1] - d[1]), (float)(dn[2] - d[2]), 0.f);
+  }
+}
+
+bool finite_all(const double* v, size_t n) {
+  for (size_t i = 0; i < n; i++)
+    if (!std::isfinite(v[i])) return false;
+  return true;
+}
+
+}  // namespace
+
+struct fa_reference {
+  fa_context* ctx = nullptr;
+  int nz = 0, ny = 0, nx = 0, nD = 0, n_dim = 0, P = 0;
+  long long N = 0;
+  fa_precision prec = FA_PREC_F32;
+  fa_scan_params scan{};
+  Geometry G;
+  std::vector<double> H;  // dense P x P
+  RefDev host{};
+  RefDev* dev = nullptr;
+  cudaStream_t stream = nullptr;
+  std::vector<Alloc> allocs;
+  std::atomic<int> n_frames{0};
+};
+
+struct fa_frame {
+  fa_reference* ref = nullptr;
+  void* data = nullptr;
+  bool half = false;
+  cudaStream_t stream = nullptr;
+  Job job{};
+  Job* job_dev = nullptr;
+  fa::FrameState* state = nullptr;
+  double* h_result = nullptr;  // pinned: [f, g(P)]
+  float4* h_dparams = nullptr;  // pinned: nD * 3
+  double* h_x = nullptr;        // pinned: P
+  fa::FrameState* h_state = nullptr;  // pinned
+  float* warp_out = nullptr;
+  std::vector<double> lastD;
+  std::vector<double> last_g;
+  double last_f = 0;
+  bool have_last = false;
+  std::mutex mu;
+  std::vector<Alloc> allocs;
+};
+
+struct fa_correlator {
+  fa_context* ctx = nullptr;
+  int nz = 0, ny = 0, nx = 0;
+  long long n_el = 0, n_complex = 0;
+  cufftHandle fwd = 0, inv = 0;
+  cudaStream_t stream = nullptr;
+  double* window = nullptr;
+  double* real = nullptr;
+  double2* spec = nullptr;
+  double2* ref_conj = nullptr;
+  float* vol = nullptr;
+  double* bval = nullptr;
+  long long* bidx = nullptr;
+  long long* d_idx = nullptr;
+  long long* h_idx = nullptr;
+  int n_blocks = 0;
+  std::mutex mu;
+  std::vector<Alloc> allocs;
+};
+
+// ================================================================== context ========================
+
+extern "C" const char* fa_last_error(void) { return g_err.c_str(); }
+
+extern "C" const char* fa_status_string(fa_status s) {
+  switch (s) {
+    case FA_OK: return "ok";
+    case FA_ERR_BAD_ARG: return "bad argument";
+    case FA_ERR_OOM: return "out of memory";
+    case FA_ERR_CUDA: return "CUDA error";
+    case FA_ERR_TIMEOUT: return "timeout";
+    case FA_ERR_UNSUPPORTED: return "unsupported";
+    case FA_ERR_NOT_FOUND: return "not found";
+    case FA_ERR_STATE: return "bad state";
+    case FA_ERR_BUSY: return "busy";
+  }
+  return "unknown";
+}
+
+extern "C" fa_status fa_gpu_support(int* supported, char* message, size_t message_len) {
+  if (!supported) return fail(FA_ERR_BAD_ARG, "supported is NULL");
+  *supported = 0;
+  auto msg = [&](const char* m) {
+    if (message && message_len) {
+      std::snprintf(message, message_len, "%s", m);
+    }
+  };
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    msg(e == cudaErrorInsufficientDriver ? "Insufficient Driver" : "No compatible GPU");
+    return FA_OK;
+  }
+  int dev = 0, major = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+  if (major != 10) {
+    msg("No compatible GPU (this build targets sm_100a)");
+    return FA_OK;
+  }
+  *supported = 1;
+  msg("");
+  return FA_OK;
+}
+
+extern "C" fa_status fa_create(const fa_config* cfg, fa_context** out) {
+  if (!out) return fail(FA_ERR_BAD_ARG, "out is NULL");
+  int dev = cfg ? cfg->device : 0;
+  FA_CU(cudaSetDevice(dev));
+  size_t free_b = 0, total_b = 0;
+  FA_CU(cudaMemGetInfo(&free_b, &total_b));
+  fa_context* c = new fa_context;
+  c->device = dev;
+  c->budget = (cfg && cfg->memory_budget) ? cfg->memory_budget : (size_t)(0.9 * (double)free_b);
+  *out = c;
+  return FA_OK;
+}
+
+extern "C" fa_status fa_destroy(fa_context* ctx) {
+  if (!ctx) return fail(FA_ERR_BAD_ARG, "ctx is NULL");
+  delete ctx;
+  return FA_OK;
+}
+
+extern "C" fa_status fa_scan_params_init(double line_duration, double interline_duration, double interframe_duration,
+                                         int n_x, int n_y, int n_z, int bidirectional, fa_scan_params* s) {
+  if (!s) return fail(FA_ERR_BAD_ARG, "out is NULL");
+  s->line_duration = line_duration;
+  s->interline_duration = interline_duration;
+  s->interframe_duration = interframe_duration;
+  s->n_x = std::max(n_x, 1);
+  s->n_y = std::max(n_y, 1);
+  s->n_z = n_z;
+  if (s->interline_duration < s->line_duration) s->interline_duration = 1.01 * s->line_duration;
+  s->pixel_duration = s->line_duration / s->n_x;
+  s->frame_duration = s->n_y * s->interline_duration;
+  s->stack_duration = (s->n_z - 1) * s->interframe_duration + s->frame_duration;
+  s->bidirectional = bidirectional ? 1 : 0;
+  return FA_OK;
+}
+
+// ================================================================== reference ======================
+
+namespace {
+
+fa_status reference_setup(fa_reference* R, const float* src, bool src_device) {
+  fa_context* ctx = R->ctx;
+  Geometry& G = R->G;
+  const long long N = R->N;
+  FA_CU(cudaStreamCreateWithFlags(&R->stream, cudaStreamNonBlocking));
+  RefDev& h = R->host;
+  h.nz = R->nz;
+  h.ny = R->ny;
+  h.nx = R->nx;
+  h.nD = R->nD;
+  h.n_dim = R->n_dim;
+  h.n_rows = G.n_rows;
+  h.N = N;
+  h.bidir = R->scan.bidirectional;
+  h.dq = G.dq;
+  h.tile_rows = G.tile_rows;
+  h.n_tiles = G.n_tiles;
+  h.P = R->P;
+  RowDesc* rows;
+  int* tile_c0;
+  int2* ctrl;
+  float *ref32, *gx, *gy, *gz;
+  double *Hd, *Hl, *tparts, *scan_dev;
+  FA_TRY(dalloc_t(ctx, G.rows.size(), &rows, R->allocs));
+  FA_TRY(dalloc_t(ctx, G.tile_c0.size(), &tile_c0, R->allocs));
+  FA_TRY(dalloc_t(ctx, G.ctrl_tiles.size(), &ctrl, R->allocs));
+  FA_TRY(dalloc_t(ctx, (size_t)N, &ref32, R->allocs));
+  FA_TRY(dalloc_t(ctx, (size_t)N, &gx, R->allocs));
+  FA_TRY(dalloc_t(ctx, (size_t)N, &gy, R->allocs));
+  FA_TRY(dalloc_t(ctx, (size_t)N, &gz, R->allocs));
+  const int nn = R->n_dim * R->n_dim;
+  FA_TRY(dalloc_t(ctx, (size_t)R->nD * nn, &Hd, R->allocs));
+  FA_TRY(dalloc_t(ctx, (size_t)R->nD * nn, &Hl, R->allocs));
+  FA_TRY(dalloc_t(ctx, 4, &scan_dev, R->allocs));
+  FA_TRY(dalloc_t(ctx, 1, &R->dev, R->allocs));
+  std::vector<Alloc> tmp;
+  fa_status st = dalloc_t(ctx, (size_t)G.n_tiles * 2 * 21, &tparts, tmp);
+  if (st != FA_OK) return st;
+  cudaStream_t s = R->stream;
+  FA_CU(cudaMemcpyAsync(rows, G.rows.data(), G.rows.size() * sizeof(RowDesc), cudaMemcpyHostToDevice, s));
+  FA_CU(cudaMemcpyAsync(tile_c0, G.tile_c0.data(), G.tile_c0.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+  FA_CU(cudaMemcpyAsync(ctrl, G.ctrl_tiles.data(), G.ctrl_tiles.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
+  FA_CU(cudaMemcpyAsync(ref32, src, (size_t)N * sizeof(float), src_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+  FA_CU(fa::launch_sobel(ref32, R->nz, R->ny, R->nx, gx, gy, gz, s));
+  h.rows = rows;
+  h.tile_c0 = tile_c0;
+  h.ctrl_tiles = ctrl;
+  h.ref32 = ref32;
+  h.gx32 = gx;
+  h.gy32 = gy;
+  h.gz32 = gz;
+  h.Hd = Hd;
+  h.Hl = Hl;
+  if (R->prec == FA_PREC_MIXED) {
+    __nv_bfloat16 *r16, *x16, *y16, *z16;
+    FA_TRY(dalloc_t(ctx, (size_t)N, &r16, R->allocs));
+    FA_TRY(dalloc_t(ctx, (size_t)N, &x16, R->allocs));
+    FA_TRY(dalloc_t(ctx, (size_t)N, &y16, R->allocs));
+    FA_TRY(dalloc_t(ctx, (size_t)N, &z16, R->allocs));
+    FA_CU(fa::launch_to_bf16(ref32, r16, N, s));
+    FA_CU(fa::launch_to_bf16(gx, x16, N, s));
+    FA_CU(fa::launch_to_bf16(gy, y16, N, s));
+    FA_CU(fa::launch_to_bf16(gz, z16, N, s));
+    h.ref16 = r16;
+    h.gx16 = x16;
+    h.gy16 = y16;
+    h.gz16 = z16;
+  }
+  FA_CU(cudaMemcpyAsync(R->dev, &h, sizeof(RefDev), cudaMemcpyHostToDevice, s));
+  const fa_scan_params p = process_scan(R->scan, R->nz, R->nD);
+  double scan4[4] = {p.pixel_duration, p.interline_duration, p.interframe_duration, p.stack_duration};
+  FA_CU(fa::launch_hessian(R->dev, h, scan4, tparts, Hd, Hl, s));
+  std::vector<double> hd((size_t)R->nD * nn), hl((size_t)R->nD * nn);
+  FA_CU(cudaMemcpyAsync(hd.data(), Hd, hd.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  FA_CU(cudaMemcpyAsync(hl.data(), Hl, hl.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  FA_CU(cudaStreamSynchronize(s));
+  dfree_all(ctx, tmp);
+  const int P = R->P, nd = R->n_dim;
+  R->H.assign((size_t)P * P, 0.0);
+  for (int i = 0; i < P; i++)
+    for (int j = 0; j < P; j++) {
+      int bi = i / nd, bj = j / nd, a = i % nd, b = j % nd;
+      double v = 0;
+      if (bi == bj)
+        v = hd[(size_t)bi * nn + a * nd + b];
+      else if (bi == bj + 1)
+        v = hl[(size_t)bi * nn + a * nd + b];
+      else if (bj == bi + 1)
+        v = hl[(size_t)bj * nn + b * nd + a];
+      R->H[(size_t)i * P + j] = v;
+    }
+  return FA_OK;
+}
+
+fa_status set_reference_impl(fa_context* ctx, const float* src, bool src_device, int nz, int ny, int nx, int nD,
+                             const fa_scan_params* scan, fa_precision precision, fa_reference** out) {
+  if (!ctx || !src || !scan || !out) return fail(FA_ERR_BAD_ARG, "NULL argument");
+  if (precision != FA_PREC_F32 && precision != FA_PREC_MIXED) return fail(FA_ERR_BAD_ARG, "unknown precision");
+  FA_CU(cudaSetDevice(ctx->device));
+  fa_reference* R = new fa_reference;
+  R->ctx = ctx;
+  R->nz = nz;
+  R->ny = ny;
+  R->nx = nx;
+  R->nD = nD;
+  R->n_dim = nz > 1 ? 3 : 2;
+  R->P = nD * R->n_dim;
+  R->N = (long long)nz * ny * nx;
+  R->prec = precision;
+  R->scan = *scan;
+  fa_status st = build_geometry(*scan, nz, ny, nx, nD, 8192, R->G);
+  if (st == FA_OK) st = reference_setup(R, src, src_device);
+  if (st != FA_OK) {
+    std::string keep = g_err;
+    if (R->stream) cudaStreamDestroy(R->stream);
+    dfree_all(ctx, R->allocs);
+    delete R;
+    g_err = keep;
+    return st;
+  }
+  *out = R;
+  return FA_OK;
+}
+
+}  // namespace
+
+extern "C" fa_status fa_set_reference(fa_context* ctx, const float* reference, int nz, int ny, int nx, int nD,
+                                      const fa_scan_params* scan, fa_precision precision, fa_reference** out) {
+  return set_reference_impl(ctx, reference, false, nz, ny, nx, nD, scan, precision, out);
+}
+
+extern "C" fa_status fa_set_reference_device(fa_context* ctx, const float* reference_device, int nz, int ny, int nx,
+                                             int nD, const fa_scan_params* scan, fa_precision precision,
+                                             fa_reference** out) {
+  return set_reference_impl(ctx, reference_device, true, nz, ny, nx, nD, scan, precision, out);
+}
+
+extern "C" fa_status fa_reference_destroy(fa_reference* R) {
+  if (!R) return fail(FA_ERR_BAD_ARG, "ref is NULL");
+  if (R->n_frames.load() != 0) return fail(FA_ERR_STATE, "frames of this reference are still registered");
+  cudaSetDevice(R->ctx->device);
+  if (R->stream) cudaStreamDestroy(R->stream);
+  dfree_all(R->ctx, R->allocs);
+  delete R;
+  return FA_OK;
+}
+
+extern "C" fa_status fa_reference_info(const fa_reference* R, int* n_dim, int* n_params) {
+  if (!R) return fail(FA_ERR_BAD_ARG, "ref is NULL");
+  if (n_dim) *n_dim = R->n_dim;
+  if (n_params) *n_params = R->P;
+  return FA_OK;
+}
+
+extern "C" fa_status fa_get_hessian(const fa_reference* R, double* H) {
+  if (!R || !H) return fail(FA_ERR_BAD_ARG, "NULL argument");
+  std::memcpy(H, R->H.data(), R->H.size() * sizeof(double));
+  return FA_OK;
+}
+
+extern "C" fa_status fa_get_gradient(const fa_reference* R, float* gx, float* gy, float* gz) {
+  if (!R) return fail(FA_ERR_BAD_ARG, "ref is NULL");
+  FA_CU(cudaSetDevice(R->ctx->device));
+  size_t n = (size_t)R->N * sizeof(float);
+  if (gx) FA_CU(cudaMemcpy(gx, R->host.gx32, n, cudaMemcpyDeviceToHost));
+  if (gy) FA_CU(cudaMemcpy(gy, R->host.gy32, n, cudaMemcpyDeviceToHost));
+  if (gz) FA_CU(cudaMemcpy(gz, R->host.gz32, n, cudaMemcpyDeviceToHost));
+  return FA_OK;
+}
+
+extern "C" fa_status fa_get_ranges(const fa_reference* R, int* ranges) {
+  if (!R || !ranges) return fail(FA_ERR_BAD_ARG, "NULL argument");
+  for (int k = 0; k < R->nD; k++) {
+    ranges[2 * k] = (k <= R->nD - 2) ? R->G.begin[k] : 0;
+    ranges[2 * k + 1] = (k <= R->nD - 2) ? R->G.end[k] : 0;
+  }
+  return FA_OK;
+}
+
+// ================================================================== frames =========================
+
+namespace {
+
+size_t work_doubles(const fa_reference* R) { return (size_t)R->P * (2 * R->n_dim) + 2 * (size_t)R->P; }
+
+fa_status frame_alloc(fa_reference* R, fa_frame** out) {
+  fa_context* ctx = R->ctx;
+  fa_frame* F = new fa_frame;
+  F->ref = R;
+  F->half = (R->prec == FA_PREC_MIXED);
+  auto cleanup = [&](fa_status st) {
+    std::string keep = g_err;
+    if (F->stream) cudaStreamDestroy(F->stream);
+    if (F->h_result) cudaFreeHost(F->h_result);
+    if (F->h_dparams) cudaFreeHost(F->h_dparams);
+    if (F->h_x) cudaFreeHost(F->h_x);
+    if (F->h_state) cudaFreeHost(F->h_state);
+    dfree_all(ctx, F->allocs);
+    delete F;
+    g_err = keep;
+    return st;
+  };
+  if (cudaStreamCreateWithFlags(&F->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return cleanup(fail(FA_ERR_CUDA, "cudaStreamCreate failed"));
+  const size_t P = (size_t)R->P;
+  fa_status st;
+  void* data;
+  if ((st = dalloc(ctx, (size_t)R->N * (F->half ? 2 : 4), &data, F->allocs)) != FA_OK) return cleanup(st);
+  F->data = data;
+  Job& j = F->job;
+  j.ref = R->dev;
+  j.frame = data;
+  if ((st = dalloc_t(ctx, (size_t)R->nD * fa::kDParamF4, &j.dparams, F->allocs)) != FA_OK) return cleanup(st);
+  if ((st = dalloc_t(ctx, (size_t)R->G.n_tiles * fa::kPartialDoubles, &j.partials, F->allocs)) != FA_OK)
+    return cleanup(st);
+  if ((st = dalloc_t(ctx, 1, &F->state, F->allocs)) != FA_OK) return cleanup(st);
+  double* pool;
+  size_t nd = 4 * P + work_doubles(R) + 1 + P;
+  if ((st = dalloc_t(ctx, nd, &pool, F->allocs)) != FA_OK) return cleanup(st);
+  j.x = pool;
+  j.g = pool + P;
+  j.p = pool + 2 * P;
+  j.gt = pool + 3 * P;
+  j.work = pool + 4 * P;
+  j.result = j.work + work_doubles(R);
+  j.state = nullptr;
+  if ((st = dalloc_t(ctx, 1, &F->job_dev, F->allocs)) != FA_OK) return cleanup(st);
+  if (cudaMallocHost(&F->h_result, (1 + P) * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost(&F->h_dparams, (size_t)R->nD * fa::kDParamF4 * sizeof(float4)) != cudaSuccess ||
+      cudaMallocHost(&F->h_x, P * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost(&F->h_state, sizeof(fa::FrameState)) != cudaSuccess)
+    return cleanup(fail(FA_ERR_OOM, "cudaMallocHost failed"));
+  if (cudaMemcpyAsync(F->job_dev, &F->job, sizeof(Job), cudaMemcpyHostToDevice, F->stream) != cudaSuccess)
+    return cleanup(fail(FA_ERR_CUDA, "job upload failed"));
+  R->n_frames++;
+  *out = F;
+  return FA_OK;
+}
+
+fa_status frame_fill(fa_frame* F, const void* src, fa_dtype dtype, bool src_device) {
+  fa_reference* R = F->ref;
+  const long long N = R->N;
+  const fa_dtype store = F->half ? FA_F16 : FA_F32;
+  size_t esz = (dtype == FA_F32) ? 4 : 2;
+  if (dtype == store && !src_device) {
+    FA_CU(cudaMemcpyAsync(F->data, src, (size_t)N * esz, cudaMemcpyHostToDevice, F->stream));
+  } else if (dtype == store && src_device) {
+    FA_CU(cudaMemcpyAsync(F->data, src, (size_t)N * esz, cudaMemcpyDeviceToDevice, F->stream));
+  } else if (src_device) {
+    FA_CU(fa::launch_convert(src, dtype, F->data, store, N, F->stream));
+  } else {
+    std::vector<Alloc> tmp;
+    void* stage;
+    FA_TRY(dalloc(R->ctx, (size_t)N * esz, &stage, tmp));
+    cudaError_t e = cudaMemcpyAsync(stage, src, (size_t)N * esz, cudaMemcpyHostToDevice, F->stream);
+    if (e == cudaSuccess) e = fa::launch_convert(stage, dtype, F->data, store, N, F->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(F->stream);
+    dfree_all(R->ctx, tmp);
+    if (e != cudaSuccess) return fail(FA_ERR_CUDA, std::string("frame upload: ") + cudaGetErrorString(e));
+  }
+  FA_CU(cudaStreamSynchronize(F->stream));
+  F->have_last = false;
+  return FA_OK;
+}
+
+fa_status register_impl(fa_reference* R, const void* data, fa_dtype dtype, bool dev, fa_frame** out) {
+  if (!R || !data || !out) return fail(FA_ERR_BAD_ARG, "NULL argument");
+  if (dtype < FA_F32 || dtype > FA_U16) return fail(FA_ERR_BAD_ARG, "unknown dtype");
+  FA_CU(cudaSetDevice(R->ctx->device));
+  fa_frame* F = nullptr;
+  FA_TRY(frame_alloc(R, &F));
+  fa_status st = frame_fill(F, data, dtype, dev);
+  if (st != FA_OK) {
+    std::string keep = g_err;
+    fa_deregister_frame(F);
+    g_err = keep;
+    return st;
+  }
+  *out = F;
+  return FA_OK;
+}
+
+}  // namespace
+
+extern "C" fa_status fa_register_frame(fa_reference* R, const void* data, fa_dtype dtype, fa_frame** out) {
+  return register_impl(R, data, dtype, false, out);
+}
+
+extern "C" fa_status fa_register_frame_device(fa_reference* R, const void* data, fa_dtype dtype, fa_frame** out) {
+  return register_impl(R, data, dtype, true, out);
+}
+
+extern "C" fa_status fa_update_frame(fa_frame* F, const void* data, fa_dtype dtype) {
+  if (!F || !data) return fail(FA_ERR_BAD_ARG, "NULL argument");
+  std::lock_guard<std::mutex> lk(F->mu);
+  FA_CU(cudaSetDevice(F->ref->ctx->device));
+  return frame_fill(F, data, dtype, false);
+}
+
+extern "C" fa_status fa_deregister_frame(fa_frame* F) {
+  if (!F) return fail(FA_ERR_BAD_ARG, "frame is NULL");
+  cudaSetDevice(F->ref->ctx->device);
+  if (F->stream) {
+    cudaStreamSynchronize(F->stream);
+    cudaStreamDestroy(F->stream);
+  }
+  if (F->h_result) cudaFreeHost(F->h_result);
+  if (F->h_dparams) cudaFreeHost(F->h_dparams);
+  if (F->h_x) cudaFreeHost(F->h_x);
+  if (F->h_state) cudaFreeHost(F->h_state);
+  F->ref->n_frames--;
+  dfree_all(F->ref->ctx, F->allocs);
+  delete F;
+  return FA_OK;
+}
+
+// ================================================================== evaluation =====================
+
+namespace {
+
+fa_status evaluate(fa_frame* F, const double* D) {
+  fa_reference* R = F->ref;
+  if (!finite_all(D, (size_t)R->nD * 3)) return fail(FA_ERR_BAD_ARG, "D has non-finite entries");
+  FA_CU(cudaSetDevice(R->ctx->device));
+  make_dparams(D, R->nD, R->n_dim, F->h_dparams);
+  const size_t np = (size_t)R->nD * fa::kDParamF4 * sizeof(float4);
+  FA_CU(cudaMemcpyAsync(F->job.dparams, F->h_dparams, np, cudaMemcpyHostToDevice, F->stream));
+  FA_CU(fa::launch_eval(F->job_dev, 1, R->G.n_tiles, R->n_dim, F->half, R->prec == FA_PREC_MIXED, F->stream));
+  FA_CU(fa::launch_reduce(F->job_dev, R->host, F->stream));
+  g_launches += 2;
+  FA_CU(cudaMemcpyAsync(F->h_result, F->job.result, (1 + R->P) * sizeof(double), cudaMemcpyDeviceToHost, F->stream));
+  FA_CU(cudaStreamSynchronize(F->stream));
+  F->last_f = F->h_result[0];
+  F->last_g.assign(F->h_result + 1, F->h_result + 1 + R->P);
+  F->lastD.assign(D, D + (size_t)R->nD * 3);
+  F->have_last = true;
+  return FA_OK;
+}
+
+}  // namespace
+
+extern "C" fa_status fa_get_error(fa_frame* F, const double* D, double* f) {
+  if (!F || !D || !f) return fail(FA_ERR_BAD_ARG, "NULL argument");
+  std::lock_guard<std::mutex> lk(F->mu);
+  FA_TRY(evaluate(F, D));
+  *f = F->last_f;
+  return FA_OK;
+}
+
+extern "C" fa_status fa_get_jacobian(fa_frame* F, const double* D, double* jac) {
+  if (!F || !D || !jac) return fail(FA_ERR_BAD_ARG, "NULL argument");
+  std::lock_guard<std::mutex> lk(F->mu);
+  const size_t n = (size_t)F->ref->nD * 3;
+  if (!F->have_last || std::memcmp(F->lastD.data(), D, n * sizeof(double)) != 0) FA_TRY(evaluate(F, D));
+  std::memcpy(jac, F->last_g.data(), F->last_g.size() * sizeof(double));
+  return FA_OK;
+}
+
+extern "C" fa_status fa_warp(fa_frame* F, const double* D, float invalid_value, float* out) {
+  if (!F || !D || !out) return fail(FA_ERR_BAD_ARG, "NULL argument");
+  std::lock_guard<std::mutex> lk(F->mu);
+  fa_reference* R = F->ref;
+  if (!finite_all(D, (size_t)R->nD * 3)) return fail(FA_ERR_BAD_ARG, "D has non-finite entries");
+  FA_CU(cudaSetDevice(R->ctx->device));
+  if (!F->warp_out) {
+    void* p;
+    FA_TRY(dalloc(R->ctx, (size_t)R->N * sizeof(float), &p, F->allocs));
+    F->warp_out = static_cast<float*>(p);
+  }
+  make_dparams(D, R->nD, R->n_dim, F->h_dparams);
+  const size_t np = (size_t)R->nD * fa::kDParamF4 * sizeof(float4);
+  FA_CU(cudaMemcpyAsync(F->job.dparams, F->h_dparams, np, cudaMemcpyHostToDevice, F->stream));
+  FA_CU(fa::launch_warp(R->dev, R->host, F->data, F->half, F->job.dparams, invalid_value, F->warp_out, F->stream));
+  g_launches += 1;
+  FA_CU(cudaMemcpyAsync(out, F->warp_out, (size_t)R->N * sizeof(float), cudaMemcpyDeviceToHost, F->stream));
+  FA_CU(cudaStreamSynchronize(F->stream));
+  F->have_last = false;  // dparams now hold D of the warp, not of the cached evaluation
+  return FA_OK;
+}
+
+// ================================================================== alignment ======================
+
+namespace {
+
+fa_status init_solve(fa_frame* F, const double* rigid, int max_iterations) {
+  fa_reference* R = F->ref;
+  fa::FrameState& S = *F->h_state;
+  std::memset(&S, 0, sizeof(S));
+  S.phase = fa::kPhaseStartZero;
+  S.max_iter = max_iterations > 0 ? max_iterations : 100;
+  for (int c = 0; c < 3; c++) S.rigid[c] = rigid ? rigid[c] : 0.0;
+  if (R->n_dim == 2) S.rigid[2] = 0.0;
+  Job j = F->job;
+  j.state = F->state;
+  FA_CU(cudaMemcpyAsync(F->state, &S, sizeof(S), cudaMemcpyHostToDevice, F->stream));
+  FA_CU(cudaMemsetAsync(j.x, 0, 4 * (size_t)R->P * sizeof(double), F->stream));
+  FA_CU(cudaMemsetAsync(j.dparams, 0, (size_t)R->nD * fa::kDParamF4 * sizeof(float4), F->stream));
+  return FA_OK;
+}
+
+fa_status finish_solve(fa_frame* F, double* D_out, fa_align_stats* stats) {
+  fa_reference* R = F->ref;
+  const int nd = R->n_dim;
+  FA_CU(cudaMemcpyAsync(F->h_x, F->job.x, (size_t)R->P * sizeof(double), cudaMemcpyDeviceToHost, F->stream));
+  FA_CU(cudaMemcpyAsync(F->h_state, F->state, sizeof(fa::FrameState), cudaMemcpyDeviceToHost, F->stream));
+  FA_CU(cudaStreamSynchronize(F->stream));
+  for (int k = 0; k < R->nD; k++) {
+    D_out[3 * k] = F->h_x[k * nd];
+    D_out[3 * k + 1] = F->h_x[k * nd + 1];
+    D_out[3 * k + 2] = nd == 3 ? F->h_x[k * nd + 2] : 0.0;
+  }
+  if (stats) {
+    const fa::FrameState& S = *F->h_state;
+    stats->iterations = S.iter;
+    stats->evaluations = S.evaluations;
+    stats->accepted = S.accepted;
+    stats->status = S.hit_max ? 1 : 0;
+    stats->f_final = S.f;
+    stats->radius_final = S.radius;
+  }
+  return FA_OK;
+}
+
+}  // namespace
+
+extern "C" fa_status fa_align_frame(fa_frame* F, const double* rigid_shift, int max_iterations, double* D_out,
+                                    fa_align_stats* stats) {
+  if (!F || !D_out) return fail(FA_ERR_BAD_ARG, "NULL argument");
+  if (rigid_shift && !finite_all(rigid_shift, 3)) return fail(FA_ERR_BAD_ARG, "rigid shift is not finite");
+  std::lock_guard<std::mutex> lk(F->mu);
+  fa_reference* R = F->ref;
+  FA_CU(cudaSetDevice(R->ctx->device));
+  FA_TRY(init_solve(F, rigid_shift, max_iterations));
+  Job j = F->job;
+  j.state = F->state;
+  FA_CU(cudaMemcpyAsync(F->job_dev, &j, sizeof(Job), cudaMemcpyHostToDevice, F->stream));
+  const int max_steps = (max_iterations > 0 ? max_iterations : 100) + 4;
+  int phase = fa::kPhaseStartZero;
+  for (int step = 0; step < max_steps && phase != fa::kPhaseDone; step++) {
+    FA_CU(fa::launch_eval(F->job_dev, 1, R->G.n_tiles, R->n_dim, F->half, R->prec == FA_PREC_MIXED, F->stream));
+    FA_CU(fa::launch_solve(F->job_dev, 1, F->stream));
+    g_launches += 2;
+    FA_CU(cudaMemcpyAsync(&F->h_state->phase, &F->state->phase, sizeof(int), cudaMemcpyDeviceToHost, F->stream));
+    FA_CU(cudaStreamSynchronize(F->stream));
+    phase = F->h_state->phase;
+  }
+  F->have_last = false;
+  FA_TRY(finish_solve(F, D_out, stats));
+  Job j0 = F->job;
+  FA_CU(cudaMemcpyAsync(F->job_dev, &j0, sizeof(Job), cudaMemcpyHostToDevice, F->stream));
+  FA_CU(cudaStreamSynchronize(F->stream));
+  return FA_OK;
+}
+
+namespace {
+
+__global__ void count_active_kernel(const Job* jobs, int n, int* out) {
+  int c = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) c += (jobs[i].state->phase != fa::kPhaseDone) ? 1 : 0;
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if (threadIdx.x == 0) *out = c;
+}
+
+}  // namespace
+
+extern "C" fa_status fa_align_batch(fa_frame* const* frames, int n, const double* rigid_shifts, int max_iterations,
+                                    double* D_out, fa_align_stats* stats) {
+  if (!frames || n <= 0 || !D_out) return fail(FA_ERR_BAD_ARG, "bad arguments");
+  fa_reference* R0 = frames[0]->ref;
+  for (int i = 0; i < n; i++) {
+    if (!frames[i]) return fail(FA_ERR_BAD_ARG, "NULL frame");
+    if (frames[i]->ref->n_dim != R0->n_dim || frames[i]->ref->prec != R0->prec || frames[i]->ref->ctx != R0->ctx)
+      return fail(FA_ERR_BAD_ARG, "batched frames must share dimensionality, precision and context");
+  }
+  if (rigid_shifts && !finite_all(rigid_shifts, (size_t)3 * n)) return fail(FA_ERR_BAD_ARG, "rigid shift not finite");
+  fa_context* ctx = R0->ctx;
+  FA_CU(cudaSetDevice(ctx->device));
+  std::vector<std::unique_lock<std::mutex>> locks;
+  for (int i = 0; i < n; i++) locks.emplace_back(frames[i]->mu);
+  cudaStream_t s = frames[0]->stream;
+  int max_tiles = 0;
+  std::vector<Job> jobs(n);
+  for (int i = 0; i < n; i++) {
+    fa_frame* F = frames[i];
+    FA_TRY(init_solve(F, rigid_shifts ? rigid_shifts + 3 * i : nullptr, max_iterations));
+    FA_CU(cudaStreamSynchronize(F->stream));
+    jobs[i] = F->job;
+    jobs[i].state = F->state;
+    max_tiles = std::max(max_tiles, F->ref->G.n_tiles);
+  }
+  std::vector<Alloc> tmp;
+  Job* jobs_dev;
+  int* d_active;
+  int* h_active;
+  FA_TRY(dalloc_t(ctx, (size_t)n, &jobs_dev, tmp));
+  fa_status st = dalloc_t(ctx, 1, &d_active, tmp);
+  if (st != FA_OK) {
+    dfree_all(ctx, tmp);
+    return st;
+  }
+  if (cudaMallocHost(&h_active, sizeof(int)) != cudaSuccess) {
+    dfree_all(ctx, tmp);
+    return fail(FA_ERR_OOM, "cudaMallocHost failed");
+  }
+  auto done = [&](fa_status r) {
+    std::string keep = g_err;
+    cudaStreamSynchronize(s);
+    cudaFreeHost(h_active);
+    dfree_all(ctx, tmp);
+    g_err = keep;
+    return r;
+  };
+  if (cudaMemcpyAsync(jobs_dev, jobs.data(), n * sizeof(Job), cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return done(fail(FA_ERR_CUDA, "job upload failed"));
+  // Iterations run as a CUDA graph of kGraphIters x (fused pass, solve), then one active count.
+  constexpr int kGraphIters = 4;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    for (int it = 0; it < kGraphIters && e == cudaSuccess; it++) {
+      e = fa::launch_eval(jobs_dev, n, max_tiles, R0->n_dim, frames[0]->half, R0->prec == FA_PREC_MIXED, s);
+      if (e == cudaSuccess) e = fa::launch_solve(jobs_dev, n, s);
+    }
+    if (e == cudaSuccess) {
+      count_active_kernel<<<1, 32, 0, s>>>(jobs_dev, n, d_active);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_active, d_active, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaError_t e2 = cudaStreamEndCapture(s, &graph);
+    if (e == cudaSuccess) e = e2;
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+  if (e != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    return done(fail(FA_ERR_CUDA, std::string("batch graph: ") + cudaGetErrorString(e)));
+  }
+  const int max_steps = (max_iterations > 0 ? max_iterations : 100) + 4;
+  for (int step = 0; step < max_steps; step += kGraphIters) {
+    e = cudaGraphLaunch(exec, s);
+    g_launches += 2 * kGraphIters + 1;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) break;
+    if (*h_active == 0) break;
+  }
+  cudaGraphExecDestroy(exec);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return done(fail(FA_ERR_CUDA, std::string("batch solve: ") + cudaGetErrorString(e)));
+  for (int i = 0; i < n; i++) {
+    fa_frame* F = frames[i];
+    fa_status r = finish_solve(F, D_out + (size_t)i * 3 * F->ref->nD, stats ? stats + i : nullptr);
+    if (r != FA_OK) return done(r);
+    F->have_last = false;
+  }
+  return done(FA_OK);
+}
+
+// ================================================================== phase correlation =============
+
+extern "C" fa_status fa_correlator_create(fa_context* ctx, const float* reference, int nz, int ny, int nx,
+                                          fa_correlator** out) {
+  if (!ctx || !reference || !out || nz < 1 || ny < 1 || nx < 1) return fail(FA_ERR_BAD_ARG, "bad arguments");
+  FA_CU(cudaSetDevice(ctx->device));
+  fa_correlator* C = new fa_correlator;
+  C->ctx = ctx;
+  C->nz = nz;
+  C->ny = ny;
+  C->nx = nx;
+  C->n_el = (long long)nz * ny * nx;
+  C->n_complex = (long long)nz * ny * (nx / 2 + 1);
+  auto cleanup = [&](fa_status st) {
+    std::string keep = g_err;
+    fa_correlator_destroy(C);
+    g_err = keep;
+    return st;
+  };
+  if (cudaStreamCreateWithFlags(&C->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return cleanup(fail(FA_ERR_CUDA, "stream"));
+  fa_status st;
+  if ((st = dalloc_t(ctx, (size_t)C->n_el, &C->window, C->allocs)) != FA_OK) return cleanup(st);
+  if ((st = dalloc_t(ctx, (size_t)C->n_el, &C->real, C->allocs)) != FA_OK) return cleanup(st);
+  if ((st = dalloc_t(ctx, (size_t)C->n_complex, &C->spec, C->allocs)) != FA_OK) return cleanup(st);
+  if ((st = dalloc_t(ctx, (size_t)C->n_complex, &C->ref_conj, C->allocs)) != FA_OK) return cleanup(st);
+  if ((st = dalloc_t(ctx, (size_t)C->n_el, &C->vol, C->allocs)) != FA_OK) return cleanup(st);
+  C->n_blocks = (int)std::min<long long>(148 * 4, (C->n_el + 255) / 256);
+  if ((st = dalloc_t(ctx, (size_t)C->n_blocks, &C->bval, C->allocs)) != FA_OK) return cleanup(st);
+  if ((st = dalloc_t(ctx, (size_t)C->n_blocks, &C->bidx, C->allocs)) != FA_OK) return cleanup(st);
+  if ((st = dalloc_t(ctx, 1, &C->d_idx, C->allocs)) != FA_OK) return cleanup(st);
+  if (cudaMallocHost(&C->h_idx, sizeof(long long)) != cudaSuccess) return cleanup(fail(FA_ERR_OOM, "pinned"));
+  // Square-root Hann window in x and y, 1 along z (VolumePhaseCorrelator.cpp:141-166).
+  auto hann = [](int n) {
+    std::vector<double> w(n, 1.0);
+    if (n > 1) {
+      const double PI = 3.14159265358979323846;
+      double f = 2.0 * PI / (n - 1);
+      for (int i = 0; i < n; i++) w[i] = std::sqrt(0.5 * (1 - std::cos(f * i)));
+    }
+    return w;
+  };
+  std::vector<double> wy = hann(ny), wx = hann(nx), win((size_t)C->n_el);
+  size_t idx = 0;
+  for (int z = 0; z < nz; z++)
+    for (int y = 0; y < ny; y++)
+      for (int x = 0; x < nx; x++) win[idx++] = 1.0 * wy[y] * wx[x];
+  if (cudaMemcpy(C->window, win.data(), win.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+    return cleanup(fail(FA_ERR_CUDA, "window upload"));
+  int dims[3] = {nz, ny, nx};
+  int rank = 3;
+  int* d = dims;
+  if (nz == 1) {
+    rank = 2;
+    d = dims + 1;
+    if (ny == 1) {
+      rank = 1;
+      d = dims + 2;
+    }
+  }
+  if (cufftPlanMany(&C->fwd, rank, d, nullptr, 1, 0, nullptr, 1, 0, CUFFT_D2Z, 1) != CUFFT_SUCCESS ||
+      cufftPlanMany(&C->inv, rank, d, nullptr, 1, 0, nullptr, 1, 0, CUFFT_Z2D, 1) != CUFFT_SUCCESS)
+    return cleanup(fail(FA_ERR_CUDA, "cufftPlanMany failed"));
+  cufftSetStream(C->fwd, C->stream);
+  cufftSetStream(C->inv, C->stream);
+  if (cudaMemcpyAsync(C->vol, reference, (size_t)C->n_el * sizeof(float), cudaMemcpyHostToDevice, C->stream) !=
+      cudaSuccess)
+    return cleanup(fail(FA_ERR_CUDA, "reference upload"));
+  if (fa::launch_phase_window(C->vol, C->window, C->real, C->n_el, C->stream) != cudaSuccess)
+    return cleanup(fail(FA_ERR_CUDA, "window kernel"));
+  if (cufftExecD2Z(C->fwd, C->real, reinterpret_cast<cufftDoubleComplex*>(C->spec)) != CUFFT_SUCCESS)
+    return cleanup(fail(FA_ERR_CUDA, "cufftExecD2Z failed"));
+  if (fa::launch_phase_conj(C->spec, C->ref_conj, C->n_complex, C->stream) != cudaSuccess)
+    return cleanup(fail(FA_ERR_CUDA, "conj kernel"));
+  if (cudaStreamSynchronize(C->stream) != cudaSuccess) return cleanup(fail(FA_ERR_CUDA, "correlator set-up"));
+  *out = C;
+  return FA_OK;
+}
+
+extern "C" fa_status fa_correlator_destroy(fa_correlator* C) {
+  if (!C) return fail(FA_ERR_BAD_ARG, "NULL correlator");
+  cudaSetDevice(C->ctx->device);
+  if (C->stream) cudaStreamSynchronize(C->stream);
+  if (C->fwd) cufftDestroy(C->fwd);
+  if (C->inv) cufftDestroy(C->inv);
+  if (C->h_idx) cudaFreeHost(C->h_idx);
+  if (C->stream) cudaStreamDestroy(C->stream);
+  dfree_all(C->ctx, C->allocs);
+  delete C;
+  return FA_OK;
+}
+
+namespace {
+
+// Window, D2Z, cross-power normalisation, Z2D and first-maximum argmax into *d_out (device).
+fa_status correlator_enqueue(fa_correlator* C, const float* vol_dev, long long* d_out) {
+  g_launches += 4;  // window, normalise, two argmax stages (the FFTs are cuFFT's)
+  FA_CU(fa::launch_phase_window(vol_dev, C->window, C->real, C->n_el, C->stream));
+  if (cufftExecD2Z(C->fwd, C->real, reinterpret_cast<cufftDoubleComplex*>(C->spec)) != CUFFT_SUCCESS)
+    return fail(FA_ERR_CUDA, "cufftExecD2Z failed");
+  FA_CU(fa::launch_phase_normalise(C->spec, C->ref_conj, C->n_complex, C->stream));
+  if (cufftExecZ2D(C->inv, reinterpret_cast<cufftDoubleComplex*>(C->spec), C->real) != CUFFT_SUCCESS)
+    return fail(FA_ERR_CUDA, "cufftExecZ2D failed");
+  FA_CU(fa::launch_phase_argmax(C->real, C->n_el, C->bval, C->bidx, C->n_blocks, d_out, C->stream));
+  return FA_OK;
+}
+
+// Peak index -> signed integer shift (VolumePhaseCorrelator.cpp:94-103).
+void unravel_shift(const fa_correlator* C, long long idx, double* shift) {
+  long long x = idx % C->nx;
+  long long y = (idx / C->nx) % C->ny;
+  long long z = idx / ((long long)C->nx * C->ny);
+  if (x > C->nx / 2) x -= C->nx;
+  if (y > C->ny / 2) y -= C->ny;
+  if (z > C->nz / 2) z -= C->nz;
+  shift[0] = (double)x;
+  shift[1] = (double)y;
+  shift[2] = (double)z;
+}
+
+fa_status correlator_run(fa_correlator* C, const float* vol_dev, double* shift) {
+  FA_TRY(correlator_enqueue(C, vol_dev, C->d_idx));
+  FA_CU(cudaMemcpyAsync(C->h_idx, C->d_idx, sizeof(long long), cudaMemcpyDeviceToHost, C->stream));
+  FA_CU(cudaStreamSynchronize(C->stream));
+  unravel_shift(C, *C->h_idx, shift);
+  return FA_OK;
+}
+
+}  // namespace
+
+extern "C" fa_status fa_correlator_shift(fa_correlator* C, const float* volume, double* shift) {
+  if (!C || !volume || !shift) return fail(FA_ERR_BAD_ARG, "NULL argument");
+  std::lock_guard<std::mutex> lk(C->mu);
+  FA_CU(cudaSetDevice(C->ctx->device));
+  FA_CU(cudaMemcpyAsync(C->vol, volume, (size_t)C->n_el * sizeof(float), cudaMemcpyHostToDevice, C->stream));
+  return correlator_run(C, C->vol, shift);
+}
+
+extern "C" fa_status fa_correlator_shift_device(fa_correlator* C, const float* volume_device, double* shift) {
+  if (!C || !volume_device || !shift) return fail(FA_ERR_BAD_ARG, "NULL argument");
+  std::lock_guard<std::mutex> lk(C->mu);
+  FA_CU(cudaSetDevice(C->ctx->device));
+  return correlator_run(C, volume_device, shift);
+}
+
+// ================================================================== test hooks ====================
+
+extern "C" fa_status fa_test_tr_subproblem(fa_context* ctx, int nD, int n_dim, const double* H, const double* g,
+                                           double radius, double* p, int* on_boundary) {
+  if (!ctx || !H || !g || !p || !on_boundary || nD < 1 || (n_dim != 2 && n_dim != 3))
+    return fail(FA_ERR_BAD_ARG, "bad arguments");
+  FA_CU(cudaSetDevice(ctx->device));
+  const int P = nD * n_dim, nn = n_dim * n_dim;
+  std::vector<double> hd((size_t)nD * nn, 0.0), hl((size_t)nD * nn, 0.0);
+  for (int b = 0; b < nD; b++)
+    for (int a = 0; a < n_dim; a++)
+      for (int c = 0; c < n_dim; c++) {
+        hd[(size_t)b * nn + a * n_dim + c] = H[(size_t)(b * n_dim + a) * P + b * n_dim + c];
+        if (b > 0) hl[(size_t)b * nn + a * n_dim + c] = H[(size_t)(b * n_dim + a) * P + (b - 1) * n_dim + c];
+      }
+  std::vector<Alloc> tmp;
+  double *dHd, *dHl, *dg, *dp, *work;
+  int* db;
+  auto done = [&](fa_status st) {
+    std::string keep = g_err;
+    dfree_all(ctx, tmp);
+    g_err = keep;
+    return st;
+  };
+  fa_status st;
+  if ((st = dalloc_t(ctx, hd.size(), &dHd, tmp)) != FA_OK) return done(st);
+  if ((st = dalloc_t(ctx, hl.size(), &dHl, tmp)) != FA_OK) return done(st);
+  if ((st = dalloc_t(ctx, (size_t)P, &dg, tmp)) != FA_OK) return done(st);
+  if ((st = dalloc_t(ctx, (size_t)P, &dp, tmp)) != FA_OK) return done(st);
+  if ((st = dalloc_t(ctx, (size_t)P * (2 * n_dim) + 2 * (size_t)P, &work, tmp)) != FA_OK) return done(st);
+  if ((st = dalloc_t(ctx, 1, &db, tmp)) != FA_OK) return done(st);
+  cudaError_t e = cudaMemcpy(dHd, hd.data(), hd.size() * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dHl, hl.data(), hl.size() * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dg, g, (size_t)P * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = fa::launch_test_subproblem(dHd, dHl, nD, n_dim, dg, radius, dp, db, work, 0);
+  if (e == cudaSuccess) e = cudaMemcpy(p, dp, (size_t)P * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(on_boundary, db, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return done(fail(FA_ERR_CUDA, std::string("subproblem: ") + cudaGetErrorString(e)));
+  return done(FA_OK);
+}
+
+// ================================================================== aligner =======================
+
+struct fa_aligner {
+  fa_context* ctx = nullptr;
+  fa_aligner_params prm{};
+  fa_reference* ref = nullptr;
+  fa_correlator* corr = nullptr;
+  int nz = 0, ny = 0, nx = 0, nD = 0;
+  int dz = 0, dy = 0, dx = 0;  // downsampled dims
+  cudaStream_t stream = nullptr;
+  std::vector<fa_frame*> slots;
+  void* staging = nullptr;     // raw frames in flight (n_stage * N * 4 bytes)
+  size_t staging_bytes = 0;
+  float* vols = nullptr;       // downsampled float frames for the correlator
+  size_t vols_count = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double last_ms = 0;
+  long long* d_idx = nullptr;  // per-frame peak indices
+  long long* h_idx = nullptr;
+  int idx_cap = 0;
+  std::vector<Alloc> allocs;   // staging / vols / d_idx
+  std::vector<Alloc> ref_allocs;
+  std::mutex mu;
+};
+
+namespace {
+
+void aligner_release_reference(fa_aligner* A) {
+  for (fa_frame* f : A->slots) fa_deregister_frame(f);
+  A->slots.clear();
+  if (A->corr) fa_correlator_destroy(A->corr);
+  A->corr = nullptr;
+  if (A->ref) fa_reference_destroy(A->ref);
+  A->ref = nullptr;
+  dfree_all(A->ctx, A->ref_allocs);
+}
+
+size_t dtype_size(fa_dtype t) { return t == FA_F32 ? 4 : 2; }
+
+fa_status aligner_grow(fa_aligner* A, int n, size_t raw_bytes) {
+  while ((int)A->slots.size() < n) {
+    fa_frame* F = nullptr;
+    FA_TRY(frame_alloc(A->ref, &F));
+    A->slots.push_back(F);
+  }
+  const size_t need = (size_t)n * raw_bytes;
+  if (A->staging_bytes < need || (int)A->vols_count < n || A->idx_cap < n) {
+    FA_CU(cudaStreamSynchronize(A->stream));
+    dfree_all(A->ctx, A->allocs);
+    if (A->h_idx) cudaFreeHost(A->h_idx);
+    A->h_idx = nullptr;
+    A->staging = nullptr;
+    A->staging_bytes = 0;
+    A->vols_count = 0;
+    A->idx_cap = 0;
+    FA_TRY(dalloc(A->ctx, need, &A->staging, A->allocs));
+    A->staging_bytes = need;
+    FA_TRY(dalloc_t(A->ctx, (size_t)n * A->dz * A->dy * A->dx, &A->vols, A->allocs));
+    A->vols_count = (size_t)n;
+    FA_TRY(dalloc_t(A->ctx, (size_t)n, &A->d_idx, A->allocs));
+    if (cudaMallocHost(&A->h_idx, (size_t)n * sizeof(long long)) != cudaSuccess)
+      return fail(FA_ERR_OOM, "cudaMallocHost failed");
+    A->idx_cap = n;
+  }
+  return FA_OK;
+}
+
+fa_status aligner_run(fa_aligner* A, const void* const* frames, fa_dtype dtype, int n, bool device_src,
+                      double* D_out, fa_align_stats* stats) {
+  if (!A->ref) return fail(FA_ERR_STATE, "Reference imaging not yet set");  // FrameWarpAligner.cpp:119
+  if (!frames || n <= 0 || !D_out) return fail(FA_ERR_BAD_ARG, "bad arguments");
+  if (dtype != FA_F32 && dtype != FA_U16) return fail(FA_ERR_BAD_ARG, "frames must be FA_F32 or FA_U16");
+  for (int i = 0; i < n; i++)
+    if (!frames[i]) return fail(FA_ERR_BAD_ARG, "NULL frame pointer");
+  FA_CU(cudaSetDevice(A->ctx->device));
+  const long long N = A->ref->N;
+  const size_t raw_bytes = (size_t)N * dtype_size(dtype);
+  FA_TRY(aligner_grow(A, n, raw_bytes));
+  const fa_dtype store = A->slots[0]->half ? FA_F16 : FA_F32;
+  const long long nds = (long long)A->dz * A->dy * A->dx;
+  cudaStream_t s = A->corr->stream;
+  if (!A->ev0) {
+    FA_CU(cudaEventCreate(&A->ev0));
+    FA_CU(cudaEventCreate(&A->ev1));
+  }
+  FA_CU(cudaEventRecord(A->ev0, s));
+  for (int i = 0; i < n; i++) {
+    const void* raw = frames[i];
+    if (!device_src) {
+      void* dst = static_cast<char*>(A->staging) + (size_t)i * raw_bytes;
+      FA_CU(cudaMemcpyAsync(dst, frames[i], raw_bytes, cudaMemcpyHostToDevice, s));
+      raw = dst;
+    }
+    FA_CU(fa::launch_offset_convert(raw, dtype, A->slots[i]->data, store, N, s));
+    g_launches += 1;
+    float* vol = A->vols + (size_t)i * nds;
+    if (A->prm.spatial_binning > 1 || dtype != FA_F32) {
+      FA_CU(fa::launch_downsample(raw, dtype, A->nz, A->ny, A->nx, A->prm.spatial_binning, vol, s));
+      g_launches += 1;
+    } else
+      vol = const_cast<float*>(static_cast<const float*>(raw));
+    FA_TRY(correlator_enqueue(A->corr, vol, A->d_idx + i));
+  }
+  FA_CU(cudaMemcpyAsync(A->h_idx, A->d_idx, (size_t)n * sizeof(long long), cudaMemcpyDeviceToHost, s));
+  FA_CU(cudaStreamSynchronize(s));
+  std::vector<double> rigid((size_t)3 * n);
+  for (int i = 0; i < n; i++) {
+    unravel_shift(A->corr, A->h_idx[i], &rigid[(size_t)3 * i]);
+    // FrameWarpAligner.cpp:186-188: x and y scaled by the phase-correlation downsampling
+    rigid[(size_t)3 * i] *= A->prm.spatial_binning;
+    rigid[(size_t)3 * i + 1] *= A->prm.spatial_binning;
+    A->slots[i]->have_last = false;
+  }
+  std::vector<fa_frame*> batch(A->slots.begin(), A->slots.begin() + n);
+  FA_TRY(fa_align_batch(batch.data(), n, rigid.data(), A->prm.max_iterations, D_out, stats));
+  FA_CU(cudaEventRecord(A->ev1, batch[0]->stream));
+  FA_CU(cudaEventSynchronize(A->ev1));
+  float ms = 0;
+  FA_CU(cudaEventElapsedTime(&ms, A->ev0, A->ev1));
+  A->last_ms = ms;
+  return FA_OK;
+}
+
+}  // namespace
+
+extern "C" fa_status fa_aligner_create(fa_context* ctx, const fa_aligner_params* params, fa_aligner** out) {
+  if (!ctx || !params || !out) return fail(FA_ERR_BAD_ARG, "NULL argument");
+  if (params->smoothing > 0.0)
+    return fail(FA_ERR_UNSUPPORTED, "Gaussian pre-smoothing (RealignmentParameters::smoothing > 0) is not built");
+  if (params->spatial_binning < 1) return fail(FA_ERR_BAD_ARG, "spatial_binning must be >= 1");
+  if (params->precision != FA_PREC_F32 && params->precision != FA_PREC_MIXED)
+    return fail(FA_ERR_BAD_ARG, "unknown precision");
+  fa_aligner* A = new fa_aligner;
+  A->ctx = ctx;
+  A->prm = *params;
+  *out = A;
+  return FA_OK;
+}
+
+extern "C" fa_status fa_aligner_destroy(fa_aligner* A) {
+  if (!A) return fail(FA_ERR_BAD_ARG, "NULL aligner");
+  cudaSetDevice(A->ctx->device);
+  aligner_release_reference(A);
+  dfree_all(A->ctx, A->allocs);
+  if (A->h_idx) cudaFreeHost(A->h_idx);
+  if (A->stream) cudaStreamDestroy(A->stream);
+  if (A->ev0) cudaEventDestroy(A->ev0);
+  if (A->ev1) cudaEventDestroy(A->ev1);
+  delete A;
+  return FA_OK;
+}
+
+extern "C" fa_status fa_aligner_set_reference(fa_aligner* A, const void* reference, fa_dtype dtype, int nz, int ny,
+                                              int nx, const fa_scan_params* scan) {
+  if (!A || !reference || !scan) return fail(FA_ERR_BAD_ARG, "NULL argument");
+  if (dtype != FA_F32 && dtype != FA_U16) return fail(FA_ERR_BAD_ARG, "reference must be FA_F32 or FA_U16");
+  std::lock_guard<std::mutex> lk(A->mu);
+  FA_CU(cudaSetDevice(A->ctx->device));
+  aligner_release_reference(A);
+  if (!A->stream) FA_CU(cudaStreamCreateWithFlags(&A->stream, cudaStreamNonBlocking));
+  const long long N = (long long)nz * ny * nx;
+  const int b = A->prm.spatial_binning;
+  A->nz = nz;
+  A->ny = ny;
+  A->nx = nx;
+  A->dz = nz;
+  A->dy = (ny + b - 1) / b;
+  A->dx = (nx + b - 1) / b;
+  A->nD = A->prm.nD > 0 ? A->prm.nD : A->prm.n_resampling_points * nz + 1;  // FrameWarpAligner.cpp:100
+  void *raw, *plus1, *down;
+  FA_TRY(dalloc(A->ctx, (size_t)N * dtype_size(dtype), &raw, A->ref_allocs));
+  FA_TRY(dalloc(A->ctx, (size_t)N * sizeof(float), &plus1, A->ref_allocs));
+  FA_TRY(dalloc(A->ctx, (size_t)A->dz * A->dy * A->dx * sizeof(float), &down, A->ref_allocs));
+  FA_CU(cudaMemcpyAsync(raw, reference, (size_t)N * dtype_size(dtype), cudaMemcpyHostToDevice, A->stream));
+  // smoothed_reference = reference + 1 (smoothing 0), FrameWarpAligner.cpp:86-90
+  FA_CU(fa::launch_offset_convert(raw, dtype, plus1, FA_F32, N, A->stream));
+  FA_CU(fa::launch_downsample(raw, dtype, nz, ny, nx, b, static_cast<float*>(down), A->stream));
+  std::vector<float> hdown((size_t)A->dz * A->dy * A->dx);
+  FA_CU(cudaMemcpyAsync(hdown.data(), down, hdown.size() * sizeof(float), cudaMemcpyDeviceToHost, A->stream));
+  FA_CU(cudaStreamSynchronize(A->stream));
+  FA_TRY(fa_correlator_create(A->ctx, hdown.data(), A->dz, A->dy, A->dx, &A->corr));
+  fa_status st = fa_set_reference_device(A->ctx, static_cast<const float*>(plus1), nz, ny, nx, A->nD, scan,
+                                         A->prm.precision, &A->ref);
+  dfree_all(A->ctx, A->ref_allocs);
+  if (st != FA_OK) {
+    std::string keep = g_err;
+    aligner_release_reference(A);
+    g_err = keep;
+  }
+  return st;
+}
+
+extern "C" fa_status fa_aligner_info(const fa_aligner* A, int* nD, int* n_dim) {
+  if (!A || !A->ref) return fail(FA_ERR_STATE, "Reference imaging not yet set");
+  if (nD) *nD = A->ref->nD;
+  if (n_dim) *n_dim = A->ref->n_dim;
+  return FA_OK;
+}
+
+extern "C" fa_status fa_aligner_add_frames(fa_aligner* A, const void* const* frames, fa_dtype dtype, int n,
+                                           double* D_out, fa_align_stats* stats) {
+  if (!A) return fail(FA_ERR_BAD_ARG, "NULL aligner");
+  std::lock_guard<std::mutex> lk(A->mu);
+  return aligner_run(A, frames, dtype, n, false, D_out, stats);
+}
+
+extern "C" fa_status fa_aligner_add_frames_device(fa_aligner* A, const void* const* frames, fa_dtype dtype, int n,
+                                                  double* D_out, fa_align_stats* stats) {
+  if (!A) return fail(FA_ERR_BAD_ARG, "NULL aligner");
+  std::lock_guard<std::mutex> lk(A->mu);
+  return aligner_run(A, frames, dtype, n, true, D_out, stats);
+}
+
+// ================================================================== measurement ===================
+
+extern "C" long long fa_kernel_launches(void) { return g_launches.load(); }
+
+extern "C" fa_status fa_aligner_last_device_ms(const fa_aligner* A, double* ms) {
+  if (!A || !ms) return fail(FA_ERR_BAD_ARG, "NULL argument");
+  *ms = A->last_ms;
+  return FA_OK;
+}
+
+extern "C" fa_status fa_profile_eval(fa_frame* const* frames, int n, const double* D, int launches,
+                                     double* ms_per_launch) {
+  if (!frames || n <= 0 || !D || launches <= 0 || !ms_per_launch) return fail(FA_ERR_BAD_ARG, "bad arguments");
+  fa_reference* R = frames[0]->ref;
+  for (int i = 0; i < n; i++)
+    if (!frames[i] || frames[i]->ref != R) return fail(FA_ERR_BAD_ARG, "frames must share one reference");
+  FA_CU(cudaSetDevice(R->ctx->device));
+  std::vector<float4> dp((size_t)R->nD * fa::kDParamF4);
+  make_dparams(D, R->nD, R->n_dim, dp.data());
+  std::vector<Job> jobs(n);
+  for (int i = 0; i < n; i++) {
+    FA_CU(cudaMemcpy(frames[i]->job.dparams, dp.data(), dp.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    jobs[i] = frames[i]->job;
+    frames[i]->have_last = false;
+  }
+  std::vector<Alloc> tmp;
+  Job* jd;
+  FA_TRY(dalloc_t(R->ctx, (size_t)n, &jd, tmp));
+  cudaStream_t s = frames[0]->stream;
+  cudaEvent_t e0, e1;
+  cudaError_t e = cudaMemcpyAsync(jd, jobs.data(), n * sizeof(Job), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  // one untimed launch, then the timed ones
+  if (e == cudaSuccess) e = fa::launch_eval(jd, n, R->G.n_tiles, R->n_dim, frames[0]->half, R->prec == FA_PREC_MIXED, s);
+  if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+  for (int l = 0; l < launches && e == cudaSuccess; l++)
+    e = fa::launch_eval(jd, n, R->G.n_tiles, R->n_dim, frames[0]->half, R->prec == FA_PREC_MIXED, s);
+  if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+  if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+  float ms = 0;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+  g_launches += launches + 1;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  dfree_all(R->ctx, tmp);
+  if (e != cudaSuccess) return fail(FA_ERR_CUDA, std::string("profile: ") + cudaGetErrorString(e));
+  *ms_per_launch = ms / launches;
+  return FA_OK;
+}

@@ -1,0 +1,103 @@
+// fa_internal.h -- device data layout shared by the kernels and the host runtime.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fa_b200.h"
+
+namespace fa {
+
+// One image row (fixed z, y) of the scan-time displacement model.
+//   scan position xs = x, or nx-1-x on odd rows of a bidirectional scan;
+//   interval Di(xs) = di0 + (xs >= xdi)                     (FrameWarper.cpp:258-260)
+//   fraction Df(xs) ~= qbase + xs * dq - (Di - di0)          (FP32; exact tables only on the host)
+//   storage range r(x) = r0 + (x >= xr)                      (D_range, FrameWarper.cpp:269-275)
+//   x == xlast marks the last voxel of a range, whose steepest-descent weight is zero
+//   (the exclusive loop ends at FrameWarper.cpp:315,333).
+struct RowDesc {
+  float qbase;
+  int di0;
+  int xdi;
+  int r0;
+  int xr;
+  int xlast;
+  int pad0;
+  int pad1;
+};
+
+// Control-point parameters for the fused pass, per control point k (3 float4):
+//   [0] integer part of D[k] (xyz), [1] fractional part of D[k], [2] D[k+1] - D[k].
+// d(x) = int(D[k]) + (frac(D[k]) + Df * (D[k+1]-D[k])) keeps the FP32 fraction exact to ~1e-7 px.
+constexpr int kDParamF4 = 3;
+
+// Partial sums of one tile: f, then g for three consecutive control points starting at c0.
+constexpr int kPartialDoubles = 12;  // [f, c0, g(3 x 3), pad]
+
+// Frame solve phases (device trust region).
+enum Phase : int {
+  kPhaseStartZero = 0,   // trial = zero displacement
+  kPhaseStartRigid = 1,  // trial = rigid shift
+  kPhaseTrial = 2,       // trial = x + p
+  kPhaseDone = 3
+};
+
+struct FrameState {
+  double f;        // f(x)
+  double f_prev;   // value at the previous stop-rule check
+  double f_start;  // f at the zero start
+  double radius;
+  int iter;
+  int accepted;
+  int evaluations;
+  int have_prev;
+  int boundary;    // last subproblem step was on the trust-region boundary
+  int phase;
+  int max_iter;
+  int hit_max;
+  double rigid[3];
+};
+
+// Everything a kernel needs about one reference (device-resident copy).
+struct RefDev {
+  int nz, ny, nx, nD, n_dim;
+  int n_rows;
+  long long N;
+  int bidir;
+  float dq;
+  int tile_rows;
+  int n_tiles;
+  int P;
+  const RowDesc* rows;
+  const int* tile_c0;      // per tile: storage range index of its first voxel
+  const int2* ctrl_tiles;  // per control point: tiles [x, y) whose partial slots may hold it
+  const float* ref32;
+  const float* gx32;
+  const float* gy32;
+  const float* gz32;
+  const __nv_bfloat16* ref16;
+  const __nv_bfloat16* gx16;
+  const __nv_bfloat16* gy16;
+  const __nv_bfloat16* gz16;
+  const double* Hd;  // nD blocks of n_dim x n_dim (diagonal), row-major
+  const double* Hl;  // nD blocks (block k couples k and k-1; block 0 unused)
+};
+
+// One frame in a fused pass / solve launch.
+struct Job {
+  const RefDev* ref;      // device pointer
+  const void* frame;      // device pointer, FP32 or FP16 (per kernel instantiation)
+  float4* dparams;        // nD * kDParamF4 (trial point of this job)
+  double* partials;       // n_tiles * kPartialDoubles
+  FrameState* state;      // solve state (may be null for a bare evaluation)
+  double* x;              // P: accepted parameters
+  double* g;              // P: gradient at x
+  double* p;              // P: trial step
+  double* gt;             // P: gradient at the trial point
+  double* work;           // solve scratch (band Cholesky etc.)
+  double* result;         // [f, g(P)] of the last pass (bare evaluation)
+};
+
+}  // namespace fa

@@ -1,0 +1,590 @@
+// fa_kernels.cu -- sm_100a kernels of the warper path.
+//
+//   sobel_kernel    Sobel3d (FrameAligner/Sobel3d.cpp:8-85), bit-exact float arithmetic
+//   hessian_*       computeSteepestDecentImages + computeHessian (FrameWarper.cpp:296-395)
+//   eval_kernel     fused warpImageInterpolated + computeErrorImage + computeJacobian
+//                   (FrameWarper.cpp:4-69,147-176): one HBM pass per frame evaluation
+//   reduce_kernel   deterministic tile -> frame reduction of f and J^T e
+//   warp_kernel     warpImageInterpolated output image
+//
+// Layout: volumes {nz, ny, nx}, x fastest. A tile is `tile_rows` consecutive image rows; the host
+// picks tile_rows so that a tile meets at most two storage ranges (three control points).
+#include "fa_device.cuh"
+
+namespace fa {
+
+// ------------------------------------------------------------------ loads ------------------------
+
+template <typename T>
+__device__ __forceinline__ float ldf(const T* p);
+template <>
+__device__ __forceinline__ float ldf<float>(const float* p) { return __ldg(p); }
+template <>
+__device__ __forceinline__ float ldf<__half>(const __half* p) { return __half2float(__ldg(p)); }
+template <>
+__device__ __forceinline__ float ldf<__nv_bfloat16>(const __nv_bfloat16* p) { return __bfloat162float(__ldg(p)); }
+
+// ------------------------------------------------------------------ Sobel3d ----------------------
+
+// One separable pass at position i of an axis of length n (Sobel3d.cpp:8-58): interior
+// f0*G(i-1) + f1*G(i) + f2*G(i+1); edges e1 = {e1a*G(0) + e1b*G(1)}, e2 = {e2a*G(n-1) + e2b*G(n-2)}.
+// Float products and sums are rounded one by one (no FMA), as in the reference build.
+template <typename G>
+__device__ __forceinline__ float pass(int i, int n, bool copy_if_single, const float* f, const float* e1,
+                                      const float* e2, G get) {
+  if (n == 1 && copy_if_single) return get(i);
+  if (i == 0) return __fadd_rn(__fmul_rn(e1[0], get(0)), __fmul_rn(e1[1], get(1)));
+  if (i == n - 1) return __fadd_rn(__fmul_rn(e2[0], get(n - 1)), __fmul_rn(e2[1], get(n - 2)));
+  return __fadd_rn(__fadd_rn(__fmul_rn(f[0], get(i - 1)), __fmul_rn(f[1], get(i))), __fmul_rn(f[2], get(i + 1)));
+}
+
+__global__ void __launch_bounds__(256) sobel_kernel(const float* __restrict__ m, int nz, int ny, int nx,
+                                                    float* __restrict__ gx, float* __restrict__ gy,
+                                                    float* __restrict__ gz) {
+  const float sm[3] = {1.0f / 4.0f, 2.0f / 4.0f, 1.0f / 4.0f};
+  const float se[2] = {2.0f / 3.0f, 2.0f / 3.0f};
+  const float dm[3] = {-0.5f, 0.0f, 0.5f};
+  const float de1[2] = {-0.5f, 0.5f};
+  const float de2[2] = {0.5f, -0.5f};
+  const long long N = (long long)nz * ny * nx;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N; p += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(p % nx);
+    const long long row = p / nx;
+    const int y = (int)(row % ny);
+    const int z = (int)(row / ny);
+    auto M = [&](int zz, int yy, int xx) { return __ldg(m + ((long long)zz * ny + yy) * nx + xx); };
+    // a = Sx(m); b = Sy(a); c = Sz(a); gz = Dz(b); gy = Dy(c)  (Sobel3d.cpp:73-79)
+    auto A = [&](int zz, int yy, int xx) { return pass(xx, nx, false, sm, se, se, [&](int k) { return M(zz, yy, k); }); };
+    auto B = [&](int zz, int yy, int xx) { return pass(yy, ny, false, sm, se, se, [&](int k) { return A(zz, k, xx); }); };
+    auto Cc = [&](int zz, int yy, int xx) { return pass(zz, nz, true, sm, se, se, [&](int k) { return A(k, yy, xx); }); };
+    gz[p] = pass(z, nz, true, dm, de1, de2, [&](int k) { return B(k, y, x); });
+    gy[p] = pass(y, ny, false, dm, de1, de2, [&](int k) { return Cc(z, k, x); });
+    // a' = Sy(m); b' = Sz(a'); gx = Dx(b')  (Sobel3d.cpp:81-84)
+    auto A2 = [&](int zz, int yy, int xx) { return pass(yy, ny, false, sm, se, se, [&](int k) { return M(zz, k, xx); }); };
+    auto B2 = [&](int zz, int yy, int xx) { return pass(zz, nz, true, sm, se, se, [&](int k) { return A2(k, yy, xx); }); };
+    gx[p] = pass(x, nx, false, dm, de1, de2, [&](int k) { return B2(z, y, k); });
+  }
+}
+
+cudaError_t launch_sobel(const float* m, int nz, int ny, int nx, float* gx, float* gy, float* gz, cudaStream_t s) {
+  long long N = (long long)nz * ny * nx;
+  int blocks = (int)((N + 255) / 256);
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  sobel_kernel<<<blocks, 256, 0, s>>>(m, nz, ny, nx, gx, gy, gz);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ conversions ------------------
+
+__global__ void to_bf16_kernel(const float* __restrict__ in, __nv_bfloat16* __restrict__ out, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = __float2bfloat16_rn(in[i]);
+}
+
+cudaError_t launch_to_bf16(const float* in, __nv_bfloat16* out, long long n, cudaStream_t s) {
+  int blocks = (int)((n + 255) / 256);
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  if (blocks < 1) blocks = 1;
+  to_bf16_kernel<<<blocks, 256, 0, s>>>(in, out, n);
+  return cudaGetLastError();
+}
+
+__device__ __forceinline__ float load_any(const void* in, int t, long long i) {
+  switch (t) {
+    case FA_F32: return static_cast<const float*>(in)[i];
+    case FA_F16: return __half2float(static_cast<const __half*>(in)[i]);
+    case FA_BF16: return __bfloat162float(static_cast<const __nv_bfloat16*>(in)[i]);
+    default: return (float)static_cast<const uint16_t*>(in)[i];
+  }
+}
+
+__global__ void convert_kernel(const void* __restrict__ in, int in_t, void* __restrict__ out, int out_t, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    float v = load_any(in, in_t, i);
+    if (out_t == FA_F16)
+      static_cast<__half*>(out)[i] = __float2half_rn(v);
+    else
+      static_cast<float*>(out)[i] = v;
+  }
+}
+
+cudaError_t launch_convert(const void* in, fa_dtype in_type, void* out, fa_dtype out_type, long long n,
+                           cudaStream_t s) {
+  int blocks = (int)((n + 255) / 256);
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  if (blocks < 1) blocks = 1;
+  convert_kernel<<<blocks, 256, 0, s>>>(in, (int)in_type, out, (int)out_type, n);
+  return cudaGetLastError();
+}
+
+// Raw frame (any dtype) -> warper storage with FrameWarpAligner's +1 offset
+// (FrameWarpAligner.cpp:142), converted to float first as the reference does (convertTo CV_32F).
+__global__ void offset_convert_kernel(const void* __restrict__ in, int in_t, void* __restrict__ out, int out_t,
+                                      long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    float v = load_any(in, in_t, i) + 1.0f;
+    if (out_t == FA_F16)
+      static_cast<__half*>(out)[i] = __float2half_rn(v);
+    else
+      static_cast<float*>(out)[i] = v;
+  }
+}
+
+cudaError_t launch_offset_convert(const void* in, fa_dtype in_type, void* out, fa_dtype out_type, long long n,
+                                  cudaStream_t s) {
+  int blocks = (int)((n + 255) / 256);
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  if (blocks < 1) blocks = 1;
+  offset_convert_kernel<<<blocks, 256, 0, s>>>(in, (int)in_type, out, (int)out_type, n);
+  return cudaGetLastError();
+}
+
+// downsample (AbstractFrameAligner.cpp:37-56): output (z, y/b, x/b) = float sum of its b x b block,
+// accumulated in the reference's loop order (y, then x).
+__global__ void downsample_kernel(const void* __restrict__ in, int in_t, int nz, int ny, int nx, int b,
+                                  float* __restrict__ out) {
+  const int nh = (ny + b - 1) / b, nw = (nx + b - 1) / b;
+  const long long n = (long long)nz * nh * nw;
+  for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < n; o += (long long)gridDim.x * blockDim.x) {
+    const int ox = (int)(o % nw);
+    const long long r = o / nw;
+    const int oy = (int)(r % nh);
+    const int z = (int)(r / nh);
+    float acc = 0.0f;
+    for (int y = oy * b; y < min(ny, oy * b + b); y++)
+      for (int x = ox * b; x < min(nx, ox * b + b); x++)
+        acc = __fadd_rn(acc, load_any(in, in_t, ((long long)z * ny + y) * nx + x));
+    out[o] = acc;
+  }
+}
+
+cudaError_t launch_downsample(const void* in, fa_dtype in_type, int nz, int ny, int nx, int b, float* out,
+                              cudaStream_t s) {
+  long long n = (long long)nz * ((ny + b - 1) / b) * ((nx + b - 1) / b);
+  int blocks = (int)((n + 255) / 256);
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  if (blocks < 1) blocks = 1;
+  downsample_kernel<<<blocks, 256, 0, s>>>(in, (int)in_type, nz, ny, nx, b, out);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ per-voxel model --------------
+
+// Interval, fraction and storage-range bookkeeping of one voxel (see RowDesc).
+struct VoxelModel {
+  int di;      // displacement interval
+  float f;     // fraction within it
+  int r;       // storage range (steepest-descent images)
+  bool last;   // last voxel of its storage range
+};
+
+__device__ __forceinline__ VoxelModel voxel_model(const RowDesc& rd, int x, int nx, bool flip, bool bidir, float dq) {
+  VoxelModel v;
+  const int xs = flip ? nx - 1 - x : x;
+  v.di = rd.di0 + (xs >= rd.xdi ? 1 : 0);
+  float f = fmaf((float)xs, dq, rd.qbase) - (float)(v.di - rd.di0);
+  v.f = fminf(fmaxf(f, 0.0f), 1.0f);
+  v.r = bidir ? rd.r0 + (x >= rd.xr ? 1 : 0) : v.di;
+  v.last = (x == rd.xlast);
+  return v;
+}
+
+// Zero-padded trilinear (bilinear for NDIM == 2) sample of the frame at (x, y, z) + d, where
+// d = int(D) + frac(D) + f * dD from the control-point parameters P (3 float4). Returns the
+// interpolated value; exactly 0 when every contributing tap is outside (getZeroPadded,
+// FrameWarper.h:39-47).
+template <int NDIM, typename FT>
+__device__ __forceinline__ float sample(const FT* __restrict__ fr, const float4* P, float f, int x, int y, int z,
+                                        int nx, int ny, int nz) {
+  const float4 n = P[0], ph = P[1], dd = P[2];
+  const float tx = fmaf(f, dd.x, ph.x);
+  const float ty = fmaf(f, dd.y, ph.y);
+  const float flx = floorf(tx), fly = floorf(ty);
+  const float wx = tx - flx, wy = ty - fly;
+  const int ix = x + (int)n.x + (int)flx;
+  const int iy = y + (int)n.y + (int)fly;
+  const bool vx0 = (unsigned)ix < (unsigned)nx, vx1 = (unsigned)(ix + 1) < (unsigned)nx;
+  const bool vy0 = (unsigned)iy < (unsigned)ny, vy1 = (unsigned)(iy + 1) < (unsigned)ny;
+  if (NDIM == 2) {
+    const long long b = (long long)iy * nx + ix;
+    const float v00 = (vy0 && vx0) ? ldf(fr + b) : 0.0f;
+    const float v01 = (vy0 && vx1) ? ldf(fr + b + 1) : 0.0f;
+    const float v10 = (vy1 && vx0) ? ldf(fr + b + nx) : 0.0f;
+    const float v11 = (vy1 && vx1) ? ldf(fr + b + nx + 1) : 0.0f;
+    const float c0 = fmaf(wx, v01 - v00, v00);
+    const float c1 = fmaf(wx, v11 - v10, v10);
+    return fmaf(wy, c1 - c0, c0);
+  } else {
+    const float tz = fmaf(f, dd.z, ph.z);
+    const float flz = floorf(tz);
+    const float wz = tz - flz;
+    const int iz = z + (int)n.z + (int)flz;
+    const bool vz0 = (unsigned)iz < (unsigned)nz, vz1 = (unsigned)(iz + 1) < (unsigned)nz;
+    const long long plane = (long long)nx * ny;
+    const long long b = ((long long)iz * ny + iy) * nx + ix;
+    const float v000 = (vz0 && vy0 && vx0) ? ldf(fr + b) : 0.0f;
+    const float v001 = (vz0 && vy0 && vx1) ? ldf(fr + b + 1) : 0.0f;
+    const float v010 = (vz0 && vy1 && vx0) ? ldf(fr + b + nx) : 0.0f;
+    const float v011 = (vz0 && vy1 && vx1) ? ldf(fr + b + nx + 1) : 0.0f;
+    const float v100 = (vz1 && vy0 && vx0) ? ldf(fr + b + plane) : 0.0f;
+    const float v101 = (vz1 && vy0 && vx1) ? ldf(fr + b + plane + 1) : 0.0f;
+    const float v110 = (vz1 && vy1 && vx0) ? ldf(fr + b + plane + nx) : 0.0f;
+    const float v111 = (vz1 && vy1 && vx1) ? ldf(fr + b + plane + nx + 1) : 0.0f;
+    const float c00 = fmaf(wx, v001 - v000, v000);
+    const float c01 = fmaf(wx, v011 - v010, v010);
+    const float c10 = fmaf(wx, v101 - v100, v100);
+    const float c11 = fmaf(wx, v111 - v110, v110);
+    const float c0 = fmaf(wy, c01 - c00, c00);
+    const float c1 = fmaf(wy, c11 - c10, c10);
+    return fmaf(wz, c1 - c0, c0);
+  }
+}
+
+// ------------------------------------------------------------------ fused evaluation -------------
+
+constexpr int kWin = 5;  // control points [c0-1, c0+4) cover every interval a tile can touch
+
+template <int NDIM, typename FT, typename RT>
+__global__ void __launch_bounds__(kEvalThreads) eval_kernel(const Job* __restrict__ jobs) {
+  const Job& job = jobs[blockIdx.y];
+  if (job.state != nullptr && job.state->phase == kPhaseDone) return;
+  const RefDev& R = *job.ref;
+  const int tile = blockIdx.x;
+  if (tile >= R.n_tiles) return;
+  const int nx = R.nx, ny = R.ny, nz = R.nz;
+  const int row_begin = tile * R.tile_rows;
+  const int row_end = min(row_begin + R.tile_rows, R.n_rows);
+  const int c0 = R.tile_c0[tile];
+  const int cw = max(c0 - 1, 0);
+  const bool bidir = R.bidir != 0;
+  const float dq = R.dq;
+
+  __shared__ float4 sD[kWin * kDParamF4];
+  __shared__ float sred[kEvalWarps][1 + 3 * NDIM];
+  for (int i = threadIdx.x; i < kWin * kDParamF4; i += blockDim.x) {
+    const int k = cw + i / kDParamF4;
+    sD[i] = (k < R.nD) ? job.dparams[k * kDParamF4 + i % kDParamF4] : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  __syncthreads();
+
+  const FT* __restrict__ fr = static_cast<const FT*>(job.frame);
+  const RT* __restrict__ tref;
+  const RT* __restrict__ tgx;
+  const RT* __restrict__ tgy;
+  const RT* __restrict__ tgz;
+  if constexpr (sizeof(RT) == 4) {
+    tref = reinterpret_cast<const RT*>(R.ref32);
+    tgx = reinterpret_cast<const RT*>(R.gx32);
+    tgy = reinterpret_cast<const RT*>(R.gy32);
+    tgz = reinterpret_cast<const RT*>(R.gz32);
+  } else {
+    tref = reinterpret_cast<const RT*>(R.ref16);
+    tgx = reinterpret_cast<const RT*>(R.gx16);
+    tgy = reinterpret_cast<const RT*>(R.gy16);
+    tgz = reinterpret_cast<const RT*>(R.gz16);
+  }
+
+  float af = 0.0f;
+  float ag[3][NDIM];
+#pragma unroll
+  for (int s = 0; s < 3; s++)
+#pragma unroll
+    for (int k = 0; k < NDIM; k++) ag[s][k] = 0.0f;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int row = row_begin + warp; row < row_end; row += kEvalWarps) {
+    const RowDesc rd = R.rows[row];
+    const int z = row / ny;
+    const int y = row - z * ny;
+    const bool flip = bidir && (y & 1);
+    const long long rowoff = (long long)row * nx;
+    for (int x = lane; x < nx; x += 32) {
+      const VoxelModel vm = voxel_model(rd, x, nx, flip, bidir, dq);
+      const float v = sample<NDIM, FT>(fr, sD + (vm.di - cw) * kDParamF4, vm.f, x, y, z, nx, ny, nz);
+      const long long p = rowoff + x;
+      const float t = ldf(tref + p);
+      // include iff the interpolated value is positive: CPU rule px == 0 -> -1, then wimg >= 0
+      // (FrameWarper.cpp:67, 16-25)
+      const float e = (v > 0.0f) ? v - t : 0.0f;
+      af = fmaf(e, e, af);
+      if (!vm.last) {
+        const float e1 = e * vm.f;           // weight of control r+1: Df
+        const float e0 = e * (1.0f - vm.f);  // weight of control r:   1 - Df
+        float gk[NDIM];
+        gk[0] = ldf(tgx + p);
+        gk[1] = ldf(tgy + p);
+        if (NDIM == 3) gk[NDIM - 1] = ldf(tgz + p);
+        if (vm.r == c0) {
+#pragma unroll
+          for (int k = 0; k < NDIM; k++) {
+            ag[0][k] = fmaf(gk[k], e0, ag[0][k]);
+            ag[1][k] = fmaf(gk[k], e1, ag[1][k]);
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < NDIM; k++) {
+            ag[1][k] = fmaf(gk[k], e0, ag[1][k]);
+            ag[2][k] = fmaf(gk[k], e1, ag[2][k]);
+          }
+        }
+      }
+    }
+  }
+
+  // FP32 butterfly across the warp, FP64 across warps (fixed order).
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    af += __shfl_xor_sync(0xffffffffu, af, o);
+#pragma unroll
+    for (int s = 0; s < 3; s++)
+#pragma unroll
+      for (int k = 0; k < NDIM; k++) ag[s][k] += __shfl_xor_sync(0xffffffffu, ag[s][k], o);
+  }
+  if (lane == 0) {
+    sred[warp][0] = af;
+#pragma unroll
+    for (int s = 0; s < 3; s++)
+#pragma unroll
+      for (int k = 0; k < NDIM; k++) sred[warp][1 + s * NDIM + k] = ag[s][k];
+  }
+  __syncthreads();
+  double* out = job.partials + (long long)tile * kPartialDoubles;
+  if (threadIdx.x < 1 + 3 * NDIM) {
+    double acc = 0.0;
+    for (int w = 0; w < kEvalWarps; w++) acc += (double)sred[w][threadIdx.x];
+    const int i = threadIdx.x;
+    if (i == 0) {
+      out[0] = acc;
+    } else {
+      const int s = (i - 1) / NDIM, k = (i - 1) % NDIM;
+      out[2 + s * 3 + k] = acc;
+    }
+  } else if (threadIdx.x == 1 + 3 * NDIM) {
+    out[1] = (double)c0;
+    if (NDIM == 2) out[2 + 0 * 3 + 2] = out[2 + 1 * 3 + 2] = out[2 + 2 * 3 + 2] = 0.0;
+  }
+}
+
+cudaError_t launch_eval(const Job* jobs_dev, int n_jobs, int max_tiles, int n_dim, bool frame_half, bool ref_bf16,
+                        cudaStream_t s) {
+  dim3 grid(max_tiles, n_jobs);
+  if (n_dim == 3) {
+    if (frame_half && ref_bf16)
+      eval_kernel<3, __half, __nv_bfloat16><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
+    else if (frame_half)
+      eval_kernel<3, __half, float><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
+    else if (ref_bf16)
+      eval_kernel<3, float, __nv_bfloat16><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
+    else
+      eval_kernel<3, float, float><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
+  } else {
+    if (frame_half && ref_bf16)
+      eval_kernel<2, __half, __nv_bfloat16><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
+    else if (frame_half)
+      eval_kernel<2, __half, float><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
+    else if (ref_bf16)
+      eval_kernel<2, float, __nv_bfloat16><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
+    else
+      eval_kernel<2, float, float><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
+  }
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ reductions -------------------
+
+__global__ void __launch_bounds__(kSolveThreads) reduce_kernel(const Job* __restrict__ job) {
+  const RefDev& R = *job->ref;
+  reduce_partials(R, job->partials, job->result, job->result + 1);
+}
+
+cudaError_t launch_reduce(const Job* job_dev, const RefDev&, cudaStream_t s) {
+  reduce_kernel<<<1, kSolveThreads, 0, s>>>(job_dev);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ warped image -----------------
+
+template <int NDIM, typename FT>
+__global__ void __launch_bounds__(256) warp_kernel(const RefDev* __restrict__ Rp, const FT* __restrict__ fr,
+                                                   const float4* __restrict__ dparams, float invalid_value,
+                                                   float* __restrict__ out) {
+  const RefDev& R = *Rp;
+  const int nx = R.nx, ny = R.ny, nz = R.nz;
+  extern __shared__ float4 sAll[];
+  for (int i = threadIdx.x; i < R.nD * kDParamF4; i += blockDim.x) sAll[i] = dparams[i];
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  for (int row = blockIdx.x * nwarps + warp; row < R.n_rows; row += gridDim.x * nwarps) {
+    const RowDesc rd = R.rows[row];
+    const int z = row / ny;
+    const int y = row - z * ny;
+    const bool flip = R.bidir && (y & 1);
+    for (int x = lane; x < nx; x += 32) {
+      const VoxelModel vm = voxel_model(rd, x, nx, flip, R.bidir != 0, R.dq);
+      float v = sample<NDIM, FT>(fr, sAll + vm.di * kDParamF4, vm.f, x, y, z, nx, ny, nz);
+      if (v == 0.0f) v = invalid_value;
+      out[(long long)row * nx + x] = v;
+    }
+  }
+}
+
+cudaError_t launch_warp(const RefDev* ref_dev, const RefDev& R, const void* frame, bool frame_half,
+                        const float4* dparams, float invalid_value, float* out, cudaStream_t s) {
+  int blocks = (R.n_rows + 7) / 8;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  size_t smem = (size_t)R.nD * kDParamF4 * sizeof(float4);
+  if (smem > 48 * 1024) {
+    cudaError_t e;
+    if (R.n_dim == 3)
+      e = frame_half ? cudaFuncSetAttribute(warp_kernel<3, __half>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                     : cudaFuncSetAttribute(warp_kernel<3, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    else
+      e = frame_half ? cudaFuncSetAttribute(warp_kernel<2, __half>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                     : cudaFuncSetAttribute(warp_kernel<2, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  if (R.n_dim == 3) {
+    if (frame_half)
+      warp_kernel<3, __half><<<blocks, 256, smem, s>>>(ref_dev, static_cast<const __half*>(frame), dparams, invalid_value, out);
+    else
+      warp_kernel<3, float><<<blocks, 256, smem, s>>>(ref_dev, static_cast<const float*>(frame), dparams, invalid_value, out);
+  } else {
+    if (frame_half)
+      warp_kernel<2, __half><<<blocks, 256, smem, s>>>(ref_dev, static_cast<const __half*>(frame), dparams, invalid_value, out);
+    else
+      warp_kernel<2, float><<<blocks, 256, smem, s>>>(ref_dev, static_cast<const float*>(frame), dparams, invalid_value, out);
+  }
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ Hessian ----------------------
+
+// Per tile and per storage-range slot s (range c0 + s): the 21 (3-D) or 10 (2-D) sums
+//   A = sum v0 v0^T (upper), B = sum v1 v1^T (upper), C = sum v1 v0^T
+// with v0 = float(grad * float(1 - Df)), v1 = float(grad * Df) and Df exact
+// (FrameWarper.cpp:258-259, 319-342), over the voxels of the range that are not its last.
+constexpr int kHessTerms = 21;
+
+template <int NDIM>
+__global__ void __launch_bounds__(256) hessian_tile_kernel(const RefDev* __restrict__ Rp, double pd, double ild,
+                                                           double ifd, double stack, double* __restrict__ parts) {
+  const RefDev& R = *Rp;
+  const int tile = blockIdx.x;
+  const int slot = blockIdx.y;
+  const int nx = R.nx, ny = R.ny;
+  const int row_begin = tile * R.tile_rows;
+  const int row_end = min(row_begin + R.tile_rows, R.n_rows);
+  const int c0 = R.tile_c0[tile];
+  const double nDm1 = (double)(R.nD - 1);
+  constexpr int NU = NDIM * (NDIM + 1) / 2;
+  double acc[2 * NU + NDIM * NDIM];
+#pragma unroll
+  for (int i = 0; i < 2 * NU + NDIM * NDIM; i++) acc[i] = 0.0;
+  for (int row = row_begin; row < row_end; row++) {
+    const RowDesc rd = R.rows[row];
+    const int z = row / ny;
+    const int y = row - z * ny;
+    const bool flip = R.bidir && (y & 1);
+    for (int x = threadIdx.x; x < nx; x += blockDim.x) {
+      const int r = R.bidir ? rd.r0 + (x >= rd.xr ? 1 : 0) : rd.di0 + (x >= rd.xdi ? 1 : 0);
+      if (r - c0 != slot || x == rd.xlast) continue;
+      const int xs = flip ? nx - 1 - x : x;
+      // t = z*interframe + y*interline + x*pixel; q = t / stack * (nD - 1) (FrameWarper.cpp:258-259)
+      const double t = __dadd_rn(__dadd_rn(__dmul_rn((double)z, ifd), __dmul_rn((double)y, ild)), __dmul_rn((double)xs, pd));
+      const double q = __dmul_rn(__ddiv_rn(t, stack), nDm1);
+      const float df = (float)(q - floor(q));
+      const float w0 = __fsub_rn(1.0f, df);
+      const long long p = (long long)row * nx + x;
+      float g[NDIM];
+      g[0] = R.gx32[p];
+      g[1] = R.gy32[p];
+      if (NDIM == 3) g[NDIM - 1] = R.gz32[p];
+      float v0[NDIM], v1[NDIM];
+#pragma unroll
+      for (int k = 0; k < NDIM; k++) {
+        v0[k] = __fmul_rn(g[k], w0);
+        v1[k] = __fmul_rn(g[k], df);
+      }
+      int u = 0;
+#pragma unroll
+      for (int a = 0; a < NDIM; a++)
+#pragma unroll
+        for (int b = a; b < NDIM; b++, u++) {
+          acc[u] += (double)__fmul_rn(v0[a], v0[b]);
+          acc[NU + u] += (double)__fmul_rn(v1[a], v1[b]);
+        }
+#pragma unroll
+      for (int a = 0; a < NDIM; a++)
+#pragma unroll
+        for (int b = 0; b < NDIM; b++) acc[2 * NU + a * NDIM + b] += (double)__fmul_rn(v1[a], v0[b]);
+    }
+  }
+  __shared__ double sacc[256];
+  double* out = parts + ((long long)tile * 2 + slot) * kHessTerms;
+  for (int i = 0; i < 2 * NU + NDIM * NDIM; i++) {
+    sacc[threadIdx.x] = acc[i];
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+      if (threadIdx.x < w) sacc[threadIdx.x] += sacc[threadIdx.x + w];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[i] = sacc[0];
+    __syncthreads();
+  }
+}
+
+// Hd[c] = sum_t A(t, c - c0_t) + B(t, c - 1 - c0_t);  Hl[c] = sum_t C(t, c - 1 - c0_t).
+template <int NDIM>
+__global__ void hessian_reduce_kernel(const RefDev* __restrict__ Rp, const double* __restrict__ parts,
+                                      double* __restrict__ Hd, double* __restrict__ Hl) {
+  const RefDev& R = *Rp;
+  constexpr int NU = NDIM * (NDIM + 1) / 2;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= R.nD) return;
+  double d[NDIM * NDIM], l[NDIM * NDIM];
+  for (int i = 0; i < NDIM * NDIM; i++) d[i] = l[i] = 0.0;
+  const int t0 = max(0, R.ctrl_tiles[c].x), t1 = R.ctrl_tiles[c].y;
+  for (int t = t0; t < t1; t++) {
+    const int ct = R.tile_c0[t];
+    for (int s = 0; s < 2; s++) {
+      const double* pt = parts + ((long long)t * 2 + s) * kHessTerms;
+      const int r = ct + s;
+      if (r == c) {
+        int u = 0;
+        for (int a = 0; a < NDIM; a++)
+          for (int b = a; b < NDIM; b++, u++) {
+            d[a * NDIM + b] += pt[u];
+            if (a != b) d[b * NDIM + a] += pt[u];
+          }
+      }
+      if (r + 1 == c) {
+        int u = 0;
+        for (int a = 0; a < NDIM; a++)
+          for (int b = a; b < NDIM; b++, u++) {
+            d[a * NDIM + b] += pt[NU + u];
+            if (a != b) d[b * NDIM + a] += pt[NU + u];
+          }
+        for (int a = 0; a < NDIM * NDIM; a++) l[a] += pt[2 * NU + a];
+      }
+    }
+  }
+  for (int i = 0; i < NDIM * NDIM; i++) {
+    Hd[c * NDIM * NDIM + i] = d[i];
+    Hl[c * NDIM * NDIM + i] = l[i];
+  }
+}
+
+cudaError_t launch_hessian(const RefDev* ref_dev, const RefDev& R, const double* scan4, double* tile_parts, double* Hd,
+                           double* Hl, cudaStream_t s) {
+  dim3 grid(R.n_tiles, 2);
+  if (R.n_dim == 3) {
+    hessian_tile_kernel<3><<<grid, 256, 0, s>>>(ref_dev, scan4[0], scan4[1], scan4[2], scan4[3], tile_parts);
+    hessian_reduce_kernel<3><<<(R.nD + 127) / 128, 128, 0, s>>>(ref_dev, tile_parts, Hd, Hl);
+  } else {
+    hessian_tile_kernel<2><<<grid, 256, 0, s>>>(ref_dev, scan4[0], scan4[1], scan4[2], scan4[3], tile_parts);
+    hessian_reduce_kernel<2><<<(R.nD + 127) / 128, 128, 0, s>>>(ref_dev, tile_parts, Hd, Hl);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace fa

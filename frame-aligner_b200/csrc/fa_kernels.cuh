@@ -1,0 +1,60 @@
+// fa_kernels.cuh -- kernel launch declarations (implemented in fa_kernels.cu, fa_solve.cu).
+#pragma once
+
+#include "fa_internal.h"
+
+namespace fa {
+
+constexpr int kEvalThreads = 256;
+constexpr int kEvalWarps = kEvalThreads / 32;
+constexpr int kSolveThreads = 128;
+
+// Exact float Sobel3d (Sobel3d.cpp:60-85) of an FP32 volume.
+cudaError_t launch_sobel(const float* m, int nz, int ny, int nx, float* gx, float* gy, float* gz,
+                         cudaStream_t s);
+
+// Per-tile Hessian partials (exact Df per voxel, FP32 products, FP64 sums) and their reduction
+// into Hd / Hl. scan4 = {pixel, interline, interframe, stack} durations after processing.
+cudaError_t launch_hessian(const RefDev* ref_dev, const RefDev& ref_host, const double* scan4, double* tile_parts,
+                           double* Hd, double* Hl, cudaStream_t s);
+
+// FP32 -> BF16 copy.
+cudaError_t launch_to_bf16(const float* in, __nv_bfloat16* out, long long n, cudaStream_t s);
+// Any input dtype -> FP32 or FP16 frame storage.
+cudaError_t launch_convert(const void* in, fa_dtype in_type, void* out, fa_dtype out_type, long long n,
+                           cudaStream_t s);
+
+// Raw frame -> storage with the +1 offset; raw -> downsampled float (block sums).
+cudaError_t launch_offset_convert(const void* in, fa_dtype in_type, void* out, fa_dtype out_type, long long n,
+                                  cudaStream_t s);
+cudaError_t launch_downsample(const void* in, fa_dtype in_type, int nz, int ny, int nx, int b, float* out,
+                              cudaStream_t s);
+
+// Fused warp + error + J^T e over all tiles of n_jobs frames (grid.y = job). frame_half selects
+// FP16 frames, ref_bf16 the BF16 reference/gradient copies.
+cudaError_t launch_eval(const Job* jobs_dev, int n_jobs, int max_tiles, int n_dim, bool frame_half, bool ref_bf16,
+                        cudaStream_t s);
+
+// Reduces one job's tile partials into result = [f, g(P)] (deterministic order).
+cudaError_t launch_reduce(const Job* job_dev, const RefDev& ref_host, cudaStream_t s);
+
+// Warped image (CpuFrameWarper::warpImageInterpolated semantics) for one frame.
+cudaError_t launch_warp(const RefDev* ref_dev, const RefDev& ref_host, const void* frame, bool frame_half,
+                        const float4* dparams, float invalid_value, float* out, cudaStream_t s);
+
+// One trust-region step for each job (grid = n_jobs): reduce partials, advance the state machine,
+// solve the next subproblem, write the next trial point's dparams.
+cudaError_t launch_solve(const Job* jobs_dev, int n_jobs, cudaStream_t s);
+
+// Test hook: the device trust-region subproblem on given dense H (P x P) and g.
+cudaError_t launch_test_subproblem(const double* Hd, const double* Hl, int nD, int nd, const double* g,
+                                   double radius, double* p_out, int* boundary_out, double* work, cudaStream_t s);
+
+// Phase correlation kernels (fa_phase.cu).
+cudaError_t launch_phase_window(const float* in, const double* window, double* out, long long n, cudaStream_t s);
+cudaError_t launch_phase_normalise(double2* spec, const double2* ref_conj, long long n, cudaStream_t s);
+cudaError_t launch_phase_argmax(const double* surf, long long n, double* block_val, long long* block_idx,
+                                int n_blocks, long long* out_idx, cudaStream_t s);
+cudaError_t launch_phase_conj(const double2* in, double2* out, long long n, cudaStream_t s);
+
+}  // namespace fa

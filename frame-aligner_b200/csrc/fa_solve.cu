@@ -1,0 +1,337 @@
+// fa_solve.cu -- device-side trust-region solver (FP64). Built with -fmad=false: every product and
+// sum is rounded separately, in the same order as the CPU statement of the algorithm, so that given
+// identical f, g and H the device takes bit-identical steps.
+//
+// Algorithm (the reference calls dlib::find_min_trust_region at FrameAligner/FrameWarpAligner.cpp:
+// 205-209 with objective_delta_stop_strategy(1e-8) and radius 40; dlib's source is not part of the
+// reference tree, so this is the project's own statement of the method):
+//   outer loop: Nocedal & Wright, Numerical Optimization (2nd ed.), Algorithm 4.1 with eta = 0,
+//     Delta_max = 1000; rho < 1/4 shrinks Delta by 4, rho > 3/4 on the boundary doubles it; a
+//     rejected step leaves f unchanged, so the |delta f| < 1e-8 rule ends the solve.
+//   subproblem: More & Sorensen (1983) Newton iteration on 1/|p(lambda)| - 1/Delta with a
+//     safeguarded bracket, eps = 0.1, at most 20 factorisations, using a block-tridiagonal
+//     Cholesky of H + lambda I (H = J^T J has n_dim x n_dim blocks, |i - j| <= 1).
+#include <float.h>
+
+#include "fa_device.cuh"
+
+namespace fa {
+
+namespace {
+
+constexpr double kDblEps = 2.220446049250313080847e-16;
+constexpr double kMinDelta = 1e-8;
+constexpr double kRadius0 = 40.0;
+constexpr double kRadiusMax = 1000.0;
+
+struct Band {
+  const double* Hd;
+  const double* Hl;
+  int nd, nD, P;
+};
+
+// Element (i, j) of the dense Hessian.
+__device__ __forceinline__ double hval(const Band& B, int i, int j) {
+  const int bi = i / B.nd, bj = j / B.nd;
+  const int a = i - bi * B.nd, b = j - bj * B.nd;
+  const int nn = B.nd * B.nd;
+  if (bi == bj) return B.Hd[bi * nn + a * B.nd + b];
+  if (bi == bj + 1) return B.Hl[bi * nn + a * B.nd + b];
+  if (bj == bi + 1) return B.Hl[bj * nn + b * B.nd + a];
+  return 0.0;
+}
+
+// Lower band of L: row i holds columns [(bi-1)*nd, (bi+1)*nd), stored at L[i*W + k - (bi-1)*nd].
+__device__ __forceinline__ int kstart(const Band& B, int i) {
+  const int k = (i / B.nd - 1) * B.nd;
+  return k < 0 ? 0 : k;
+}
+__device__ __forceinline__ double& lref(const Band& B, double* L, int i, int k) {
+  return L[i * 2 * B.nd + k - (i / B.nd - 1) * B.nd];
+}
+__device__ __forceinline__ double lval(const Band& B, const double* L, int i, int k) {
+  if (k < kstart(B, i) || k > i) return 0.0;
+  return L[i * 2 * B.nd + k - (i / B.nd - 1) * B.nd];
+}
+
+// Cholesky of H + lambda I, row by row, summing the nonzero band terms in ascending k (the dense
+// algorithm's order: its skipped terms are exact zeros).
+__device__ int band_chol(const Band& B, double lambda, double* L) {
+  for (int i = 0; i < B.P; i++) {
+    const int ki = kstart(B, i);
+    for (int j = ki; j <= i; j++) {
+      double s = hval(B, i, j) + (i == j ? lambda : 0.0);
+      const int kj = kstart(B, j);
+      for (int k = (ki > kj ? ki : kj); k < j; k++) s -= lref(B, L, i, k) * lref(B, L, j, k);
+      if (i == j) {
+        if (!(s > 0.0)) return -1;
+        lref(B, L, i, i) = sqrt(s);
+      } else {
+        lref(B, L, i, j) = s / lref(B, L, j, j);
+      }
+    }
+  }
+  return 0;
+}
+
+__device__ void band_forward(const Band& B, const double* L, const double* b, double* y) {
+  for (int i = 0; i < B.P; i++) {
+    double s = b[i];
+    for (int k = kstart(B, i); k < i; k++) s -= lval(B, L, i, k) * y[k];
+    y[i] = s / lval(B, L, i, i);
+  }
+}
+
+__device__ void band_backward(const Band& B, const double* L, const double* y, double* x) {
+  for (int i = B.P - 1; i >= 0; i--) {
+    double s = y[i];
+    int kend = (i / B.nd + 2) * B.nd;
+    if (kend > B.P) kend = B.P;
+    for (int k = i + 1; k < kend; k++) s -= lval(B, L, k, i) * x[k];
+    x[i] = s / lval(B, L, i, i);
+  }
+}
+
+__device__ double norm2(int n, const double* v) {
+  double s = 0;
+  for (int i = 0; i < n; i++) s += v[i] * v[i];
+  return sqrt(s);
+}
+
+// Returns 1 when the step lies on the trust-region boundary. work: P*(2*nd) + 2*P doubles.
+__device__ int subproblem(const Band& B, const double* g, double radius, double eps, int max_iter, double* p,
+                          double* work) {
+  const int P = B.P;
+  double* L = work;
+  double* y = work + P * 2 * B.nd;
+  double* rhs = y + P;
+  const double gnorm = norm2(P, g);
+  if (gnorm == 0.0) {
+    for (int i = 0; i < P; i++) p[i] = 0.0;
+    return 0;
+  }
+  double hinf = 0, mindiag = hval(B, 0, 0);
+  for (int i = 0; i < P; i++) {
+    double r = 0;
+    int j0 = (i / B.nd - 1) * B.nd, j1 = (i / B.nd + 2) * B.nd;
+    if (j0 < 0) j0 = 0;
+    if (j1 > P) j1 = P;
+    for (int j = j0; j < j1; j++) r += fabs(hval(B, i, j));
+    if (r > hinf) hinf = r;
+    const double d = hval(B, i, i);
+    if (d < mindiag) mindiag = d;
+  }
+  double lam_hi = gnorm / radius + hinf;
+  double lam_lo = gnorm / radius - hinf;
+  if (-mindiag > lam_lo) lam_lo = -mindiag;
+  if (lam_lo < 0) lam_lo = 0;
+  int have_p = 0, boundary = 1;
+  double lambda = 0.0;
+  for (int i = 0; i < P; i++) rhs[i] = -g[i];
+  for (int it = 0; it < max_iter; it++) {
+    if (band_chol(B, lambda, L) != 0) {
+      if (lambda > lam_lo) lam_lo = lambda;
+      const double a = sqrt(lam_lo * lam_hi), b = lam_lo + 0.001 * (lam_hi - lam_lo);
+      lambda = a > b ? a : b;
+      continue;
+    }
+    band_forward(B, L, rhs, y);
+    band_backward(B, L, y, p);
+    have_p = 1;
+    const double pn = norm2(P, p);
+    if (lambda == 0.0 && pn <= radius) {
+      boundary = 0;
+      break;
+    }
+    if (fabs(pn - radius) <= eps * radius) break;
+    if (pn < radius) {
+      if (lambda < lam_hi) lam_hi = lambda;
+    } else {
+      if (lambda > lam_lo) lam_lo = lambda;
+    }
+    band_forward(B, L, p, y);
+    const double qn = norm2(P, y);
+    const double r = pn / qn;
+    double next = lambda + r * r * (pn - radius) / radius;
+    if (!(next > lam_lo && next < lam_hi)) {
+      const double a = sqrt(lam_lo * lam_hi), b = lam_lo + 0.001 * (lam_hi - lam_lo);
+      next = a > b ? a : b;
+    }
+    lambda = next;
+  }
+  if (!have_p) {
+    for (int i = 0; i < P; i++) p[i] = -g[i] * (radius / gnorm);
+  } else if (boundary) {
+    const double pn = norm2(P, p);
+    if (pn > radius) {
+      const double s = radius / pn;
+      for (int i = 0; i < P; i++) p[i] *= s;
+    }
+  }
+  return boundary;
+}
+
+// Predicted reduction -(g.p + 0.5 p.H.p) with the dense algorithm's summation order.
+__device__ double predicted(const Band& B, const double* g, const double* p) {
+  double gp = 0, pHp = 0;
+  for (int i = 0; i < B.P; i++) {
+    double s = 0;
+    int j0 = (i / B.nd - 1) * B.nd, j1 = (i / B.nd + 2) * B.nd;
+    if (j0 < 0) j0 = 0;
+    if (j1 > B.P) j1 = B.P;
+    for (int j = j0; j < j1; j++) s += hval(B, i, j) * p[j];
+    gp += g[i] * p[i];
+    pHp += p[i] * s;
+  }
+  return -(gp + 0.5 * pHp);
+}
+
+// Start a new trust-region iteration if the stop rule allows it. Returns false when done.
+__device__ bool loop_top(FrameState* S, const Band& B, const double* g, double* p, double* work) {
+  if (S->max_iter > 0 && S->iter >= S->max_iter) {
+    S->hit_max = 1;
+    return false;
+  }
+  if (S->have_prev && fabs(S->f - S->f_prev) < kMinDelta) return false;
+  S->have_prev = 1;
+  S->f_prev = S->f;
+  S->iter++;
+  S->boundary = subproblem(B, g, S->radius, 0.1, 20, p, work);
+  return true;
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kSolveThreads) solve_kernel(const Job* __restrict__ jobs) {
+  const Job& job = jobs[blockIdx.x];
+  FrameState* S = job.state;
+  if (S->phase == kPhaseDone) return;
+  const RefDev& R = *job.ref;
+  __shared__ double s_f;
+  reduce_partials(R, job.partials, &s_f, job.gt);
+  __syncthreads();
+  const int P = R.P, nd = R.n_dim;
+  if (threadIdx.x == 0) {
+    Band B{R.Hd, R.Hl, nd, R.nD, P};
+    const double ft = s_f;
+    double* x = job.x;
+    double* g = job.g;
+    double* p = job.p;
+    const double* gt = job.gt;
+    bool go_top = false, done = false;
+    int next = kPhaseTrial;
+    S->evaluations++;
+    switch (S->phase) {
+      case kPhaseStartZero: {
+        S->f_start = ft;
+        for (int i = 0; i < P; i++) g[i] = gt[i];
+        bool rigid = false;
+        for (int c = 0; c < nd; c++) rigid = rigid || (S->rigid[c] != 0.0);
+        if (rigid) {
+          for (int k = 0; k < R.nD; k++)
+            for (int c = 0; c < nd; c++) p[k * nd + c] = S->rigid[c];
+          next = kPhaseStartRigid;
+        } else {
+          S->f = ft;
+          go_top = true;
+        }
+        break;
+      }
+      case kPhaseStartRigid: {
+        // Starting points {0, 0, rigid}: std::min_element keeps the first minimum
+        // (FrameWarpAligner.cpp:194-198).
+        if (ft < S->f_start) {
+          for (int i = 0; i < P; i++) {
+            x[i] = p[i];
+            g[i] = gt[i];
+          }
+          S->f = ft;
+        } else {
+          S->f = S->f_start;
+        }
+        go_top = true;
+        break;
+      }
+      case kPhaseTrial: {
+        const double pred = predicted(B, g, p);
+        const double meas = S->f - ft;
+        if (fabs(pred) <= fabs(meas) * kDblEps) {
+          done = true;
+          break;
+        }
+        const double rho = meas / fabs(pred);
+        if (!isfinite(rho)) {
+          done = true;
+          break;
+        }
+        if (rho < 0.25) {
+          S->radius *= 0.25;
+          if (S->radius <= kRadius0 * kDblEps) {
+            done = true;
+            break;
+          }
+        } else if (rho > 0.75 && S->boundary) {
+          S->radius = 2 * S->radius < kRadiusMax ? 2 * S->radius : kRadiusMax;
+        }
+        if (rho > 0) {
+          for (int i = 0; i < P; i++) {
+            x[i] = x[i] + p[i];
+            g[i] = gt[i];
+          }
+          S->f = ft;
+          S->accepted++;
+        }
+        if (!loop_top(S, B, g, p, job.work)) done = true;
+        break;
+      }
+      default:
+        done = true;
+    }
+    if (go_top) {
+      for (int i = 0; i < P; i++) p[i] = 0.0;
+      S->radius = kRadius0;
+      S->iter = 0;
+      S->have_prev = 0;
+      if (!loop_top(S, B, g, p, job.work)) done = true;
+    }
+    S->phase = done ? kPhaseDone : next;
+  }
+  __syncthreads();
+  if (S->phase == kPhaseDone) return;
+  // Next trial point D = x + p, as the fused pass's control-point parameters.
+  for (int k = threadIdx.x; k < R.nD; k += blockDim.x) {
+    double d[3], dn[3];
+    for (int c = 0; c < 3; c++) {
+      d[c] = c < nd ? job.x[k * nd + c] + job.p[k * nd + c] : 0.0;
+      dn[c] = (c < nd && k + 1 < R.nD) ? job.x[(k + 1) * nd + c] + job.p[(k + 1) * nd + c] : d[c];
+    }
+    float4 a, b, e;
+    const double f0 = floor(d[0]), f1 = floor(d[1]), f2 = floor(d[2]);
+    a = make_float4((float)f0, (float)f1, (float)f2, 0.f);
+    b = make_float4((float)(d[0] - f0), (float)(d[1] - f1), (float)(d[2] - f2), 0.f);
+    e = make_float4((float)(dn[0] - d[0]), (float)(dn[1] - d[1]), (float)(dn[2] - d[2]), 0.f);
+    job.dparams[k * kDParamF4 + 0] = a;
+    job.dparams[k * kDParamF4 + 1] = b;
+    job.dparams[k * kDParamF4 + 2] = e;
+  }
+}
+
+cudaError_t launch_solve(const Job* jobs_dev, int n_jobs, cudaStream_t s) {
+  solve_kernel<<<n_jobs, kSolveThreads, 0, s>>>(jobs_dev);
+  return cudaGetLastError();
+}
+
+__global__ void test_subproblem_kernel(const double* Hd, const double* Hl, int nD, int nd, const double* g,
+                                       double radius, double* p, int* boundary, double* work) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  Band B{Hd, Hl, nd, nD, nD * nd};
+  *boundary = subproblem(B, g, radius, 0.1, 20, p, work);
+}
+
+cudaError_t launch_test_subproblem(const double* Hd, const double* Hl, int nD, int nd, const double* g,
+                                   double radius, double* p_out, int* boundary_out, double* work, cudaStream_t s) {
+  test_subproblem_kernel<<<1, 32, 0, s>>>(Hd, Hl, nD, nd, g, radius, p_out, boundary_out, work);
+  return cudaGetLastError();
+}
+
+}  // namespace fa

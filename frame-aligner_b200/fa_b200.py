@@ -1,0 +1,469 @@
+"""Python binding of the C ABI in include/fa_b200.h (ctypes over the in-tree libfa_b200.so).
+
+The classes mirror the reference's warper interface (FrameAligner/FrameWarper.h:95-143 and
+FrameAligner/GpuFrameWarper.h:31-72) so that tests read like the reference's own call sequence:
+
+    w = B200FrameWarper(ctx)
+    w.setReference(reference, nD, scan_params)       # AbstractFrameWarper::setReference
+    w.registerFrame(frame)                           # GpuFrameWarper::registerFrame
+    f = w.getError(frame, D)                         # getError -> sum of squared errors
+    jac = w.getJacobian(frame, D)                    # getJacobian -> J^T e
+    wimg = w.warpImageInterpolated(frame, D, -1)     # warpImageInterpolated
+    w.deregisterFrame(frame)
+
+There is no CPU fallback: if libfa_b200.so is missing or no sm_100 device is present, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfa_b200.so")
+
+FA_OK = 0
+STATUS = {0: "ok", 1: "bad argument", 2: "out of memory", 3: "CUDA error", 4: "timeout", 5: "unsupported",
+          6: "not found", 7: "bad state", 8: "busy"}
+F32, F16, BF16, U16 = 0, 1, 2, 3
+PREC_F32, PREC_MIXED = 0, 1
+_DTYPES = {np.dtype(np.float32): F32, np.dtype(np.float16): F16, np.dtype(np.uint16): U16}
+
+
+class FaError(RuntimeError):
+    def __init__(self, status, message):
+        self.status = status
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+
+
+class ScanParams(C.Structure):
+    """ImageScanParameters fields (FrameAligner/ImageScanParameters.h:22-31)."""
+    _fields_ = [
+        ("line_duration", C.c_double),
+        ("interline_duration", C.c_double),
+        ("pixel_duration", C.c_double),
+        ("frame_duration", C.c_double),
+        ("interframe_duration", C.c_double),
+        ("stack_duration", C.c_double),
+        ("n_x", C.c_int),
+        ("n_y", C.c_int),
+        ("n_z", C.c_int),
+        ("bidirectional", C.c_int),
+    ]
+
+
+class Config(C.Structure):
+    _fields_ = [("device", C.c_int), ("memory_budget", C.c_size_t)]
+
+
+class AlignerParams(C.Structure):
+    """RealignmentParameters fields read by the aligner (FrameAligner/AbstractFrameAligner.h:31-48)."""
+    _fields_ = [
+        ("spatial_binning", C.c_int),
+        ("n_resampling_points", C.c_int),
+        ("nD", C.c_int),
+        ("smoothing", C.c_double),
+        ("precision", C.c_int),
+        ("max_iterations", C.c_int),
+    ]
+
+
+class AlignStats(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int),
+        ("evaluations", C.c_int),
+        ("accepted", C.c_int),
+        ("status", C.c_int),
+        ("f_final", C.c_double),
+        ("radius_final", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_vp = C.c_void_p
+
+# (name, argtypes) for every entry point declared in include/fa_b200.h
+SIGNATURES = {
+    "fa_gpu_support": [C.POINTER(C.c_int), C.c_char_p, C.c_size_t],
+    "fa_create": [C.POINTER(Config), C.POINTER(_vp)],
+    "fa_destroy": [_vp],
+    "fa_last_error": [],
+    "fa_status_string": [C.c_int],
+    "fa_scan_params_init": [C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
+                            C.POINTER(ScanParams)],
+    "fa_set_reference": [_vp, _f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(ScanParams), C.c_int,
+                         C.POINTER(_vp)],
+    "fa_set_reference_device": [_vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(ScanParams), C.c_int,
+                                C.POINTER(_vp)],
+    "fa_reference_destroy": [_vp],
+    "fa_reference_info": [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)],
+    "fa_get_hessian": [_vp, _f64p],
+    "fa_get_gradient": [_vp, _vp, _vp, _vp],
+    "fa_get_ranges": [_vp, _i32p],
+    "fa_register_frame": [_vp, _vp, C.c_int, C.POINTER(_vp)],
+    "fa_register_frame_device": [_vp, _vp, C.c_int, C.POINTER(_vp)],
+    "fa_update_frame": [_vp, _vp, C.c_int],
+    "fa_deregister_frame": [_vp],
+    "fa_get_error": [_vp, _f64p, C.POINTER(C.c_double)],
+    "fa_get_jacobian": [_vp, _f64p, _f64p],
+    "fa_warp": [_vp, _f64p, C.c_float, _f32p],
+    "fa_align_frame": [_vp, _vp, C.c_int, _f64p, C.POINTER(AlignStats)],
+    "fa_align_batch": [_vp, C.c_int, _vp, C.c_int, _f64p, _vp],
+    "fa_correlator_create": [_vp, _f32p, C.c_int, C.c_int, C.c_int, C.POINTER(_vp)],
+    "fa_correlator_destroy": [_vp],
+    "fa_correlator_shift": [_vp, _f32p, _f64p],
+    "fa_correlator_shift_device": [_vp, _vp, _f64p],
+    "fa_aligner_create": [_vp, C.c_void_p, C.POINTER(_vp)],
+    "fa_aligner_destroy": [_vp],
+    "fa_aligner_set_reference": [_vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(ScanParams)],
+    "fa_aligner_info": [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)],
+    "fa_aligner_add_frames": [_vp, _vp, C.c_int, C.c_int, _f64p, _vp],
+    "fa_aligner_add_frames_device": [_vp, _vp, C.c_int, C.c_int, _f64p, _vp],
+    "fa_kernel_launches": [],
+    "fa_aligner_last_device_ms": [_vp, C.POINTER(C.c_double)],
+    "fa_profile_eval": [_vp, C.c_int, _f64p, C.c_int, C.POINTER(C.c_double)],
+    "fa_test_tr_subproblem": [_vp, C.c_int, C.c_int, _f64p, _f64p, C.c_double, _f64p, C.POINTER(C.c_int)],
+}
+
+
+def lib():
+    """Loads libfa_b200.so. Raises if it is missing: there is no fallback path."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with __graft_entry__.build() "
+                               "(make -C frame-aligner_b200)")
+        L = C.CDLL(LIB_PATH)
+        for name, args in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = C.c_int
+        L.fa_kernel_launches.restype = C.c_longlong
+        L.fa_last_error.restype = C.c_char_p
+        L.fa_status_string.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def check(status):
+    if status != FA_OK:
+        raise FaError(status, lib().fa_last_error().decode(errors="replace"))
+
+
+def gpu_support():
+    ok = C.c_int(0)
+    msg = C.create_string_buffer(256)
+    check(lib().fa_gpu_support(C.byref(ok), msg, 256))
+    return bool(ok.value), msg.value.decode()
+
+
+def scan_params(line, interline, interframe, nx, ny, nz, bidirectional=False) -> ScanParams:
+    """ImageScanParameters constructor (FrameAligner/ImageScanParameters.h:7-20)."""
+    s = ScanParams()
+    check(lib().fa_scan_params_init(line, interline, interframe, nx, ny, nz, int(bidirectional), C.byref(s)))
+    return s
+
+
+def _c64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Context:
+    def __init__(self, device=0, memory_budget=0):
+        self._h = _vp()
+        cfg = Config(device, memory_budget)
+        check(lib().fa_create(C.byref(cfg), C.byref(self._h)))
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().fa_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Reference:
+    """A reference volume with its device-resident gradient and Hessian."""
+
+    def __init__(self, ctx: Context, reference, nD, scan: ScanParams, precision=PREC_F32, device_ptr=None,
+                 shape=None):
+        self.ctx = ctx
+        self._h = _vp()
+        if device_ptr is not None:
+            nz, ny, nx = shape
+            check(lib().fa_set_reference_device(ctx._h, device_ptr, nz, ny, nx, int(nD), C.byref(scan), precision,
+                                                C.byref(self._h)))
+        else:
+            ref = np.ascontiguousarray(reference, dtype=np.float32)
+            if ref.ndim == 2:
+                ref = ref[None]
+            nz, ny, nx = ref.shape
+            check(lib().fa_set_reference(ctx._h, ref, nz, ny, nx, int(nD), C.byref(scan), precision,
+                                         C.byref(self._h)))
+        self.dims = (nz, ny, nx)
+        self.nD = int(nD)
+        self.precision = precision
+        nd, P = C.c_int(), C.c_int()
+        check(lib().fa_reference_info(self._h, C.byref(nd), C.byref(P)))
+        self.n_dim, self.P = nd.value, P.value
+        self.N = nz * ny * nx
+
+    def hessian(self):
+        H = np.empty((self.P, self.P), np.float64)
+        check(lib().fa_get_hessian(self._h, H))
+        return H
+
+    def gradient(self):
+        g = [np.empty(self.dims, np.float32) for _ in range(3)]
+        check(lib().fa_get_gradient(self._h, *[x.ctypes.data for x in g]))
+        return g
+
+    def ranges(self):
+        r = np.empty(2 * self.nD, np.int32)
+        check(lib().fa_get_ranges(self._h, r))
+        return r.reshape(self.nD, 2)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            check(lib().fa_reference_destroy(self._h))
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Frame:
+    """A registered frame (device copy in the reference's storage precision)."""
+
+    def __init__(self, ref: Reference, data=None, device_ptr=None, dtype=F32):
+        self.ref = ref
+        self._h = _vp()
+        if device_ptr is not None:
+            check(lib().fa_register_frame_device(ref._h, device_ptr, dtype, C.byref(self._h)))
+        else:
+            arr = np.ascontiguousarray(data)
+            if arr.dtype not in _DTYPES:
+                arr = arr.astype(np.float32)
+            self._keep = arr
+            check(lib().fa_register_frame(ref._h, arr.ctypes.data, _DTYPES[arr.dtype], C.byref(self._h)))
+            self._keep = None
+
+    def update(self, data):
+        arr = np.ascontiguousarray(data)
+        if arr.dtype not in _DTYPES:
+            arr = arr.astype(np.float32)
+        check(lib().fa_update_frame(self._h, arr.ctypes.data, _DTYPES[arr.dtype]))
+
+    def get_error(self, D):
+        f = C.c_double()
+        check(lib().fa_get_error(self._h, _c64(D).ravel(), C.byref(f)))
+        return f.value
+
+    def get_jacobian(self, D):
+        j = np.empty(self.ref.P, np.float64)
+        check(lib().fa_get_jacobian(self._h, _c64(D).ravel(), j))
+        return j
+
+    def warp(self, D, invalid_value=0.0):
+        out = np.empty(self.ref.N, np.float32)
+        check(lib().fa_warp(self._h, _c64(D).ravel(), float(invalid_value), out))
+        return out.reshape(self.ref.dims)
+
+    def align(self, rigid_shift=None, max_iterations=100):
+        D = np.empty((self.ref.nD, 3), np.float64)
+        st = AlignStats()
+        rs = None if rigid_shift is None else _c64(rigid_shift)
+        check(lib().fa_align_frame(self._h, None if rs is None else rs.ctypes.data, max_iterations, D,
+                                   C.byref(st)))
+        return D, st.as_dict()
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            check(lib().fa_deregister_frame(self._h))
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def align_batch(frames, rigid_shifts=None, max_iterations=100):
+    n = len(frames)
+    handles = (_vp * n)(*[f._h.value for f in frames])
+    nD = frames[0].ref.nD
+    D = np.empty((n, nD, 3), np.float64)
+    stats = (AlignStats * n)()
+    rs = None if rigid_shifts is None else _c64(rigid_shifts)
+    check(lib().fa_align_batch(C.cast(handles, _vp), n, None if rs is None else rs.ctypes.data, max_iterations, D,
+                               C.cast(stats, _vp)))
+    return D, [s.as_dict() for s in stats]
+
+
+class Correlator:
+    """VolumePhaseCorrelator (FrameAligner/VolumePhaseCorrelator.h:29-43) on the device."""
+
+    def __init__(self, ctx: Context, reference):
+        ref = np.ascontiguousarray(reference, dtype=np.float32)
+        if ref.ndim == 2:
+            ref = ref[None]
+        self.dims = ref.shape
+        self._h = _vp()
+        check(lib().fa_correlator_create(ctx._h, ref, *ref.shape, C.byref(self._h)))
+
+    def compute_shift(self, volume):
+        s = np.empty(3, np.float64)
+        vol = np.ascontiguousarray(volume, dtype=np.float32).reshape(self.dims)
+        check(lib().fa_correlator_shift(self._h, vol, s))
+        return s
+
+    def compute_shift_device(self, ptr):
+        s = np.empty(3, np.float64)
+        check(lib().fa_correlator_shift_device(self._h, ptr, s))
+        return s
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().fa_correlator_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Aligner:
+    """FrameWarpAligner's setReference / addFrame flow, batched (fa_aligner_*)."""
+
+    def __init__(self, ctx: Context, spatial_binning=1, n_resampling_points=30, nD=0, precision=PREC_MIXED,
+                 max_iterations=100, smoothing=0.0):
+        self.ctx = ctx
+        self._h = _vp()
+        prm = AlignerParams(spatial_binning, n_resampling_points, nD, smoothing, precision, max_iterations)
+        check(lib().fa_aligner_create(ctx._h, C.byref(prm), C.byref(self._h)))
+
+    def set_reference(self, reference, scan: ScanParams):
+        ref = np.ascontiguousarray(reference)
+        if ref.dtype not in (np.float32, np.uint16):
+            ref = ref.astype(np.float32)
+        if ref.ndim == 2:
+            ref = ref[None]
+        self.dims = ref.shape
+        check(lib().fa_aligner_set_reference(self._h, ref.ctypes.data, _DTYPES[ref.dtype], *ref.shape, C.byref(scan)))
+        nD, nd = C.c_int(), C.c_int()
+        check(lib().fa_aligner_info(self._h, C.byref(nD), C.byref(nd)))
+        self.nD, self.n_dim = nD.value, nd.value
+
+    def add_frames(self, frames):
+        """frames: sequence of host arrays (float32 or uint16), one per frame."""
+        arrs = [np.ascontiguousarray(f) for f in frames]
+        dt = arrs[0].dtype
+        if dt not in (np.float32, np.uint16):
+            arrs = [a.astype(np.float32) for a in arrs]
+            dt = np.dtype(np.float32)
+        n = len(arrs)
+        ptrs = (_vp * n)(*[a.ctypes.data for a in arrs])
+        D = np.empty((n, self.nD, 3), np.float64)
+        stats = (AlignStats * n)()
+        check(lib().fa_aligner_add_frames(self._h, C.cast(ptrs, _vp), _DTYPES[dt], n, D, C.cast(stats, _vp)))
+        return D, [s.as_dict() for s in stats]
+
+    def last_device_ms(self):
+        ms = C.c_double()
+        check(lib().fa_aligner_last_device_ms(self._h, C.byref(ms)))
+        return ms.value
+
+    def add_frames_device(self, ptrs, dtype, n):
+        arr = (_vp * n)(*ptrs)
+        D = np.empty((n, self.nD, 3), np.float64)
+        stats = (AlignStats * n)()
+        check(lib().fa_aligner_add_frames_device(self._h, C.cast(arr, _vp), dtype, n, D, C.cast(stats, _vp)))
+        return D, [s.as_dict() for s in stats]
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().fa_aligner_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def kernel_launches():
+    return int(lib().fa_kernel_launches())
+
+
+def profile_eval(frames, D, launches=20):
+    n = len(frames)
+    handles = (_vp * n)(*[f._h.value for f in frames])
+    ms = C.c_double()
+    check(lib().fa_profile_eval(C.cast(handles, _vp), n, _c64(D).ravel(), launches, C.byref(ms)))
+    return ms.value
+
+
+def test_tr_subproblem(ctx: Context, nD, n_dim, H, g, radius):
+    P = nD * n_dim
+    p = np.empty(P, np.float64)
+    b = C.c_int()
+    check(lib().fa_test_tr_subproblem(ctx._h, nD, n_dim, _c64(H), _c64(g), radius, p, C.byref(b)))
+    return p, bool(b.value)
+
+
+class B200FrameWarper:
+    """AbstractFrameWarper-shaped facade (FrameAligner/FrameWarper.h:95-143) over the C ABI.
+
+    Frames are identified by the identity of the numpy array passed to registerFrame, the way the
+    reference identifies cv::Mat frames by their data pointer (GpuFrameWarper.h:55)."""
+
+    def __init__(self, ctx: Context, precision=PREC_F32):
+        self.ctx = ctx
+        self.precision = precision
+        self.reference = None
+        self.frames = {}
+
+    def setReference(self, reference, nD, scan: ScanParams):
+        self.reference = Reference(self.ctx, reference, nD, scan, self.precision)
+        self.n_dim = self.reference.n_dim
+        self.dims = list(self.reference.dims)
+        self.H = self.reference.hessian()
+
+    def registerFrame(self, frame):
+        self.frames[id(frame)] = Frame(self.reference, frame)
+
+    def deregisterFrame(self, frame):
+        fr = self.frames.pop(id(frame))
+        fr.close()
+
+    def _frame(self, frame):
+        if id(frame) not in self.frames:
+            raise FaError(6, "Unrecognised frame")  # GpuFrameWarper.cpp:162-167
+        return self.frames[id(frame)]
+
+    def getError(self, frame, D):
+        return self._frame(frame).get_error(D)
+
+    def getJacobian(self, frame, D):
+        return self._frame(frame).get_jacobian(D)
+
+    def warpImageInterpolated(self, frame, D, invalid_value=0):
+        return self._frame(frame).warp(D, invalid_value)

@@ -1,0 +1,245 @@
+/*
+ * fa_b200.h -- C ABI of the B200 (sm_100a) frame-aligner warper library.
+ *
+ * This library replaces the GPU warper of flimfit/frame-aligner (class GpuFrameWarper,
+ * FrameAligner/GpuFrameWarper.h:31-72) behind the warper interface AbstractFrameWarper
+ * (FrameAligner/FrameWarper.h:95-143). Every entry point is plain C: pointers, sizes, status codes.
+ * Paths in the citations are relative to the reference project's root.
+ *
+ * Conventions
+ *  - Volumes are {nz, ny, nx} row-major, x fastest (FrameAligner/Cv3dUtils.cpp:6-8: Z=0, Y=1, X=2).
+ *  - A displacement set D is nD control points of 3 doubles (x, y, z), the memory layout of
+ *    std::vector<cv::Point3d>. For single-plane data (nz == 1, n_dim == 2) the z component is
+ *    ignored.
+ *  - Parameter vectors (Jacobians, Hessians) use OptimisationModel's order
+ *    [D0.x, D0.y, (D0.z), D1.x, ...] (FrameAligner/OptimisationModel.cpp:14-27), P = nD * n_dim.
+ *  - Pointers named host_* or documented as host memory are ordinary (pageable or pinned) host
+ *    memory; pointers documented as device memory must be CUDA device allocations on the
+ *    context's device.
+ *  - Every function returns fa_status. The library never resets the device; on FA_ERR_CUDA the
+ *    context stays usable unless the CUDA error was sticky. fa_last_error() describes the last
+ *    failure on the calling thread.
+ */
+#ifndef FA_B200_H
+#define FA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  FA_OK = 0,
+  FA_ERR_BAD_ARG = 1,      /* invalid argument (the reference would throw or has undefined behaviour) */
+  FA_ERR_OOM = 2,          /* device memory or the context's memory budget is exhausted */
+  FA_ERR_CUDA = 3,         /* a CUDA runtime / cuFFT call failed */
+  FA_ERR_TIMEOUT = 4,      /* a bounded wait ran out */
+  FA_ERR_UNSUPPORTED = 5,  /* valid for the reference but outside what this library implements */
+  FA_ERR_NOT_FOUND = 6,    /* unknown handle / request id */
+  FA_ERR_STATE = 7,        /* call out of order (e.g. no reference set) */
+  FA_ERR_BUSY = 8          /* no free slot; retry later */
+} fa_status;
+
+typedef enum { FA_F32 = 0, FA_F16 = 1, FA_BF16 = 2, FA_U16 = 3 } fa_dtype;
+
+/* Fields of ImageScanParameters (FrameAligner/ImageScanParameters.h:22-31), after construction. */
+typedef struct {
+  double line_duration;
+  double interline_duration;
+  double pixel_duration;
+  double frame_duration;
+  double interframe_duration;
+  double stack_duration;
+  int n_x, n_y, n_z;
+  int bidirectional;
+} fa_scan_params;
+
+typedef struct fa_context fa_context;
+typedef struct fa_reference fa_reference;
+typedef struct fa_frame fa_frame;
+typedef struct fa_correlator fa_correlator;
+
+typedef struct {
+  int device;            /* CUDA device ordinal */
+  size_t memory_budget;  /* bytes of device memory the context may hold; 0 = 90% of free memory */
+} fa_config;
+
+/* Storage precision of a reference's device copies (the FP32 copy always exists: the Gauss-Newton
+   Hessian and the plain path use it). */
+typedef enum {
+  FA_PREC_F32 = 0,   /* plain path: FP32 reference, gradient and frames */
+  FA_PREC_MIXED = 1  /* BF16 reference + gradient, FP16 frames, FP32 accumulation, FP64 solve */
+} fa_precision;
+
+/* ---------------------------------------------------------------- context --------------------- */
+
+/* GpuFrameWarper::getGpuSupportInformation (FrameAligner/GpuFrameWarper.cpp:16-44): *supported = 1
+   when a compute-capability 10.x device is visible; message receives a short reason otherwise. */
+fa_status fa_gpu_support(int* supported, char* message, size_t message_len);
+fa_status fa_create(const fa_config* cfg, fa_context** out);
+fa_status fa_destroy(fa_context* ctx);
+/* Message of the last failure on this thread (static storage, valid until the next call). */
+const char* fa_last_error(void);
+const char* fa_status_string(fa_status s);
+
+/* ImageScanParameters::ImageScanParameters (FrameAligner/ImageScanParameters.h:7-20). The
+   reference constructor leaves `bidirectional` uninitialised; here it is an argument. */
+fa_status fa_scan_params_init(double line_duration, double interline_duration, double interframe_duration, int n_x,
+                              int n_y, int n_z, int bidirectional, fa_scan_params* out);
+
+/* ---------------------------------------------------------------- reference ------------------- */
+
+/* AbstractFrameWarper::setReference (FrameAligner/FrameWarper.cpp:186-205) followed by
+   GpuFrameWarper::setupReferenceInformation (FrameAligner/GpuFrameWarper.cpp:75-152):
+   interval tables, Sobel gradient, steepest-descent weights and the constant block-tridiagonal
+   Hessian H = J^T J, all on the device. `reference` is host memory (nz*ny*nx floats, the smoothed
+   reference with FrameWarpAligner's +1 offset already applied). Errors: FA_ERR_BAD_ARG for
+   nx < 2, ny < 2, nD < 2 or a scan that does not reach interval nD-2 (the reference throws
+   "Something went wrong", FrameWarper.cpp:280-281); FA_ERR_UNSUPPORTED when a control interval is
+   skipped, shorter than one image row, or (bidirectional) not increasing in storage order. */
+fa_status fa_set_reference(fa_context* ctx, const float* reference, int nz, int ny, int nx, int nD,
+                           const fa_scan_params* scan, fa_precision precision, fa_reference** out);
+/* Same, with the reference already in device memory (FP32). */
+fa_status fa_set_reference_device(fa_context* ctx, const float* reference_device, int nz, int ny, int nx, int nD,
+                                  const fa_scan_params* scan, fa_precision precision, fa_reference** out);
+fa_status fa_reference_destroy(fa_reference* ref);
+/* n_dim (2 or 3, FrameWarper.cpp:198) and the parameter count P = nD * n_dim. */
+fa_status fa_reference_info(const fa_reference* ref, int* n_dim, int* n_params);
+/* The member H read by OptimisationModel (OptimisationModel.cpp:61): dense P x P, row-major,
+   host memory. */
+fa_status fa_get_hessian(const fa_reference* ref, double* H);
+/* The Sobel3d gradient images (Sobel3d.cpp:60-85), host memory, nz*ny*nx floats each; gz may be
+   NULL. */
+fa_status fa_get_gradient(const fa_reference* ref, float* gx, float* gy, float* gz);
+/* D_range (FrameWarper.cpp:239-293): 2*nD ints {begin, end}; the unused last entry is {0, 0}. */
+fa_status fa_get_ranges(const fa_reference* ref, int* ranges);
+
+/* ---------------------------------------------------------------- frames ---------------------- */
+
+/* GpuFrameWarper::registerFrame (FrameAligner/GpuFrameWarper.cpp:46-64): copies one frame
+   (host memory, nz*ny*nx elements of `dtype`, FrameWarpAligner's +1 offset already applied) into
+   device memory in the reference's storage precision. Frames are independent: each owns its
+   stream and scratch, so different frames may be used from different threads concurrently. */
+fa_status fa_register_frame(fa_reference* ref, const void* data, fa_dtype dtype, fa_frame** out);
+/* Same, source in device memory. */
+fa_status fa_register_frame_device(fa_reference* ref, const void* data_device, fa_dtype dtype, fa_frame** out);
+/* Replaces a registered frame's pixels (host memory) without reallocating. */
+fa_status fa_update_frame(fa_frame* frame, const void* data, fa_dtype dtype);
+/* GpuFrameWarper::deregisterFrame (FrameAligner/GpuFrameWarper.cpp:66-73). */
+fa_status fa_deregister_frame(fa_frame* frame);
+
+/* ---------------------------------------------------------------- evaluation ------------------ */
+
+/* CpuFrameWarper::getError / GpuFrameWarper::getError (FrameWarper.cpp:169-176,
+   GpuFrameWarper.cpp:182-190): the sum of squared errors over voxels whose interpolated value is
+   positive. One fused pass also forms J^T e, which fa_get_jacobian returns for the same D. */
+fa_status fa_get_error(fa_frame* frame, const double* D, double* f);
+/* AbstractFrameWarper::computeJacobian / GpuFrameWarper::getJacobian (FrameWarper.cpp:147-167,
+   GpuFrameWarper.cpp:192-235): g = J^T e (P doubles, host memory). Reuses the pass of the last
+   fa_get_error on this frame when D is identical; otherwise runs one. */
+fa_status fa_get_jacobian(fa_frame* frame, const double* D, double* jac);
+/* CpuFrameWarper::warpImageInterpolated (FrameWarper.cpp:31-69): trilinear (bilinear for a single
+   plane) zero-padded resampling at x + d(x); exact zeros become invalid_value. out: host memory,
+   nz*ny*nx floats. */
+fa_status fa_warp(fa_frame* frame, const double* D, float invalid_value, float* out);
+
+/* ---------------------------------------------------------------- alignment ------------------- */
+
+typedef struct {
+  int iterations;        /* trust-region iterations (subproblem solves) */
+  int evaluations;       /* fused error+gradient passes, starting points included */
+  int accepted;          /* accepted steps */
+  int status;            /* 0 = converged by the stop rule, 1 = hit max_iterations */
+  double f_final;        /* sum of squared errors at the returned D */
+  double radius_final;
+} fa_align_stats;
+
+/* The solve of FrameWarpAligner::addFrame (FrameAligner/FrameWarpAligner.cpp:194-219) on the
+   device: starting points {0, rigid_shift} (first minimum wins), then the trust region
+   (radius 40, stop when |delta f| < 1e-8) with the constant Hessian. rigid_shift: 3 doubles (x, y,
+   z), already scaled by the phase-correlation binning, or NULL for none. max_iterations <= 0
+   means 100. D_out: nD*3 doubles, host memory. The host drives the iterations (one fused pass and
+   one solve launch per iteration, the plain single-frame path). */
+fa_status fa_align_frame(fa_frame* frame, const double* rigid_shift, int max_iterations, double* D_out,
+                         fa_align_stats* stats);
+
+/* Batched solve: n frames of one reference advance together, one fused multi-frame pass plus one
+   multi-frame solve launch per trust-region iteration, iterations captured in a CUDA graph and
+   run without host round-trips. rigid_shifts: n*3 doubles or NULL. D_out: n*nD*3 doubles, stats:
+   n entries (may be NULL); host memory. Results per frame equal the frame aligned alone. */
+fa_status fa_align_batch(fa_frame* const* frames, int n, const double* rigid_shifts, int max_iterations,
+                         double* D_out, fa_align_stats* stats);
+
+/* ---------------------------------------------------------------- phase correlation ----------- */
+
+/* VolumePhaseCorrelator (FrameAligner/VolumePhaseCorrelator.cpp:29-139): FP64 cuFFT R2C of the
+   windowed volume, hand-written cross-power normalisation and first-maximum argmax, integer
+   shift wrapped to (-n/2, n/2]. `reference` is host memory (nz*ny*nx floats). */
+fa_status fa_correlator_create(fa_context* ctx, const float* reference, int nz, int ny, int nx, fa_correlator** out);
+fa_status fa_correlator_destroy(fa_correlator* c);
+/* shift: 3 doubles (x, y, z). volume: host memory. */
+fa_status fa_correlator_shift(fa_correlator* c, const float* volume, double* shift);
+/* Same, volume in device memory. */
+fa_status fa_correlator_shift_device(fa_correlator* c, const float* volume_device, double* shift);
+
+/* ---------------------------------------------------------------- aligner --------------------- */
+
+/* The per-frame flow of FrameWarpAligner (FrameAligner/FrameWarpAligner.cpp:77-105 setReference,
+   117-219 addFrame) on the device: the +1 offset, the phase-correlation rigid start on the
+   downsampled raw data, the starting-point choice and the trust-region solve, for a batch of
+   frames at a time. RealignmentParameters (FrameAligner/AbstractFrameAligner.h:31-48) fields that
+   this path reads are mirrored here. */
+typedef struct fa_aligner fa_aligner;
+
+typedef struct {
+  int spatial_binning;       /* RealignmentParameters::spatial_binning: phase-correlation downsampling */
+  int n_resampling_points;   /* nD = n_resampling_points * n_z + 1 (FrameWarpAligner.cpp:100) ... */
+  int nD;                    /* ... unless nD > 0, which sets the control-point count directly */
+  double smoothing;          /* must be 0: the Gaussian pre-smoothing (FrameWarpAligner.cpp:46-64) is not built */
+  fa_precision precision;
+  int max_iterations;        /* <= 0: 100 */
+} fa_aligner_params;
+
+fa_status fa_aligner_create(fa_context* ctx, const fa_aligner_params* params, fa_aligner** out);
+fa_status fa_aligner_destroy(fa_aligner* a);
+/* FrameWarpAligner::setReference: `reference` is the raw reference (host memory, nz*ny*nx elements
+   of dtype FA_F32 or FA_U16). */
+fa_status fa_aligner_set_reference(fa_aligner* a, const void* reference, fa_dtype dtype, int nz, int ny, int nx,
+                                   const fa_scan_params* scan);
+/* The control-point count and parameter layout of the current reference. */
+fa_status fa_aligner_info(const fa_aligner* a, int* nD, int* n_dim);
+/* FrameWarpAligner::addFrame for n raw frames (host memory; frames[i] points at nz*ny*nx elements of
+   dtype). D_out: n*nD*3 doubles, stats: n entries or NULL; host memory. */
+fa_status fa_aligner_add_frames(fa_aligner* a, const void* const* frames, fa_dtype dtype, int n, double* D_out,
+                                fa_align_stats* stats);
+/* Same, frames already in device memory (frames[i] device pointers). */
+fa_status fa_aligner_add_frames_device(fa_aligner* a, const void* const* frames, fa_dtype dtype, int n,
+                                       double* D_out, fa_align_stats* stats);
+
+/* ---------------------------------------------------------------- measurement ----------------- */
+
+/* Number of this library's kernels launched so far in the process (graph replays included). */
+long long fa_kernel_launches(void);
+/* Device time (CUDA events on the library's streams) of the last fa_aligner_add_frames* call, ms. */
+fa_status fa_aligner_last_device_ms(const fa_aligner* a, double* ms);
+/* Times the fused warp + error + J^T e pass alone: `launches` back-to-back launches over n
+   registered frames (of one reference) at displacement D (nD*3 doubles, host memory), bracketed by
+   CUDA events on the launching stream. ms_per_launch receives the average duration. */
+fa_status fa_profile_eval(fa_frame* const* frames, int n, const double* D, int launches, double* ms_per_launch);
+
+/* ---------------------------------------------------------------- test hooks ------------------ */
+
+/* Runs the device trust-region subproblem solver (the step computation inside dlib's
+   find_min_trust_region, called at FrameAligner/FrameWarpAligner.cpp:205-209) once on a given dense
+   block-tridiagonal H (P x P, P = nD * n_dim, host memory) and gradient g; writes the step p and
+   whether it lies on the trust-region boundary. Lets tests compare the device solver with the
+   CPU statement of the same algorithm on identical inputs. */
+fa_status fa_test_tr_subproblem(fa_context* ctx, int nD, int n_dim, const double* H, const double* g, double radius,
+                                double* p, int* on_boundary);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FA_B200_H */

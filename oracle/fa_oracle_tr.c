@@ -14,7 +14,7 @@
  *    p = subproblem(H, g, Delta)
  *    f_new = f(x + p); predicted = -(g.p + 0.5 p.H.p); measured = f - f_new
  *    stop if |predicted| <= |measured| * DBL_EPSILON (the model step has vanished)
- *    rho = measured / |predicted|
+ *    rho = measured / |predicted|; stop if rho is not finite
  *    rho < 0.25 -> Delta *= 0.25 (stop if Delta <= Delta_0 * DBL_EPSILON)
  *    else rho > 0.75 and the step was on the trust-region boundary -> Delta = min(1000, 2 Delta)
  *    rho > 0 -> accept: x += p, f = f_new, g = g(x)
@@ -180,6 +180,7 @@ int or_trust_region(int P, const double* H, double* x, double radius0, double mi
     double measured = fx - fn;
     if (fabs(predicted) <= fabs(measured) * DBL_EPSILON) break;
     double rho = measured / fabs(predicted);
+    if (!isfinite(rho)) break;
     if (rho < 0.25) {
       radius *= 0.25;
       if (radius <= radius0 * DBL_EPSILON) break;

@@ -274,15 +274,44 @@ static void* mt_worker(void* arg) {
 // fr_mt_create) so that fr_mt_align measures alignment only.
 void* fr_mt_create(const float* ref, int nz, int ny, int nx, int nD, double line, double interline, double interframe,
                    int bidirectional, int n_threads, char* err) {
-  std::vector<Handle*>* v = new std::vector<Handle*>();
+  // Warpers are set up in parallel, one per worker thread.
+  std::vector<Handle*> hs((size_t)n_threads, nullptr);
+  std::vector<pthread_t> th((size_t)n_threads);
+  struct Arg {
+    const float* ref;
+    int nz, ny, nx, nD;
+    double line, interline, interframe;
+    int bidir;
+    Handle** out;
+    char err[128];
+  };
+  std::vector<Arg> args((size_t)n_threads);
   for (int t = 0; t < n_threads; t++) {
-    Handle* h = create(ref, nz, ny, nx, nD, line, interline, interframe, bidirectional, err);
-    if (!h) {
-      for (Handle* x : *v) delete x;
-      delete v;
-      return nullptr;
+    args[(size_t)t] = Arg{ref, nz, ny, nx, nD, line, interline, interframe, bidirectional, &hs[(size_t)t], {0}};
+    pthread_create(&th[(size_t)t], nullptr,
+                   [](void* p) -> void* {
+                     Arg* a = static_cast<Arg*>(p);
+                     *a->out = create(a->ref, a->nz, a->ny, a->nx, a->nD, a->line, a->interline, a->interframe,
+                                      a->bidir, a->err);
+                     return nullptr;
+                   },
+                   &args[(size_t)t]);
+  }
+  for (int t = 0; t < n_threads; t++) pthread_join(th[(size_t)t], nullptr);
+  std::vector<Handle*>* v = new std::vector<Handle*>();
+  bool ok = true;
+  for (int t = 0; t < n_threads; t++) {
+    if (!hs[(size_t)t]) {
+      ok = false;
+      if (err) std::snprintf(err, 128, "%s", args[(size_t)t].err);
+    } else {
+      v->push_back(hs[(size_t)t]);
     }
-    v->push_back(h);
+  }
+  if (!ok) {
+    for (Handle* x : *v) delete x;
+    delete v;
+    return nullptr;
   }
   return v;
 }
