@@ -300,7 +300,10 @@ __global__ void __launch_bounds__(kEvalThreads) eval_kernel(const Job* __restric
     const long long rowoff = (long long)row * nx;
     for (int x = lane; x < nx; x += 32) {
       const VoxelModel vm = voxel_model(rd, x, nx, flip, bidir, dq);
-      const float v = sample<NDIM, FT>(fr, sD + (vm.di - cw) * kDParamF4, vm.f, x, y, z, nx, ny, nz);
+      // the host geometry guarantees c0-1 <= di <= c0+2; the clamp only keeps the shared-memory
+      // window in bounds
+      const int wi = min(max(vm.di - cw, 0), kWin - 2);
+      const float v = sample<NDIM, FT>(fr, sD + wi * kDParamF4, vm.f, x, y, z, nx, ny, nz);
       const long long p = rowoff + x;
       const float t = ldf(tref + p);
       // include iff the interpolated value is positive: CPU rule px == 0 -> -1, then wimg >= 0
@@ -421,7 +424,8 @@ __global__ void __launch_bounds__(256) warp_kernel(const RefDev* __restrict__ Rp
     const bool flip = R.bidir && (y & 1);
     for (int x = lane; x < nx; x += 32) {
       const VoxelModel vm = voxel_model(rd, x, nx, flip, R.bidir != 0, R.dq);
-      float v = sample<NDIM, FT>(fr, sAll + vm.di * kDParamF4, vm.f, x, y, z, nx, ny, nz);
+      const int di = min(max(vm.di, 0), R.nD - 2);
+      float v = sample<NDIM, FT>(fr, sAll + di * kDParamF4, vm.f, x, y, z, nx, ny, nz);
       if (v == 0.0f) v = invalid_value;
       out[(long long)row * nx + x] = v;
     }
