@@ -260,7 +260,7 @@ struct fa_reference {
   fa_precision prec = FA_PREC_F32;
   fa_scan_params scan{};
   Geometry G;
-  std::vector<double> H;  // dense P x P
+  std::vector<double> hd, hl;  // host copies of the Hessian blocks (diagonal, sub-diagonal)
   RefDev host{};
   RefDev* dev = nullptr;
   cudaStream_t stream = nullptr;
@@ -467,25 +467,12 @@ fa_status reference_setup(fa_reference* R, const float* src, bool src_device) {
   const fa_scan_params p = process_scan(R->scan, R->nz, R->nD);
   double scan4[4] = {p.pixel_duration, p.interline_duration, p.interframe_duration, p.stack_duration};
   FA_CU(fa::launch_hessian(R->dev, h, scan4, tparts, Hd, Hl, s));
-  std::vector<double> hd((size_t)R->nD * nn), hl((size_t)R->nD * nn);
-  FA_CU(cudaMemcpyAsync(hd.data(), Hd, hd.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-  FA_CU(cudaMemcpyAsync(hl.data(), Hl, hl.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  R->hd.assign((size_t)R->nD * nn, 0.0);
+  R->hl.assign((size_t)R->nD * nn, 0.0);
+  FA_CU(cudaMemcpyAsync(R->hd.data(), Hd, R->hd.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  FA_CU(cudaMemcpyAsync(R->hl.data(), Hl, R->hl.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
   FA_CU(cudaStreamSynchronize(s));
   dfree_all(ctx, tmp);
-  const int P = R->P, nd = R->n_dim;
-  R->H.assign((size_t)P * P, 0.0);
-  for (int i = 0; i < P; i++)
-    for (int j = 0; j < P; j++) {
-      int bi = i / nd, bj = j / nd, a = i % nd, b = j % nd;
-      double v = 0;
-      if (bi == bj)
-        v = hd[(size_t)bi * nn + a * nd + b];
-      else if (bi == bj + 1)
-        v = hl[(size_t)bi * nn + a * nd + b];
-      else if (bj == bi + 1)
-        v = hl[(size_t)bj * nn + b * nd + a];
-      R->H[(size_t)i * P + j] = v;
-    }
   return FA_OK;
 }
 
@@ -551,7 +538,19 @@ extern "C" fa_status fa_reference_info(const fa_reference* R, int* n_dim, int* n
 
 extern "C" fa_status fa_get_hessian(const fa_reference* R, double* H) {
   if (!R || !H) return fail(FA_ERR_BAD_ARG, "NULL argument");
-  std::memcpy(H, R->H.data(), R->H.size() * sizeof(double));
+  const int P = R->P, nd = R->n_dim, nn = nd * nd;
+  for (int i = 0; i < P; i++)
+    for (int j = 0; j < P; j++) {
+      const int bi = i / nd, bj = j / nd, a = i % nd, b = j % nd;
+      double v = 0;
+      if (bi == bj)
+        v = R->hd[(size_t)bi * nn + a * nd + b];
+      else if (bi == bj + 1)
+        v = R->hl[(size_t)bi * nn + a * nd + b];
+      else if (bj == bi + 1)
+        v = R->hl[(size_t)bj * nn + b * nd + a];
+      H[(size_t)i * P + j] = v;
+    }
   return FA_OK;
 }
 
