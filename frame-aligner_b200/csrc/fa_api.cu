@@ -1400,3 +1400,26 @@ extern "C" fa_status fa_profile_eval(fa_frame* const* frames, int n, const doubl
   *ms_per_launch = ms / launches;
   return FA_OK;
 }
+
+// ================================================================== static-scratch evaluation ======
+
+namespace fa {
+
+fa_status static_eval_prepare(const fa_reference* R, const RefDev** dev, const RefDev** host, int* nD, int* n_dim,
+                              bool* mixed) {
+  if (cudaSetDevice(R->ctx->device) != cudaSuccess) return fail(FA_ERR_CUDA, "cudaSetDevice failed");
+  *dev = R->dev;
+  *host = &R->host;
+  *nD = R->nD;
+  *n_dim = R->n_dim;
+  *mixed = R->prec == FA_PREC_MIXED;
+  return FA_OK;
+}
+
+fa_status static_eval_fail(fa_status s, const char* msg) { return fail(s, msg); }
+
+void static_eval_dparams(const double* D, int nD, int n_dim, float4* out) { make_dparams(D, nD, n_dim, out); }
+
+void static_eval_count_launches(int n) { g_launches += n; }
+
+}  // namespace fa

@@ -126,6 +126,7 @@ SIGNATURES = {
     "fa_aligner_info": [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)],
     "fa_aligner_add_frames": [_vp, _vp, C.c_int, C.c_int, _f64p, _vp],
     "fa_aligner_add_frames_device": [_vp, _vp, C.c_int, C.c_int, _f64p, _vp],
+    "fa_get_error_jacobian_static": [_vp, _vp, C.c_int, _f64p, C.POINTER(C.c_double), _f64p],
     "fa_kernel_launches": [],
     "fa_aligner_last_device_ms": [_vp, C.POINTER(C.c_double)],
     "fa_profile_eval": [_vp, C.c_int, _f64p, C.c_int, C.POINTER(C.c_double)],
@@ -407,6 +408,15 @@ class Aligner:
             self.close()
         except Exception:
             pass
+
+
+def get_error_jacobian_static(ref: Reference, frame_ptr, dtype, D):
+    """fa_get_error_jacobian_static: evaluation of a frame in the caller's device memory with the
+    library's fixed static scratch (no allocation inside the call)."""
+    f = C.c_double()
+    jac = np.empty(ref.P, np.float64)
+    check(lib().fa_get_error_jacobian_static(ref._h, frame_ptr, dtype, _c64(D).ravel(), C.byref(f), jac))
+    return f.value, jac
 
 
 def kernel_launches():

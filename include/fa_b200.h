@@ -218,6 +218,24 @@ fa_status fa_aligner_add_frames(fa_aligner* a, const void* const* frames, fa_dty
 fa_status fa_aligner_add_frames_device(fa_aligner* a, const void* const* frames, fa_dtype dtype, int n,
                                        double* D_out, fa_align_stats* stats);
 
+/* ---------------------------------------------------------------- static-scratch evaluation --- */
+
+/* No counterpart in the reference. For callers that cannot call cudaMalloc when they evaluate a
+   frame (a host application that has reserved the device memory pool for its own allocator, or a
+   real-time acquisition loop that must not allocate between frames): the same fused error + J^T e
+   pass as fa_get_error / fa_get_jacobian on a frame held in the caller's own device memory
+   (frame_device: nz*ny*nx elements, FA_F32 for an FA_PREC_F32 reference, FA_F16 for FA_PREC_MIXED,
+   +1 offset applied), with every piece of scratch in one fixed 2 MiB device array inside the
+   library, which each GPU that loads the library holds until exit. The call allocates no device or
+   host memory; it runs on the legacy default stream and returns when f (host double) and jac (P host
+   doubles) are written. Volumes whose scratch would exceed 2 MiB (about 21,000 tiles of the fused
+   pass) are rejected with FA_ERR_BAD_ARG. The first call on each device looks up the array's device
+   address (cudaGetSymbolAddress) with that device current; make it before any stream capture. All
+   calls share the array, so calls that overlap on the GPU (other threads, other streams) race and
+   must be serialised by the caller. */
+fa_status fa_get_error_jacobian_static(const fa_reference* ref, const void* frame_device, fa_dtype dtype,
+                                       const double* D, double* f, double* jac);
+
 /* ---------------------------------------------------------------- measurement ----------------- */
 
 /* Number of this library's kernels launched so far in the process (graph replays included). */
