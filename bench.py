@@ -79,52 +79,55 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+    """nvidia-smi clocks and throttle reasons, polled every 200 ms on a thread while running."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.rows = []
-        self.proc = None
+        self._stop = threading.Event()
+
+    def _poll(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                for line in out.stdout.strip().splitlines():
+                    self.rows.append([x.strip() for x in line.split(",")])
+            except (OSError, subprocess.SubprocessError):
+                return
+            self._stop.wait(0.2)
 
     def __enter__(self):
-        try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
-        except (OSError, FileNotFoundError):
-            self.proc = None
+        self.thread = threading.Thread(target=self._poll, daemon=True)
+        self.thread.start()
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
-
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+        self._stop.set()
+        self.thread.join(timeout=10)
 
     def summary(self):
-        if not self.rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        def num(s):
+            try:
+                return float(s)
+            except ValueError:
+                return None
+
+        sm = [num(r[0]) for r in self.rows if r and num(r[0]) is not None]
+        mx = [num(r[1]) for r in self.rows if len(r) > 1 and num(r[1]) is not None]
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = set()
         for r in self.rows:
             for i, n in enumerate(names):
-                if len(r) > 5 + i and r[5 + i].lower().startswith("active"):
+                if len(r) > 3 + i and r[3 + i].lower().startswith("active"):
                     reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx) if mx else None,
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
@@ -263,8 +266,10 @@ def run_ours(args, rank, world, local):
         ref_m = fa.Reference(ctx, acq.reference + 1, acq.nD, scan, fa.PREC_MIXED)
         frs = [fa.Frame(ref_m, (acq.frames[k] + 1).astype(np.float16)) for k in range(n)]
         ms = fa.profile_eval(frs, acq.D_true[0], 20)
-        bytes_per_voxel = 2 + 2 + 3 * 2  # fp16 frame + bf16 reference + 3 bf16 gradient planes
-        algo_bytes = n * N * bytes_per_voxel
+        # Unique bytes one launch needs: each FP16 frame once, plus the BF16 reference and three
+        # gradient planes once (the frames of a batch share them; after the first frame they are L2
+        # hits, so counting them per frame would inflate the figure).
+        algo_bytes = n * N * 2 + N * (2 + 3 * 2)
         achieved = algo_bytes / (ms / 1000.0) / 1e9
         peak, peak_kind = load_peaks()
         traffic = None
@@ -275,6 +280,7 @@ def run_ours(args, rank, world, local):
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                     "traffic": traffic, "kernel": "eval_kernel<3, half, bf16> (fused warp+error+J^T e)",
                     "algorithmic_bytes_per_launch": algo_bytes, "ms_per_launch": ms,
+                    "bytes_per_unit": "2 B per voxel per frame + 8 B per voxel of the shared reference",
                     "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind if peak_kind == "measured" else "fallback 6.65 TB/s"}
         for f in frs:
             f.close()

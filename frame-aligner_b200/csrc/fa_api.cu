@@ -211,6 +211,8 @@ fa_status build_geometry(const fa_scan_params& scan, int nz, int ny, int nx, int
     d.xr = nx;
     if (r0 + 1 <= nD - 2 && G.begin[r0 + 1] < s0 + nx) d.xr = (int)(G.begin[r0 + 1] - s0);
     d.xlast = -1;
+    d.y = row % ny;
+    d.z = row / ny;
     const long long e = G.end[r0];
     if (e >= s0 && e < s0 + nx) d.xlast = (int)(e - s0);
     G.rows[row] = d;
@@ -721,7 +723,8 @@ fa_status evaluate(fa_frame* F, const double* D) {
   make_dparams(D, R->nD, R->n_dim, F->h_dparams);
   const size_t np = (size_t)R->nD * fa::kDParamF4 * sizeof(float4);
   FA_CU(cudaMemcpyAsync(F->job.dparams, F->h_dparams, np, cudaMemcpyHostToDevice, F->stream));
-  FA_CU(fa::launch_eval(F->job_dev, 1, R->G.n_tiles, R->n_dim, F->half, R->prec == FA_PREC_MIXED, F->stream));
+  FA_CU(fa::launch_eval(F->job_dev, 1, R->G.n_tiles, R->n_dim, F->half, R->prec == FA_PREC_MIXED, F->stream,
+                          R->nx % 4 == 0));
   FA_CU(fa::launch_reduce(F->job_dev, R->host, F->stream));
   g_launches += 2;
   FA_CU(cudaMemcpyAsync(F->h_result, F->job.result, (1 + R->P) * sizeof(double), cudaMemcpyDeviceToHost, F->stream));
@@ -833,7 +836,8 @@ extern "C" fa_status fa_align_frame(fa_frame* F, const double* rigid_shift, int 
   const int max_steps = (max_iterations > 0 ? max_iterations : 100) + 4;
   int phase = fa::kPhaseStartZero;
   for (int step = 0; step < max_steps && phase != fa::kPhaseDone; step++) {
-    FA_CU(fa::launch_eval(F->job_dev, 1, R->G.n_tiles, R->n_dim, F->half, R->prec == FA_PREC_MIXED, F->stream));
+    FA_CU(fa::launch_eval(F->job_dev, 1, R->G.n_tiles, R->n_dim, F->half, R->prec == FA_PREC_MIXED, F->stream,
+                          R->nx % 4 == 0));
     FA_CU(fa::launch_solve(F->job_dev, 1, F->stream));
     g_launches += 2;
     FA_CU(cudaMemcpyAsync(&F->h_state->phase, &F->state->phase, sizeof(int), cudaMemcpyDeviceToHost, F->stream));
@@ -875,6 +879,7 @@ extern "C" fa_status fa_align_batch(fa_frame* const* frames, int n, const double
   for (int i = 0; i < n; i++) locks.emplace_back(frames[i]->mu);
   cudaStream_t s = frames[0]->stream;
   int max_tiles = 0;
+  bool vec4 = true;
   std::vector<Job> jobs(n);
   for (int i = 0; i < n; i++) {
     fa_frame* F = frames[i];
@@ -883,6 +888,7 @@ extern "C" fa_status fa_align_batch(fa_frame* const* frames, int n, const double
     jobs[i] = F->job;
     jobs[i].state = F->state;
     max_tiles = std::max(max_tiles, F->ref->G.n_tiles);
+    vec4 = vec4 && (F->ref->nx % 4 == 0);
   }
   std::vector<Alloc> tmp;
   Job* jobs_dev;
@@ -915,7 +921,7 @@ extern "C" fa_status fa_align_batch(fa_frame* const* frames, int n, const double
   cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
     for (int it = 0; it < kGraphIters && e == cudaSuccess; it++) {
-      e = fa::launch_eval(jobs_dev, n, max_tiles, R0->n_dim, frames[0]->half, R0->prec == FA_PREC_MIXED, s);
+      e = fa::launch_eval(jobs_dev, n, max_tiles, R0->n_dim, frames[0]->half, R0->prec == FA_PREC_MIXED, s, vec4);
       if (e == cudaSuccess) e = fa::launch_solve(jobs_dev, n, s);
     }
     if (e == cudaSuccess) {
@@ -1384,10 +1390,12 @@ extern "C" fa_status fa_profile_eval(fa_frame* const* frames, int n, const doubl
   if (e == cudaSuccess) e = cudaEventCreate(&e0);
   if (e == cudaSuccess) e = cudaEventCreate(&e1);
   // one untimed launch, then the timed ones
-  if (e == cudaSuccess) e = fa::launch_eval(jd, n, R->G.n_tiles, R->n_dim, frames[0]->half, R->prec == FA_PREC_MIXED, s);
+  const bool v4 = R->nx % 4 == 0;
+  if (e == cudaSuccess)
+    e = fa::launch_eval(jd, n, R->G.n_tiles, R->n_dim, frames[0]->half, R->prec == FA_PREC_MIXED, s, v4);
   if (e == cudaSuccess) e = cudaEventRecord(e0, s);
   for (int l = 0; l < launches && e == cudaSuccess; l++)
-    e = fa::launch_eval(jd, n, R->G.n_tiles, R->n_dim, frames[0]->half, R->prec == FA_PREC_MIXED, s);
+    e = fa::launch_eval(jd, n, R->G.n_tiles, R->n_dim, frames[0]->half, R->prec == FA_PREC_MIXED, s, v4);
   if (e == cudaSuccess) e = cudaEventRecord(e1, s);
   if (e == cudaSuccess) e = cudaEventSynchronize(e1);
   float ms = 0;

@@ -1,0 +1,350 @@
+// fa_eval4.cu -- the fused warp + error + J^T e pass with four consecutive voxels per lane
+// (image rows whose length is a multiple of 4).
+//
+// Same arithmetic contract as eval_kernel (FrameWarper.cpp:4-69,147-176 restated on the device):
+// per voxel the scan-time interval and fraction, the displacement d = D[i] + f (D[i+1] - D[i]),
+// the zero-padded trilinear sample of the frame at x + d, the masked error, its square, and the
+// two control points' J^T e contributions (1 - f) grad e and f grad e.
+//
+// Why four voxels per lane: along an image row the sample position advances by one voxel plus a
+// displacement that changes by ~1e-5 px per voxel, so four neighbours almost always share the
+// integer tap offset. They then need only five frame values per tap row, fetched as one aligned
+// 8-element window (two 64-bit loads for FP16, two 128-bit loads for FP32) and shifted into place,
+// instead of eight gathers per voxel; the reference and gradient planes are read with one vector
+// load per plane. Lanes whose four voxels straddle an interval boundary, a range end, a change of
+// the integer offset or the volume edge take the per-voxel path.
+#include "fa_device.cuh"
+
+namespace fa {
+
+namespace {
+
+// Four consecutive reference / gradient values starting at a multiple of 4.
+__device__ __forceinline__ void load4(const float* p, float* v) {
+  const float4 a = __ldg(reinterpret_cast<const float4*>(p));
+  v[0] = a.x;
+  v[1] = a.y;
+  v[2] = a.z;
+  v[3] = a.w;
+}
+__device__ __forceinline__ void load4(const __nv_bfloat16* p, float* v) {
+  const uint2 a = __ldg(reinterpret_cast<const uint2*>(p));
+  v[0] = __uint_as_float(a.x << 16);
+  v[1] = __uint_as_float(a.x & 0xffff0000u);
+  v[2] = __uint_as_float(a.y << 16);
+  v[3] = __uint_as_float(a.y & 0xffff0000u);
+}
+
+// Five consecutive frame values v[k] = p[s + k], k = 0..4, from the aligned 8-element window at p
+// (p is 8-element aligned in FP16 units or 4-element aligned in FP32 units; s in [0, 3]).
+__device__ __forceinline__ void window5(const __half* p, int s, float* v) {
+  const uint2 lo = __ldg(reinterpret_cast<const uint2*>(p));
+  const uint2 hi = __ldg(reinterpret_cast<const uint2*>(p + 4));
+  const bool e = (s >> 1) != 0;
+  const unsigned sh = (unsigned)(s & 1) * 16u;
+  const unsigned A = e ? lo.y : lo.x;
+  const unsigned B = e ? hi.x : lo.y;
+  const unsigned C = e ? hi.y : hi.x;
+  const unsigned p0 = __funnelshift_r(A, B, sh);
+  const unsigned p1 = __funnelshift_r(B, C, sh);
+  const unsigned p2 = __funnelshift_r(C, hi.y, sh);
+  const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&p0));
+  const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&p1));
+  v[0] = a.x;
+  v[1] = a.y;
+  v[2] = b.x;
+  v[3] = b.y;
+  v[4] = __half2float(__ushort_as_half((unsigned short)(p2 & 0xffffu)));
+}
+__device__ __forceinline__ void window5(const float* p, int s, float* v) {
+  const float4 a = __ldg(reinterpret_cast<const float4*>(p));
+  const float4 b = __ldg(reinterpret_cast<const float4*>(p + 4));
+  const bool e = (s >> 1) != 0, o = (s & 1) != 0;
+  const float r0 = e ? a.z : a.x, r1 = e ? a.w : a.y, r2 = e ? b.x : a.z, r3 = e ? b.y : a.w, r4 = e ? b.z : b.x,
+              r5 = e ? b.w : b.y;
+  v[0] = o ? r1 : r0;
+  v[1] = o ? r2 : r1;
+  v[2] = o ? r3 : r2;
+  v[3] = o ? r4 : r3;
+  v[4] = o ? r5 : r4;
+}
+
+// Edge version: v[k] = frame value at column ix + k of the row starting at `row`, zero outside the
+// row or when the whole tap row lies outside the volume (getZeroPadded, FrameWarper.h:39-47).
+template <typename FT>
+__device__ __forceinline__ void masked5(const FT* row, bool row_valid, int ix, int nx, float* v) {
+#pragma unroll
+  for (int k = 0; k < 5; k++) v[k] = (row_valid && (unsigned)(ix + k) < (unsigned)nx) ? ldf(row + ix + k) : 0.0f;
+}
+
+}  // namespace
+
+template <int NDIM, typename FT, typename RT>
+__global__ void __launch_bounds__(kEvalThreads, 2) eval4_kernel(const Job* __restrict__ jobs) {
+  const Job& job = jobs[blockIdx.y];
+  if (job.state != nullptr && job.state->phase == kPhaseDone) return;
+  const RefDev& R = *job.ref;
+  const int tile = blockIdx.x;
+  if (tile >= R.n_tiles) return;
+  const int nx = R.nx, ny = R.ny, nz = R.nz;
+  const int row_begin = tile * R.tile_rows;
+  const int row_end = min(row_begin + R.tile_rows, R.n_rows);
+  const int c0 = R.tile_c0[tile];
+  const int cw = max(c0 - 1, 0);
+  const bool bidir = R.bidir != 0;
+  const float dq = R.dq;
+
+  __shared__ float4 sD[kWin * kDParamF4];
+  __shared__ float sred[kEvalWarps][1 + 3 * NDIM];
+  for (int i = threadIdx.x; i < kWin * kDParamF4; i += blockDim.x) {
+    const int k = cw + i / kDParamF4;
+    sD[i] = (k < R.nD) ? job.dparams[k * kDParamF4 + i % kDParamF4] : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  __syncthreads();
+
+  const FT* __restrict__ fr = static_cast<const FT*>(job.frame);
+  const RT* __restrict__ tref;
+  const RT* __restrict__ tg[3];
+  if constexpr (sizeof(RT) == 4) {
+    tref = reinterpret_cast<const RT*>(R.ref32);
+    tg[0] = reinterpret_cast<const RT*>(R.gx32);
+    tg[1] = reinterpret_cast<const RT*>(R.gy32);
+    tg[2] = reinterpret_cast<const RT*>(R.gz32);
+  } else {
+    tref = reinterpret_cast<const RT*>(R.ref16);
+    tg[0] = reinterpret_cast<const RT*>(R.gx16);
+    tg[1] = reinterpret_cast<const RT*>(R.gy16);
+    tg[2] = reinterpret_cast<const RT*>(R.gz16);
+  }
+
+  float af = 0.0f;
+  float ag[3][NDIM];
+#pragma unroll
+  for (int s = 0; s < 3; s++)
+#pragma unroll
+    for (int k = 0; k < NDIM; k++) ag[s][k] = 0.0f;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int segs = (nx + 127) >> 7;
+  const int rows_here = row_end - row_begin;
+  // When the number of 128-voxel segments per row divides the warp count (row lengths 128, 256,
+  // 512, 1024), each warp keeps one segment and steps over rows; otherwise items are enumerated.
+  const bool fixed_seg = (kEvalWarps % segs) == 0;
+  const int row_step = fixed_seg ? kEvalWarps / segs : 0;
+  const int n_items = fixed_seg ? (warp / segs < rows_here ? (rows_here - warp / segs + row_step - 1) / row_step : 0)
+                                : (rows_here * segs - warp + kEvalWarps - 1) / kEvalWarps;
+  const long long plane = (long long)nx * ny;
+  for (int item = 0; item < n_items; item++) {
+    int row, x0;
+    if (fixed_seg) {
+      row = row_begin + warp / segs + item * row_step;
+      x0 = (warp % segs) * 128 + lane * 4;
+    } else {
+      const int it = warp + item * kEvalWarps;
+      const int rr = it / segs;
+      row = row_begin + rr;
+      x0 = (it - rr * segs) * 128 + lane * 4;
+    }
+    if (x0 >= nx) continue;
+    const RowDesc rd = R.rows[row];
+    const int z = rd.z;
+    const int y = rd.y;
+    const bool flip = bidir && (y & 1);
+    const long long p0 = (long long)row * nx + x0;
+    float t4[4], g4[NDIM][4];
+    load4(tref + p0, t4);
+#pragma unroll
+    for (int k = 0; k < NDIM; k++) load4(tg[k] + p0, g4[k]);
+
+    // Do the four voxels share interval, storage range and integer tap offsets, away from edges?
+    const int xs0 = flip ? nx - 1 - x0 : x0;
+    const int xs3 = flip ? xs0 - 3 : xs0 + 3;
+    const int di = rd.di0 + (xs0 >= rd.xdi ? 1 : 0);
+    const int di3 = rd.di0 + (xs3 >= rd.xdi ? 1 : 0);
+    const int r = bidir ? rd.r0 + (x0 >= rd.xr ? 1 : 0) : di;
+    const int r3 = bidir ? rd.r0 + (x0 + 3 >= rd.xr ? 1 : 0) : di3;
+    bool fast = (di == di3) && (r == r3) && (rd.xlast < x0 || rd.xlast > x0 + 3);
+    const float4* P = sD + min(max(di - cw, 0), kWin - 2) * kDParamF4;
+    const float f0 = fmaf((float)xs0, dq, rd.qbase) - (float)(di - rd.di0);
+    const float fs = flip ? -dq : dq;
+    const float4 n = P[0], ph = P[1], dd = P[2];
+    const float t0x = fmaf(f0, dd.x, ph.x), t0y = fmaf(f0, dd.y, ph.y);
+    const float sx = fs * dd.x, sy = fs * dd.y;
+    const float flx = floorf(t0x), fly = floorf(t0y);
+    fast = fast && floorf(fmaf(3.0f, sx, t0x)) == flx && floorf(fmaf(3.0f, sy, t0y)) == fly;
+    const int ix = x0 + (int)n.x + (int)flx;
+    const int iy = y + (int)n.y + (int)fly;
+    bool inside = ix >= 0 && ix + 4 <= nx - 1 && iy >= 0 && iy + 1 <= ny - 1;
+    float t0z = 0.f, sz = 0.f, flz = 0.f;
+    int iz = 0;
+    if (NDIM == 3) {
+      t0z = fmaf(f0, dd.z, ph.z);
+      sz = fs * dd.z;
+      flz = floorf(t0z);
+      fast = fast && floorf(fmaf(3.0f, sz, t0z)) == flz;
+      iz = z + (int)n.z + (int)flz;
+      inside = inside && iz >= 0 && iz + 1 <= nz - 1;
+    }
+
+    float acc0[NDIM], acc1[NDIM];  // J^T e of controls r and r+1 for this lane's voxels
+#pragma unroll
+    for (int k = 0; k < NDIM; k++) acc0[k] = acc1[k] = 0.0f;
+
+    if (fast) {
+      float v[NDIM == 3 ? 4 : 2][5];
+      if (inside) {
+        const int a = ix & ~3, s = ix & 3;
+        const long long rb = ((long long)iz * ny + iy) * nx + a;
+        window5(fr + rb, s, v[0]);
+        window5(fr + rb + nx, s, v[1]);
+        if (NDIM == 3) {
+          window5(fr + rb + plane, s, v[NDIM == 3 ? 2 : 0]);
+          window5(fr + rb + plane + nx, s, v[NDIM == 3 ? 3 : 1]);
+        }
+      } else {
+        // tap rows (y, z), (y+1, z), (y, z+1), (y+1, z+1); rows outside the volume read zeros
+        const bool y0v = (unsigned)iy < (unsigned)ny, y1v = (unsigned)(iy + 1) < (unsigned)ny;
+        const bool z0v = NDIM == 2 || (unsigned)iz < (unsigned)nz;
+        const bool z1v = NDIM == 2 || (unsigned)(iz + 1) < (unsigned)nz;
+        const long long rb = ((long long)iz * ny + iy) * nx;
+        masked5(fr + rb, y0v && z0v, ix, nx, v[0]);
+        masked5(fr + rb + nx, y1v && z0v, ix, nx, v[1]);
+        if (NDIM == 3) {
+          masked5(fr + rb + plane, y0v && z1v, ix, nx, v[NDIM == 3 ? 2 : 0]);
+          masked5(fr + rb + plane + nx, y1v && z1v, ix, nx, v[NDIM == 3 ? 3 : 1]);
+        }
+      }
+      const float wx0 = t0x - flx, wy0 = t0y - fly, wz0 = t0z - flz;
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const float wx = fmaf((float)j, sx, wx0), wy = fmaf((float)j, sy, wy0);
+        const float c00 = fmaf(wx, v[0][j + 1] - v[0][j], v[0][j]);
+        const float c01 = fmaf(wx, v[1][j + 1] - v[1][j], v[1][j]);
+        float val = fmaf(wy, c01 - c00, c00);
+        if (NDIM == 3) {
+          const float wz = fmaf((float)j, sz, wz0);
+          const float c10 = fmaf(wx, v[NDIM == 3 ? 2 : 0][j + 1] - v[NDIM == 3 ? 2 : 0][j], v[NDIM == 3 ? 2 : 0][j]);
+          const float c11 = fmaf(wx, v[NDIM == 3 ? 3 : 1][j + 1] - v[NDIM == 3 ? 3 : 1][j], v[NDIM == 3 ? 3 : 1][j]);
+          const float c1 = fmaf(wy, c11 - c10, c10);
+          val = fmaf(wz, c1 - val, val);
+        }
+        const float e = (val > 0.0f) ? val - t4[j] : 0.0f;
+        af = fmaf(e, e, af);
+        const float fj = fmaf((float)j, fs, f0);
+        const float e1 = e * fj;
+        const float e0 = e - e1;
+#pragma unroll
+        for (int k = 0; k < NDIM; k++) {
+          acc0[k] = fmaf(g4[k][j], e0, acc0[k]);
+          acc1[k] = fmaf(g4[k][j], e1, acc1[k]);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const int x = x0 + j;
+        const VoxelModel vm = voxel_model(rd, x, nx, flip, bidir, dq);
+        const int wi = min(max(vm.di - cw, 0), kWin - 2);
+        const float val = sample<NDIM, FT>(fr, sD + wi * kDParamF4, vm.f, x, y, z, nx, ny, nz);
+        const float e = (val > 0.0f) ? val - t4[j] : 0.0f;
+        af = fmaf(e, e, af);
+        if (!vm.last) {
+          const float e1 = e * vm.f;
+          const float e0 = e * (1.0f - vm.f);
+          if (vm.r == r) {
+#pragma unroll
+            for (int k = 0; k < NDIM; k++) {
+              acc0[k] = fmaf(g4[k][j], e0, acc0[k]);
+              acc1[k] = fmaf(g4[k][j], e1, acc1[k]);
+            }
+          } else {
+            // voxel in the following range: controls r+1 and r+2
+            const int s2 = vm.r - c0;
+#pragma unroll
+            for (int k = 0; k < NDIM; k++) {
+              if (s2 == 1) {
+                ag[1][k] = fmaf(g4[k][j], e0, ag[1][k]);
+                ag[2][k] = fmaf(g4[k][j], e1, ag[2][k]);
+              } else {
+                ag[0][k] = fmaf(g4[k][j], e0, ag[0][k]);
+                ag[1][k] = fmaf(g4[k][j], e1, ag[1][k]);
+              }
+            }
+          }
+        }
+      }
+    }
+    if (r == c0) {
+#pragma unroll
+      for (int k = 0; k < NDIM; k++) {
+        ag[0][k] += acc0[k];
+        ag[1][k] += acc1[k];
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < NDIM; k++) {
+        ag[1][k] += acc0[k];
+        ag[2][k] += acc1[k];
+      }
+    }
+  }
+
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    af += __shfl_xor_sync(0xffffffffu, af, o);
+#pragma unroll
+    for (int s = 0; s < 3; s++)
+#pragma unroll
+      for (int k = 0; k < NDIM; k++) ag[s][k] += __shfl_xor_sync(0xffffffffu, ag[s][k], o);
+  }
+  if (lane == 0) {
+    sred[warp][0] = af;
+#pragma unroll
+    for (int s = 0; s < 3; s++)
+#pragma unroll
+      for (int k = 0; k < NDIM; k++) sred[warp][1 + s * NDIM + k] = ag[s][k];
+  }
+  __syncthreads();
+  double* out = job.partials + (long long)tile * kPartialDoubles;
+  if (threadIdx.x < 1 + 3 * NDIM) {
+    double acc = 0.0;
+    for (int w = 0; w < kEvalWarps; w++) acc += (double)sred[w][threadIdx.x];
+    const int i = threadIdx.x;
+    if (i == 0) {
+      out[0] = acc;
+    } else {
+      const int s = (i - 1) / NDIM, k = (i - 1) % NDIM;
+      out[2 + s * 3 + k] = acc;
+    }
+  } else if (threadIdx.x == 1 + 3 * NDIM) {
+    out[1] = (double)c0;
+    if (NDIM == 2) out[2 + 0 * 3 + 2] = out[2 + 1 * 3 + 2] = out[2 + 2 * 3 + 2] = 0.0;
+  }
+}
+
+cudaError_t launch_eval4(const Job* jobs_dev, int n_jobs, int max_tiles, int n_dim, bool frame_half, bool ref_bf16,
+                         cudaStream_t s) {
+  dim3 grid(max_tiles, n_jobs);
+  if (n_dim == 3) {
+    if (frame_half && ref_bf16)
+      eval4_kernel<3, __half, __nv_bfloat16><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
+    else if (frame_half)
+      eval4_kernel<3, __half, float><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
+    else if (ref_bf16)
+      eval4_kernel<3, float, __nv_bfloat16><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
+    else
+      eval4_kernel<3, float, float><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
+  } else {
+    if (frame_half && ref_bf16)
+      eval4_kernel<2, __half, __nv_bfloat16><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
+    else if (frame_half)
+      eval4_kernel<2, __half, float><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
+    else if (ref_bf16)
+      eval4_kernel<2, float, __nv_bfloat16><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
+    else
+      eval4_kernel<2, float, float><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace fa

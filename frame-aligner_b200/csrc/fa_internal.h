@@ -24,8 +24,8 @@ struct RowDesc {
   int r0;
   int xr;
   int xlast;
-  int pad0;
-  int pad1;
+  int y;  // image row index within its plane
+  int z;  // plane index
 };
 
 // Control-point parameters for the fused pass, per control point k (3 float4):

@@ -13,17 +13,6 @@
 
 namespace fa {
 
-// ------------------------------------------------------------------ loads ------------------------
-
-template <typename T>
-__device__ __forceinline__ float ldf(const T* p);
-template <>
-__device__ __forceinline__ float ldf<float>(const float* p) { return __ldg(p); }
-template <>
-__device__ __forceinline__ float ldf<__half>(const __half* p) { return __half2float(__ldg(p)); }
-template <>
-__device__ __forceinline__ float ldf<__nv_bfloat16>(const __nv_bfloat16* p) { return __bfloat162float(__ldg(p)); }
-
 // ------------------------------------------------------------------ Sobel3d ----------------------
 
 // One separable pass at position i of an axis of length n (Sobel3d.cpp:8-58): interior
@@ -168,81 +157,7 @@ cudaError_t launch_downsample(const void* in, fa_dtype in_type, int nz, int ny, 
   return cudaGetLastError();
 }
 
-// ------------------------------------------------------------------ per-voxel model --------------
-
-// Interval, fraction and storage-range bookkeeping of one voxel (see RowDesc).
-struct VoxelModel {
-  int di;      // displacement interval
-  float f;     // fraction within it
-  int r;       // storage range (steepest-descent images)
-  bool last;   // last voxel of its storage range
-};
-
-__device__ __forceinline__ VoxelModel voxel_model(const RowDesc& rd, int x, int nx, bool flip, bool bidir, float dq) {
-  VoxelModel v;
-  const int xs = flip ? nx - 1 - x : x;
-  v.di = rd.di0 + (xs >= rd.xdi ? 1 : 0);
-  float f = fmaf((float)xs, dq, rd.qbase) - (float)(v.di - rd.di0);
-  v.f = fminf(fmaxf(f, 0.0f), 1.0f);
-  v.r = bidir ? rd.r0 + (x >= rd.xr ? 1 : 0) : v.di;
-  v.last = (x == rd.xlast);
-  return v;
-}
-
-// Zero-padded trilinear (bilinear for NDIM == 2) sample of the frame at (x, y, z) + d, where
-// d = int(D) + frac(D) + f * dD from the control-point parameters P (3 float4). Returns the
-// interpolated value; exactly 0 when every contributing tap is outside (getZeroPadded,
-// FrameWarper.h:39-47).
-template <int NDIM, typename FT>
-__device__ __forceinline__ float sample(const FT* __restrict__ fr, const float4* P, float f, int x, int y, int z,
-                                        int nx, int ny, int nz) {
-  const float4 n = P[0], ph = P[1], dd = P[2];
-  const float tx = fmaf(f, dd.x, ph.x);
-  const float ty = fmaf(f, dd.y, ph.y);
-  const float flx = floorf(tx), fly = floorf(ty);
-  const float wx = tx - flx, wy = ty - fly;
-  const int ix = x + (int)n.x + (int)flx;
-  const int iy = y + (int)n.y + (int)fly;
-  const bool vx0 = (unsigned)ix < (unsigned)nx, vx1 = (unsigned)(ix + 1) < (unsigned)nx;
-  const bool vy0 = (unsigned)iy < (unsigned)ny, vy1 = (unsigned)(iy + 1) < (unsigned)ny;
-  if (NDIM == 2) {
-    const long long b = (long long)iy * nx + ix;
-    const float v00 = (vy0 && vx0) ? ldf(fr + b) : 0.0f;
-    const float v01 = (vy0 && vx1) ? ldf(fr + b + 1) : 0.0f;
-    const float v10 = (vy1 && vx0) ? ldf(fr + b + nx) : 0.0f;
-    const float v11 = (vy1 && vx1) ? ldf(fr + b + nx + 1) : 0.0f;
-    const float c0 = fmaf(wx, v01 - v00, v00);
-    const float c1 = fmaf(wx, v11 - v10, v10);
-    return fmaf(wy, c1 - c0, c0);
-  } else {
-    const float tz = fmaf(f, dd.z, ph.z);
-    const float flz = floorf(tz);
-    const float wz = tz - flz;
-    const int iz = z + (int)n.z + (int)flz;
-    const bool vz0 = (unsigned)iz < (unsigned)nz, vz1 = (unsigned)(iz + 1) < (unsigned)nz;
-    const long long plane = (long long)nx * ny;
-    const long long b = ((long long)iz * ny + iy) * nx + ix;
-    const float v000 = (vz0 && vy0 && vx0) ? ldf(fr + b) : 0.0f;
-    const float v001 = (vz0 && vy0 && vx1) ? ldf(fr + b + 1) : 0.0f;
-    const float v010 = (vz0 && vy1 && vx0) ? ldf(fr + b + nx) : 0.0f;
-    const float v011 = (vz0 && vy1 && vx1) ? ldf(fr + b + nx + 1) : 0.0f;
-    const float v100 = (vz1 && vy0 && vx0) ? ldf(fr + b + plane) : 0.0f;
-    const float v101 = (vz1 && vy0 && vx1) ? ldf(fr + b + plane + 1) : 0.0f;
-    const float v110 = (vz1 && vy1 && vx0) ? ldf(fr + b + plane + nx) : 0.0f;
-    const float v111 = (vz1 && vy1 && vx1) ? ldf(fr + b + plane + nx + 1) : 0.0f;
-    const float c00 = fmaf(wx, v001 - v000, v000);
-    const float c01 = fmaf(wx, v011 - v010, v010);
-    const float c10 = fmaf(wx, v101 - v100, v100);
-    const float c11 = fmaf(wx, v111 - v110, v110);
-    const float c0 = fmaf(wy, c01 - c00, c00);
-    const float c1 = fmaf(wy, c11 - c10, c10);
-    return fmaf(wz, c1 - c0, c0);
-  }
-}
-
 // ------------------------------------------------------------------ fused evaluation -------------
-
-constexpr int kWin = 5;  // control points [c0-1, c0+4) cover every interval a tile can touch
 
 template <int NDIM, typename FT, typename RT>
 __global__ void __launch_bounds__(kEvalThreads) eval_kernel(const Job* __restrict__ jobs) {
@@ -368,8 +283,12 @@ __global__ void __launch_bounds__(kEvalThreads) eval_kernel(const Job* __restric
   }
 }
 
+cudaError_t launch_eval4(const Job* jobs_dev, int n_jobs, int max_tiles, int n_dim, bool frame_half, bool ref_bf16,
+                         cudaStream_t s);
+
 cudaError_t launch_eval(const Job* jobs_dev, int n_jobs, int max_tiles, int n_dim, bool frame_half, bool ref_bf16,
-                        cudaStream_t s) {
+                        cudaStream_t s, bool rows_multiple_of_4) {
+  if (rows_multiple_of_4) return launch_eval4(jobs_dev, n_jobs, max_tiles, n_dim, frame_half, ref_bf16, s);
   dim3 grid(max_tiles, n_jobs);
   if (n_dim == 3) {
     if (frame_half && ref_bf16)

@@ -32,8 +32,9 @@ cudaError_t launch_downsample(const void* in, fa_dtype in_type, int nz, int ny, 
 
 // Fused warp + error + J^T e over all tiles of n_jobs frames (grid.y = job). frame_half selects
 // FP16 frames, ref_bf16 the BF16 reference/gradient copies.
+// rows_multiple_of_4 selects the four-voxels-per-lane kernel (every job's nx % 4 == 0).
 cudaError_t launch_eval(const Job* jobs_dev, int n_jobs, int max_tiles, int n_dim, bool frame_half, bool ref_bf16,
-                        cudaStream_t s);
+                        cudaStream_t s, bool rows_multiple_of_4);
 
 // Reduces one job's tile partials into result = [f, g(P)] (deterministic order).
 cudaError_t launch_reduce(const Job* job_dev, const RefDev& ref_host, cudaStream_t s);
