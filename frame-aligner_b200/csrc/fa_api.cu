@@ -273,7 +273,7 @@ struct fa_reference {
 struct fa_frame {
   fa_reference* ref = nullptr;
   void* data = nullptr;
-  bool half = false;
+  int kind = fa::kFrameF32;
   cudaStream_t stream = nullptr;
   Job job{};
   Job* job_dev = nullptr;
@@ -295,20 +295,27 @@ struct fa_correlator {
   fa_context* ctx = nullptr;
   int nz = 0, ny = 0, nx = 0;
   long long n_el = 0, n_complex = 0;
-  cufftHandle fwd = 0, inv = 0;
+  int cap = 0;                          // frames per batched FFT
+  cufftHandle fwd = 0, inv = 0;         // batch of cap frames
+  cufftHandle fwd1 = 0, inv1 = 0;       // single frame
   cudaStream_t stream = nullptr;
-  double* window = nullptr;
-  double* real = nullptr;
-  double2* spec = nullptr;
-  double2* ref_conj = nullptr;
-  float* vol = nullptr;
+  double* wy = nullptr;                 // square-root Hann window along y
+  double* wx = nullptr;                 // ... and along x (1 along z)
+  double* real = nullptr;               // cap * n_el
+  double2* spec = nullptr;              // cap * n_complex
+  double2* ref_conj = nullptr;          // n_complex
+  float* vol = nullptr;                 // one host-uploaded volume
+  const void** d_ptrs = nullptr;        // device array of input pointers
+  const void** h_ptrs = nullptr;        // pinned staging of the same
+  int ptr_cap = 0;
   double* bval = nullptr;
   long long* bidx = nullptr;
-  long long* d_idx = nullptr;
+  long long* d_idx = nullptr;           // one peak index per frame (ptr_cap)
   long long* h_idx = nullptr;
-  int n_blocks = 0;
+  int n_blocks = 0;                     // argmax blocks per frame
   std::mutex mu;
   std::vector<Alloc> allocs;
+  std::vector<Alloc> ptr_allocs;
 };
 
 // ================================================================== context ========================
@@ -579,13 +586,15 @@ extern "C" fa_status fa_get_ranges(const fa_reference* R, int* ranges) {
 
 namespace {
 
-size_t work_doubles(const fa_reference* R) { return (size_t)R->P * (2 * R->n_dim) + 2 * (size_t)R->P; }
+size_t work_doubles(const fa_reference* R) { return (size_t)R->P * (2 * R->n_dim) + 3 * (size_t)R->P; }
 
-fa_status frame_alloc(fa_reference* R, fa_frame** out) {
+int default_kind(const fa_reference* R) { return R->prec == FA_PREC_MIXED ? fa::kFrameF16 : fa::kFrameF32; }
+
+fa_status frame_alloc(fa_reference* R, int kind, fa_frame** out) {
   fa_context* ctx = R->ctx;
   fa_frame* F = new fa_frame;
   F->ref = R;
-  F->half = (R->prec == FA_PREC_MIXED);
+  F->kind = kind;
   auto cleanup = [&](fa_status st) {
     std::string keep = g_err;
     if (F->stream) cudaStreamDestroy(F->stream);
@@ -603,7 +612,8 @@ fa_status frame_alloc(fa_reference* R, fa_frame** out) {
   const size_t P = (size_t)R->P;
   fa_status st;
   void* data;
-  if ((st = dalloc(ctx, (size_t)R->N * (F->half ? 2 : 4), &data, F->allocs)) != FA_OK) return cleanup(st);
+  if ((st = dalloc(ctx, (size_t)R->N * (kind == fa::kFrameF32 ? 4 : 2), &data, F->allocs)) != FA_OK)
+    return cleanup(st);
   F->data = data;
   Job& j = F->job;
   j.ref = R->dev;
@@ -638,7 +648,7 @@ fa_status frame_alloc(fa_reference* R, fa_frame** out) {
 fa_status frame_fill(fa_frame* F, const void* src, fa_dtype dtype, bool src_device) {
   fa_reference* R = F->ref;
   const long long N = R->N;
-  const fa_dtype store = F->half ? FA_F16 : FA_F32;
+  const fa_dtype store = F->kind == fa::kFrameF16 ? FA_F16 : FA_F32;
   size_t esz = (dtype == FA_F32) ? 4 : 2;
   if (dtype == store && !src_device) {
     FA_CU(cudaMemcpyAsync(F->data, src, (size_t)N * esz, cudaMemcpyHostToDevice, F->stream));
@@ -666,7 +676,7 @@ fa_status register_impl(fa_reference* R, const void* data, fa_dtype dtype, bool 
   if (dtype < FA_F32 || dtype > FA_U16) return fail(FA_ERR_BAD_ARG, "unknown dtype");
   FA_CU(cudaSetDevice(R->ctx->device));
   fa_frame* F = nullptr;
-  FA_TRY(frame_alloc(R, &F));
+  FA_TRY(frame_alloc(R, default_kind(R), &F));
   fa_status st = frame_fill(F, data, dtype, dev);
   if (st != FA_OK) {
     std::string keep = g_err;
@@ -723,7 +733,7 @@ fa_status evaluate(fa_frame* F, const double* D) {
   make_dparams(D, R->nD, R->n_dim, F->h_dparams);
   const size_t np = (size_t)R->nD * fa::kDParamF4 * sizeof(float4);
   FA_CU(cudaMemcpyAsync(F->job.dparams, F->h_dparams, np, cudaMemcpyHostToDevice, F->stream));
-  FA_CU(fa::launch_eval(F->job_dev, 1, R->G.n_tiles, R->n_dim, F->half, R->prec == FA_PREC_MIXED, F->stream,
+  FA_CU(fa::launch_eval(F->job_dev, 1, R->G.n_tiles, R->n_dim, F->kind, R->prec == FA_PREC_MIXED, F->stream,
                           R->nx % 4 == 0));
   FA_CU(fa::launch_reduce(F->job_dev, R->host, F->stream));
   g_launches += 2;
@@ -769,7 +779,7 @@ extern "C" fa_status fa_warp(fa_frame* F, const double* D, float invalid_value, 
   make_dparams(D, R->nD, R->n_dim, F->h_dparams);
   const size_t np = (size_t)R->nD * fa::kDParamF4 * sizeof(float4);
   FA_CU(cudaMemcpyAsync(F->job.dparams, F->h_dparams, np, cudaMemcpyHostToDevice, F->stream));
-  FA_CU(fa::launch_warp(R->dev, R->host, F->data, F->half, F->job.dparams, invalid_value, F->warp_out, F->stream));
+  FA_CU(fa::launch_warp(R->dev, R->host, F->data, F->kind, F->job.dparams, invalid_value, F->warp_out, F->stream));
   g_launches += 1;
   FA_CU(cudaMemcpyAsync(out, F->warp_out, (size_t)R->N * sizeof(float), cudaMemcpyDeviceToHost, F->stream));
   FA_CU(cudaStreamSynchronize(F->stream));
@@ -836,9 +846,9 @@ extern "C" fa_status fa_align_frame(fa_frame* F, const double* rigid_shift, int 
   const int max_steps = (max_iterations > 0 ? max_iterations : 100) + 4;
   int phase = fa::kPhaseStartZero;
   for (int step = 0; step < max_steps && phase != fa::kPhaseDone; step++) {
-    FA_CU(fa::launch_eval(F->job_dev, 1, R->G.n_tiles, R->n_dim, F->half, R->prec == FA_PREC_MIXED, F->stream,
+    FA_CU(fa::launch_eval(F->job_dev, 1, R->G.n_tiles, R->n_dim, F->kind, R->prec == FA_PREC_MIXED, F->stream,
                           R->nx % 4 == 0));
-    FA_CU(fa::launch_solve(F->job_dev, 1, F->stream));
+    FA_CU(fa::launch_solve(F->job_dev, 1, R->nD, R->n_dim, F->stream));
     g_launches += 2;
     FA_CU(cudaMemcpyAsync(&F->h_state->phase, &F->state->phase, sizeof(int), cudaMemcpyDeviceToHost, F->stream));
     FA_CU(cudaStreamSynchronize(F->stream));
@@ -863,14 +873,19 @@ __global__ void count_active_kernel(const Job* jobs, int n, int* out) {
 
 }  // namespace
 
-extern "C" fa_status fa_align_batch(fa_frame* const* frames, int n, const double* rigid_shifts, int max_iterations,
-                                    double* D_out, fa_align_stats* stats) {
+namespace {
+
+// Batched solve; frame_data (optional) replaces each frame's own device data pointer for this call.
+fa_status align_batch_impl(fa_frame* const* frames, int n, const double* rigid_shifts, int max_iterations,
+                           double* D_out, fa_align_stats* stats, const void* const* frame_data) {
   if (!frames || n <= 0 || !D_out) return fail(FA_ERR_BAD_ARG, "bad arguments");
+  for (int i = 0; i < n; i++)
+    if (!frames[i]) return fail(FA_ERR_BAD_ARG, "NULL frame");
   fa_reference* R0 = frames[0]->ref;
   for (int i = 0; i < n; i++) {
-    if (!frames[i]) return fail(FA_ERR_BAD_ARG, "NULL frame");
-    if (frames[i]->ref->n_dim != R0->n_dim || frames[i]->ref->prec != R0->prec || frames[i]->ref->ctx != R0->ctx)
-      return fail(FA_ERR_BAD_ARG, "batched frames must share dimensionality, precision and context");
+    if (frames[i]->ref->n_dim != R0->n_dim || frames[i]->ref->prec != R0->prec || frames[i]->ref->ctx != R0->ctx ||
+        frames[i]->kind != frames[0]->kind)
+      return fail(FA_ERR_BAD_ARG, "batched frames must share dimensionality, precision, storage and context");
   }
   if (rigid_shifts && !finite_all(rigid_shifts, (size_t)3 * n)) return fail(FA_ERR_BAD_ARG, "rigid shift not finite");
   fa_context* ctx = R0->ctx;
@@ -878,7 +893,7 @@ extern "C" fa_status fa_align_batch(fa_frame* const* frames, int n, const double
   std::vector<std::unique_lock<std::mutex>> locks;
   for (int i = 0; i < n; i++) locks.emplace_back(frames[i]->mu);
   cudaStream_t s = frames[0]->stream;
-  int max_tiles = 0;
+  int max_tiles = 0, max_nD = 0;
   bool vec4 = true;
   std::vector<Job> jobs(n);
   for (int i = 0; i < n; i++) {
@@ -887,8 +902,10 @@ extern "C" fa_status fa_align_batch(fa_frame* const* frames, int n, const double
     FA_CU(cudaStreamSynchronize(F->stream));
     jobs[i] = F->job;
     jobs[i].state = F->state;
+    if (frame_data) jobs[i].frame = frame_data[i];
     max_tiles = std::max(max_tiles, F->ref->G.n_tiles);
     vec4 = vec4 && (F->ref->nx % 4 == 0);
+    max_nD = std::max(max_nD, F->ref->nD);
   }
   std::vector<Alloc> tmp;
   Job* jobs_dev;
@@ -921,8 +938,8 @@ extern "C" fa_status fa_align_batch(fa_frame* const* frames, int n, const double
   cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
     for (int it = 0; it < kGraphIters && e == cudaSuccess; it++) {
-      e = fa::launch_eval(jobs_dev, n, max_tiles, R0->n_dim, frames[0]->half, R0->prec == FA_PREC_MIXED, s, vec4);
-      if (e == cudaSuccess) e = fa::launch_solve(jobs_dev, n, s);
+      e = fa::launch_eval(jobs_dev, n, max_tiles, R0->n_dim, frames[0]->kind, R0->prec == FA_PREC_MIXED, s, vec4);
+      if (e == cudaSuccess) e = fa::launch_solve(jobs_dev, n, max_nD, R0->n_dim, s);
     }
     if (e == cudaSuccess) {
       count_active_kernel<<<1, 32, 0, s>>>(jobs_dev, n, d_active);
@@ -957,110 +974,56 @@ extern "C" fa_status fa_align_batch(fa_frame* const* frames, int n, const double
   return done(FA_OK);
 }
 
+}  // namespace
+
+extern "C" fa_status fa_align_batch(fa_frame* const* frames, int n, const double* rigid_shifts, int max_iterations,
+                                    double* D_out, fa_align_stats* stats) {
+  return align_batch_impl(frames, n, rigid_shifts, max_iterations, D_out, stats, nullptr);
+}
+
 // ================================================================== phase correlation =============
-
-extern "C" fa_status fa_correlator_create(fa_context* ctx, const float* reference, int nz, int ny, int nx,
-                                          fa_correlator** out) {
-  if (!ctx || !reference || !out || nz < 1 || ny < 1 || nx < 1) return fail(FA_ERR_BAD_ARG, "bad arguments");
-  FA_CU(cudaSetDevice(ctx->device));
-  fa_correlator* C = new fa_correlator;
-  C->ctx = ctx;
-  C->nz = nz;
-  C->ny = ny;
-  C->nx = nx;
-  C->n_el = (long long)nz * ny * nx;
-  C->n_complex = (long long)nz * ny * (nx / 2 + 1);
-  auto cleanup = [&](fa_status st) {
-    std::string keep = g_err;
-    fa_correlator_destroy(C);
-    g_err = keep;
-    return st;
-  };
-  if (cudaStreamCreateWithFlags(&C->stream, cudaStreamNonBlocking) != cudaSuccess)
-    return cleanup(fail(FA_ERR_CUDA, "stream"));
-  fa_status st;
-  if ((st = dalloc_t(ctx, (size_t)C->n_el, &C->window, C->allocs)) != FA_OK) return cleanup(st);
-  if ((st = dalloc_t(ctx, (size_t)C->n_el, &C->real, C->allocs)) != FA_OK) return cleanup(st);
-  if ((st = dalloc_t(ctx, (size_t)C->n_complex, &C->spec, C->allocs)) != FA_OK) return cleanup(st);
-  if ((st = dalloc_t(ctx, (size_t)C->n_complex, &C->ref_conj, C->allocs)) != FA_OK) return cleanup(st);
-  if ((st = dalloc_t(ctx, (size_t)C->n_el, &C->vol, C->allocs)) != FA_OK) return cleanup(st);
-  C->n_blocks = (int)std::min<long long>(148 * 4, (C->n_el + 255) / 256);
-  if ((st = dalloc_t(ctx, (size_t)C->n_blocks, &C->bval, C->allocs)) != FA_OK) return cleanup(st);
-  if ((st = dalloc_t(ctx, (size_t)C->n_blocks, &C->bidx, C->allocs)) != FA_OK) return cleanup(st);
-  if ((st = dalloc_t(ctx, 1, &C->d_idx, C->allocs)) != FA_OK) return cleanup(st);
-  if (cudaMallocHost(&C->h_idx, sizeof(long long)) != cudaSuccess) return cleanup(fail(FA_ERR_OOM, "pinned"));
-  // Square-root Hann window in x and y, 1 along z (VolumePhaseCorrelator.cpp:141-166).
-  auto hann = [](int n) {
-    std::vector<double> w(n, 1.0);
-    if (n > 1) {
-      const double PI = 3.14159265358979323846;
-      double f = 2.0 * PI / (n - 1);
-      for (int i = 0; i < n; i++) w[i] = std::sqrt(0.5 * (1 - std::cos(f * i)));
-    }
-    return w;
-  };
-  std::vector<double> wy = hann(ny), wx = hann(nx), win((size_t)C->n_el);
-  size_t idx = 0;
-  for (int z = 0; z < nz; z++)
-    for (int y = 0; y < ny; y++)
-      for (int x = 0; x < nx; x++) win[idx++] = 1.0 * wy[y] * wx[x];
-  if (cudaMemcpy(C->window, win.data(), win.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
-    return cleanup(fail(FA_ERR_CUDA, "window upload"));
-  int dims[3] = {nz, ny, nx};
-  int rank = 3;
-  int* d = dims;
-  if (nz == 1) {
-    rank = 2;
-    d = dims + 1;
-    if (ny == 1) {
-      rank = 1;
-      d = dims + 2;
-    }
-  }
-  if (cufftPlanMany(&C->fwd, rank, d, nullptr, 1, 0, nullptr, 1, 0, CUFFT_D2Z, 1) != CUFFT_SUCCESS ||
-      cufftPlanMany(&C->inv, rank, d, nullptr, 1, 0, nullptr, 1, 0, CUFFT_Z2D, 1) != CUFFT_SUCCESS)
-    return cleanup(fail(FA_ERR_CUDA, "cufftPlanMany failed"));
-  cufftSetStream(C->fwd, C->stream);
-  cufftSetStream(C->inv, C->stream);
-  if (cudaMemcpyAsync(C->vol, reference, (size_t)C->n_el * sizeof(float), cudaMemcpyHostToDevice, C->stream) !=
-      cudaSuccess)
-    return cleanup(fail(FA_ERR_CUDA, "reference upload"));
-  if (fa::launch_phase_window(C->vol, C->window, C->real, C->n_el, C->stream) != cudaSuccess)
-    return cleanup(fail(FA_ERR_CUDA, "window kernel"));
-  if (cufftExecD2Z(C->fwd, C->real, reinterpret_cast<cufftDoubleComplex*>(C->spec)) != CUFFT_SUCCESS)
-    return cleanup(fail(FA_ERR_CUDA, "cufftExecD2Z failed"));
-  if (fa::launch_phase_conj(C->spec, C->ref_conj, C->n_complex, C->stream) != cudaSuccess)
-    return cleanup(fail(FA_ERR_CUDA, "conj kernel"));
-  if (cudaStreamSynchronize(C->stream) != cudaSuccess) return cleanup(fail(FA_ERR_CUDA, "correlator set-up"));
-  *out = C;
-  return FA_OK;
-}
-
-extern "C" fa_status fa_correlator_destroy(fa_correlator* C) {
-  if (!C) return fail(FA_ERR_BAD_ARG, "NULL correlator");
-  cudaSetDevice(C->ctx->device);
-  if (C->stream) cudaStreamSynchronize(C->stream);
-  if (C->fwd) cufftDestroy(C->fwd);
-  if (C->inv) cufftDestroy(C->inv);
-  if (C->h_idx) cudaFreeHost(C->h_idx);
-  if (C->stream) cudaStreamDestroy(C->stream);
-  dfree_all(C->ctx, C->allocs);
-  delete C;
-  return FA_OK;
-}
 
 namespace {
 
-// Window, D2Z, cross-power normalisation, Z2D and first-maximum argmax into *d_out (device).
-fa_status correlator_enqueue(fa_correlator* C, const float* vol_dev, long long* d_out) {
-  g_launches += 4;  // window, normalise, two argmax stages (the FFTs are cuFFT's)
-  FA_CU(fa::launch_phase_window(vol_dev, C->window, C->real, C->n_el, C->stream));
-  if (cufftExecD2Z(C->fwd, C->real, reinterpret_cast<cufftDoubleComplex*>(C->spec)) != CUFFT_SUCCESS)
-    return fail(FA_ERR_CUDA, "cufftExecD2Z failed");
-  FA_CU(fa::launch_phase_normalise(C->spec, C->ref_conj, C->n_complex, C->stream));
-  if (cufftExecZ2D(C->inv, reinterpret_cast<cufftDoubleComplex*>(C->spec), C->real) != CUFFT_SUCCESS)
-    return fail(FA_ERR_CUDA, "cufftExecZ2D failed");
-  FA_CU(fa::launch_phase_argmax(C->real, C->n_el, C->bval, C->bidx, C->n_blocks, d_out, C->stream));
+// Pointer staging for a batch of n inputs (pinned host + device arrays), grown on demand.
+fa_status correlator_reserve(fa_correlator* C, int n) {
+  if (n <= C->ptr_cap) return FA_OK;
+  FA_CU(cudaStreamSynchronize(C->stream));
+  dfree_all(C->ctx, C->ptr_allocs);
+  if (C->h_ptrs) cudaFreeHost(C->h_ptrs);
+  if (C->h_idx) cudaFreeHost(C->h_idx);
+  C->h_ptrs = nullptr;
+  C->h_idx = nullptr;
+  C->ptr_cap = 0;
+  FA_TRY(dalloc_t(C->ctx, (size_t)n, &C->d_ptrs, C->ptr_allocs));
+  FA_TRY(dalloc_t(C->ctx, (size_t)n, &C->d_idx, C->ptr_allocs));
+  if (cudaMallocHost(&C->h_ptrs, (size_t)n * sizeof(void*)) != cudaSuccess ||
+      cudaMallocHost(&C->h_idx, (size_t)n * sizeof(long long)) != cudaSuccess)
+    return fail(FA_ERR_OOM, "cudaMallocHost failed");
+  C->ptr_cap = n;
+  return FA_OK;
+}
+
+// Window, D2Z, cross-power normalisation, Z2D and first-maximum argmax for n volumes (device
+// pointers, FP32 or raw uint16) in batches of C->cap; peak indices to C->d_idx[0..n).
+fa_status correlator_enqueue(fa_correlator* C, const void* const* vols, int in_kind, int n) {
+  FA_TRY(correlator_reserve(C, n));
+  for (int i = 0; i < n; i++) C->h_ptrs[i] = vols[i];
+  FA_CU(cudaMemcpyAsync(C->d_ptrs, C->h_ptrs, (size_t)n * sizeof(void*), cudaMemcpyHostToDevice, C->stream));
+  for (int c0 = 0; c0 < n;) {
+    const int m = (n - c0 >= C->cap) ? C->cap : 1;
+    cufftHandle fwd = (m == C->cap) ? C->fwd : C->fwd1;
+    cufftHandle inv = (m == C->cap) ? C->inv : C->inv1;
+    FA_CU(fa::launch_phase_window(C->d_ptrs + c0, in_kind, C->wy, C->wx, C->ny, C->nx, C->n_el, m, C->real, C->stream));
+    if (cufftExecD2Z(fwd, C->real, reinterpret_cast<cufftDoubleComplex*>(C->spec)) != CUFFT_SUCCESS)
+      return fail(FA_ERR_CUDA, "cufftExecD2Z failed");
+    FA_CU(fa::launch_phase_normalise(C->spec, C->ref_conj, C->n_complex, m, C->stream));
+    if (cufftExecZ2D(inv, reinterpret_cast<cufftDoubleComplex*>(C->spec), C->real) != CUFFT_SUCCESS)
+      return fail(FA_ERR_CUDA, "cufftExecZ2D failed");
+    FA_CU(fa::launch_phase_argmax(C->real, C->n_el, m, C->bval, C->bidx, C->n_blocks, C->d_idx + c0, C->stream));
+    g_launches += 4;  // window, normalise, two argmax stages (the FFTs are cuFFT's)
+    c0 += m;
+  }
   return FA_OK;
 }
 
@@ -1077,29 +1040,144 @@ void unravel_shift(const fa_correlator* C, long long idx, double* shift) {
   shift[2] = (double)z;
 }
 
-fa_status correlator_run(fa_correlator* C, const float* vol_dev, double* shift) {
-  FA_TRY(correlator_enqueue(C, vol_dev, C->d_idx));
-  FA_CU(cudaMemcpyAsync(C->h_idx, C->d_idx, sizeof(long long), cudaMemcpyDeviceToHost, C->stream));
+fa_status correlator_read(fa_correlator* C, int n, double* shifts) {
+  FA_CU(cudaMemcpyAsync(C->h_idx, C->d_idx, (size_t)n * sizeof(long long), cudaMemcpyDeviceToHost, C->stream));
   FA_CU(cudaStreamSynchronize(C->stream));
-  unravel_shift(C, *C->h_idx, shift);
+  for (int i = 0; i < n; i++) unravel_shift(C, C->h_idx[i], shifts + 3 * i);
+  return FA_OK;
+}
+
+fa_status correlator_plan(fa_correlator* C, int batch, cufftHandle* fwd, cufftHandle* inv) {
+  int dims[3] = {C->nz, C->ny, C->nx};
+  int rank = 3;
+  int* d = dims;
+  if (C->nz == 1) {
+    rank = 2;
+    d = dims + 1;
+    if (C->ny == 1) {
+      rank = 1;
+      d = dims + 2;
+    }
+  }
+  // Basic layout: batches contiguous, n_el reals apart on the real side, n_complex on the complex side.
+  if (cufftPlanMany(fwd, rank, d, nullptr, 1, 0, nullptr, 1, 0, CUFFT_D2Z, batch) != CUFFT_SUCCESS ||
+      cufftPlanMany(inv, rank, d, nullptr, 1, 0, nullptr, 1, 0, CUFFT_Z2D, batch) != CUFFT_SUCCESS)
+    return fail(FA_ERR_CUDA, "cufftPlanMany failed");
+  cufftSetStream(*fwd, C->stream);
+  cufftSetStream(*inv, C->stream);
+  return FA_OK;
+}
+
+fa_status correlator_create_impl(fa_context* ctx, const void* reference, bool ref_device, int nz, int ny, int nx,
+                                 int cap, fa_correlator** out) {
+  if (!ctx || !reference || !out || nz < 1 || ny < 1 || nx < 1) return fail(FA_ERR_BAD_ARG, "bad arguments");
+  FA_CU(cudaSetDevice(ctx->device));
+  fa_correlator* C = new fa_correlator;
+  C->ctx = ctx;
+  C->nz = nz;
+  C->ny = ny;
+  C->nx = nx;
+  C->n_el = (long long)nz * ny * nx;
+  C->n_complex = (long long)nz * ny * (nx / 2 + 1);
+  C->cap = cap < 1 ? 1 : cap;
+  auto cleanup = [&](fa_status st) {
+    std::string keep = g_err;
+    fa_correlator_destroy(C);
+    g_err = keep;
+    return st;
+  };
+  if (cudaStreamCreateWithFlags(&C->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return cleanup(fail(FA_ERR_CUDA, "stream"));
+  fa_status st;
+  if ((st = dalloc_t(ctx, (size_t)ny, &C->wy, C->allocs)) != FA_OK) return cleanup(st);
+  if ((st = dalloc_t(ctx, (size_t)nx, &C->wx, C->allocs)) != FA_OK) return cleanup(st);
+  if ((st = dalloc_t(ctx, (size_t)C->n_el * C->cap, &C->real, C->allocs)) != FA_OK) return cleanup(st);
+  if ((st = dalloc_t(ctx, (size_t)C->n_complex * C->cap, &C->spec, C->allocs)) != FA_OK) return cleanup(st);
+  if ((st = dalloc_t(ctx, (size_t)C->n_complex, &C->ref_conj, C->allocs)) != FA_OK) return cleanup(st);
+  if ((st = dalloc_t(ctx, (size_t)C->n_el, &C->vol, C->allocs)) != FA_OK) return cleanup(st);
+  C->n_blocks = (int)std::min<long long>(std::max(1, 148 * 4 / C->cap), (C->n_el + 255) / 256);
+  if ((st = dalloc_t(ctx, (size_t)C->n_blocks * C->cap, &C->bval, C->allocs)) != FA_OK) return cleanup(st);
+  if ((st = dalloc_t(ctx, (size_t)C->n_blocks * C->cap, &C->bidx, C->allocs)) != FA_OK) return cleanup(st);
+  // Square-root Hann window in x and y, 1 along z (VolumePhaseCorrelator.cpp:141-166).
+  auto hann = [](int n) {
+    std::vector<double> w(n, 1.0);
+    if (n > 1) {
+      const double PI = 3.14159265358979323846;
+      double f = 2.0 * PI / (n - 1);
+      for (int i = 0; i < n; i++) w[i] = std::sqrt(0.5 * (1 - std::cos(f * i)));
+    }
+    return w;
+  };
+  std::vector<double> wy = hann(ny), wx = hann(nx);
+  if (cudaMemcpy(C->wy, wy.data(), wy.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(C->wx, wx.data(), wx.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+    return cleanup(fail(FA_ERR_CUDA, "window upload"));
+  if ((st = correlator_plan(C, C->cap, &C->fwd, &C->inv)) != FA_OK) return cleanup(st);
+  if (C->cap > 1) {
+    if ((st = correlator_plan(C, 1, &C->fwd1, &C->inv1)) != FA_OK) return cleanup(st);
+  } else {
+    C->fwd1 = C->fwd;
+    C->inv1 = C->inv;
+  }
+  if (cudaMemcpyAsync(C->vol, reference, (size_t)C->n_el * sizeof(float),
+                      ref_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, C->stream) != cudaSuccess)
+    return cleanup(fail(FA_ERR_CUDA, "reference upload"));
+  if ((st = correlator_reserve(C, 1)) != FA_OK) return cleanup(st);
+  C->h_ptrs[0] = C->vol;
+  if (cudaMemcpyAsync(C->d_ptrs, C->h_ptrs, sizeof(void*), cudaMemcpyHostToDevice, C->stream) != cudaSuccess ||
+      fa::launch_phase_window(C->d_ptrs, fa::kFrameF32, C->wy, C->wx, ny, nx, C->n_el, 1, C->real, C->stream) !=
+          cudaSuccess)
+    return cleanup(fail(FA_ERR_CUDA, "window kernel"));
+  if (cufftExecD2Z(C->fwd1, C->real, reinterpret_cast<cufftDoubleComplex*>(C->spec)) != CUFFT_SUCCESS)
+    return cleanup(fail(FA_ERR_CUDA, "cufftExecD2Z failed"));
+  if (fa::launch_phase_conj(C->spec, C->ref_conj, C->n_complex, C->stream) != cudaSuccess)
+    return cleanup(fail(FA_ERR_CUDA, "conj kernel"));
+  if (cudaStreamSynchronize(C->stream) != cudaSuccess) return cleanup(fail(FA_ERR_CUDA, "correlator set-up"));
+  *out = C;
   return FA_OK;
 }
 
 }  // namespace
+
+extern "C" fa_status fa_correlator_create(fa_context* ctx, const float* reference, int nz, int ny, int nx,
+                                          fa_correlator** out) {
+  return correlator_create_impl(ctx, reference, false, nz, ny, nx, 1, out);
+}
+
+extern "C" fa_status fa_correlator_destroy(fa_correlator* C) {
+  if (!C) return fail(FA_ERR_BAD_ARG, "NULL correlator");
+  cudaSetDevice(C->ctx->device);
+  if (C->stream) cudaStreamSynchronize(C->stream);
+  if (C->fwd1 && C->fwd1 != C->fwd) cufftDestroy(C->fwd1);
+  if (C->inv1 && C->inv1 != C->inv) cufftDestroy(C->inv1);
+  if (C->fwd) cufftDestroy(C->fwd);
+  if (C->inv) cufftDestroy(C->inv);
+  if (C->h_ptrs) cudaFreeHost(C->h_ptrs);
+  if (C->h_idx) cudaFreeHost(C->h_idx);
+  if (C->stream) cudaStreamDestroy(C->stream);
+  dfree_all(C->ctx, C->ptr_allocs);
+  dfree_all(C->ctx, C->allocs);
+  delete C;
+  return FA_OK;
+}
 
 extern "C" fa_status fa_correlator_shift(fa_correlator* C, const float* volume, double* shift) {
   if (!C || !volume || !shift) return fail(FA_ERR_BAD_ARG, "NULL argument");
   std::lock_guard<std::mutex> lk(C->mu);
   FA_CU(cudaSetDevice(C->ctx->device));
   FA_CU(cudaMemcpyAsync(C->vol, volume, (size_t)C->n_el * sizeof(float), cudaMemcpyHostToDevice, C->stream));
-  return correlator_run(C, C->vol, shift);
+  const void* v = C->vol;
+  FA_TRY(correlator_enqueue(C, &v, fa::kFrameF32, 1));
+  return correlator_read(C, 1, shift);
 }
 
 extern "C" fa_status fa_correlator_shift_device(fa_correlator* C, const float* volume_device, double* shift) {
   if (!C || !volume_device || !shift) return fail(FA_ERR_BAD_ARG, "NULL argument");
   std::lock_guard<std::mutex> lk(C->mu);
   FA_CU(cudaSetDevice(C->ctx->device));
-  return correlator_run(C, volume_device, shift);
+  const void* v = volume_device;
+  FA_TRY(correlator_enqueue(C, &v, fa::kFrameF32, 1));
+  return correlator_read(C, 1, shift);
 }
 
 // ================================================================== test hooks ====================
@@ -1131,7 +1209,7 @@ extern "C" fa_status fa_test_tr_subproblem(fa_context* ctx, int nD, int n_dim, c
   if ((st = dalloc_t(ctx, hl.size(), &dHl, tmp)) != FA_OK) return done(st);
   if ((st = dalloc_t(ctx, (size_t)P, &dg, tmp)) != FA_OK) return done(st);
   if ((st = dalloc_t(ctx, (size_t)P, &dp, tmp)) != FA_OK) return done(st);
-  if ((st = dalloc_t(ctx, (size_t)P * (2 * n_dim) + 2 * (size_t)P, &work, tmp)) != FA_OK) return done(st);
+  if ((st = dalloc_t(ctx, (size_t)P * (2 * n_dim) + 3 * (size_t)P, &work, tmp)) != FA_OK) return done(st);
   if ((st = dalloc_t(ctx, 1, &db, tmp)) != FA_OK) return done(st);
   cudaError_t e = cudaMemcpy(dHd, hd.data(), hd.size() * sizeof(double), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(dHl, hl.data(), hl.size() * sizeof(double), cudaMemcpyHostToDevice);
@@ -1154,16 +1232,14 @@ struct fa_aligner {
   int dz = 0, dy = 0, dx = 0;  // downsampled dims
   cudaStream_t stream = nullptr;
   std::vector<fa_frame*> slots;
-  void* staging = nullptr;     // raw frames in flight (n_stage * N * 4 bytes)
+  int slot_kind = -1;
+  void* staging = nullptr;     // raw frames copied from the host when they need a conversion pass
   size_t staging_bytes = 0;
-  float* vols = nullptr;       // downsampled float frames for the correlator
+  float* vols = nullptr;       // downsampled frames for the correlator (spatial_binning > 1)
   size_t vols_count = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = 0;
-  long long* d_idx = nullptr;  // per-frame peak indices
-  long long* h_idx = nullptr;
-  int idx_cap = 0;
-  std::vector<Alloc> allocs;   // staging / vols / d_idx
+  std::vector<Alloc> allocs;   // staging / vols
   std::vector<Alloc> ref_allocs;
   std::mutex mu;
 };
@@ -1173,6 +1249,7 @@ namespace {
 void aligner_release_reference(fa_aligner* A) {
   for (fa_frame* f : A->slots) fa_deregister_frame(f);
   A->slots.clear();
+  A->slot_kind = -1;
   if (A->corr) fa_correlator_destroy(A->corr);
   A->corr = nullptr;
   if (A->ref) fa_reference_destroy(A->ref);
@@ -1182,30 +1259,40 @@ void aligner_release_reference(fa_aligner* A) {
 
 size_t dtype_size(fa_dtype t) { return t == FA_F32 ? 4 : 2; }
 
-fa_status aligner_grow(fa_aligner* A, int n, size_t raw_bytes) {
+// Slot storage for a batch: raw uint16 counts (the kernels add the +1) when the input is uint16
+// and the reference is mixed precision; otherwise FP16 / FP32 values with the +1 applied.
+int slot_kind_for(const fa_aligner* A, fa_dtype dtype) {
+  if (A->prm.precision == FA_PREC_MIXED) return dtype == FA_U16 ? fa::kFrameRawU16 : fa::kFrameF16;
+  return fa::kFrameF32;
+}
+
+fa_status aligner_grow(fa_aligner* A, int n, int kind, size_t staging_need) {
+  if (A->slot_kind != kind) {
+    for (fa_frame* f : A->slots) fa_deregister_frame(f);
+    A->slots.clear();
+    A->slot_kind = kind;
+  }
   while ((int)A->slots.size() < n) {
     fa_frame* F = nullptr;
-    FA_TRY(frame_alloc(A->ref, &F));
+    FA_TRY(frame_alloc(A->ref, kind, &F));
     A->slots.push_back(F);
   }
-  const size_t need = (size_t)n * raw_bytes;
-  if (A->staging_bytes < need || (int)A->vols_count < n || A->idx_cap < n) {
-    FA_CU(cudaStreamSynchronize(A->stream));
+  const bool need_vols = A->prm.spatial_binning > 1;
+  if (A->staging_bytes < staging_need || (need_vols && (int)A->vols_count < n)) {
+    FA_CU(cudaStreamSynchronize(A->corr->stream));
     dfree_all(A->ctx, A->allocs);
-    if (A->h_idx) cudaFreeHost(A->h_idx);
-    A->h_idx = nullptr;
     A->staging = nullptr;
     A->staging_bytes = 0;
+    A->vols = nullptr;
     A->vols_count = 0;
-    A->idx_cap = 0;
-    FA_TRY(dalloc(A->ctx, need, &A->staging, A->allocs));
-    A->staging_bytes = need;
-    FA_TRY(dalloc_t(A->ctx, (size_t)n * A->dz * A->dy * A->dx, &A->vols, A->allocs));
-    A->vols_count = (size_t)n;
-    FA_TRY(dalloc_t(A->ctx, (size_t)n, &A->d_idx, A->allocs));
-    if (cudaMallocHost(&A->h_idx, (size_t)n * sizeof(long long)) != cudaSuccess)
-      return fail(FA_ERR_OOM, "cudaMallocHost failed");
-    A->idx_cap = n;
+    if (staging_need) {
+      FA_TRY(dalloc(A->ctx, staging_need, &A->staging, A->allocs));
+      A->staging_bytes = staging_need;
+    }
+    if (need_vols) {
+      FA_TRY(dalloc_t(A->ctx, (size_t)n * A->dz * A->dy * A->dx, &A->vols, A->allocs));
+      A->vols_count = (size_t)n;
+    }
   }
   return FA_OK;
 }
@@ -1220,44 +1307,72 @@ fa_status aligner_run(fa_aligner* A, const void* const* frames, fa_dtype dtype, 
   FA_CU(cudaSetDevice(A->ctx->device));
   const long long N = A->ref->N;
   const size_t raw_bytes = (size_t)N * dtype_size(dtype);
-  FA_TRY(aligner_grow(A, n, raw_bytes));
-  const fa_dtype store = A->slots[0]->half ? FA_F16 : FA_F32;
-  const long long nds = (long long)A->dz * A->dy * A->dx;
+  const int kind = slot_kind_for(A, dtype);
+  // Raw uint16 slots take the frames as they are: from the host straight into the slot, from the
+  // device by pointer (no copy). Other storage needs a conversion pass, from a staging copy of host
+  // frames.
+  const bool direct = kind == fa::kFrameRawU16;
+  FA_TRY(aligner_grow(A, n, kind, (direct || device_src) ? 0 : (size_t)n * raw_bytes));
   cudaStream_t s = A->corr->stream;
   if (!A->ev0) {
     FA_CU(cudaEventCreate(&A->ev0));
     FA_CU(cudaEventCreate(&A->ev1));
   }
   FA_CU(cudaEventRecord(A->ev0, s));
+  std::vector<const void*> raw((size_t)n), data((size_t)n);
   for (int i = 0; i < n; i++) {
-    const void* raw = frames[i];
-    if (!device_src) {
-      void* dst = static_cast<char*>(A->staging) + (size_t)i * raw_bytes;
-      FA_CU(cudaMemcpyAsync(dst, frames[i], raw_bytes, cudaMemcpyHostToDevice, s));
-      raw = dst;
-    }
-    FA_CU(fa::launch_offset_convert(raw, dtype, A->slots[i]->data, store, N, s));
-    g_launches += 1;
-    float* vol = A->vols + (size_t)i * nds;
-    if (A->prm.spatial_binning > 1 || dtype != FA_F32) {
-      FA_CU(fa::launch_downsample(raw, dtype, A->nz, A->ny, A->nx, A->prm.spatial_binning, vol, s));
+    fa_frame* F = A->slots[i];
+    if (direct) {
+      // Zero-copy needs the vector loads' alignment (16 bytes); otherwise copy into the slot.
+      if (device_src && (reinterpret_cast<uintptr_t>(frames[i]) & 15u) == 0) {
+        raw[i] = frames[i];
+      } else if (device_src) {
+        FA_CU(cudaMemcpyAsync(F->data, frames[i], raw_bytes, cudaMemcpyDeviceToDevice, s));
+        raw[i] = F->data;
+      } else {
+        FA_CU(cudaMemcpyAsync(F->data, frames[i], raw_bytes, cudaMemcpyHostToDevice, s));
+        raw[i] = F->data;
+      }
+      data[i] = raw[i];
+    } else {
+      if (device_src) {
+        raw[i] = frames[i];
+      } else {
+        void* dst = static_cast<char*>(A->staging) + (size_t)i * raw_bytes;
+        FA_CU(cudaMemcpyAsync(dst, frames[i], raw_bytes, cudaMemcpyHostToDevice, s));
+        raw[i] = dst;
+      }
+      FA_CU(fa::launch_offset_convert(raw[i], dtype, F->data, kind == fa::kFrameF16 ? FA_F16 : FA_F32, N, s));
       g_launches += 1;
-    } else
-      vol = const_cast<float*>(static_cast<const float*>(raw));
-    FA_TRY(correlator_enqueue(A->corr, vol, A->d_idx + i));
+      data[i] = F->data;
+    }
   }
-  FA_CU(cudaMemcpyAsync(A->h_idx, A->d_idx, (size_t)n * sizeof(long long), cudaMemcpyDeviceToHost, s));
-  FA_CU(cudaStreamSynchronize(s));
+  // Phase correlation on the raw frames (FrameWarpAligner.cpp:181-190), downsampled when binning.
+  std::vector<const void*> cin((size_t)n);
+  int cin_kind = dtype == FA_U16 ? fa::kFrameRawU16 : fa::kFrameF32;
+  if (A->prm.spatial_binning > 1) {
+    const long long nds = (long long)A->dz * A->dy * A->dx;
+    for (int i = 0; i < n; i++) {
+      float* vol = A->vols + (size_t)i * nds;
+      FA_CU(fa::launch_downsample(raw[i], dtype, A->nz, A->ny, A->nx, A->prm.spatial_binning, vol, s));
+      g_launches += 1;
+      cin[i] = vol;
+    }
+    cin_kind = fa::kFrameF32;
+  } else {
+    cin = raw;
+  }
+  FA_TRY(correlator_enqueue(A->corr, cin.data(), cin_kind, n));
   std::vector<double> rigid((size_t)3 * n);
+  FA_TRY(correlator_read(A->corr, n, rigid.data()));
   for (int i = 0; i < n; i++) {
-    unravel_shift(A->corr, A->h_idx[i], &rigid[(size_t)3 * i]);
     // FrameWarpAligner.cpp:186-188: x and y scaled by the phase-correlation downsampling
     rigid[(size_t)3 * i] *= A->prm.spatial_binning;
     rigid[(size_t)3 * i + 1] *= A->prm.spatial_binning;
     A->slots[i]->have_last = false;
   }
   std::vector<fa_frame*> batch(A->slots.begin(), A->slots.begin() + n);
-  FA_TRY(fa_align_batch(batch.data(), n, rigid.data(), A->prm.max_iterations, D_out, stats));
+  FA_TRY(align_batch_impl(batch.data(), n, rigid.data(), A->prm.max_iterations, D_out, stats, data.data()));
   FA_CU(cudaEventRecord(A->ev1, batch[0]->stream));
   FA_CU(cudaEventSynchronize(A->ev1));
   float ms = 0;
@@ -1287,7 +1402,6 @@ extern "C" fa_status fa_aligner_destroy(fa_aligner* A) {
   cudaSetDevice(A->ctx->device);
   aligner_release_reference(A);
   dfree_all(A->ctx, A->allocs);
-  if (A->h_idx) cudaFreeHost(A->h_idx);
   if (A->stream) cudaStreamDestroy(A->stream);
   if (A->ev0) cudaEventDestroy(A->ev0);
   if (A->ev1) cudaEventDestroy(A->ev1);
@@ -1320,12 +1434,12 @@ extern "C" fa_status fa_aligner_set_reference(fa_aligner* A, const void* referen
   // smoothed_reference = reference + 1 (smoothing 0), FrameWarpAligner.cpp:86-90
   FA_CU(fa::launch_offset_convert(raw, dtype, plus1, FA_F32, N, A->stream));
   FA_CU(fa::launch_downsample(raw, dtype, nz, ny, nx, b, static_cast<float*>(down), A->stream));
-  std::vector<float> hdown((size_t)A->dz * A->dy * A->dx);
-  FA_CU(cudaMemcpyAsync(hdown.data(), down, hdown.size() * sizeof(float), cudaMemcpyDeviceToHost, A->stream));
   FA_CU(cudaStreamSynchronize(A->stream));
-  FA_TRY(fa_correlator_create(A->ctx, hdown.data(), A->dz, A->dy, A->dx, &A->corr));
-  fa_status st = fa_set_reference_device(A->ctx, static_cast<const float*>(plus1), nz, ny, nx, A->nD, scan,
-                                         A->prm.precision, &A->ref);
+  // Frames go through the correlator in batches of up to 16 (one batched cuFFT plan).
+  fa_status st = correlator_create_impl(A->ctx, down, true, A->dz, A->dy, A->dx, 16, &A->corr);
+  if (st == FA_OK)
+    st = fa_set_reference_device(A->ctx, static_cast<const float*>(plus1), nz, ny, nx, A->nD, scan, A->prm.precision,
+                                 &A->ref);
   dfree_all(A->ctx, A->ref_allocs);
   if (st != FA_OK) {
     std::string keep = g_err;
@@ -1392,10 +1506,10 @@ extern "C" fa_status fa_profile_eval(fa_frame* const* frames, int n, const doubl
   // one untimed launch, then the timed ones
   const bool v4 = R->nx % 4 == 0;
   if (e == cudaSuccess)
-    e = fa::launch_eval(jd, n, R->G.n_tiles, R->n_dim, frames[0]->half, R->prec == FA_PREC_MIXED, s, v4);
+    e = fa::launch_eval(jd, n, R->G.n_tiles, R->n_dim, frames[0]->kind, R->prec == FA_PREC_MIXED, s, v4);
   if (e == cudaSuccess) e = cudaEventRecord(e0, s);
   for (int l = 0; l < launches && e == cudaSuccess; l++)
-    e = fa::launch_eval(jd, n, R->G.n_tiles, R->n_dim, frames[0]->half, R->prec == FA_PREC_MIXED, s, v4);
+    e = fa::launch_eval(jd, n, R->G.n_tiles, R->n_dim, frames[0]->kind, R->prec == FA_PREC_MIXED, s, v4);
   if (e == cudaSuccess) e = cudaEventRecord(e1, s);
   if (e == cudaSuccess) e = cudaEventSynchronize(e1);
   float ms = 0;

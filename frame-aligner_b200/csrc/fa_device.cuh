@@ -16,6 +16,38 @@ __device__ __forceinline__ float ldf<__half>(const __half* p) { return __half2fl
 template <>
 __device__ __forceinline__ float ldf<__nv_bfloat16>(const __nv_bfloat16* p) { return __bfloat162float(__ldg(p)); }
 
+// Raw uint16 photon count; reads return count + 1 (exact: 2^23 + u is representable, so the magic
+// constant subtraction yields u + 1 without a conversion instruction).
+struct RawU16 {
+  unsigned short v;
+};
+__device__ __forceinline__ float u16_plus1(unsigned u) { return __uint_as_float(0x4B000000u | u) - 8388607.0f; }
+template <>
+__device__ __forceinline__ float ldf<RawU16>(const RawU16* p) {
+  return u16_plus1(__ldg(reinterpret_cast<const unsigned short*>(p)));
+}
+
+// Compile-time kernel configuration: dimensionality, frame storage type, reference storage type.
+template <int N, typename FT, typename RT>
+struct KCfg {
+  static constexpr int nd = N;
+  using F = FT;
+  using R = RT;
+};
+
+// Calls f(KCfg<...>{}) for the runtime combination (n_dim, frame kind, BF16 reference or not).
+template <typename Fn>
+inline cudaError_t dispatch_cfg(int n_dim, int kind, bool ref_bf16, Fn&& f) {
+  if (n_dim == 3) {
+    if (kind == kFrameRawU16) return ref_bf16 ? f(KCfg<3, RawU16, __nv_bfloat16>{}) : f(KCfg<3, RawU16, float>{});
+    if (kind == kFrameF16) return ref_bf16 ? f(KCfg<3, __half, __nv_bfloat16>{}) : f(KCfg<3, __half, float>{});
+    return ref_bf16 ? f(KCfg<3, float, __nv_bfloat16>{}) : f(KCfg<3, float, float>{});
+  }
+  if (kind == kFrameRawU16) return ref_bf16 ? f(KCfg<2, RawU16, __nv_bfloat16>{}) : f(KCfg<2, RawU16, float>{});
+  if (kind == kFrameF16) return ref_bf16 ? f(KCfg<2, __half, __nv_bfloat16>{}) : f(KCfg<2, __half, float>{});
+  return ref_bf16 ? f(KCfg<2, float, __nv_bfloat16>{}) : f(KCfg<2, float, float>{});
+}
+
 // ------------------------------------------------------------------ per-voxel model --------------
 
 // Interval, fraction and storage-range bookkeeping of one voxel (see RowDesc).

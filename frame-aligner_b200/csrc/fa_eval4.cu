@@ -56,6 +56,23 @@ __device__ __forceinline__ void window5(const __half* p, int s, float* v) {
   v[3] = b.y;
   v[4] = __half2float(__ushort_as_half((unsigned short)(p2 & 0xffffu)));
 }
+__device__ __forceinline__ void window5(const RawU16* p, int s, float* v) {
+  const uint2 lo = __ldg(reinterpret_cast<const uint2*>(p));
+  const uint2 hi = __ldg(reinterpret_cast<const uint2*>(p + 4));
+  const bool e = (s >> 1) != 0;
+  const unsigned sh = (unsigned)(s & 1) * 16u;
+  const unsigned A = e ? lo.y : lo.x;
+  const unsigned B = e ? hi.x : lo.y;
+  const unsigned C = e ? hi.y : hi.x;
+  const unsigned p0 = __funnelshift_r(A, B, sh);
+  const unsigned p1 = __funnelshift_r(B, C, sh);
+  const unsigned p2 = __funnelshift_r(C, hi.y, sh);
+  v[0] = u16_plus1(p0 & 0xffffu);
+  v[1] = u16_plus1(p0 >> 16);
+  v[2] = u16_plus1(p1 & 0xffffu);
+  v[3] = u16_plus1(p1 >> 16);
+  v[4] = u16_plus1(p2 & 0xffffu);
+}
 __device__ __forceinline__ void window5(const float* p, int s, float* v) {
   const float4 a = __ldg(reinterpret_cast<const float4*>(p));
   const float4 b = __ldg(reinterpret_cast<const float4*>(p + 4));
@@ -322,29 +339,14 @@ __global__ void __launch_bounds__(kEvalThreads, 2) eval4_kernel(const Job* __res
   }
 }
 
-cudaError_t launch_eval4(const Job* jobs_dev, int n_jobs, int max_tiles, int n_dim, bool frame_half, bool ref_bf16,
+cudaError_t launch_eval4(const Job* jobs_dev, int n_jobs, int max_tiles, int n_dim, int frame_kind, bool ref_bf16,
                          cudaStream_t s) {
-  dim3 grid(max_tiles, n_jobs);
-  if (n_dim == 3) {
-    if (frame_half && ref_bf16)
-      eval4_kernel<3, __half, __nv_bfloat16><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
-    else if (frame_half)
-      eval4_kernel<3, __half, float><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
-    else if (ref_bf16)
-      eval4_kernel<3, float, __nv_bfloat16><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
-    else
-      eval4_kernel<3, float, float><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
-  } else {
-    if (frame_half && ref_bf16)
-      eval4_kernel<2, __half, __nv_bfloat16><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
-    else if (frame_half)
-      eval4_kernel<2, __half, float><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
-    else if (ref_bf16)
-      eval4_kernel<2, float, __nv_bfloat16><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
-    else
-      eval4_kernel<2, float, float><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
-  }
-  return cudaGetLastError();
+  const dim3 grid(max_tiles, n_jobs);
+  return dispatch_cfg(n_dim, frame_kind, ref_bf16, [&](auto c) {
+    using C = decltype(c);
+    eval4_kernel<C::nd, typename C::F, typename C::R><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
+    return cudaGetLastError();
+  });
 }
 
 }  // namespace fa

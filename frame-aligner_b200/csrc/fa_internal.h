@@ -36,6 +36,10 @@ constexpr int kDParamF4 = 3;
 // Partial sums of one tile: f, then g for three consecutive control points starting at c0.
 constexpr int kPartialDoubles = 12;  // [f, c0, g(3 x 3), pad]
 
+// Storage of a frame slot: FP32 or FP16 values (the +1 offset of FrameWarpAligner.cpp:142 already
+// applied), or raw uint16 photon counts to which the kernels add 1 when they read them.
+enum FrameKind : int { kFrameF32 = 0, kFrameF16 = 1, kFrameRawU16 = 2 };
+
 // Frame solve phases (device trust region).
 enum Phase : int {
   kPhaseStartZero = 0,   // trial = zero displacement

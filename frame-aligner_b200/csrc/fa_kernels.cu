@@ -283,33 +283,18 @@ __global__ void __launch_bounds__(kEvalThreads) eval_kernel(const Job* __restric
   }
 }
 
-cudaError_t launch_eval4(const Job* jobs_dev, int n_jobs, int max_tiles, int n_dim, bool frame_half, bool ref_bf16,
+cudaError_t launch_eval4(const Job* jobs_dev, int n_jobs, int max_tiles, int n_dim, int frame_kind, bool ref_bf16,
                          cudaStream_t s);
 
-cudaError_t launch_eval(const Job* jobs_dev, int n_jobs, int max_tiles, int n_dim, bool frame_half, bool ref_bf16,
+cudaError_t launch_eval(const Job* jobs_dev, int n_jobs, int max_tiles, int n_dim, int frame_kind, bool ref_bf16,
                         cudaStream_t s, bool rows_multiple_of_4) {
-  if (rows_multiple_of_4) return launch_eval4(jobs_dev, n_jobs, max_tiles, n_dim, frame_half, ref_bf16, s);
-  dim3 grid(max_tiles, n_jobs);
-  if (n_dim == 3) {
-    if (frame_half && ref_bf16)
-      eval_kernel<3, __half, __nv_bfloat16><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
-    else if (frame_half)
-      eval_kernel<3, __half, float><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
-    else if (ref_bf16)
-      eval_kernel<3, float, __nv_bfloat16><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
-    else
-      eval_kernel<3, float, float><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
-  } else {
-    if (frame_half && ref_bf16)
-      eval_kernel<2, __half, __nv_bfloat16><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
-    else if (frame_half)
-      eval_kernel<2, __half, float><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
-    else if (ref_bf16)
-      eval_kernel<2, float, __nv_bfloat16><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
-    else
-      eval_kernel<2, float, float><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
-  }
-  return cudaGetLastError();
+  if (rows_multiple_of_4) return launch_eval4(jobs_dev, n_jobs, max_tiles, n_dim, frame_kind, ref_bf16, s);
+  const dim3 grid(max_tiles, n_jobs);
+  return dispatch_cfg(n_dim, frame_kind, ref_bf16, [&](auto c) {
+    using C = decltype(c);
+    eval_kernel<C::nd, typename C::F, typename C::R><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
+    return cudaGetLastError();
+  });
 }
 
 // ------------------------------------------------------------------ reductions -------------------
@@ -351,33 +336,21 @@ __global__ void __launch_bounds__(256) warp_kernel(const RefDev* __restrict__ Rp
   }
 }
 
-cudaError_t launch_warp(const RefDev* ref_dev, const RefDev& R, const void* frame, bool frame_half,
+cudaError_t launch_warp(const RefDev* ref_dev, const RefDev& R, const void* frame, int frame_kind,
                         const float4* dparams, float invalid_value, float* out, cudaStream_t s) {
   int blocks = (R.n_rows + 7) / 8;
   if (blocks > 148 * 8) blocks = 148 * 8;
-  size_t smem = (size_t)R.nD * kDParamF4 * sizeof(float4);
-  if (smem > 48 * 1024) {
-    cudaError_t e;
-    if (R.n_dim == 3)
-      e = frame_half ? cudaFuncSetAttribute(warp_kernel<3, __half>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-                     : cudaFuncSetAttribute(warp_kernel<3, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    else
-      e = frame_half ? cudaFuncSetAttribute(warp_kernel<2, __half>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-                     : cudaFuncSetAttribute(warp_kernel<2, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-  }
-  if (R.n_dim == 3) {
-    if (frame_half)
-      warp_kernel<3, __half><<<blocks, 256, smem, s>>>(ref_dev, static_cast<const __half*>(frame), dparams, invalid_value, out);
-    else
-      warp_kernel<3, float><<<blocks, 256, smem, s>>>(ref_dev, static_cast<const float*>(frame), dparams, invalid_value, out);
-  } else {
-    if (frame_half)
-      warp_kernel<2, __half><<<blocks, 256, smem, s>>>(ref_dev, static_cast<const __half*>(frame), dparams, invalid_value, out);
-    else
-      warp_kernel<2, float><<<blocks, 256, smem, s>>>(ref_dev, static_cast<const float*>(frame), dparams, invalid_value, out);
-  }
-  return cudaGetLastError();
+  const size_t smem = (size_t)R.nD * kDParamF4 * sizeof(float4);
+  return dispatch_cfg(R.n_dim, frame_kind, false, [&](auto c) {
+    using C = decltype(c);
+    auto kern = warp_kernel<C::nd, typename C::F>;
+    if (smem > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+    }
+    kern<<<blocks, 256, smem, s>>>(ref_dev, static_cast<const typename C::F*>(frame), dparams, invalid_value, out);
+    return cudaGetLastError();
+  });
 }
 
 // ------------------------------------------------------------------ Hessian ----------------------

@@ -30,32 +30,34 @@ cudaError_t launch_offset_convert(const void* in, fa_dtype in_type, void* out, f
 cudaError_t launch_downsample(const void* in, fa_dtype in_type, int nz, int ny, int nx, int b, float* out,
                               cudaStream_t s);
 
-// Fused warp + error + J^T e over all tiles of n_jobs frames (grid.y = job). frame_half selects
-// FP16 frames, ref_bf16 the BF16 reference/gradient copies.
-// rows_multiple_of_4 selects the four-voxels-per-lane kernel (every job's nx % 4 == 0).
-cudaError_t launch_eval(const Job* jobs_dev, int n_jobs, int max_tiles, int n_dim, bool frame_half, bool ref_bf16,
+// Fused warp + error + J^T e over all tiles of n_jobs frames (grid.y = job). frame_kind is a
+// FrameKind, ref_bf16 selects the BF16 reference/gradient copies, rows_multiple_of_4 the
+// four-voxels-per-lane kernel (every job's nx % 4 == 0).
+cudaError_t launch_eval(const Job* jobs_dev, int n_jobs, int max_tiles, int n_dim, int frame_kind, bool ref_bf16,
                         cudaStream_t s, bool rows_multiple_of_4);
 
 // Reduces one job's tile partials into result = [f, g(P)] (deterministic order).
 cudaError_t launch_reduce(const Job* job_dev, const RefDev& ref_host, cudaStream_t s);
 
 // Warped image (CpuFrameWarper::warpImageInterpolated semantics) for one frame.
-cudaError_t launch_warp(const RefDev* ref_dev, const RefDev& ref_host, const void* frame, bool frame_half,
+cudaError_t launch_warp(const RefDev* ref_dev, const RefDev& ref_host, const void* frame, int frame_kind,
                         const float4* dparams, float invalid_value, float* out, cudaStream_t s);
 
 // One trust-region step for each job (grid = n_jobs): reduce partials, advance the state machine,
 // solve the next subproblem, write the next trial point's dparams.
-cudaError_t launch_solve(const Job* jobs_dev, int n_jobs, cudaStream_t s);
+// max_nD / n_dim size the shared-memory staging (frames above about 200 KB work in global memory).
+cudaError_t launch_solve(const Job* jobs_dev, int n_jobs, int max_nD, int n_dim, cudaStream_t s);
 
 // Test hook: the device trust-region subproblem on given dense H (P x P) and g.
 cudaError_t launch_test_subproblem(const double* Hd, const double* Hl, int nD, int nd, const double* g,
                                    double radius, double* p_out, int* boundary_out, double* work, cudaStream_t s);
 
-// Phase correlation kernels (fa_phase.cu).
-cudaError_t launch_phase_window(const float* in, const double* window, double* out, long long n, cudaStream_t s);
-cudaError_t launch_phase_normalise(double2* spec, const double2* ref_conj, long long n, cudaStream_t s);
-cudaError_t launch_phase_argmax(const double* surf, long long n, double* block_val, long long* block_idx,
-                                int n_blocks, long long* out_idx, cudaStream_t s);
+// Phase correlation kernels (fa_phase.cu), each over a batch of frames.
+cudaError_t launch_phase_window(const void* const* vols, int in_kind, const double* wy, const double* wx, int ny,
+                                int nx, long long n_el, int batch, double* out, cudaStream_t s);
+cudaError_t launch_phase_normalise(double2* spec, const double2* ref_conj, long long n, int batch, cudaStream_t s);
+cudaError_t launch_phase_argmax(const double* surf, long long n, int batch, double* block_val, long long* block_idx,
+                                int blocks_per_frame, long long* out_idx, cudaStream_t s);
 cudaError_t launch_phase_conj(const double2* in, double2* out, long long n, cudaStream_t s);
 
 }  // namespace fa

@@ -55,8 +55,9 @@ __device__ __forceinline__ double lval(const Band& B, const double* L, int i, in
 }
 
 // Cholesky of H + lambda I, row by row, summing the nonzero band terms in ascending k (the dense
-// algorithm's order: its skipped terms are exact zeros).
-__device__ int band_chol(const Band& B, double lambda, double* L) {
+// algorithm's order: its skipped terms are exact zeros). inv[i] = 1 / L_ii; off-diagonal entries
+// and the triangular solves multiply by it.
+__device__ int band_chol(const Band& B, double lambda, double* L, double* inv) {
   for (int i = 0; i < B.P; i++) {
     const int ki = kstart(B, i);
     for (int j = ki; j <= i; j++) {
@@ -65,30 +66,32 @@ __device__ int band_chol(const Band& B, double lambda, double* L) {
       for (int k = (ki > kj ? ki : kj); k < j; k++) s -= lref(B, L, i, k) * lref(B, L, j, k);
       if (i == j) {
         if (!(s > 0.0)) return -1;
-        lref(B, L, i, i) = sqrt(s);
+        const double d = sqrt(s);
+        lref(B, L, i, i) = d;
+        inv[i] = 1.0 / d;
       } else {
-        lref(B, L, i, j) = s / lref(B, L, j, j);
+        lref(B, L, i, j) = s * inv[j];
       }
     }
   }
   return 0;
 }
 
-__device__ void band_forward(const Band& B, const double* L, const double* b, double* y) {
+__device__ void band_forward(const Band& B, const double* L, const double* inv, const double* b, double* y) {
   for (int i = 0; i < B.P; i++) {
     double s = b[i];
     for (int k = kstart(B, i); k < i; k++) s -= lval(B, L, i, k) * y[k];
-    y[i] = s / lval(B, L, i, i);
+    y[i] = s * inv[i];
   }
 }
 
-__device__ void band_backward(const Band& B, const double* L, const double* y, double* x) {
+__device__ void band_backward(const Band& B, const double* L, const double* inv, const double* y, double* x) {
   for (int i = B.P - 1; i >= 0; i--) {
     double s = y[i];
     int kend = (i / B.nd + 2) * B.nd;
     if (kend > B.P) kend = B.P;
     for (int k = i + 1; k < kend; k++) s -= lval(B, L, k, i) * x[k];
-    x[i] = s / lval(B, L, i, i);
+    x[i] = s * inv[i];
   }
 }
 
@@ -98,12 +101,13 @@ __device__ double norm2(int n, const double* v) {
   return sqrt(s);
 }
 
-// Returns 1 when the step lies on the trust-region boundary. work: P*(2*nd) + 2*P doubles.
+// Returns 1 when the step lies on the trust-region boundary. work: P*(2*nd) + 3*P doubles.
 __device__ int subproblem(const Band& B, const double* g, double radius, double eps, int max_iter, double* p,
                           double* work) {
   const int P = B.P;
   double* L = work;
-  double* y = work + P * 2 * B.nd;
+  double* inv = work + P * 2 * B.nd;
+  double* y = inv + P;
   double* rhs = y + P;
   const double gnorm = norm2(P, g);
   if (gnorm == 0.0) {
@@ -129,14 +133,14 @@ __device__ int subproblem(const Band& B, const double* g, double radius, double 
   double lambda = 0.0;
   for (int i = 0; i < P; i++) rhs[i] = -g[i];
   for (int it = 0; it < max_iter; it++) {
-    if (band_chol(B, lambda, L) != 0) {
+    if (band_chol(B, lambda, L, inv) != 0) {
       if (lambda > lam_lo) lam_lo = lambda;
       const double a = sqrt(lam_lo * lam_hi), b = lam_lo + 0.001 * (lam_hi - lam_lo);
       lambda = a > b ? a : b;
       continue;
     }
-    band_forward(B, L, rhs, y);
-    band_backward(B, L, y, p);
+    band_forward(B, L, inv, rhs, y);
+    band_backward(B, L, inv, y, p);
     have_p = 1;
     const double pn = norm2(P, p);
     if (lambda == 0.0 && pn <= radius) {
@@ -149,7 +153,7 @@ __device__ int subproblem(const Band& B, const double* g, double radius, double 
     } else {
       if (lambda > lam_lo) lam_lo = lambda;
     }
-    band_forward(B, L, p, y);
+    band_forward(B, L, inv, p, y);
     const double qn = norm2(P, y);
     const double r = pn / qn;
     double next = lambda + r * r * (pn - radius) / radius;
@@ -202,7 +206,15 @@ __device__ bool loop_top(FrameState* S, const Band& B, const double* g, double* 
 
 }  // namespace
 
-__global__ void __launch_bounds__(kSolveThreads) solve_kernel(const Job* __restrict__ jobs) {
+// Doubles of shared memory one frame's solve uses when staged: Hessian blocks, band factor,
+// 1/L_ii, two work vectors, g and p.
+__host__ __device__ inline long long solve_smem_doubles(int nD, int nd) {
+  const long long P = (long long)nD * nd;
+  return 2LL * nD * nd * nd + P * 2 * nd + 5 * P;
+}
+
+__global__ void __launch_bounds__(kSolveThreads) solve_kernel(const Job* __restrict__ jobs, int smem_cap_doubles) {
+  extern __shared__ double s_dyn[];
   const Job& job = jobs[blockIdx.x];
   FrameState* S = job.state;
   if (S->phase == kPhaseDone) return;
@@ -210,13 +222,41 @@ __global__ void __launch_bounds__(kSolveThreads) solve_kernel(const Job* __restr
   __shared__ double s_f;
   reduce_partials(R, job.partials, &s_f, job.gt);
   __syncthreads();
+  // Stage the Hessian blocks, g and p in shared memory when they fit; otherwise work in global.
+  const int nn = R.n_dim * R.n_dim;
+  const bool staged = solve_smem_doubles(R.nD, R.n_dim) <= smem_cap_doubles;
+  const double* Hd = R.Hd;
+  const double* Hl = R.Hl;
+  double* work = job.work;
+  double* gv = job.g;
+  double* pv = job.p;
+  if (staged) {
+    double* sHd = s_dyn;
+    double* sHl = sHd + R.nD * nn;
+    double* sg = sHl + R.nD * nn;
+    double* sp = sg + R.P;
+    for (int i = threadIdx.x; i < R.nD * nn; i += blockDim.x) {
+      sHd[i] = R.Hd[i];
+      sHl[i] = R.Hl[i];
+    }
+    for (int i = threadIdx.x; i < R.P; i += blockDim.x) {
+      sg[i] = job.g[i];
+      sp[i] = job.p[i];
+    }
+    Hd = sHd;
+    Hl = sHl;
+    gv = sg;
+    pv = sp;
+    work = sp + R.P;
+    __syncthreads();
+  }
   const int P = R.P, nd = R.n_dim;
   if (threadIdx.x == 0) {
-    Band B{R.Hd, R.Hl, nd, R.nD, P};
+    Band B{Hd, Hl, nd, R.nD, P};
     const double ft = s_f;
     double* x = job.x;
-    double* g = job.g;
-    double* p = job.p;
+    double* g = gv;
+    double* p = pv;
     const double* gt = job.gt;
     bool go_top = false, done = false;
     int next = kPhaseTrial;
@@ -281,7 +321,7 @@ __global__ void __launch_bounds__(kSolveThreads) solve_kernel(const Job* __restr
           S->f = ft;
           S->accepted++;
         }
-        if (!loop_top(S, B, g, p, job.work)) done = true;
+        if (!loop_top(S, B, g, p, work)) done = true;
         break;
       }
       default:
@@ -292,11 +332,18 @@ __global__ void __launch_bounds__(kSolveThreads) solve_kernel(const Job* __restr
       S->radius = kRadius0;
       S->iter = 0;
       S->have_prev = 0;
-      if (!loop_top(S, B, g, p, job.work)) done = true;
+      if (!loop_top(S, B, g, p, work)) done = true;
     }
     S->phase = done ? kPhaseDone : next;
   }
   __syncthreads();
+  if (staged) {
+    for (int i = threadIdx.x; i < P; i += blockDim.x) {
+      job.g[i] = gv[i];
+      job.p[i] = pv[i];
+    }
+    __syncthreads();
+  }
   if (S->phase == kPhaseDone) return;
   // Next trial point D = x + p, as the fused pass's control-point parameters.
   for (int k = threadIdx.x; k < R.nD; k += blockDim.x) {
@@ -316,8 +363,15 @@ __global__ void __launch_bounds__(kSolveThreads) solve_kernel(const Job* __restr
   }
 }
 
-cudaError_t launch_solve(const Job* jobs_dev, int n_jobs, cudaStream_t s) {
-  solve_kernel<<<n_jobs, kSolveThreads, 0, s>>>(jobs_dev);
+cudaError_t launch_solve(const Job* jobs_dev, int n_jobs, int max_nD, int n_dim, cudaStream_t s) {
+  constexpr long long kCapBytes = 200 * 1024;
+  long long need = solve_smem_doubles(max_nD, n_dim) * (long long)sizeof(double);
+  int smem = need <= kCapBytes ? (int)need : 0;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+  }
+  solve_kernel<<<n_jobs, kSolveThreads, smem, s>>>(jobs_dev, smem / (int)sizeof(double));
   return cudaGetLastError();
 }
 
@@ -325,7 +379,7 @@ __global__ void test_subproblem_kernel(const double* Hd, const double* Hl, int n
                                        double radius, double* p, int* boundary, double* work) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   Band B{Hd, Hl, nd, nD, nD * nd};
-  *boundary = subproblem(B, g, radius, 0.1, 20, p, work);
+  *boundary = subproblem(B, g, radius, 0.1, 20, p, work);  // work: P*(2*nd) + 3*P doubles
 }
 
 cudaError_t launch_test_subproblem(const double* Hd, const double* Hl, int nD, int nd, const double* g,

@@ -26,7 +26,9 @@
  *  definite and |p(0)| <= Delta the Newton step is returned. Otherwise Newton iterations on
  *  1/|p(lambda)| - 1/Delta with the update lambda += (|p|/|q|)^2 (|p| - Delta)/Delta, q = L^-1 p,
  *  kept inside the bracket [lambda_L, lambda_U] (lambda_U = |g|/Delta + |H|_inf,
- *  lambda_L = max(0, -min H_ii, |g|/Delta - |H|_inf)); a failed Cholesky raises lambda_L.
+ *  lambda_L = max(0, -min H_ii, |g|/Delta - |H|_inf)); a failed Cholesky raises lambda_L. The
+ *  Cholesky factor keeps 1/L_ii per row; off-diagonal entries and the triangular solves multiply by
+ *  it rather than divide.
  *  Stop when ||p| - Delta| <= eps * Delta (eps = 0.1) or after 20 iterations; a final step longer
  *  than Delta is scaled back onto the boundary.
  */
@@ -37,8 +39,10 @@
 
 #include "fa_oracle.h"
 
-/* Dense Cholesky of A + lambda I into L (lower, row-major). Returns 0 on success. */
-static int chol_shift(int n, const double* A, double lambda, double* L) {
+/* Dense Cholesky of A + lambda I into L (lower, row-major) with inv[i] = 1 / L[i][i]; the
+   off-diagonal entries and the triangular solves multiply by inv instead of dividing.
+   Returns 0 on success. */
+static int chol_shift(int n, const double* A, double lambda, double* L, double* inv) {
   for (int i = 0; i < n; i++) {
     for (int j = 0; j <= i; j++) {
       double s = A[(size_t)i * n + j] + (i == j ? lambda : 0.0);
@@ -46,8 +50,9 @@ static int chol_shift(int n, const double* A, double lambda, double* L) {
       if (i == j) {
         if (!(s > 0.0)) return -1;
         L[(size_t)i * n + i] = sqrt(s);
+        inv[i] = 1.0 / L[(size_t)i * n + i];
       } else {
-        L[(size_t)i * n + j] = s / L[(size_t)j * n + j];
+        L[(size_t)i * n + j] = s * inv[j];
       }
     }
     for (int j = i + 1; j < n; j++) L[(size_t)i * n + j] = 0.0;
@@ -55,19 +60,19 @@ static int chol_shift(int n, const double* A, double lambda, double* L) {
   return 0;
 }
 
-static void forward(int n, const double* L, const double* b, double* y) {
+static void forward(int n, const double* L, const double* inv, const double* b, double* y) {
   for (int i = 0; i < n; i++) {
     double s = b[i];
     for (int k = 0; k < i; k++) s -= L[(size_t)i * n + k] * y[k];
-    y[i] = s / L[(size_t)i * n + i];
+    y[i] = s * inv[i];
   }
 }
 
-static void backward(int n, const double* L, const double* y, double* x) {
+static void backward(int n, const double* L, const double* inv, const double* y, double* x) {
   for (int i = n - 1; i >= 0; i--) {
     double s = y[i];
     for (int k = i + 1; k < n; k++) s -= L[(size_t)k * n + i] * x[k];
-    x[i] = s / L[(size_t)i * n + i];
+    x[i] = s * inv[i];
   }
 }
 
@@ -95,20 +100,21 @@ int or_tr_subproblem(int P, const double* H, const double* g, double radius, dou
   if (-mindiag > lam_lo) lam_lo = -mindiag;
   if (lam_lo < 0) lam_lo = 0;
   double* L = (double*)malloc(sizeof(double) * (size_t)P * P);
+  double* inv = (double*)malloc(sizeof(double) * (size_t)P);
   double* y = (double*)malloc(sizeof(double) * (size_t)P);
   double* rhs = (double*)malloc(sizeof(double) * (size_t)P);
   int have_p = 0, boundary = 1;
   double lambda = 0.0;
   for (int i = 0; i < P; i++) rhs[i] = -g[i];
   for (int it = 0; it < max_iter; it++) {
-    if (chol_shift(P, H, lambda, L) != 0) {
+    if (chol_shift(P, H, lambda, L, inv) != 0) {
       if (lambda > lam_lo) lam_lo = lambda;
       double a = sqrt(lam_lo * lam_hi), b = lam_lo + 0.001 * (lam_hi - lam_lo);
       lambda = a > b ? a : b;
       continue;
     }
-    forward(P, L, rhs, y);
-    backward(P, L, y, p);
+    forward(P, L, inv, rhs, y);
+    backward(P, L, inv, y, p);
     have_p = 1;
     double pn = norm2(P, p);
     if (lambda == 0.0 && pn <= radius) {
@@ -121,7 +127,7 @@ int or_tr_subproblem(int P, const double* H, const double* g, double radius, dou
     } else {
       if (lambda > lam_lo) lam_lo = lambda;
     }
-    forward(P, L, p, y); /* q = L^-1 p */
+    forward(P, L, inv, p, y); /* q = L^-1 p */
     double qn = norm2(P, y);
     double r = pn / qn;
     double next = lambda + r * r * (pn - radius) / radius;
@@ -141,6 +147,7 @@ int or_tr_subproblem(int P, const double* H, const double* g, double radius, dou
     }
   }
   free(L);
+  free(inv);
   free(y);
   free(rhs);
   return boundary;

@@ -203,3 +203,27 @@ def test_errors_are_reported(ctx):
     with pytest.raises(fa.FaError) as e:
         fr.get_error(D)
     assert e.value.status == 1
+
+
+@pytest.mark.parametrize("precision", [fa.PREC_F32, fa.PREC_MIXED])
+def test_aligner_raw_frames_against_oracle(ctx, precision):
+    """fa_aligner_*: raw uint16 frames in (host and device), +1 offset, phase-correlation start and
+    the batched solve on the device; D within 0.01 px RMS of the CPU solve of the same frames."""
+    import torch
+
+    acq = S.make_config(S.CONFIG0, n_frames=5)
+    nz, ny, nx = acq.reference.shape
+    line, il, ifr = acq.scan
+    ow = O.OracleWarper(acq.reference + 1, acq.nD, O.scan_init(line, il, ifr, nx, ny, nz))
+    al = fa.Aligner(ctx, nD=acq.nD, precision=precision)
+    al.set_reference(acq.reference, fa.scan_params(line, il, ifr, nx, ny, nz))
+    raw = np.ascontiguousarray(acq.frames.astype(np.uint16))
+    D_host, st = al.add_frames([raw[k] for k in range(5)])
+    dev = torch.from_numpy(raw.view(np.int16)).to("cuda:0")
+    torch.cuda.synchronize()
+    D_dev, _ = al.add_frames_device([dev[k].data_ptr() for k in range(5)], fa.U16, 5)
+    assert np.array_equal(D_host, D_dev)
+    for k in range(5):
+        shift = O.phase_shift(acq.reference, acq.frames[k])
+        D_cpu, _ = ow.align_frame(acq.frames[k] + 1, shift, 100)
+        assert _rms(D_host[k], D_cpu, 2) <= 0.01, (k, _rms(D_host[k], D_cpu, 2))
