@@ -864,11 +864,35 @@ extern "C" fa_status fa_align_frame(fa_frame* F, const double* rigid_shift, int 
 
 namespace {
 
-__global__ void count_active_kernel(const Job* jobs, int n, int* out) {
-  int c = 0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) c += (jobs[i].state->phase != fa::kPhaseDone) ? 1 : 0;
-  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-  if (threadIdx.x == 0) *out = c;
+// Indices of the frames still being solved, in ascending order, and their count.
+__global__ void compact_active_kernel(const Job* jobs, int n, int* active, int* n_active) {
+  __shared__ int warp_base[32];
+  __shared__ int base, total;
+  if (threadIdx.x == 0) base = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int c = 0; c < n; c += blockDim.x) {
+    const int i = c + threadIdx.x;
+    const bool f = i < n && jobs[i].state->phase != fa::kPhaseDone;
+    const unsigned m = __ballot_sync(0xffffffffu, f);
+    if (lane == 0) warp_base[w] = __popc(m);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int acc = 0;
+      for (int k = 0; k < (int)(blockDim.x >> 5); k++) {
+        const int t = warp_base[k];
+        warp_base[k] = acc;
+        acc += t;
+      }
+      total = acc;
+    }
+    __syncthreads();
+    if (f) active[base + warp_base[w] + __popc(m & ((1u << lane) - 1u))] = i;
+    __syncthreads();
+    if (threadIdx.x == 0) base += total;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *n_active = base;
 }
 
 }  // namespace
@@ -910,9 +934,11 @@ fa_status align_batch_impl(fa_frame* const* frames, int n, const double* rigid_s
   std::vector<Alloc> tmp;
   Job* jobs_dev;
   int* d_active;
+  int* d_list;
   int* h_active;
   FA_TRY(dalloc_t(ctx, (size_t)n, &jobs_dev, tmp));
   fa_status st = dalloc_t(ctx, 1, &d_active, tmp);
+  if (st == FA_OK) st = dalloc_t(ctx, (size_t)n, &d_list, tmp);
   if (st != FA_OK) {
     dfree_all(ctx, tmp);
     return st;
@@ -931,6 +957,15 @@ fa_status align_batch_impl(fa_frame* const* frames, int n, const double* rigid_s
   };
   if (cudaMemcpyAsync(jobs_dev, jobs.data(), n * sizeof(Job), cudaMemcpyHostToDevice, s) != cudaSuccess)
     return done(fail(FA_ERR_CUDA, "job upload failed"));
+  std::vector<int> all(n);
+  for (int i = 0; i < n; i++) all[i] = i;
+  *h_active = n;
+  if (cudaMemcpyAsync(d_list, all.data(), n * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(d_active, h_active, sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return done(fail(FA_ERR_CUDA, "active list upload failed"));
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
   // Iterations run as a CUDA graph of kGraphIters x (fused pass, solve), then one active count.
   constexpr int kGraphIters = 4;
   cudaGraph_t graph = nullptr;
@@ -938,12 +973,16 @@ fa_status align_batch_impl(fa_frame* const* frames, int n, const double* rigid_s
   cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
     for (int it = 0; it < kGraphIters && e == cudaSuccess; it++) {
-      e = fa::launch_eval(jobs_dev, n, max_tiles, R0->n_dim, frames[0]->kind, R0->prec == FA_PREC_MIXED, s, vec4);
+      if (vec4)
+        e = fa::launch_eval4_active(jobs_dev, d_list, d_active, n, max_tiles, R0->n_dim, frames[0]->kind,
+                                    R0->prec == FA_PREC_MIXED, 2 * sms, s);
+      else
+        e = fa::launch_eval(jobs_dev, n, max_tiles, R0->n_dim, frames[0]->kind, R0->prec == FA_PREC_MIXED, s, false);
       if (e == cudaSuccess) e = fa::launch_solve(jobs_dev, n, max_nD, R0->n_dim, s);
-    }
-    if (e == cudaSuccess) {
-      count_active_kernel<<<1, 32, 0, s>>>(jobs_dev, n, d_active);
-      e = cudaGetLastError();
+      if (e == cudaSuccess) {
+        compact_active_kernel<<<1, 1024, 0, s>>>(jobs_dev, n, d_list, d_active);
+        e = cudaGetLastError();
+      }
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(h_active, d_active, sizeof(int), cudaMemcpyDeviceToHost, s);
     cudaError_t e2 = cudaStreamEndCapture(s, &graph);
@@ -957,7 +996,7 @@ fa_status align_batch_impl(fa_frame* const* frames, int n, const double* rigid_s
   const int max_steps = (max_iterations > 0 ? max_iterations : 100) + 4;
   for (int step = 0; step < max_steps; step += kGraphIters) {
     e = cudaGraphLaunch(exec, s);
-    g_launches += 2 * kGraphIters + 1;
+    g_launches += 3 * kGraphIters;
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) break;
     if (*h_active == 0) break;

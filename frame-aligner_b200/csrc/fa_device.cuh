@@ -140,10 +140,12 @@ __device__ __forceinline__ void reduce_partials(const RefDev& R, const double* _
     const int c = i / nd, k = i % nd;
     const int2 tr = R.ctrl_tiles[c];
     double a = 0.0;
+#pragma unroll 8
     for (int t = tr.x; t < tr.y; t++) {
       const double* pt = parts + (long long)t * kPartialDoubles;
-      const int s = c - (int)pt[1];
-      if (s >= 0 && s < 3) a += pt[2 + s * 3 + k];
+      const int s = c - R.tile_c0[t];
+      const double v = (s >= 0 && s < 3) ? pt[2 + s * 3 + k] : 0.0;
+      a += v;
     }
     g_out[i] = a;
   }

@@ -96,13 +96,9 @@ __device__ __forceinline__ void masked5(const FT* row, bool row_valid, int ix, i
 
 }  // namespace
 
+// One tile of one frame: the whole CTA cooperates; all threads must call it together.
 template <int NDIM, typename FT, typename RT>
-__global__ void __launch_bounds__(kEvalThreads, 2) eval4_kernel(const Job* __restrict__ jobs) {
-  const Job& job = jobs[blockIdx.y];
-  if (job.state != nullptr && job.state->phase == kPhaseDone) return;
-  const RefDev& R = *job.ref;
-  const int tile = blockIdx.x;
-  if (tile >= R.n_tiles) return;
+__device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, const int tile) {
   const int nx = R.nx, ny = R.ny, nz = R.nz;
   const int row_begin = tile * R.tile_rows;
   const int row_end = min(row_begin + R.tile_rows, R.n_rows);
@@ -339,12 +335,52 @@ __global__ void __launch_bounds__(kEvalThreads, 2) eval4_kernel(const Job* __res
   }
 }
 
+template <int NDIM, typename FT, typename RT>
+__global__ void __launch_bounds__(kEvalThreads, 2) eval4_kernel(const Job* __restrict__ jobs) {
+  const Job& job = jobs[blockIdx.y];
+  if (job.state != nullptr && job.state->phase == kPhaseDone) return;
+  const RefDev& R = *job.ref;
+  const int tile = blockIdx.x;
+  if (tile >= R.n_tiles) return;
+  eval4_tile<NDIM, FT, RT>(job, R, tile);
+}
+
+// Persistent form for batched solves: a fixed grid walks the (active frame, tile) items of the
+// compacted active list, so frames that have converged cost nothing.
+template <int NDIM, typename FT, typename RT>
+__global__ void __launch_bounds__(kEvalThreads, 2) eval4_active_kernel(const Job* __restrict__ jobs,
+                                                                     const int* __restrict__ active,
+                                                                     const int* __restrict__ n_active, int max_tiles) {
+  const long long n_items = (long long)(*n_active) * max_tiles;
+  for (long long item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int a = (int)(item / max_tiles);
+    const int tile = (int)(item - (long long)a * max_tiles);
+    const Job& job = jobs[active[a]];
+    const RefDev& R = *job.ref;
+    if (tile >= R.n_tiles) continue;
+    eval4_tile<NDIM, FT, RT>(job, R, tile);
+    __syncthreads();  // the next item reuses the shared-memory window
+  }
+}
+
 cudaError_t launch_eval4(const Job* jobs_dev, int n_jobs, int max_tiles, int n_dim, int frame_kind, bool ref_bf16,
                          cudaStream_t s) {
   const dim3 grid(max_tiles, n_jobs);
   return dispatch_cfg(n_dim, frame_kind, ref_bf16, [&](auto c) {
     using C = decltype(c);
     eval4_kernel<C::nd, typename C::F, typename C::R><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
+    return cudaGetLastError();
+  });
+}
+
+cudaError_t launch_eval4_active(const Job* jobs_dev, const int* active, const int* n_active, int n_jobs, int max_tiles,
+                                int n_dim, int frame_kind, bool ref_bf16, int grid, cudaStream_t s) {
+  const long long most = (long long)n_jobs * max_tiles;
+  const int g = (int)(most < grid ? most : grid);
+  return dispatch_cfg(n_dim, frame_kind, ref_bf16, [&](auto c) {
+    using C = decltype(c);
+    eval4_active_kernel<C::nd, typename C::F, typename C::R><<<g, kEvalThreads, 0, s>>>(jobs_dev, active, n_active,
+                                                                                      max_tiles);
     return cudaGetLastError();
   });
 }

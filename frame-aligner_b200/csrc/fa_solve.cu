@@ -24,14 +24,17 @@ constexpr double kMinDelta = 1e-8;
 constexpr double kRadius0 = 40.0;
 constexpr double kRadiusMax = 1000.0;
 
+template <int ND>
 struct Band {
+  static constexpr int nd = ND;
   const double* Hd;
   const double* Hl;
-  int nd, nD, P;
+  int nD, P;
 };
 
 // Element (i, j) of the dense Hessian.
-__device__ __forceinline__ double hval(const Band& B, int i, int j) {
+template <int ND>
+__device__ __forceinline__ double hval(const Band<ND>& B, int i, int j) {
   const int bi = i / B.nd, bj = j / B.nd;
   const int a = i - bi * B.nd, b = j - bj * B.nd;
   const int nn = B.nd * B.nd;
@@ -42,14 +45,17 @@ __device__ __forceinline__ double hval(const Band& B, int i, int j) {
 }
 
 // Lower band of L: row i holds columns [(bi-1)*nd, (bi+1)*nd), stored at L[i*W + k - (bi-1)*nd].
-__device__ __forceinline__ int kstart(const Band& B, int i) {
+template <int ND>
+__device__ __forceinline__ int kstart(const Band<ND>& B, int i) {
   const int k = (i / B.nd - 1) * B.nd;
   return k < 0 ? 0 : k;
 }
-__device__ __forceinline__ double& lref(const Band& B, double* L, int i, int k) {
+template <int ND>
+__device__ __forceinline__ double& lref(const Band<ND>& B, double* L, int i, int k) {
   return L[i * 2 * B.nd + k - (i / B.nd - 1) * B.nd];
 }
-__device__ __forceinline__ double lval(const Band& B, const double* L, int i, int k) {
+template <int ND>
+__device__ __forceinline__ double lval(const Band<ND>& B, const double* L, int i, int k) {
   if (k < kstart(B, i) || k > i) return 0.0;
   return L[i * 2 * B.nd + k - (i / B.nd - 1) * B.nd];
 }
@@ -57,7 +63,8 @@ __device__ __forceinline__ double lval(const Band& B, const double* L, int i, in
 // Cholesky of H + lambda I, row by row, summing the nonzero band terms in ascending k (the dense
 // algorithm's order: its skipped terms are exact zeros). inv[i] = 1 / L_ii; off-diagonal entries
 // and the triangular solves multiply by it.
-__device__ int band_chol(const Band& B, double lambda, double* L, double* inv) {
+template <int ND>
+__device__ int band_chol(const Band<ND>& B, double lambda, double* L, double* inv) {
   for (int i = 0; i < B.P; i++) {
     const int ki = kstart(B, i);
     for (int j = ki; j <= i; j++) {
@@ -77,7 +84,8 @@ __device__ int band_chol(const Band& B, double lambda, double* L, double* inv) {
   return 0;
 }
 
-__device__ void band_forward(const Band& B, const double* L, const double* inv, const double* b, double* y) {
+template <int ND>
+__device__ void band_forward(const Band<ND>& B, const double* L, const double* inv, const double* b, double* y) {
   for (int i = 0; i < B.P; i++) {
     double s = b[i];
     for (int k = kstart(B, i); k < i; k++) s -= lval(B, L, i, k) * y[k];
@@ -85,7 +93,8 @@ __device__ void band_forward(const Band& B, const double* L, const double* inv, 
   }
 }
 
-__device__ void band_backward(const Band& B, const double* L, const double* inv, const double* y, double* x) {
+template <int ND>
+__device__ void band_backward(const Band<ND>& B, const double* L, const double* inv, const double* y, double* x) {
   for (int i = B.P - 1; i >= 0; i--) {
     double s = y[i];
     int kend = (i / B.nd + 2) * B.nd;
@@ -102,7 +111,8 @@ __device__ double norm2(int n, const double* v) {
 }
 
 // Returns 1 when the step lies on the trust-region boundary. work: P*(2*nd) + 3*P doubles.
-__device__ int subproblem(const Band& B, const double* g, double radius, double eps, int max_iter, double* p,
+template <int ND>
+__device__ int subproblem(const Band<ND>& B, const double* g, double radius, double eps, int max_iter, double* p,
                           double* work) {
   const int P = B.P;
   double* L = work;
@@ -176,7 +186,8 @@ __device__ int subproblem(const Band& B, const double* g, double radius, double 
 }
 
 // Predicted reduction -(g.p + 0.5 p.H.p) with the dense algorithm's summation order.
-__device__ double predicted(const Band& B, const double* g, const double* p) {
+template <int ND>
+__device__ double predicted(const Band<ND>& B, const double* g, const double* p) {
   double gp = 0, pHp = 0;
   for (int i = 0; i < B.P; i++) {
     double s = 0;
@@ -191,7 +202,8 @@ __device__ double predicted(const Band& B, const double* g, const double* p) {
 }
 
 // Start a new trust-region iteration if the stop rule allows it. Returns false when done.
-__device__ bool loop_top(FrameState* S, const Band& B, const double* g, double* p, double* work) {
+template <int ND>
+__device__ bool loop_top(FrameState* S, const Band<ND>& B, const double* g, double* p, double* work) {
   if (S->max_iter > 0 && S->iter >= S->max_iter) {
     S->hit_max = 1;
     return false;
@@ -213,7 +225,96 @@ __host__ __device__ inline long long solve_smem_doubles(int nD, int nd) {
   return 2LL * nD * nd * nd + P * 2 * nd + 5 * P;
 }
 
-__global__ void __launch_bounds__(kSolveThreads) solve_kernel(const Job* __restrict__ jobs, int smem_cap_doubles) {
+// The trust-region state machine for one frame after a fused pass at its trial point (thread 0).
+template <int ND>
+__device__ void state_step(const Job& job, FrameState* S, const RefDev& R, const double* Hd, const double* Hl,
+                           double* gv, double* pv, double* work, double ft) {
+  const int P = R.P, nd = ND;
+  Band<ND> B{Hd, Hl, R.nD, P};
+  double* x = job.x;
+  double* g = gv;
+  double* p = pv;
+  const double* gt = job.gt;
+  bool go_top = false, done = false;
+  int next = kPhaseTrial;
+  S->evaluations++;
+  switch (S->phase) {
+    case kPhaseStartZero: {
+      S->f_start = ft;
+      for (int i = 0; i < P; i++) g[i] = gt[i];
+      bool rigid = false;
+      for (int c = 0; c < nd; c++) rigid = rigid || (S->rigid[c] != 0.0);
+      if (rigid) {
+        for (int k = 0; k < R.nD; k++)
+          for (int c = 0; c < nd; c++) p[k * nd + c] = S->rigid[c];
+        next = kPhaseStartRigid;
+      } else {
+        S->f = ft;
+        go_top = true;
+      }
+      break;
+    }
+    case kPhaseStartRigid: {
+      // Starting points {0, 0, rigid}: std::min_element keeps the first minimum
+      // (FrameWarpAligner.cpp:194-198).
+      if (ft < S->f_start) {
+        for (int i = 0; i < P; i++) {
+          x[i] = p[i];
+          g[i] = gt[i];
+        }
+        S->f = ft;
+      } else {
+        S->f = S->f_start;
+      }
+      go_top = true;
+      break;
+    }
+    case kPhaseTrial: {
+      const double pred = predicted(B, g, p);
+      const double meas = S->f - ft;
+      if (fabs(pred) <= fabs(meas) * kDblEps) {
+        done = true;
+        break;
+      }
+      const double rho = meas / fabs(pred);
+      if (!isfinite(rho)) {
+        done = true;
+        break;
+      }
+      if (rho < 0.25) {
+        S->radius *= 0.25;
+        if (S->radius <= kRadius0 * kDblEps) {
+          done = true;
+          break;
+        }
+      } else if (rho > 0.75 && S->boundary) {
+        S->radius = 2 * S->radius < kRadiusMax ? 2 * S->radius : kRadiusMax;
+      }
+      if (rho > 0) {
+        for (int i = 0; i < P; i++) {
+          x[i] = x[i] + p[i];
+          g[i] = gt[i];
+        }
+        S->f = ft;
+        S->accepted++;
+      }
+      if (!loop_top(S, B, g, p, work)) done = true;
+      break;
+    }
+    default:
+      done = true;
+  }
+  if (go_top) {
+    for (int i = 0; i < P; i++) p[i] = 0.0;
+    S->radius = kRadius0;
+    S->iter = 0;
+    S->have_prev = 0;
+    if (!loop_top(S, B, g, p, work)) done = true;
+  }
+  S->phase = done ? kPhaseDone : next;
+  }
+
+__global__ void __launch_bounds__(kSolveThreads, 1) solve_kernel(const Job* __restrict__ jobs, int smem_cap_doubles) {
   extern __shared__ double s_dyn[];
   const Job& job = jobs[blockIdx.x];
   FrameState* S = job.state;
@@ -252,89 +353,10 @@ __global__ void __launch_bounds__(kSolveThreads) solve_kernel(const Job* __restr
   }
   const int P = R.P, nd = R.n_dim;
   if (threadIdx.x == 0) {
-    Band B{Hd, Hl, nd, R.nD, P};
-    const double ft = s_f;
-    double* x = job.x;
-    double* g = gv;
-    double* p = pv;
-    const double* gt = job.gt;
-    bool go_top = false, done = false;
-    int next = kPhaseTrial;
-    S->evaluations++;
-    switch (S->phase) {
-      case kPhaseStartZero: {
-        S->f_start = ft;
-        for (int i = 0; i < P; i++) g[i] = gt[i];
-        bool rigid = false;
-        for (int c = 0; c < nd; c++) rigid = rigid || (S->rigid[c] != 0.0);
-        if (rigid) {
-          for (int k = 0; k < R.nD; k++)
-            for (int c = 0; c < nd; c++) p[k * nd + c] = S->rigid[c];
-          next = kPhaseStartRigid;
-        } else {
-          S->f = ft;
-          go_top = true;
-        }
-        break;
-      }
-      case kPhaseStartRigid: {
-        // Starting points {0, 0, rigid}: std::min_element keeps the first minimum
-        // (FrameWarpAligner.cpp:194-198).
-        if (ft < S->f_start) {
-          for (int i = 0; i < P; i++) {
-            x[i] = p[i];
-            g[i] = gt[i];
-          }
-          S->f = ft;
-        } else {
-          S->f = S->f_start;
-        }
-        go_top = true;
-        break;
-      }
-      case kPhaseTrial: {
-        const double pred = predicted(B, g, p);
-        const double meas = S->f - ft;
-        if (fabs(pred) <= fabs(meas) * kDblEps) {
-          done = true;
-          break;
-        }
-        const double rho = meas / fabs(pred);
-        if (!isfinite(rho)) {
-          done = true;
-          break;
-        }
-        if (rho < 0.25) {
-          S->radius *= 0.25;
-          if (S->radius <= kRadius0 * kDblEps) {
-            done = true;
-            break;
-          }
-        } else if (rho > 0.75 && S->boundary) {
-          S->radius = 2 * S->radius < kRadiusMax ? 2 * S->radius : kRadiusMax;
-        }
-        if (rho > 0) {
-          for (int i = 0; i < P; i++) {
-            x[i] = x[i] + p[i];
-            g[i] = gt[i];
-          }
-          S->f = ft;
-          S->accepted++;
-        }
-        if (!loop_top(S, B, g, p, work)) done = true;
-        break;
-      }
-      default:
-        done = true;
-    }
-    if (go_top) {
-      for (int i = 0; i < P; i++) p[i] = 0.0;
-      S->radius = kRadius0;
-      S->iter = 0;
-      S->have_prev = 0;
-      if (!loop_top(S, B, g, p, work)) done = true;
-    }
-    S->phase = done ? kPhaseDone : next;
+    if (R.n_dim == 3)
+      state_step<3>(job, S, R, Hd, Hl, gv, pv, work, s_f);
+    else
+      state_step<2>(job, S, R, Hd, Hl, gv, pv, work, s_f);
   }
   __syncthreads();
   if (staged) {
@@ -378,8 +400,14 @@ cudaError_t launch_solve(const Job* jobs_dev, int n_jobs, int max_nD, int n_dim,
 __global__ void test_subproblem_kernel(const double* Hd, const double* Hl, int nD, int nd, const double* g,
                                        double radius, double* p, int* boundary, double* work) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  Band B{Hd, Hl, nd, nD, nD * nd};
-  *boundary = subproblem(B, g, radius, 0.1, 20, p, work);  // work: P*(2*nd) + 3*P doubles
+  // work: P*(2*nd) + 3*P doubles
+  if (nd == 3) {
+    Band<3> B{Hd, Hl, nD, nD * 3};
+    *boundary = subproblem(B, g, radius, 0.1, 20, p, work);
+  } else {
+    Band<2> B{Hd, Hl, nD, nD * 2};
+    *boundary = subproblem(B, g, radius, 0.1, 20, p, work);
+  }
 }
 
 cudaError_t launch_test_subproblem(const double* Hd, const double* Hl, int nD, int nd, const double* g,
