@@ -44,63 +44,110 @@ __device__ __forceinline__ double hval(const Band<ND>& B, int i, int j) {
   return 0.0;
 }
 
-// Lower band of L: row i holds columns [(bi-1)*nd, (bi+1)*nd), stored at L[i*W + k - (bi-1)*nd].
-template <int ND>
-__device__ __forceinline__ int kstart(const Band<ND>& B, int i) {
-  const int k = (i / B.nd - 1) * B.nd;
-  return k < 0 ? 0 : k;
-}
-template <int ND>
-__device__ __forceinline__ double& lref(const Band<ND>& B, double* L, int i, int k) {
-  return L[i * 2 * B.nd + k - (i / B.nd - 1) * B.nd];
-}
-template <int ND>
-__device__ __forceinline__ double lval(const Band<ND>& B, const double* L, int i, int k) {
-  if (k < kstart(B, i) || k > i) return 0.0;
-  return L[i * 2 * B.nd + k - (i / B.nd - 1) * B.nd];
-}
+// Band factor storage: row i of block b holds 2*n_dim entries, the columns of block b-1 then those of
+// block b.
 
-// Cholesky of H + lambda I, row by row, summing the nonzero band terms in ascending k (the dense
-// algorithm's order: its skipped terms are exact zeros). inv[i] = 1 / L_ii; off-diagonal entries
-// and the triangular solves multiply by it.
+// Cholesky of H + lambda I by block rows, fully unrolled over the n_dim x n_dim blocks. Each entry
+// L_ij accumulates A_ij (+ lambda) minus L_ik L_jk over ascending k -- the previous block's columns
+// first, then the earlier columns of its own block -- which is the dense algorithm's order (its
+// other terms are exact zeros). inv[i] = 1 / L_ii; off-diagonal entries multiply by it.
 template <int ND>
 __device__ int band_chol(const Band<ND>& B, double lambda, double* L, double* inv) {
-  for (int i = 0; i < B.P; i++) {
-    const int ki = kstart(B, i);
-    for (int j = ki; j <= i; j++) {
-      double s = hval(B, i, j) + (i == j ? lambda : 0.0);
-      const int kj = kstart(B, j);
-      for (int k = (ki > kj ? ki : kj); k < j; k++) s -= lref(B, L, i, k) * lref(B, L, j, k);
-      if (i == j) {
-        if (!(s > 0.0)) return -1;
-        const double d = sqrt(s);
-        lref(B, L, i, i) = d;
-        inv[i] = 1.0 / d;
-      } else {
-        lref(B, L, i, j) = s * inv[j];
+  constexpr int NN = ND * ND;
+  double C[ND][ND];   // L rows of block b, columns of block b-1
+  double Dg[ND][ND];  // L rows of block b, its own columns (lower triangle)
+  double Dp[ND][ND];  // previous block's own-column L (rows of block b-1)
+#pragma unroll
+  for (int r = 0; r < ND; r++)
+#pragma unroll
+    for (int c = 0; c < ND; c++) Dp[r][c] = 0.0;
+  for (int b = 0; b < B.nD; b++) {
+    const double* hd = B.Hd + b * NN;
+    const double* hl = B.Hl + b * NN;
+    const int i0 = b * ND;
+    if (b > 0) {
+#pragma unroll
+      for (int r = 0; r < ND; r++)
+#pragma unroll
+        for (int c = 0; c < ND; c++) {
+          double s = hl[r * ND + c];
+#pragma unroll
+          for (int k = 0; k < c; k++) s -= C[r][k] * Dp[c][k];
+          C[r][c] = s * inv[i0 - ND + c];
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < ND; r++) {
+#pragma unroll
+      for (int c = 0; c <= r; c++) {
+        double s = hd[r * ND + c] + (r == c ? lambda : 0.0);
+        if (b > 0) {
+#pragma unroll
+          for (int k = 0; k < ND; k++) s -= C[r][k] * C[c][k];
+        }
+#pragma unroll
+        for (int k = 0; k < c; k++) s -= Dg[r][k] * Dg[c][k];
+        if (r == c) {
+          if (!(s > 0.0)) return -1;
+          const double d = sqrt(s);
+          Dg[r][r] = d;
+          inv[i0 + r] = 1.0 / d;
+        } else {
+          Dg[r][c] = s * inv[i0 + c];
+        }
+      }
+    }
+    // store row i0 + r as [block b-1 columns | block b columns] (2 * ND entries)
+#pragma unroll
+    for (int r = 0; r < ND; r++) {
+      double* row = L + (i0 + r) * 2 * ND;
+#pragma unroll
+      for (int c = 0; c < ND; c++) {
+        row[c] = b > 0 ? C[r][c] : 0.0;
+        row[ND + c] = c <= r ? Dg[r][c] : 0.0;
+        Dp[r][c] = c <= r ? Dg[r][c] : 0.0;
       }
     }
   }
   return 0;
 }
 
+// L y = b by block rows (ascending k per entry, as the dense forward substitution).
 template <int ND>
 __device__ void band_forward(const Band<ND>& B, const double* L, const double* inv, const double* b, double* y) {
-  for (int i = 0; i < B.P; i++) {
-    double s = b[i];
-    for (int k = kstart(B, i); k < i; k++) s -= lval(B, L, i, k) * y[k];
-    y[i] = s * inv[i];
+  for (int blk = 0; blk < B.nD; blk++) {
+    const int i0 = blk * ND;
+#pragma unroll
+    for (int r = 0; r < ND; r++) {
+      const double* row = L + (i0 + r) * 2 * ND;
+      double s = b[i0 + r];
+      if (blk > 0) {
+#pragma unroll
+        for (int k = 0; k < ND; k++) s -= row[k] * y[i0 - ND + k];
+      }
+#pragma unroll
+      for (int k = 0; k < r; k++) s -= row[ND + k] * y[i0 + k];
+      y[i0 + r] = s * inv[i0 + r];
+    }
   }
 }
 
+// L^T x = y by block rows from the end (ascending k per entry, as the dense back substitution).
 template <int ND>
 __device__ void band_backward(const Band<ND>& B, const double* L, const double* inv, const double* y, double* x) {
-  for (int i = B.P - 1; i >= 0; i--) {
-    double s = y[i];
-    int kend = (i / B.nd + 2) * B.nd;
-    if (kend > B.P) kend = B.P;
-    for (int k = i + 1; k < kend; k++) s -= lval(B, L, k, i) * x[k];
-    x[i] = s * inv[i];
+  for (int blk = B.nD - 1; blk >= 0; blk--) {
+    const int i0 = blk * ND;
+#pragma unroll
+    for (int r = ND - 1; r >= 0; r--) {
+      double s = y[i0 + r];
+#pragma unroll
+      for (int k = r + 1; k < ND; k++) s -= L[(i0 + k) * 2 * ND + ND + r] * x[i0 + k];
+      if (blk + 1 < B.nD) {
+#pragma unroll
+        for (int k = 0; k < ND; k++) s -= L[(i0 + ND + k) * 2 * ND + r] * x[i0 + ND + k];
+      }
+      x[i0 + r] = s * inv[i0 + r];
+    }
   }
 }
 
@@ -110,7 +157,6 @@ __device__ double norm2(int n, const double* v) {
   return sqrt(s);
 }
 
-// Returns 1 when the step lies on the trust-region boundary. work: P*(2*nd) + 3*P doubles.
 template <int ND>
 __device__ int subproblem(const Band<ND>& B, const double* g, double radius, double eps, int max_iter, double* p,
                           double* work) {
