@@ -199,7 +199,7 @@ def run_ours(args, rank, world, local):
     nz, ny, nx = acq.reference.shape
     line, il, ifr = acq.scan
     scan = fa.scan_params(line, il, ifr, nx, ny, nz)
-    ctx = fa.Context(device=local)
+    ctx = fa.Context(device=local, autotune=True)
     al = fa.Aligner(ctx, nD=acq.nD, precision=fa.PREC_MIXED, max_iterations=100)
     al.set_reference(acq.reference, scan)
     raw_u16 = np.ascontiguousarray(acq.frames.astype(np.uint16))
@@ -264,6 +264,7 @@ def run_ours(args, rank, world, local):
     if rank == 0:
         # roofline of the fused evaluation kernel: algorithmic bytes per launch / event-timed duration
         ref_m = fa.Reference(ctx, acq.reference + 1, acq.nD, scan, fa.PREC_MIXED)
+        tile_voxels, ctas_per_sm = ref_m.tuning()
         frs = [fa.Frame(ref_m, (acq.frames[k] + 1).astype(np.float16)) for k in range(n)]
         ms = fa.profile_eval(frs, acq.D_true[0], 20)
         # Unique bytes one launch needs: each FP16 frame once, plus the BF16 reference and three
@@ -281,6 +282,7 @@ def run_ours(args, rank, world, local):
                     "traffic": traffic, "kernel": "eval_kernel<3, half, bf16> (fused warp+error+J^T e)",
                     "algorithmic_bytes_per_launch": algo_bytes, "ms_per_launch": ms,
                     "bytes_per_unit": "2 B per voxel per frame + 8 B per voxel of the shared reference",
+                    "tuning": {"tile_voxels": tile_voxels, "ctas_per_sm": ctas_per_sm},
                     "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind if peak_kind == "measured" else "fallback 6.65 TB/s"}
         for f in frs:
             f.close()

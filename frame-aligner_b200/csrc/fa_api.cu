@@ -3,6 +3,8 @@
 // single-frame and batched trust-region drivers, and the phase correlator.
 #include <cufft.h>
 
+#include <map>
+
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -49,6 +51,7 @@ struct Alloc {
 
 struct fa_context {
   int device = 0;
+  int autotune = 0;
   size_t budget = 0;
   std::atomic<size_t> used{0};
   std::mutex mu;
@@ -112,6 +115,7 @@ struct Geometry {
   std::vector<int> begin, end;        // storage D_range
   std::vector<RowDesc> rows;
   float dq;
+  long long lmin;
   int tile_rows, n_tiles;
   std::vector<int> tile_c0;
   std::vector<int2> ctrl_tiles;
@@ -134,6 +138,24 @@ struct ScanEval {
     return (int)ip;
   }
 };
+
+// Tiles of whole rows, about target_tile_voxels each, never longer than the shortest storage range
+// (so a tile meets at most two ranges); per tile its first range, per control point its tile span.
+void assign_tiles(Geometry& G, int target_tile_voxels) {
+  const int nx = G.nx, nD = G.nD;
+  int tr = std::max(1, target_tile_voxels / nx);
+  tr = (int)std::min<long long>(tr, std::max<long long>(1, G.lmin / nx));
+  G.tile_rows = tr;
+  G.n_tiles = (G.n_rows + tr - 1) / tr;
+  G.tile_c0.resize(G.n_tiles);
+  for (int t = 0; t < G.n_tiles; t++) G.tile_c0[t] = G.rows[(size_t)t * tr].r0;
+  G.ctrl_tiles.resize(nD);
+  for (int c = 0; c < nD; c++) {
+    int a = (int)(std::lower_bound(G.tile_c0.begin(), G.tile_c0.end(), c - 2) - G.tile_c0.begin());
+    int b = (int)(std::upper_bound(G.tile_c0.begin(), G.tile_c0.end(), c) - G.tile_c0.begin());
+    G.ctrl_tiles[c] = make_int2(a, b);
+  }
+}
 
 fa_status build_geometry(const fa_scan_params& scan, int nz, int ny, int nx, int nD, int target_tile_voxels,
                          Geometry& G) {
@@ -217,18 +239,8 @@ fa_status build_geometry(const fa_scan_params& scan, int nz, int ny, int nx, int
     if (e >= s0 && e < s0 + nx) d.xlast = (int)(e - s0);
     G.rows[row] = d;
   }
-  int tr = std::max(1, target_tile_voxels / nx);
-  tr = (int)std::min<long long>(tr, std::max<long long>(1, lmin / nx));
-  G.tile_rows = tr;
-  G.n_tiles = (G.n_rows + tr - 1) / tr;
-  G.tile_c0.resize(G.n_tiles);
-  for (int t = 0; t < G.n_tiles; t++) G.tile_c0[t] = G.rows[(size_t)t * tr].r0;
-  G.ctrl_tiles.resize(nD);
-  for (int c = 0; c < nD; c++) {
-    int a = (int)(std::lower_bound(G.tile_c0.begin(), G.tile_c0.end(), c - 2) - G.tile_c0.begin());
-    int b = (int)(std::upper_bound(G.tile_c0.begin(), G.tile_c0.end(), c) - G.tile_c0.begin());
-    G.ctrl_tiles[c] = make_int2(a, b);
-  }
+  G.lmin = lmin;
+  assign_tiles(G, target_tile_voxels);
   return FA_OK;
 }
 
@@ -262,6 +274,8 @@ struct fa_reference {
   fa_precision prec = FA_PREC_F32;
   fa_scan_params scan{};
   Geometry G;
+  int* tile_c0_dev = nullptr;
+  int2* ctrl_dev = nullptr;
   std::vector<double> hd, hl;  // host copies of the Hessian blocks (diagonal, sub-diagonal)
   RefDev host{};
   RefDev* dev = nullptr;
@@ -373,6 +387,7 @@ extern "C" fa_status fa_create(const fa_config* cfg, fa_context** out) {
   fa_context* c = new fa_context;
   c->device = dev;
   c->budget = (cfg && cfg->memory_budget) ? cfg->memory_budget : (size_t)(0.9 * (double)free_b);
+  c->autotune = cfg ? cfg->autotune : 0;
   *out = c;
   return FA_OK;
 }
@@ -404,6 +419,139 @@ extern "C" fa_status fa_scan_params_init(double line_duration, double interline_
 
 namespace {
 
+// Re-tiles a reference for a new target tile size and uploads the tables and RefDev.
+fa_status retile(fa_reference* R, int target_tile_voxels) {
+  assign_tiles(R->G, target_tile_voxels);
+  R->host.tile_rows = R->G.tile_rows;
+  R->host.n_tiles = R->G.n_tiles;
+  cudaStream_t s = R->stream;
+  FA_CU(cudaMemcpyAsync(R->tile_c0_dev, R->G.tile_c0.data(), R->G.tile_c0.size() * sizeof(int),
+                        cudaMemcpyHostToDevice, s));
+  FA_CU(cudaMemcpyAsync(R->ctrl_dev, R->G.ctrl_tiles.data(), R->G.ctrl_tiles.size() * sizeof(int2),
+                        cudaMemcpyHostToDevice, s));
+  FA_CU(cudaMemcpyAsync(R->dev, &R->host, sizeof(RefDev), cudaMemcpyHostToDevice, s));
+  FA_CU(cudaStreamSynchronize(s));
+  return FA_OK;
+}
+
+struct TuneResult {
+  int target, mb, grid_mult;
+  double ms;
+};
+std::mutex g_tune_mu;
+std::map<std::string, TuneResult> g_tune_cache;
+
+// The project's autotuner for the fused pass: times each (tile size, CTAs per SM) candidate on a
+// batch of 8 synthetic frames (the reference itself, slightly displaced) with the persistent kernel
+// the batched solver uses, keeps the fastest, and caches the choice per volume shape, control-point
+// count and precision for the life of the process.
+fa_status autotune(fa_reference* R) {
+  char keyb[128];
+  std::snprintf(keyb, sizeof(keyb), "%d,%d,%d,%d,%d,%d", R->nz, R->ny, R->nx, R->nD, (int)R->prec,
+                R->scan.bidirectional);
+  const std::string key(keyb);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      R->host.tune_mb = it->second.mb;
+      R->host.tune_grid_mult = it->second.grid_mult;
+      return retile(R, it->second.target);
+    }
+  }
+  fa_context* ctx = R->ctx;
+  const int K = 8;
+  const long long N = R->N;
+  const int kind = R->prec == FA_PREC_MIXED ? fa::kFrameF16 : fa::kFrameF32;
+  std::vector<Alloc> tmp;
+  auto done = [&](fa_status st) {
+    std::string keep = g_err;
+    cudaStreamSynchronize(R->stream);
+    dfree_all(ctx, tmp);
+    g_err = keep;
+    return st;
+  };
+  void* frame;
+  float4* dp;
+  double* parts;
+  Job* jobs_dev;
+  int *list, *cnt;
+  fa_status st = dalloc(ctx, (size_t)N * (kind == fa::kFrameF16 ? 2 : 4), &frame, tmp);
+  if (st == FA_OK) st = dalloc_t(ctx, (size_t)R->nD * fa::kDParamF4, &dp, tmp);
+  if (st == FA_OK) st = dalloc_t(ctx, (size_t)K * R->G.n_rows * fa::kPartialDoubles, &parts, tmp);
+  if (st == FA_OK) st = dalloc_t(ctx, (size_t)K, &jobs_dev, tmp);
+  if (st == FA_OK) st = dalloc_t(ctx, (size_t)K, &list, tmp);
+  if (st == FA_OK) st = dalloc_t(ctx, 1, &cnt, tmp);
+  if (st != FA_OK) return done(st);
+  cudaStream_t s = R->stream;
+  cudaError_t e = fa::launch_convert(R->host.ref32, FA_F32, frame, kind == fa::kFrameF16 ? FA_F16 : FA_F32, N, s);
+  std::vector<double> D((size_t)R->nD * 3);
+  for (int k = 0; k < R->nD; k++) {
+    D[3 * k] = 0.3 + 0.01 * k;
+    D[3 * k + 1] = -0.2;
+    D[3 * k + 2] = R->n_dim == 3 ? 0.1 : 0.0;
+  }
+  std::vector<float4> hdp((size_t)R->nD * fa::kDParamF4);
+  make_dparams(D.data(), R->nD, R->n_dim, hdp.data());
+  std::vector<Job> jobs(K);
+  std::vector<int> all(K);
+  for (int i = 0; i < K; i++) {
+    Job j{};
+    j.ref = R->dev;
+    j.frame = frame;
+    j.dparams = dp;
+    j.partials = parts + (size_t)i * R->G.n_rows * fa::kPartialDoubles;
+    jobs[i] = j;
+    all[i] = i;
+  }
+  const int kcount = K;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dp, hdp.data(), hdp.size() * sizeof(float4), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(jobs_dev, jobs.data(), K * sizeof(Job), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(list, all.data(), K * sizeof(int), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(cnt, &kcount, sizeof(int), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return done(fail(FA_ERR_CUDA, std::string("autotune set-up: ") + cudaGetErrorString(e)));
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  TuneResult best{8192, 2, 2, 1e30};
+  const int targets[] = {2048, 4096, 8192, 16384, 32768};
+  const int mbs[] = {2, 3, 4};
+  for (int target : targets) {
+    if (retile(R, target) != FA_OK) break;
+    for (int mb : mbs) {
+      const bool mixed = R->prec == FA_PREC_MIXED;
+      auto launch = [&]() {
+        return fa::launch_eval4_active(jobs_dev, list, cnt, K, R->G.n_tiles, R->n_dim, kind, mixed, mb, mb * sms, s);
+      };
+      e = launch();
+      if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+      for (int r = 0; r < 3 && e == cudaSuccess; r++) e = launch();
+      if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+      float ms = 0;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+      g_launches += 4;
+      if (e != cudaSuccess) break;
+      if (ms < best.ms) best = TuneResult{target, mb, mb, ms};
+    }
+    if (e != cudaSuccess) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e != cudaSuccess) return done(fail(FA_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e)));
+  R->host.tune_mb = best.mb;
+  R->host.tune_grid_mult = best.grid_mult;
+  fa_status r = retile(R, best.target);
+  if (r == FA_OK) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = best;
+  }
+  return done(r);
+}
+
 fa_status reference_setup(fa_reference* R, const float* src, bool src_device) {
   fa_context* ctx = R->ctx;
   Geometry& G = R->G;
@@ -422,13 +570,15 @@ fa_status reference_setup(fa_reference* R, const float* src, bool src_device) {
   h.tile_rows = G.tile_rows;
   h.n_tiles = G.n_tiles;
   h.P = R->P;
+  h.tune_mb = 2;
+  h.tune_grid_mult = 2;
   RowDesc* rows;
   int* tile_c0;
   int2* ctrl;
   float *ref32, *gx, *gy, *gz;
   double *Hd, *Hl, *tparts, *scan_dev;
   FA_TRY(dalloc_t(ctx, G.rows.size(), &rows, R->allocs));
-  FA_TRY(dalloc_t(ctx, G.tile_c0.size(), &tile_c0, R->allocs));
+  FA_TRY(dalloc_t(ctx, (size_t)G.n_rows, &tile_c0, R->allocs));  // room for any tile size
   FA_TRY(dalloc_t(ctx, G.ctrl_tiles.size(), &ctrl, R->allocs));
   FA_TRY(dalloc_t(ctx, (size_t)N, &ref32, R->allocs));
   FA_TRY(dalloc_t(ctx, (size_t)N, &gx, R->allocs));
@@ -441,6 +591,8 @@ fa_status reference_setup(fa_reference* R, const float* src, bool src_device) {
   FA_TRY(dalloc_t(ctx, 1, &R->dev, R->allocs));
   std::vector<Alloc> tmp;
   fa_status st = dalloc_t(ctx, (size_t)G.n_tiles * 2 * 21, &tparts, tmp);
+  R->tile_c0_dev = tile_c0;
+  R->ctrl_dev = ctrl;
   if (st != FA_OK) return st;
   cudaStream_t s = R->stream;
   FA_CU(cudaMemcpyAsync(rows, G.rows.data(), G.rows.size() * sizeof(RowDesc), cudaMemcpyHostToDevice, s));
@@ -482,6 +634,7 @@ fa_status reference_setup(fa_reference* R, const float* src, bool src_device) {
   FA_CU(cudaMemcpyAsync(R->hl.data(), Hl, R->hl.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
   FA_CU(cudaStreamSynchronize(s));
   dfree_all(ctx, tmp);
+  if (ctx->autotune && R->nx % 4 == 0) FA_TRY(autotune(R));
   return FA_OK;
 }
 
@@ -536,6 +689,22 @@ extern "C" fa_status fa_reference_destroy(fa_reference* R) {
   dfree_all(R->ctx, R->allocs);
   delete R;
   return FA_OK;
+}
+
+extern "C" fa_status fa_reference_tuning(const fa_reference* R, int* tile_voxels, int* ctas_per_sm) {
+  if (!R) return fail(FA_ERR_BAD_ARG, "ref is NULL");
+  if (tile_voxels) *tile_voxels = R->G.tile_rows * R->nx;
+  if (ctas_per_sm) *ctas_per_sm = R->host.tune_mb;
+  return FA_OK;
+}
+
+extern "C" fa_status fa_reference_retune(fa_reference* R, int tile_voxels, int ctas_per_sm) {
+  if (!R || tile_voxels < 1 || ctas_per_sm < 2 || ctas_per_sm > 4) return fail(FA_ERR_BAD_ARG, "bad arguments");
+  if (R->n_frames.load() != 0) return fail(FA_ERR_STATE, "frames of this reference are registered");
+  FA_CU(cudaSetDevice(R->ctx->device));
+  R->host.tune_mb = ctas_per_sm;
+  R->host.tune_grid_mult = ctas_per_sm;
+  return retile(R, tile_voxels);
 }
 
 extern "C" fa_status fa_reference_info(const fa_reference* R, int* n_dim, int* n_params) {
@@ -734,7 +903,7 @@ fa_status evaluate(fa_frame* F, const double* D) {
   const size_t np = (size_t)R->nD * fa::kDParamF4 * sizeof(float4);
   FA_CU(cudaMemcpyAsync(F->job.dparams, F->h_dparams, np, cudaMemcpyHostToDevice, F->stream));
   FA_CU(fa::launch_eval(F->job_dev, 1, R->G.n_tiles, R->n_dim, F->kind, R->prec == FA_PREC_MIXED, F->stream,
-                          R->nx % 4 == 0));
+                          R->nx % 4 == 0, R->host.tune_mb));
   FA_CU(fa::launch_reduce(F->job_dev, R->host, F->stream));
   g_launches += 2;
   FA_CU(cudaMemcpyAsync(F->h_result, F->job.result, (1 + R->P) * sizeof(double), cudaMemcpyDeviceToHost, F->stream));
@@ -847,7 +1016,7 @@ extern "C" fa_status fa_align_frame(fa_frame* F, const double* rigid_shift, int 
   int phase = fa::kPhaseStartZero;
   for (int step = 0; step < max_steps && phase != fa::kPhaseDone; step++) {
     FA_CU(fa::launch_eval(F->job_dev, 1, R->G.n_tiles, R->n_dim, F->kind, R->prec == FA_PREC_MIXED, F->stream,
-                          R->nx % 4 == 0));
+                          R->nx % 4 == 0, R->host.tune_mb));
     FA_CU(fa::launch_solve(F->job_dev, 1, R->nD, R->n_dim, F->stream));
     g_launches += 2;
     FA_CU(cudaMemcpyAsync(&F->h_state->phase, &F->state->phase, sizeof(int), cudaMemcpyDeviceToHost, F->stream));
@@ -975,7 +1144,7 @@ fa_status align_batch_impl(fa_frame* const* frames, int n, const double* rigid_s
     for (int it = 0; it < kGraphIters && e == cudaSuccess; it++) {
       if (vec4)
         e = fa::launch_eval4_active(jobs_dev, d_list, d_active, n, max_tiles, R0->n_dim, frames[0]->kind,
-                                    R0->prec == FA_PREC_MIXED, 2 * sms, s);
+                                    R0->prec == FA_PREC_MIXED, R0->host.tune_mb, R0->host.tune_grid_mult * sms, s);
       else
         e = fa::launch_eval(jobs_dev, n, max_tiles, R0->n_dim, frames[0]->kind, R0->prec == FA_PREC_MIXED, s, false);
       if (e == cudaSuccess) e = fa::launch_solve(jobs_dev, n, max_nD, R0->n_dim, s);
@@ -1545,10 +1714,10 @@ extern "C" fa_status fa_profile_eval(fa_frame* const* frames, int n, const doubl
   // one untimed launch, then the timed ones
   const bool v4 = R->nx % 4 == 0;
   if (e == cudaSuccess)
-    e = fa::launch_eval(jd, n, R->G.n_tiles, R->n_dim, frames[0]->kind, R->prec == FA_PREC_MIXED, s, v4);
+    e = fa::launch_eval(jd, n, R->G.n_tiles, R->n_dim, frames[0]->kind, R->prec == FA_PREC_MIXED, s, v4, R->host.tune_mb);
   if (e == cudaSuccess) e = cudaEventRecord(e0, s);
   for (int l = 0; l < launches && e == cudaSuccess; l++)
-    e = fa::launch_eval(jd, n, R->G.n_tiles, R->n_dim, frames[0]->kind, R->prec == FA_PREC_MIXED, s, v4);
+    e = fa::launch_eval(jd, n, R->G.n_tiles, R->n_dim, frames[0]->kind, R->prec == FA_PREC_MIXED, s, v4, R->host.tune_mb);
   if (e == cudaSuccess) e = cudaEventRecord(e1, s);
   if (e == cudaSuccess) e = cudaEventSynchronize(e1);
   float ms = 0;

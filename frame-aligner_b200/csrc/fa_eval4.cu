@@ -13,6 +13,8 @@
 // instead of eight gathers per voxel; the reference and gradient planes are read with one vector
 // load per plane. Lanes whose four voxels straddle an interval boundary, a range end, a change of
 // the integer offset or the volume edge take the per-voxel path.
+#include <type_traits>
+
 #include "fa_device.cuh"
 
 namespace fa {
@@ -335,8 +337,8 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
   }
 }
 
-template <int NDIM, typename FT, typename RT>
-__global__ void __launch_bounds__(kEvalThreads, 2) eval4_kernel(const Job* __restrict__ jobs) {
+template <int NDIM, typename FT, typename RT, int MB>
+__global__ void __launch_bounds__(kEvalThreads, MB) eval4_kernel(const Job* __restrict__ jobs) {
   const Job& job = jobs[blockIdx.y];
   if (job.state != nullptr && job.state->phase == kPhaseDone) return;
   const RefDev& R = *job.ref;
@@ -347,8 +349,8 @@ __global__ void __launch_bounds__(kEvalThreads, 2) eval4_kernel(const Job* __res
 
 // Persistent form for batched solves: a fixed grid walks the (active frame, tile) items of the
 // compacted active list, so frames that have converged cost nothing.
-template <int NDIM, typename FT, typename RT>
-__global__ void __launch_bounds__(kEvalThreads, 2) eval4_active_kernel(const Job* __restrict__ jobs,
+template <int NDIM, typename FT, typename RT, int MB>
+__global__ void __launch_bounds__(kEvalThreads, MB) eval4_active_kernel(const Job* __restrict__ jobs,
                                                                      const int* __restrict__ active,
                                                                      const int* __restrict__ n_active, int max_tiles) {
   const long long n_items = (long long)(*n_active) * max_tiles;
@@ -363,25 +365,36 @@ __global__ void __launch_bounds__(kEvalThreads, 2) eval4_active_kernel(const Job
   }
 }
 
+template <typename Fn>
+inline cudaError_t dispatch_mb(int mb, Fn&& f) {
+  if (mb >= 4) return f(std::integral_constant<int, 4>{});
+  if (mb == 3) return f(std::integral_constant<int, 3>{});
+  return f(std::integral_constant<int, 2>{});
+}
+
 cudaError_t launch_eval4(const Job* jobs_dev, int n_jobs, int max_tiles, int n_dim, int frame_kind, bool ref_bf16,
-                         cudaStream_t s) {
+                         int mb, cudaStream_t s) {
   const dim3 grid(max_tiles, n_jobs);
   return dispatch_cfg(n_dim, frame_kind, ref_bf16, [&](auto c) {
     using C = decltype(c);
-    eval4_kernel<C::nd, typename C::F, typename C::R><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
-    return cudaGetLastError();
+    return dispatch_mb(mb, [&](auto m) {
+      eval4_kernel<C::nd, typename C::F, typename C::R, decltype(m)::value><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
+      return cudaGetLastError();
+    });
   });
 }
 
 cudaError_t launch_eval4_active(const Job* jobs_dev, const int* active, const int* n_active, int n_jobs, int max_tiles,
-                                int n_dim, int frame_kind, bool ref_bf16, int grid, cudaStream_t s) {
+                                int n_dim, int frame_kind, bool ref_bf16, int mb, int grid, cudaStream_t s) {
   const long long most = (long long)n_jobs * max_tiles;
   const int g = (int)(most < grid ? most : grid);
   return dispatch_cfg(n_dim, frame_kind, ref_bf16, [&](auto c) {
     using C = decltype(c);
-    eval4_active_kernel<C::nd, typename C::F, typename C::R><<<g, kEvalThreads, 0, s>>>(jobs_dev, active, n_active,
-                                                                                      max_tiles);
-    return cudaGetLastError();
+    return dispatch_mb(mb, [&](auto m) {
+      eval4_active_kernel<C::nd, typename C::F, typename C::R, decltype(m)::value>
+          <<<g, kEvalThreads, 0, s>>>(jobs_dev, active, n_active, max_tiles);
+      return cudaGetLastError();
+    });
   });
 }
 

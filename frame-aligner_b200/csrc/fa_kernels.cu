@@ -284,11 +284,11 @@ __global__ void __launch_bounds__(kEvalThreads) eval_kernel(const Job* __restric
 }
 
 cudaError_t launch_eval4(const Job* jobs_dev, int n_jobs, int max_tiles, int n_dim, int frame_kind, bool ref_bf16,
-                         cudaStream_t s);
+                         int mb, cudaStream_t s);
 
 cudaError_t launch_eval(const Job* jobs_dev, int n_jobs, int max_tiles, int n_dim, int frame_kind, bool ref_bf16,
-                        cudaStream_t s, bool rows_multiple_of_4) {
-  if (rows_multiple_of_4) return launch_eval4(jobs_dev, n_jobs, max_tiles, n_dim, frame_kind, ref_bf16, s);
+                        cudaStream_t s, bool rows_multiple_of_4, int mb) {
+  if (rows_multiple_of_4) return launch_eval4(jobs_dev, n_jobs, max_tiles, n_dim, frame_kind, ref_bf16, mb, s);
   const dim3 grid(max_tiles, n_jobs);
   return dispatch_cfg(n_dim, frame_kind, ref_bf16, [&](auto c) {
     using C = decltype(c);

@@ -34,12 +34,12 @@ cudaError_t launch_downsample(const void* in, fa_dtype in_type, int nz, int ny, 
 // FrameKind, ref_bf16 selects the BF16 reference/gradient copies, rows_multiple_of_4 the
 // four-voxels-per-lane kernel (every job's nx % 4 == 0).
 cudaError_t launch_eval(const Job* jobs_dev, int n_jobs, int max_tiles, int n_dim, int frame_kind, bool ref_bf16,
-                        cudaStream_t s, bool rows_multiple_of_4);
+                        cudaStream_t s, bool rows_multiple_of_4, int mb = 2);
 
 // Persistent fused pass over the compacted active list: grid CTAs walk the (active[a], tile) items
 // for a < *n_active (rows must be multiples of 4).
 cudaError_t launch_eval4_active(const Job* jobs_dev, const int* active, const int* n_active, int n_jobs, int max_tiles,
-                                int n_dim, int frame_kind, bool ref_bf16, int grid, cudaStream_t s);
+                                int n_dim, int frame_kind, bool ref_bf16, int mb, int grid, cudaStream_t s);
 
 // Reduces one job's tile partials into result = [f, g(P)] (deterministic order).
 cudaError_t launch_reduce(const Job* job_dev, const RefDev& ref_host, cudaStream_t s);

@@ -54,7 +54,7 @@ class ScanParams(C.Structure):
 
 
 class Config(C.Structure):
-    _fields_ = [("device", C.c_int), ("memory_budget", C.c_size_t)]
+    _fields_ = [("device", C.c_int), ("memory_budget", C.c_size_t), ("autotune", C.c_int)]
 
 
 class AlignerParams(C.Structure):
@@ -104,6 +104,8 @@ SIGNATURES = {
                                 C.POINTER(_vp)],
     "fa_reference_destroy": [_vp],
     "fa_reference_info": [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)],
+    "fa_reference_tuning": [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)],
+    "fa_reference_retune": [_vp, C.c_int, C.c_int],
     "fa_get_hessian": [_vp, _f64p],
     "fa_get_gradient": [_vp, _vp, _vp, _vp],
     "fa_get_ranges": [_vp, _i32p],
@@ -177,9 +179,9 @@ def _c64(a):
 
 
 class Context:
-    def __init__(self, device=0, memory_budget=0):
+    def __init__(self, device=0, memory_budget=0, autotune=False):
         self._h = _vp()
-        cfg = Config(device, memory_budget)
+        cfg = Config(device, memory_budget, int(autotune))
         check(lib().fa_create(C.byref(cfg), C.byref(self._h)))
 
     def close(self):
@@ -229,6 +231,14 @@ class Reference:
         g = [np.empty(self.dims, np.float32) for _ in range(3)]
         check(lib().fa_get_gradient(self._h, *[x.ctypes.data for x in g]))
         return g
+
+    def tuning(self):
+        t, m = C.c_int(), C.c_int()
+        check(lib().fa_reference_tuning(self._h, C.byref(t), C.byref(m)))
+        return t.value, m.value
+
+    def retune(self, tile_voxels, ctas_per_sm):
+        check(lib().fa_reference_retune(self._h, tile_voxels, ctas_per_sm))
 
     def ranges(self):
         r = np.empty(2 * self.nD, np.int32)

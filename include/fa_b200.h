@@ -64,6 +64,8 @@ typedef struct fa_correlator fa_correlator;
 typedef struct {
   int device;            /* CUDA device ordinal */
   size_t memory_budget;  /* bytes of device memory the context may hold; 0 = 90% of free memory */
+  int autotune;          /* 1: fa_set_reference times the fused pass's tile shapes on the device and keeps
+                            the fastest (cached per volume shape for the process); 0: fixed defaults */
 } fa_config;
 
 /* Storage precision of a reference's device copies (the FP32 copy always exists: the Gauss-Newton
@@ -107,6 +109,12 @@ fa_status fa_set_reference_device(fa_context* ctx, const float* reference_device
 fa_status fa_reference_destroy(fa_reference* ref);
 /* n_dim (2 or 3, FrameWarper.cpp:198) and the parameter count P = nD * n_dim. */
 fa_status fa_reference_info(const fa_reference* ref, int* n_dim, int* n_params);
+/* Tile shape of the fused pass (voxels per tile, CTAs per SM its register budget targets), as chosen
+   by the autotuner or set by fa_reference_retune. No counterpart in the reference. */
+fa_status fa_reference_tuning(const fa_reference* ref, int* tile_voxels, int* ctas_per_sm);
+/* Forces a tile shape (tile_voxels rounded down to whole image rows and capped by the shortest
+   control interval; ctas_per_sm in 2..4). Only while no frame of the reference is registered. */
+fa_status fa_reference_retune(fa_reference* ref, int tile_voxels, int ctas_per_sm);
 /* The member H read by OptimisationModel (OptimisationModel.cpp:61): dense P x P, row-major,
    host memory. */
 fa_status fa_get_hessian(const fa_reference* ref, double* H);

@@ -227,3 +227,39 @@ def test_aligner_raw_frames_against_oracle(ctx, precision):
         shift = O.phase_shift(acq.reference, acq.frames[k])
         D_cpu, _ = ow.align_frame(acq.frames[k] + 1, shift, 100)
         assert _rms(D_host[k], D_cpu, 2) <= 0.01, (k, _rms(D_host[k], D_cpu, 2))
+
+
+def test_tile_shapes_agree(ctx):
+    """Every tile shape the autotuner may pick gives the same f and J^T e (the partial sums only
+    change grouping): relative 1e-6 for f, 1e-5 of max|J^T e|."""
+    acq = _acq((4, 64, 128), 13, 1, 17)
+    nz, ny, nx = acq.reference.shape
+    line, il, ifr = acq.scan
+    D = acq.D_true[0]
+    results = []
+    for tile, mb in [(512, 2), (2048, 3), (8192, 4), (32768, 2)]:
+        ref = fa.Reference(ctx, acq.reference + 1, 13, fa.scan_params(line, il, ifr, nx, ny, nz), fa.PREC_MIXED)
+        ref.retune(tile, mb)
+        fr = fa.Frame(ref, acq.frames[0] + 1)
+        results.append((fr.get_error(D), fr.get_jacobian(D), fr.align(None, 100)[0]))
+        fr.close()
+    f0, j0, d0 = results[0]
+    for f, j, d in results[1:]:
+        assert abs(f - f0) <= 1e-6 * f0
+        assert np.max(np.abs(j - j0)) <= 1e-5 * np.max(np.abs(j0))
+        assert _rms(d, d0, 3) <= 0.01
+
+
+def test_autotuned_context(ctx):
+    tuned = fa.Context(autotune=True)
+    acq = _acq((2, 64, 128), 9, 1, 18)
+    nz, ny, nx = acq.reference.shape
+    line, il, ifr = acq.scan
+    ref = fa.Reference(tuned, acq.reference + 1, 9, fa.scan_params(line, il, ifr, nx, ny, nz), fa.PREC_MIXED)
+    tile, mb = ref.tuning()
+    assert tile % nx == 0 and 2 <= mb <= 4
+    fr = fa.Frame(ref, acq.frames[0] + 1)
+    ref_plain = fa.Reference(ctx, acq.reference + 1, 9, fa.scan_params(line, il, ifr, nx, ny, nz), fa.PREC_MIXED)
+    fr_plain = fa.Frame(ref_plain, acq.frames[0] + 1)
+    f1, f2 = fr.get_error(acq.D_true[0]), fr_plain.get_error(acq.D_true[0])
+    assert abs(f1 - f2) <= 1e-6 * f2
