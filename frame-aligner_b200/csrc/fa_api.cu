@@ -461,7 +461,6 @@ fa_status autotune(fa_reference* R) {
   }
   fa_context* ctx = R->ctx;
   const int K = 8;
-  const long long N = R->N;
   const int kind = R->prec == FA_PREC_MIXED ? fa::kFrameF16 : fa::kFrameF32;
   std::vector<Alloc> tmp;
   auto done = [&](fa_status st) {
@@ -476,7 +475,12 @@ fa_status autotune(fa_reference* R) {
   double* parts;
   Job* jobs_dev;
   int *list, *cnt;
-  fa_status st = dalloc(ctx, (size_t)N * (kind == fa::kFrameF16 ? 2 : 4), &frame, tmp);
+  const int hz = R->nz > 1 ? fa::kHaloZ : 0;
+  const int pitch = R->nx + 2 * fa::kHaloX;
+  const long long plane = (long long)pitch * (R->ny + 2 * fa::kHaloY);
+  const size_t esz = kind == fa::kFrameF16 ? 2 : 4;
+  const size_t elems = (size_t)plane * (R->nz + 2 * hz);
+  fa_status st = dalloc(ctx, elems * esz, &frame, tmp);
   if (st == FA_OK) st = dalloc_t(ctx, (size_t)R->nD * fa::kDParamF4, &dp, tmp);
   if (st == FA_OK) st = dalloc_t(ctx, (size_t)K * R->G.n_rows * fa::kPartialDoubles, &parts, tmp);
   if (st == FA_OK) st = dalloc_t(ctx, (size_t)K, &jobs_dev, tmp);
@@ -484,7 +488,10 @@ fa_status autotune(fa_reference* R) {
   if (st == FA_OK) st = dalloc_t(ctx, 1, &cnt, tmp);
   if (st != FA_OK) return done(st);
   cudaStream_t s = R->stream;
-  cudaError_t e = fa::launch_convert(R->host.ref32, FA_F32, frame, kind == fa::kFrameF16 ? FA_F16 : FA_F32, N, s);
+  void* interior = static_cast<char*>(frame) + ((long long)hz * plane + (long long)fa::kHaloY * pitch + fa::kHaloX) * esz;
+  cudaError_t e = cudaMemsetAsync(frame, 0, elems * esz, s);
+  if (e == cudaSuccess)
+    e = fa::launch_to_slot(R->host.ref32, FA_F32, interior, kind, R->nz, R->ny, R->nx, pitch, plane, false, s);
   std::vector<double> D((size_t)R->nD * 3);
   for (int k = 0; k < R->nD; k++) {
     D[3 * k] = 0.3 + 0.01 * k;
@@ -498,7 +505,10 @@ fa_status autotune(fa_reference* R) {
   for (int i = 0; i < K; i++) {
     Job j{};
     j.ref = R->dev;
-    j.frame = frame;
+    j.frame = interior;
+    j.fplane = plane;
+    j.fpitch = pitch;
+    j.fpad = 1;
     j.dparams = dp;
     j.partials = parts + (size_t)i * R->G.n_rows * fa::kPartialDoubles;
     jobs[i] = j;
@@ -781,12 +791,23 @@ fa_status frame_alloc(fa_reference* R, int kind, fa_frame** out) {
   const size_t P = (size_t)R->P;
   fa_status st;
   void* data;
-  if ((st = dalloc(ctx, (size_t)R->N * (kind == fa::kFrameF32 ? 4 : 2), &data, F->allocs)) != FA_OK)
-    return cleanup(st);
-  F->data = data;
+  // Frame slot with a zero halo (kHaloX columns, kHaloY rows, kHaloZ planes on each side).
+  const int hz = R->nz > 1 ? fa::kHaloZ : 0;
+  const int pitch = R->nx + 2 * fa::kHaloX;
+  const long long plane = (long long)pitch * (R->ny + 2 * fa::kHaloY);
+  const size_t esz = kind == fa::kFrameF32 ? 4 : 2;
+  const size_t elems = (size_t)plane * (R->nz + 2 * hz);
+  if ((st = dalloc(ctx, elems * esz, &data, F->allocs)) != FA_OK) return cleanup(st);
+  if (cudaMemsetAsync(data, 0, elems * esz, F->stream) != cudaSuccess)
+    return cleanup(fail(FA_ERR_CUDA, "halo clear failed"));
+  const long long origin = (long long)hz * plane + (long long)fa::kHaloY * pitch + fa::kHaloX;
+  F->data = static_cast<char*>(data) + origin * esz;  // voxel (0, 0, 0)
   Job& j = F->job;
   j.ref = R->dev;
-  j.frame = data;
+  j.frame = F->data;
+  j.fplane = plane;
+  j.fpitch = pitch;
+  j.fpad = 1;
   if ((st = dalloc_t(ctx, (size_t)R->nD * fa::kDParamF4, &j.dparams, F->allocs)) != FA_OK) return cleanup(st);
   if ((st = dalloc_t(ctx, (size_t)R->G.n_tiles * fa::kPartialDoubles, &j.partials, F->allocs)) != FA_OK)
     return cleanup(st);
@@ -814,28 +835,29 @@ fa_status frame_alloc(fa_reference* R, int kind, fa_frame** out) {
   return FA_OK;
 }
 
+// Copies a dense frame (host or device, any dtype, values as stored: the +1 offset already applied)
+// into the slot's interior.
 fa_status frame_fill(fa_frame* F, const void* src, fa_dtype dtype, bool src_device) {
   fa_reference* R = F->ref;
   const long long N = R->N;
-  const fa_dtype store = F->kind == fa::kFrameF16 ? FA_F16 : FA_F32;
-  size_t esz = (dtype == FA_F32) ? 4 : 2;
-  if (dtype == store && !src_device) {
-    FA_CU(cudaMemcpyAsync(F->data, src, (size_t)N * esz, cudaMemcpyHostToDevice, F->stream));
-  } else if (dtype == store && src_device) {
-    FA_CU(cudaMemcpyAsync(F->data, src, (size_t)N * esz, cudaMemcpyDeviceToDevice, F->stream));
-  } else if (src_device) {
-    FA_CU(fa::launch_convert(src, dtype, F->data, store, N, F->stream));
-  } else {
-    std::vector<Alloc> tmp;
+  const size_t esz = (dtype == FA_F32) ? 4 : 2;
+  std::vector<Alloc> tmp;
+  const void* dense = src;
+  if (!src_device) {
     void* stage;
     FA_TRY(dalloc(R->ctx, (size_t)N * esz, &stage, tmp));
     cudaError_t e = cudaMemcpyAsync(stage, src, (size_t)N * esz, cudaMemcpyHostToDevice, F->stream);
-    if (e == cudaSuccess) e = fa::launch_convert(stage, dtype, F->data, store, N, F->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(F->stream);
-    dfree_all(R->ctx, tmp);
-    if (e != cudaSuccess) return fail(FA_ERR_CUDA, std::string("frame upload: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess) {
+      dfree_all(R->ctx, tmp);
+      return fail(FA_ERR_CUDA, std::string("frame upload: ") + cudaGetErrorString(e));
+    }
+    dense = stage;
   }
-  FA_CU(cudaStreamSynchronize(F->stream));
+  cudaError_t e = fa::launch_to_slot(dense, dtype, F->data, F->kind, R->nz, R->ny, R->nx, F->job.fpitch, F->job.fplane,
+                                     false, F->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(F->stream);
+  dfree_all(R->ctx, tmp);
+  if (e != cudaSuccess) return fail(FA_ERR_CUDA, std::string("frame upload: ") + cudaGetErrorString(e));
   F->have_last = false;
   return FA_OK;
 }
@@ -948,7 +970,8 @@ extern "C" fa_status fa_warp(fa_frame* F, const double* D, float invalid_value, 
   make_dparams(D, R->nD, R->n_dim, F->h_dparams);
   const size_t np = (size_t)R->nD * fa::kDParamF4 * sizeof(float4);
   FA_CU(cudaMemcpyAsync(F->job.dparams, F->h_dparams, np, cudaMemcpyHostToDevice, F->stream));
-  FA_CU(fa::launch_warp(R->dev, R->host, F->data, F->kind, F->job.dparams, invalid_value, F->warp_out, F->stream));
+  FA_CU(fa::launch_warp(R->dev, R->host, F->data, F->job.fplane, F->job.fpitch, F->kind, F->job.dparams, invalid_value,
+                        F->warp_out, F->stream));
   g_launches += 1;
   FA_CU(cudaMemcpyAsync(out, F->warp_out, (size_t)R->N * sizeof(float), cudaMemcpyDeviceToHost, F->stream));
   FA_CU(cudaStreamSynchronize(F->stream));
@@ -1333,7 +1356,7 @@ fa_status correlator_create_impl(fa_context* ctx, const void* reference, bool re
   if ((st = correlator_reserve(C, 1)) != FA_OK) return cleanup(st);
   C->h_ptrs[0] = C->vol;
   if (cudaMemcpyAsync(C->d_ptrs, C->h_ptrs, sizeof(void*), cudaMemcpyHostToDevice, C->stream) != cudaSuccess ||
-      fa::launch_phase_window(C->d_ptrs, fa::kFrameF32, C->wy, C->wx, ny, nx, C->n_el, 1, C->real, C->stream) !=
+      fa::launch_phase_window(C->d_ptrs, FA_F32, C->wy, C->wx, ny, nx, C->n_el, 1, C->real, C->stream) !=
           cudaSuccess)
     return cleanup(fail(FA_ERR_CUDA, "window kernel"));
   if (cufftExecD2Z(C->fwd1, C->real, reinterpret_cast<cufftDoubleComplex*>(C->spec)) != CUFFT_SUCCESS)
@@ -1375,7 +1398,7 @@ extern "C" fa_status fa_correlator_shift(fa_correlator* C, const float* volume, 
   FA_CU(cudaSetDevice(C->ctx->device));
   FA_CU(cudaMemcpyAsync(C->vol, volume, (size_t)C->n_el * sizeof(float), cudaMemcpyHostToDevice, C->stream));
   const void* v = C->vol;
-  FA_TRY(correlator_enqueue(C, &v, fa::kFrameF32, 1));
+  FA_TRY(correlator_enqueue(C, &v, FA_F32, 1));
   return correlator_read(C, 1, shift);
 }
 
@@ -1384,7 +1407,7 @@ extern "C" fa_status fa_correlator_shift_device(fa_correlator* C, const float* v
   std::lock_guard<std::mutex> lk(C->mu);
   FA_CU(cudaSetDevice(C->ctx->device));
   const void* v = volume_device;
-  FA_TRY(correlator_enqueue(C, &v, fa::kFrameF32, 1));
+  FA_TRY(correlator_enqueue(C, &v, FA_F32, 1));
   return correlator_read(C, 1, shift);
 }
 
@@ -1516,48 +1539,31 @@ fa_status aligner_run(fa_aligner* A, const void* const* frames, fa_dtype dtype, 
   const long long N = A->ref->N;
   const size_t raw_bytes = (size_t)N * dtype_size(dtype);
   const int kind = slot_kind_for(A, dtype);
-  // Raw uint16 slots take the frames as they are: from the host straight into the slot, from the
-  // device by pointer (no copy). Other storage needs a conversion pass, from a staging copy of host
-  // frames.
-  const bool direct = kind == fa::kFrameRawU16;
-  FA_TRY(aligner_grow(A, n, kind, (direct || device_src) ? 0 : (size_t)n * raw_bytes));
+  // Raw frames (host frames via a staging copy) go through the correlator as they are and into the
+  // slots with the +1 offset (count + 1 for uint16 slots).
+  FA_TRY(aligner_grow(A, n, kind, device_src ? 0 : (size_t)n * raw_bytes));
   cudaStream_t s = A->corr->stream;
   if (!A->ev0) {
     FA_CU(cudaEventCreate(&A->ev0));
     FA_CU(cudaEventCreate(&A->ev1));
   }
   FA_CU(cudaEventRecord(A->ev0, s));
-  std::vector<const void*> raw((size_t)n), data((size_t)n);
+  std::vector<const void*> raw((size_t)n);
   for (int i = 0; i < n; i++) {
     fa_frame* F = A->slots[i];
-    if (direct) {
-      // Zero-copy needs the vector loads' alignment (16 bytes); otherwise copy into the slot.
-      if (device_src && (reinterpret_cast<uintptr_t>(frames[i]) & 15u) == 0) {
-        raw[i] = frames[i];
-      } else if (device_src) {
-        FA_CU(cudaMemcpyAsync(F->data, frames[i], raw_bytes, cudaMemcpyDeviceToDevice, s));
-        raw[i] = F->data;
-      } else {
-        FA_CU(cudaMemcpyAsync(F->data, frames[i], raw_bytes, cudaMemcpyHostToDevice, s));
-        raw[i] = F->data;
-      }
-      data[i] = raw[i];
+    if (device_src) {
+      raw[i] = frames[i];
     } else {
-      if (device_src) {
-        raw[i] = frames[i];
-      } else {
-        void* dst = static_cast<char*>(A->staging) + (size_t)i * raw_bytes;
-        FA_CU(cudaMemcpyAsync(dst, frames[i], raw_bytes, cudaMemcpyHostToDevice, s));
-        raw[i] = dst;
-      }
-      FA_CU(fa::launch_offset_convert(raw[i], dtype, F->data, kind == fa::kFrameF16 ? FA_F16 : FA_F32, N, s));
-      g_launches += 1;
-      data[i] = F->data;
+      void* dst = static_cast<char*>(A->staging) + (size_t)i * raw_bytes;
+      FA_CU(cudaMemcpyAsync(dst, frames[i], raw_bytes, cudaMemcpyHostToDevice, s));
+      raw[i] = dst;
     }
+    FA_CU(fa::launch_to_slot(raw[i], dtype, F->data, kind, A->nz, A->ny, A->nx, F->job.fpitch, F->job.fplane, true, s));
+    g_launches += 1;
   }
   // Phase correlation on the raw frames (FrameWarpAligner.cpp:181-190), downsampled when binning.
   std::vector<const void*> cin((size_t)n);
-  int cin_kind = dtype == FA_U16 ? fa::kFrameRawU16 : fa::kFrameF32;
+  int cin_kind = dtype;
   if (A->prm.spatial_binning > 1) {
     const long long nds = (long long)A->dz * A->dy * A->dx;
     for (int i = 0; i < n; i++) {
@@ -1566,7 +1572,7 @@ fa_status aligner_run(fa_aligner* A, const void* const* frames, fa_dtype dtype, 
       g_launches += 1;
       cin[i] = vol;
     }
-    cin_kind = fa::kFrameF32;
+    cin_kind = FA_F32;
   } else {
     cin = raw;
   }
@@ -1580,7 +1586,7 @@ fa_status aligner_run(fa_aligner* A, const void* const* frames, fa_dtype dtype, 
     A->slots[i]->have_last = false;
   }
   std::vector<fa_frame*> batch(A->slots.begin(), A->slots.begin() + n);
-  FA_TRY(align_batch_impl(batch.data(), n, rigid.data(), A->prm.max_iterations, D_out, stats, data.data()));
+  FA_TRY(align_batch_impl(batch.data(), n, rigid.data(), A->prm.max_iterations, D_out, stats, nullptr));
   FA_CU(cudaEventRecord(A->ev1, batch[0]->stream));
   FA_CU(cudaEventSynchronize(A->ev1));
   float ms = 0;

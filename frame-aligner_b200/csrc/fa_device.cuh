@@ -16,15 +16,16 @@ __device__ __forceinline__ float ldf<__half>(const __half* p) { return __half2fl
 template <>
 __device__ __forceinline__ float ldf<__nv_bfloat16>(const __nv_bfloat16* p) { return __bfloat162float(__ldg(p)); }
 
-// Raw uint16 photon count; reads return count + 1 (exact: 2^23 + u is representable, so the magic
-// constant subtraction yields u + 1 without a conversion instruction).
+// uint16 frame storage holding photon count + 1 (FrameWarpAligner.cpp:142), saturated at 65535; the
+// zero halo stays zero. Reads are exact: 2^23 + u is representable, so subtracting the magic
+// constant converts without a conversion instruction.
 struct RawU16 {
   unsigned short v;
 };
-__device__ __forceinline__ float u16_plus1(unsigned u) { return __uint_as_float(0x4B000000u | u) - 8388607.0f; }
+__device__ __forceinline__ float u16f(unsigned u) { return __uint_as_float(0x4B000000u | u) - 8388608.0f; }
 template <>
 __device__ __forceinline__ float ldf<RawU16>(const RawU16* p) {
-  return u16_plus1(__ldg(reinterpret_cast<const unsigned short*>(p)));
+  return u16f(__ldg(reinterpret_cast<const unsigned short*>(p)));
 }
 
 // Compile-time kernel configuration: dimensionality, frame storage type, reference storage type.
@@ -74,8 +75,8 @@ __device__ __forceinline__ VoxelModel voxel_model(const RowDesc& rd, int x, int 
 // interpolated value; exactly 0 when every contributing tap is outside (getZeroPadded,
 // FrameWarper.h:39-47).
 template <int NDIM, typename FT>
-__device__ __forceinline__ float sample(const FT* __restrict__ fr, const float4* P, float f, int x, int y, int z,
-                                        int nx, int ny, int nz) {
+__device__ __forceinline__ float sample(const FT* __restrict__ fr, long long fplane, int fpitch, const float4* P, float f,
+                                        int x, int y, int z, int nx, int ny, int nz) {
   const float4 n = P[0], ph = P[1], dd = P[2];
   const float tx = fmaf(f, dd.x, ph.x);
   const float ty = fmaf(f, dd.y, ph.y);
@@ -86,11 +87,11 @@ __device__ __forceinline__ float sample(const FT* __restrict__ fr, const float4*
   const bool vx0 = (unsigned)ix < (unsigned)nx, vx1 = (unsigned)(ix + 1) < (unsigned)nx;
   const bool vy0 = (unsigned)iy < (unsigned)ny, vy1 = (unsigned)(iy + 1) < (unsigned)ny;
   if (NDIM == 2) {
-    const long long b = (long long)iy * nx + ix;
+    const long long b = (long long)iy * fpitch + ix;
     const float v00 = (vy0 && vx0) ? ldf(fr + b) : 0.0f;
     const float v01 = (vy0 && vx1) ? ldf(fr + b + 1) : 0.0f;
-    const float v10 = (vy1 && vx0) ? ldf(fr + b + nx) : 0.0f;
-    const float v11 = (vy1 && vx1) ? ldf(fr + b + nx + 1) : 0.0f;
+    const float v10 = (vy1 && vx0) ? ldf(fr + b + fpitch) : 0.0f;
+    const float v11 = (vy1 && vx1) ? ldf(fr + b + fpitch + 1) : 0.0f;
     const float c0 = fmaf(wx, v01 - v00, v00);
     const float c1 = fmaf(wx, v11 - v10, v10);
     return fmaf(wy, c1 - c0, c0);
@@ -100,16 +101,15 @@ __device__ __forceinline__ float sample(const FT* __restrict__ fr, const float4*
     const float wz = tz - flz;
     const int iz = z + (int)n.z + (int)flz;
     const bool vz0 = (unsigned)iz < (unsigned)nz, vz1 = (unsigned)(iz + 1) < (unsigned)nz;
-    const long long plane = (long long)nx * ny;
-    const long long b = ((long long)iz * ny + iy) * nx + ix;
+    const long long b = (long long)iz * fplane + (long long)iy * fpitch + ix;
     const float v000 = (vz0 && vy0 && vx0) ? ldf(fr + b) : 0.0f;
     const float v001 = (vz0 && vy0 && vx1) ? ldf(fr + b + 1) : 0.0f;
-    const float v010 = (vz0 && vy1 && vx0) ? ldf(fr + b + nx) : 0.0f;
-    const float v011 = (vz0 && vy1 && vx1) ? ldf(fr + b + nx + 1) : 0.0f;
-    const float v100 = (vz1 && vy0 && vx0) ? ldf(fr + b + plane) : 0.0f;
-    const float v101 = (vz1 && vy0 && vx1) ? ldf(fr + b + plane + 1) : 0.0f;
-    const float v110 = (vz1 && vy1 && vx0) ? ldf(fr + b + plane + nx) : 0.0f;
-    const float v111 = (vz1 && vy1 && vx1) ? ldf(fr + b + plane + nx + 1) : 0.0f;
+    const float v010 = (vz0 && vy1 && vx0) ? ldf(fr + b + fpitch) : 0.0f;
+    const float v011 = (vz0 && vy1 && vx1) ? ldf(fr + b + fpitch + 1) : 0.0f;
+    const float v100 = (vz1 && vy0 && vx0) ? ldf(fr + b + fplane) : 0.0f;
+    const float v101 = (vz1 && vy0 && vx1) ? ldf(fr + b + fplane + 1) : 0.0f;
+    const float v110 = (vz1 && vy1 && vx0) ? ldf(fr + b + fplane + fpitch) : 0.0f;
+    const float v111 = (vz1 && vy1 && vx1) ? ldf(fr + b + fplane + fpitch + 1) : 0.0f;
     const float c00 = fmaf(wx, v001 - v000, v000);
     const float c01 = fmaf(wx, v011 - v010, v010);
     const float c10 = fmaf(wx, v101 - v100, v100);

@@ -69,11 +69,11 @@ __device__ __forceinline__ void window5(const RawU16* p, int s, float* v) {
   const unsigned p0 = __funnelshift_r(A, B, sh);
   const unsigned p1 = __funnelshift_r(B, C, sh);
   const unsigned p2 = __funnelshift_r(C, hi.y, sh);
-  v[0] = u16_plus1(p0 & 0xffffu);
-  v[1] = u16_plus1(p0 >> 16);
-  v[2] = u16_plus1(p1 & 0xffffu);
-  v[3] = u16_plus1(p1 >> 16);
-  v[4] = u16_plus1(p2 & 0xffffu);
+  v[0] = __uint_as_float(__byte_perm(p0, 0x4B000000u, 0x7610)) - 8388608.0f;
+  v[1] = __uint_as_float(__byte_perm(p0, 0x4B000000u, 0x7632)) - 8388608.0f;
+  v[2] = __uint_as_float(__byte_perm(p1, 0x4B000000u, 0x7610)) - 8388608.0f;
+  v[3] = __uint_as_float(__byte_perm(p1, 0x4B000000u, 0x7632)) - 8388608.0f;
+  v[4] = __uint_as_float(__byte_perm(p2, 0x4B000000u, 0x7610)) - 8388608.0f;
 }
 __device__ __forceinline__ void window5(const float* p, int s, float* v) {
   const float4 a = __ldg(reinterpret_cast<const float4*>(p));
@@ -148,7 +148,9 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
   const int row_step = fixed_seg ? kEvalWarps / segs : 0;
   const int n_items = fixed_seg ? (warp / segs < rows_here ? (rows_here - warp / segs + row_step - 1) / row_step : 0)
                                 : (rows_here * segs - warp + kEvalWarps - 1) / kEvalWarps;
-  const long long plane = (long long)nx * ny;
+  const long long plane = job.fplane;
+  const int pitch = job.fpitch;
+  const bool padded = job.fpad != 0;
   for (int item = 0; item < n_items; item++) {
     int row, x0;
     if (fixed_seg) {
@@ -207,26 +209,40 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
 
     if (fast) {
       float v[NDIM == 3 ? 4 : 2][5];
-      if (inside) {
-        const int a = ix & ~3, s = ix & 3;
-        const long long rb = ((long long)iz * ny + iy) * nx + a;
+      if (padded) {
+        // Clamp into the zero halo: a window that would lie wholly outside the volume along an
+        // axis reads halo zeros instead, exactly as the unclamped taps would read zero padding.
+        const int cx = min(max(ix, -kHaloX), nx + kHaloX - 5);
+        const int cy = min(max(iy, -kHaloY), ny + kHaloY - 2);
+        const int cz = NDIM == 3 ? min(max(iz, -kHaloZ), nz + kHaloZ - 2) : 0;
+        const int a = cx & ~3, s = cx - a;
+        const long long rb = (long long)cz * plane + (long long)cy * pitch + a;
         window5(fr + rb, s, v[0]);
-        window5(fr + rb + nx, s, v[1]);
+        window5(fr + rb + pitch, s, v[1]);
         if (NDIM == 3) {
           window5(fr + rb + plane, s, v[NDIM == 3 ? 2 : 0]);
-          window5(fr + rb + plane + nx, s, v[NDIM == 3 ? 3 : 1]);
+          window5(fr + rb + plane + pitch, s, v[NDIM == 3 ? 3 : 1]);
+        }
+      } else if (inside) {
+        const int a = ix & ~3, s = ix & 3;
+        const long long rb = (long long)iz * plane + (long long)iy * pitch + a;
+        window5(fr + rb, s, v[0]);
+        window5(fr + rb + pitch, s, v[1]);
+        if (NDIM == 3) {
+          window5(fr + rb + plane, s, v[NDIM == 3 ? 2 : 0]);
+          window5(fr + rb + plane + pitch, s, v[NDIM == 3 ? 3 : 1]);
         }
       } else {
         // tap rows (y, z), (y+1, z), (y, z+1), (y+1, z+1); rows outside the volume read zeros
         const bool y0v = (unsigned)iy < (unsigned)ny, y1v = (unsigned)(iy + 1) < (unsigned)ny;
         const bool z0v = NDIM == 2 || (unsigned)iz < (unsigned)nz;
         const bool z1v = NDIM == 2 || (unsigned)(iz + 1) < (unsigned)nz;
-        const long long rb = ((long long)iz * ny + iy) * nx;
+        const long long rb = (long long)iz * plane + (long long)iy * pitch;
         masked5(fr + rb, y0v && z0v, ix, nx, v[0]);
-        masked5(fr + rb + nx, y1v && z0v, ix, nx, v[1]);
+        masked5(fr + rb + pitch, y1v && z0v, ix, nx, v[1]);
         if (NDIM == 3) {
           masked5(fr + rb + plane, y0v && z1v, ix, nx, v[NDIM == 3 ? 2 : 0]);
-          masked5(fr + rb + plane + nx, y1v && z1v, ix, nx, v[NDIM == 3 ? 3 : 1]);
+          masked5(fr + rb + plane + pitch, y1v && z1v, ix, nx, v[NDIM == 3 ? 3 : 1]);
         }
       }
       const float wx0 = t0x - flx, wy0 = t0y - fly, wz0 = t0z - flz;
@@ -260,7 +276,7 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
         const int x = x0 + j;
         const VoxelModel vm = voxel_model(rd, x, nx, flip, bidir, dq);
         const int wi = min(max(vm.di - cw, 0), kWin - 2);
-        const float val = sample<NDIM, FT>(fr, sD + wi * kDParamF4, vm.f, x, y, z, nx, ny, nz);
+        const float val = sample<NDIM, FT>(fr, plane, pitch, sD + wi * kDParamF4, vm.f, x, y, z, nx, ny, nz);
         const float e = (val > 0.0f) ? val - t4[j] : 0.0f;
         af = fmaf(e, e, af);
         if (!vm.last) {

@@ -92,9 +92,19 @@ struct RefDev {
 };
 
 // One frame in a fused pass / solve launch.
+// Zero halo around every frame slot: taps that leave the volume read these zeros, which is the
+// reference's zero padding (getZeroPadded, FrameWarper.h:39-47) without per-tap bounds checks.
+// X is a multiple of 4 so that every 4-element window of a row stays aligned.
+constexpr int kHaloX = 8;
+constexpr int kHaloY = 2;
+constexpr int kHaloZ = 2;  // planes, for volumes with nz > 1
+
 struct Job {
   const RefDev* ref;      // device pointer
-  const void* frame;      // device pointer, FP32 or FP16 (per kernel instantiation)
+  const void* frame;      // device pointer to voxel (0, 0, 0); FrameKind storage
+  long long fplane;       // elements between planes of the frame
+  int fpitch;             // elements between rows of the frame
+  int fpad;               // 1: the frame carries the kHalo* zero halo
   float4* dparams;        // nD * kDParamF4 (trial point of this job)
   double* partials;       // n_tiles * kPartialDoubles
   FrameState* state;      // solve state (may be null for a bare evaluation)

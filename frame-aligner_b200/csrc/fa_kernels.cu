@@ -128,6 +128,38 @@ cudaError_t launch_offset_convert(const void* in, fa_dtype in_type, void* out, f
   return cudaGetLastError();
 }
 
+// Raw or converted values into a frame slot's interior (row pitch fpitch, plane stride fplane, out
+// pointing at voxel (0,0,0)); add_one applies FrameWarpAligner's +1 (FrameWarpAligner.cpp:142).
+__global__ void to_slot_kernel(const void* __restrict__ in, int in_t, void* __restrict__ out, int out_kind, int ny,
+                               int nx, int n_rows, int fpitch, long long fplane, int add_one) {
+  for (int row = blockIdx.x; row < n_rows; row += gridDim.x) {
+    const int y = row % ny, z = row / ny;
+    const long long ib = (long long)row * nx;
+    const long long ob = (long long)z * fplane + (long long)y * fpitch;
+    for (int x = threadIdx.x; x < nx; x += blockDim.x) {
+      if (out_kind == kFrameRawU16) {
+        // count + 1, saturated (a raw count of 65535 is stored as 65535)
+        const unsigned c = static_cast<const unsigned short*>(in)[ib + x] + (add_one ? 1u : 0u);
+        static_cast<unsigned short*>(out)[ob + x] = (unsigned short)(c > 65535u ? 65535u : c);
+      } else {
+        const float v = load_any(in, in_t, ib + x) + (add_one ? 1.0f : 0.0f);
+        if (out_kind == kFrameF16)
+          static_cast<__half*>(out)[ob + x] = __float2half_rn(v);
+        else
+          static_cast<float*>(out)[ob + x] = v;
+      }
+    }
+  }
+}
+
+cudaError_t launch_to_slot(const void* in, fa_dtype in_type, void* out, int out_kind, int nz, int ny, int nx,
+                           int fpitch, long long fplane, bool add_one, cudaStream_t s) {
+  const int n_rows = nz * ny;
+  int blocks = n_rows < 148 * 16 ? n_rows : 148 * 16;
+  to_slot_kernel<<<blocks, 256, 0, s>>>(in, (int)in_type, out, out_kind, ny, nx, n_rows, fpitch, fplane, add_one ? 1 : 0);
+  return cudaGetLastError();
+}
+
 // downsample (AbstractFrameAligner.cpp:37-56): output (z, y/b, x/b) = float sum of its b x b block,
 // accumulated in the reference's loop order (y, then x).
 __global__ void downsample_kernel(const void* __restrict__ in, int in_t, int nz, int ny, int nx, int b,
@@ -218,7 +250,7 @@ __global__ void __launch_bounds__(kEvalThreads) eval_kernel(const Job* __restric
       // the host geometry guarantees c0-1 <= di <= c0+2; the clamp only keeps the shared-memory
       // window in bounds
       const int wi = min(max(vm.di - cw, 0), kWin - 2);
-      const float v = sample<NDIM, FT>(fr, sD + wi * kDParamF4, vm.f, x, y, z, nx, ny, nz);
+      const float v = sample<NDIM, FT>(fr, job.fplane, job.fpitch, sD + wi * kDParamF4, vm.f, x, y, z, nx, ny, nz);
       const long long p = rowoff + x;
       const float t = ldf(tref + p);
       // include iff the interpolated value is positive: CPU rule px == 0 -> -1, then wimg >= 0
@@ -313,8 +345,8 @@ cudaError_t launch_reduce(const Job* job_dev, const RefDev&, cudaStream_t s) {
 
 template <int NDIM, typename FT>
 __global__ void __launch_bounds__(256) warp_kernel(const RefDev* __restrict__ Rp, const FT* __restrict__ fr,
-                                                   const float4* __restrict__ dparams, float invalid_value,
-                                                   float* __restrict__ out) {
+                                                   long long fplane, int fpitch, const float4* __restrict__ dparams,
+                                                   float invalid_value, float* __restrict__ out) {
   const RefDev& R = *Rp;
   const int nx = R.nx, ny = R.ny, nz = R.nz;
   extern __shared__ float4 sAll[];
@@ -329,15 +361,15 @@ __global__ void __launch_bounds__(256) warp_kernel(const RefDev* __restrict__ Rp
     for (int x = lane; x < nx; x += 32) {
       const VoxelModel vm = voxel_model(rd, x, nx, flip, R.bidir != 0, R.dq);
       const int di = min(max(vm.di, 0), R.nD - 2);
-      float v = sample<NDIM, FT>(fr, sAll + di * kDParamF4, vm.f, x, y, z, nx, ny, nz);
+      float v = sample<NDIM, FT>(fr, fplane, fpitch, sAll + di * kDParamF4, vm.f, x, y, z, nx, ny, nz);
       if (v == 0.0f) v = invalid_value;
       out[(long long)row * nx + x] = v;
     }
   }
 }
 
-cudaError_t launch_warp(const RefDev* ref_dev, const RefDev& R, const void* frame, int frame_kind,
-                        const float4* dparams, float invalid_value, float* out, cudaStream_t s) {
+cudaError_t launch_warp(const RefDev* ref_dev, const RefDev& R, const void* frame, long long fplane, int fpitch,
+                        int frame_kind, const float4* dparams, float invalid_value, float* out, cudaStream_t s) {
   int blocks = (R.n_rows + 7) / 8;
   if (blocks > 148 * 8) blocks = 148 * 8;
   const size_t smem = (size_t)R.nD * kDParamF4 * sizeof(float4);
@@ -348,7 +380,8 @@ cudaError_t launch_warp(const RefDev* ref_dev, const RefDev& R, const void* fram
       cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (e != cudaSuccess) return e;
     }
-    kern<<<blocks, 256, smem, s>>>(ref_dev, static_cast<const typename C::F*>(frame), dparams, invalid_value, out);
+    kern<<<blocks, 256, smem, s>>>(ref_dev, static_cast<const typename C::F*>(frame), fplane, fpitch, dparams,
+                                   invalid_value, out);
     return cudaGetLastError();
   });
 }

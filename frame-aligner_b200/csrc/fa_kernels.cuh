@@ -24,6 +24,10 @@ cudaError_t launch_to_bf16(const float* in, __nv_bfloat16* out, long long n, cud
 cudaError_t launch_convert(const void* in, fa_dtype in_type, void* out, fa_dtype out_type, long long n,
                            cudaStream_t s);
 
+// Dense frame (any dtype) -> a frame slot's interior (pitch / plane stride), optionally with +1.
+cudaError_t launch_to_slot(const void* in, fa_dtype in_type, void* out, int out_kind, int nz, int ny, int nx,
+                           int fpitch, long long fplane, bool add_one, cudaStream_t s);
+
 // Raw frame -> storage with the +1 offset; raw -> downsampled float (block sums).
 cudaError_t launch_offset_convert(const void* in, fa_dtype in_type, void* out, fa_dtype out_type, long long n,
                                   cudaStream_t s);
@@ -45,7 +49,8 @@ cudaError_t launch_eval4_active(const Job* jobs_dev, const int* active, const in
 cudaError_t launch_reduce(const Job* job_dev, const RefDev& ref_host, cudaStream_t s);
 
 // Warped image (CpuFrameWarper::warpImageInterpolated semantics) for one frame.
-cudaError_t launch_warp(const RefDev* ref_dev, const RefDev& ref_host, const void* frame, int frame_kind,
+cudaError_t launch_warp(const RefDev* ref_dev, const RefDev& ref_host, const void* frame, long long fplane, int fpitch,
+                        int frame_kind,
                         const float4* dparams, float invalid_value, float* out, cudaStream_t s);
 
 // One trust-region step for each job (grid = n_jobs): reduce partials, advance the state machine,

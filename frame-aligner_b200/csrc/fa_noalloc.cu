@@ -87,6 +87,9 @@ extern "C" fa_status fa_get_error_jacobian_static(const fa_reference* ref, const
   fa::Job job{};
   job.ref = dev;
   job.frame = frame_device;
+  job.fplane = (long long)host->nx * host->ny;  // the caller's dense frame, no halo
+  job.fpitch = host->nx;
+  job.fpad = 0;
   job.dparams = reinterpret_cast<float4*>(base + off_dp);
   job.result = reinterpret_cast<double*>(base + off_res);
   job.partials = reinterpret_cast<double*>(base + off_parts);

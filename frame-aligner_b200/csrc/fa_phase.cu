@@ -12,7 +12,8 @@ namespace fa {
 
 // Windowed FP64 input of a batch of frames: out[b][i] = double(vol_b[i]) * ((1 * wy[y]) * wx[x]) --
 // the reference's window (1 along z) formed as in VolumePhaseCorrelator.cpp:141-153, applied as at
-// :62-63. vol_b is FP32 or raw uint16 (the correlator sees the frames without the +1 offset).
+// :62-63. vol_b is dense FP32 or uint16 (in_kind is an fa_dtype); the correlator sees the raw frames,
+// without the +1 offset.
 __global__ void phase_window_kernel(const void* const* __restrict__ vols, int in_kind, const double* __restrict__ wy,
                                     const double* __restrict__ wx, int ny, int nx, int n_rows,
                                     double* __restrict__ out) {
@@ -25,8 +26,8 @@ __global__ void phase_window_kernel(const void* const* __restrict__ vols, int in
     const long long base = (long long)row * nx;
     for (int x = threadIdx.x; x < nx; x += blockDim.x) {
       const long long i = base + x;
-      const float v = in_kind == kFrameRawU16 ? (float)static_cast<const unsigned short*>(vol)[i]
-                                              : static_cast<const float*>(vol)[i];
+      const float v = in_kind == FA_U16 ? (float)static_cast<const unsigned short*>(vol)[i]
+                                        : static_cast<const float*>(vol)[i];
       o[i] = __dmul_rn((double)v, __dmul_rn(wrow, wx[x]));
     }
   }
