@@ -13,9 +13,12 @@ one solve launch per iteration, captured in a CUDA graph).
   e2e    the same through fa_aligner_add_frames with raw uint16 frames in pinned host memory,
          host->device copies and the D readback inside the timed region (wall clock)
 
-Extra keys: `plain_fp32` (the FP32 single-frame path, host-driven iterations, one frame at a time),
-`roofline` (the fused evaluation kernel against the measured HBM copy bandwidth), `cpu_baseline`
-(the reference's CPU warper, compiled from its own sources, on a bounded sample), `clocks`.
+Extra keys: `plain_fp32` (the FP32 single-frame path, host-driven iterations, one frame at a time,
+timed both with frames resident in HBM and from host memory, so that each ratio compares like with
+like), `serving` (the served stream: eight acquisitions of different sizes, Poisson arrivals at
+2000 frames/s, 40 GB admission budget, warm start; p50/p99 latency and throughput), `roofline`
+(the fused evaluation kernel against the measured HBM copy bandwidth), `cpu_baseline` (the
+reference's CPU warper, compiled from its own sources, on a bounded sample), `clocks`.
 
 --impl reference times the reference CPU path on this host's cores (rank 0 only).
 """
@@ -36,20 +39,26 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 import fa_synth as S  # noqa: E402
 
-METRIC = "aligned frames/s (512x512x16, nD=32)"
+METRIC = "aligned frames/s at \u22640.01px RMS vs CPU ref; warp+J\u1d40J HBM GB/s; p99 frame latency"
 UNIT = "frames/s"
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--frames", type=int, default=50)
     ap.add_argument("--plain-frames", type=int, default=8)
     ap.add_argument("--cpu-frames", type=int, default=0, help="CPU baseline sample size (0 = one per thread)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=3.0, help="length of the Poisson arrival stream")
+    ap.add_argument("--serve-rate", type=float, default=2000.0, help="total arrivals per second")
+    ap.add_argument("--serve-pool", type=int, default=6, help="distinct frames per served acquisition")
+    ap.add_argument("--serve-lags", type=int, nargs="+", default=[1, 4],
+                    help="warm-start lags to serve with (1 = the previous frame's solution)")
     return ap.parse_args()
 
 
@@ -79,7 +88,7 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons, polled every 200 ms on a thread while running."""
+    """nvidia-smi clocks and throttle reasons, polled every 100 ms on a thread while running."""
 
     Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -99,7 +108,7 @@ class ClockSampler:
                     self.rows.append([x.strip() for x in line.split(",")])
             except (OSError, subprocess.SubprocessError):
                 return
-            self._stop.wait(0.2)
+            self._stop.wait(0.1)
 
     def __enter__(self):
         self.thread = threading.Thread(target=self._poll, daemon=True)
@@ -157,6 +166,107 @@ def cpu_baseline(acq, n_threads, n_frames):
     return {"value": n_frames / dt, "unit": UNIT, "cores": n_threads, "kind": kind,
             "sample": "%d frames of the 512x512x16 nD=32 workload, non-rigid solve only (rigid shifts "
                       "precomputed), %.1f s, %d threads" % (n_frames, dt, n_threads)}, D, shifts
+
+
+def measure_plain(fa, ctx, acq, scan, pf, local):
+    """The plain FP32 single-frame path: one frame at a time, the phase correlation and then the
+    solve with the host driving every iteration (fa_align_frame). Timed two ways, like the batched
+    figures: frames already in HBM (`value`), and from pinned host memory with the upload inside the
+    timed region (`e2e`)."""
+    import ctypes as C
+    import torch
+
+    ref32 = fa.Reference(ctx, acq.reference + 1, acq.nD, scan, fa.PREC_F32)
+    corr = fa.Correlator(ctx, acq.reference)
+    raw = torch.from_numpy(np.ascontiguousarray(acq.frames[:pf])).to(f"cuda:{local}")  # correlator input
+    plus1 = raw + 1.0                                                                   # FrameWarpAligner's +1
+    torch.cuda.synchronize()
+    frs = [fa.Frame(ref32, device_ptr=plus1[k].data_ptr()) for k in range(pf)]
+    frs[0].align(corr.compute_shift_device(raw[0].data_ptr()), 100)  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(pf):
+        frs[k].align(corr.compute_shift_device(raw[k].data_ptr()), 100)
+    dev_fps = pf / (time.perf_counter() - t0)
+    host_raw = torch.from_numpy(np.ascontiguousarray(acq.frames[:pf])).pin_memory()
+    host_p1 = torch.from_numpy(np.ascontiguousarray(acq.frames[:pf] + 1)).pin_memory()
+    shift = np.empty(3, np.float64)
+    t0 = time.perf_counter()
+    for k in range(pf):
+        fa.check(fa.lib().fa_update_frame(frs[0]._h, C.c_void_p(host_p1[k].data_ptr()), fa.F32))
+        fa.check(fa.lib().fa_correlator_shift(corr._h, host_raw[k].numpy(), shift))
+        frs[0].align(shift, 100)
+    e2e_fps = pf / (time.perf_counter() - t0)
+    for f in frs:
+        f.close()
+    corr.close()
+    ref32.close()
+    return {"value": dev_fps, "e2e": e2e_fps, "unit": UNIT, "frames": pf,
+            "note": "FP32 single-frame path (fa_align_frame: host-driven trust-region iterations) after the "
+                    "device phase correlation; value with frames in HBM, e2e with each frame uploaded from "
+                    "pinned host memory inside the timed region"}
+
+
+def serving_data(args):
+    """The served-stream acquisitions and their frames as raw uint16 in pinned host memory."""
+    import torch
+
+    acqs = S.config3_acquisitions(n_frames=args.serve_pool)
+    pools = [torch.from_numpy(np.ascontiguousarray(a.frames.astype(np.uint16)).view(np.int16)).pin_memory()
+             for a in acqs]
+    return acqs, pools
+
+
+def measure_serving(fa, ctx, args, acqs, pools, lag):
+    """The served stream: eight acquisitions (256x256x1 ... 1024x1024x4, nD 16-64), frames arriving as
+    a Poisson process at args.serve_rate in total, each acquisition's frames drawn in order from a
+    pool of args.serve_pool frames (raw uint16 in pinned host memory); warm start from the solution of
+    the frame `lag` positions earlier in the same acquisition; 40 GB admission budget.
+    Latency = submission -> result on the host."""
+    srv = fa.Server(ctx, memory_budget=40 << 30, warm_start=lag)
+    ids = []
+    for a in acqs:
+        nz, ny, nx = a.reference.shape
+        line, il, ifr = a.scan
+        ids.append(srv.add_acquisition(a.reference, fa.scan_params(line, il, ifr, nx, ny, nz), frame_dtype=np.uint16,
+                                       nD=a.nD, precision=fa.PREC_MIXED))
+    n_acq = len(acqs)
+    # warm-up: every acquisition's pool once (graphs, slots, cuFFT plans)
+    warm = [srv.submit_ptr(ids[j], pools[j][k].data_ptr(), False) for k in range(args.serve_pool)
+            for j in range(n_acq)]
+    for t in warm:
+        srv.wait(t, 300.0)
+    srv.reset_stats()
+    rng = np.random.Generator(np.random.PCG64(3333))
+    n = max(1, int(args.serve_rate * args.serve_seconds))
+    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, n))
+    which = rng.integers(0, n_acq, n)
+    nxt = [0] * n_acq
+    tickets = []
+    t0 = time.perf_counter()
+    for i in range(n):
+        target = t0 + arrivals[i]
+        while True:
+            d = target - time.perf_counter()
+            if d <= 0:
+                break
+            if d > 2e-4:
+                time.sleep(d - 1e-4)
+        j = int(which[i])
+        tickets.append(srv.submit_ptr(ids[j], pools[j][nxt[j] % args.serve_pool].data_ptr(), False))
+        nxt[j] += 1
+    t_sub = time.perf_counter() - t0
+    iters = []
+    for t in tickets:
+        _, st, _ = srv.wait(t, 300.0)
+        iters.append(st["iterations"])
+    stats = srv.stats()
+    srv.close()
+    return {"warm_start_lag": lag, "arrival_rate": args.serve_rate, "arrival_rate_achieved": n / t_sub,
+            "frames": n, "p50_ms": stats["p50_ms"], "p99_ms": stats["p99_ms"], "mean_ms": stats["mean_ms"],
+            "max_ms": stats["max_ms"], "frames_per_s": stats["frames_per_s"],
+            "peak_in_flight": stats["peak_in_flight"], "peak_slot_gb": stats["peak_slot_bytes"] / 1e9,
+            "graph_launches": stats["graph_launches"], "iterations_mean": float(np.mean(iters))}
 
 
 def run_reference(args, rank, world):
@@ -287,21 +397,7 @@ def run_ours(args, rank, world, local):
         for f in frs:
             f.close()
         ref_m.close()
-        # plain FP32 single-frame path: one frame at a time, host-driven iterations
-        ref32 = fa.Reference(ctx, acq.reference + 1, acq.nD, scan, fa.PREC_F32)
-        corr = fa.Correlator(ctx, acq.reference)
-        pf = min(args.plain_frames, n)
-        fr32 = fa.Frame(ref32, acq.frames[0] + 1)
-        fr32.align(corr.compute_shift(acq.frames[0]), 100)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for k in range(pf):
-            fr32.update(acq.frames[k] + 1)
-            fr32.align(corr.compute_shift(acq.frames[k]), 100)
-        plain_fps = pf / (time.perf_counter() - t0)
-        fr32.close()
-        corr.close()
-        ref32.close()
+        plain = measure_plain(fa, ctx, acq, scan, min(args.plain_frames, n), local)
         cb = None
         D_cpu = None
         if not args.no_cpu:
@@ -310,6 +406,16 @@ def run_ours(args, rank, world, local):
                 cb, D_cpu, _ = cpu_baseline(acq, nt, args.cpu_frames or min(nt, n))
             except Exception as ex:  # the baseline is reported, never required
                 cb = {"value": None, "unit": UNIT, "cores": 0, "kind": "unavailable", "sample": str(ex)[:200]}
+        serving = None
+        if not args.no_serve:
+            sacqs, spools = serving_data(args)
+            serving = {"workload": "8 acquisitions " + ", ".join(
+                           "%dx%dx%d nD=%d" % (a.reference.shape[2], a.reference.shape[1], a.reference.shape[0], a.nD)
+                           for a in sacqs),
+                       "memory_budget_gb": 40 * 2 ** 30 / 1e9,
+                       "frames_from": "pinned host memory (raw uint16), %d distinct frames per acquisition"
+                                      % args.serve_pool,
+                       "runs": [measure_serving(fa, ctx, args, sacqs, spools, lag) for lag in args.serve_lags]}
         rms_vs_cpu = None
         if D_cpu is not None:
             k = D_cpu.shape[0]
@@ -320,9 +426,10 @@ def run_ours(args, rank, world, local):
                "data": "synthetic (seeded blob acquisition, Poisson noise)", "config": config_dict(n, world),
                "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cb,
                "clocks": clk.summary(),
-               "plain_fp32": {"value": plain_fps, "unit": UNIT, "frames": pf,
-                              "note": "FP32 single-frame path, host-driven trust-region iterations"},
-               "batched_over_plain": value / world / plain_fps,
+               "plain_fp32": plain,
+               "batched_over_plain": value / world / plain["value"],
+               "e2e_over_plain_e2e": e2e["value"] / world / plain["e2e"],
+               "serving": serving,
                "displacement_rms_vs_cpu_px": rms_vs_cpu,
                "iterations": {"mean": float(np.mean(iters)), "max": int(np.max(iters))}}
     if pg:

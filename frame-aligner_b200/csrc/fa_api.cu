@@ -1,26 +1,22 @@
 // fa_api.cu -- host runtime behind the C ABI (include/fa_b200.h): device memory under a budget,
 // reference set-up (exact scan geometry, Sobel, Hessian), frame slots, fused evaluations, the
 // single-frame and batched trust-region drivers, and the phase correlator.
-#include <cufft.h>
-
-#include <map>
-
 #include <algorithm>
-#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
-#include <string>
-#include <vector>
+#include <map>
 
-#include "fa_kernels.cuh"
+#include "fa_runtime.h"
 
 using fa::Job;
 using fa::RefDev;
 using fa::RowDesc;
+using namespace fa_rt;
 
-namespace {
+// ================================================================== runtime helpers ================
+
+namespace fa_rt {
 
 thread_local std::string g_err;
 std::atomic<long long> g_launches{0};
@@ -29,35 +25,6 @@ fa_status fail(fa_status s, const std::string& msg) {
   g_err = msg;
   return s;
 }
-
-#define FA_CU(call)                                                                             \
-  do {                                                                                          \
-    cudaError_t e_ = (call);                                                                    \
-    if (e_ != cudaSuccess) return fail(FA_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
-  } while (0)
-
-#define FA_TRY(call)                  \
-  do {                                \
-    fa_status s_ = (call);            \
-    if (s_ != FA_OK) return s_;       \
-  } while (0)
-
-struct Alloc {
-  void* p;
-  size_t n;
-};
-
-}  // namespace
-
-struct fa_context {
-  int device = 0;
-  int autotune = 0;
-  size_t budget = 0;
-  std::atomic<size_t> used{0};
-  std::mutex mu;
-};
-
-namespace {
 
 fa_status dalloc(fa_context* ctx, size_t bytes, void** out, std::vector<Alloc>& owner) {
   if (bytes == 0) bytes = 16;
@@ -78,14 +45,6 @@ fa_status dalloc(fa_context* ctx, size_t bytes, void** out, std::vector<Alloc>& 
   return FA_OK;
 }
 
-template <typename T>
-fa_status dalloc_t(fa_context* ctx, size_t count, T** out, std::vector<Alloc>& owner) {
-  void* p = nullptr;
-  FA_TRY(dalloc(ctx, count * sizeof(T), &p, owner));
-  *out = static_cast<T*>(p);
-  return FA_OK;
-}
-
 void dfree_all(fa_context* ctx, std::vector<Alloc>& owner) {
   for (auto& a : owner) {
     cudaFree(a.p);
@@ -93,6 +52,10 @@ void dfree_all(fa_context* ctx, std::vector<Alloc>& owner) {
   }
   owner.clear();
 }
+
+}  // namespace fa_rt
+
+namespace {
 
 // ImageScanParameters fields after AbstractFrameWarper::processScanParameters
 // (FrameWarper.cpp:223-236).
@@ -105,21 +68,6 @@ fa_scan_params process_scan(const fa_scan_params& in, int nz, int nD) {
   }
   return out;
 }
-
-// Exact scan geometry, computed on the host in double with the reference's expressions
-// (FrameWarper.cpp:252-283), without per-voxel tables.
-struct Geometry {
-  int nz, ny, nx, nD, n_rows;
-  long long N;
-  std::vector<long long> scan_begin;  // first scan index of interval k (k = 0..nD-2)
-  std::vector<int> begin, end;        // storage D_range
-  std::vector<RowDesc> rows;
-  float dq;
-  long long lmin;
-  int tile_rows, n_tiles;
-  std::vector<int> tile_c0;
-  std::vector<int2> ctrl_tiles;
-};
 
 struct ScanEval {
   fa_scan_params p;
@@ -267,71 +215,6 @@ bool finite_all(const double* v, size_t n) {
 
 }  // namespace
 
-struct fa_reference {
-  fa_context* ctx = nullptr;
-  int nz = 0, ny = 0, nx = 0, nD = 0, n_dim = 0, P = 0;
-  long long N = 0;
-  fa_precision prec = FA_PREC_F32;
-  fa_scan_params scan{};
-  Geometry G;
-  int* tile_c0_dev = nullptr;
-  int2* ctrl_dev = nullptr;
-  std::vector<double> hd, hl;  // host copies of the Hessian blocks (diagonal, sub-diagonal)
-  RefDev host{};
-  RefDev* dev = nullptr;
-  cudaStream_t stream = nullptr;
-  std::vector<Alloc> allocs;
-  std::atomic<int> n_frames{0};
-};
-
-struct fa_frame {
-  fa_reference* ref = nullptr;
-  void* data = nullptr;
-  int kind = fa::kFrameF32;
-  cudaStream_t stream = nullptr;
-  Job job{};
-  Job* job_dev = nullptr;
-  fa::FrameState* state = nullptr;
-  double* h_result = nullptr;  // pinned: [f, g(P)]
-  float4* h_dparams = nullptr;  // pinned: nD * 3
-  double* h_x = nullptr;        // pinned: P
-  fa::FrameState* h_state = nullptr;  // pinned
-  float* warp_out = nullptr;
-  std::vector<double> lastD;
-  std::vector<double> last_g;
-  double last_f = 0;
-  bool have_last = false;
-  std::mutex mu;
-  std::vector<Alloc> allocs;
-};
-
-struct fa_correlator {
-  fa_context* ctx = nullptr;
-  int nz = 0, ny = 0, nx = 0;
-  long long n_el = 0, n_complex = 0;
-  int cap = 0;                          // frames per batched FFT
-  cufftHandle fwd = 0, inv = 0;         // batch of cap frames
-  cufftHandle fwd1 = 0, inv1 = 0;       // single frame
-  cudaStream_t stream = nullptr;
-  double* wy = nullptr;                 // square-root Hann window along y
-  double* wx = nullptr;                 // ... and along x (1 along z)
-  double* real = nullptr;               // cap * n_el
-  double2* spec = nullptr;              // cap * n_complex
-  double2* ref_conj = nullptr;          // n_complex
-  float* vol = nullptr;                 // one host-uploaded volume
-  const void** d_ptrs = nullptr;        // device array of input pointers
-  const void** h_ptrs = nullptr;        // pinned staging of the same
-  int ptr_cap = 0;
-  double* bval = nullptr;
-  long long* bidx = nullptr;
-  long long* d_idx = nullptr;           // one peak index per frame (ptr_cap)
-  long long* h_idx = nullptr;
-  int n_blocks = 0;                     // argmax blocks per frame
-  std::mutex mu;
-  std::vector<Alloc> allocs;
-  std::vector<Alloc> ptr_allocs;
-};
-
 // ================================================================== context ========================
 
 extern "C" const char* fa_last_error(void) { return g_err.c_str(); }
@@ -474,7 +357,7 @@ fa_status autotune(fa_reference* R) {
   float4* dp;
   double* parts;
   Job* jobs_dev;
-  int *list, *cnt;
+  int *list, *cnt, *prefix;
   const int hz = R->nz > 1 ? fa::kHaloZ : 0;
   const int pitch = R->nx + 2 * fa::kHaloX;
   const long long plane = (long long)pitch * (R->ny + 2 * fa::kHaloY);
@@ -486,6 +369,7 @@ fa_status autotune(fa_reference* R) {
   if (st == FA_OK) st = dalloc_t(ctx, (size_t)K, &jobs_dev, tmp);
   if (st == FA_OK) st = dalloc_t(ctx, (size_t)K, &list, tmp);
   if (st == FA_OK) st = dalloc_t(ctx, 1, &cnt, tmp);
+  if (st == FA_OK) st = dalloc_t(ctx, (size_t)K + 1, &prefix, tmp);
   if (st != FA_OK) return done(st);
   cudaStream_t s = R->stream;
   void* interior = static_cast<char*>(frame) + ((long long)hz * plane + (long long)fa::kHaloY * pitch + fa::kHaloX) * esz;
@@ -529,12 +413,18 @@ fa_status autotune(fa_reference* R) {
   TuneResult best{8192, 2, 2, 1e30};
   const int targets[] = {2048, 4096, 8192, 16384, 32768};
   const int mbs[] = {2, 3, 4};
+  std::vector<int> hprefix(K + 1);
   for (int target : targets) {
     if (retile(R, target) != FA_OK) break;
+    for (int i = 0; i <= K; i++) hprefix[i] = i * R->G.n_tiles;
+    e = cudaMemcpyAsync(prefix, hprefix.data(), (K + 1) * sizeof(int), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) break;
     for (int mb : mbs) {
       const bool mixed = R->prec == FA_PREC_MIXED;
       auto launch = [&]() {
-        return fa::launch_eval4_active(jobs_dev, list, cnt, K, R->G.n_tiles, R->n_dim, kind, mixed, mb, mb * sms, s);
+        return fa::launch_eval4_active(jobs_dev, list, cnt, prefix, (long long)K * R->G.n_tiles, R->n_dim, kind, mixed,
+                                       mb, mb * sms, s);
       };
       e = launch();
       if (e == cudaSuccess) e = cudaEventRecord(e0, s);
@@ -769,6 +659,10 @@ size_t work_doubles(const fa_reference* R) { return (size_t)R->P * (2 * R->n_dim
 
 int default_kind(const fa_reference* R) { return R->prec == FA_PREC_MIXED ? fa::kFrameF16 : fa::kFrameF32; }
 
+}  // namespace
+
+namespace fa_rt {
+
 fa_status frame_alloc(fa_reference* R, int kind, fa_frame** out) {
   fa_context* ctx = R->ctx;
   fa_frame* F = new fa_frame;
@@ -834,6 +728,10 @@ fa_status frame_alloc(fa_reference* R, int kind, fa_frame** out) {
   *out = F;
   return FA_OK;
 }
+
+}  // namespace fa_rt
+
+namespace {
 
 // Copies a dense frame (host or device, any dtype, values as stored: the +1 offset already applied)
 // into the slot's interior.
@@ -1056,41 +954,6 @@ extern "C" fa_status fa_align_frame(fa_frame* F, const double* rigid_shift, int 
 
 namespace {
 
-// Indices of the frames still being solved, in ascending order, and their count.
-__global__ void compact_active_kernel(const Job* jobs, int n, int* active, int* n_active) {
-  __shared__ int warp_base[32];
-  __shared__ int base, total;
-  if (threadIdx.x == 0) base = 0;
-  __syncthreads();
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int c = 0; c < n; c += blockDim.x) {
-    const int i = c + threadIdx.x;
-    const bool f = i < n && jobs[i].state->phase != fa::kPhaseDone;
-    const unsigned m = __ballot_sync(0xffffffffu, f);
-    if (lane == 0) warp_base[w] = __popc(m);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int acc = 0;
-      for (int k = 0; k < (int)(blockDim.x >> 5); k++) {
-        const int t = warp_base[k];
-        warp_base[k] = acc;
-        acc += t;
-      }
-      total = acc;
-    }
-    __syncthreads();
-    if (f) active[base + warp_base[w] + __popc(m & ((1u << lane) - 1u))] = i;
-    __syncthreads();
-    if (threadIdx.x == 0) base += total;
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) *n_active = base;
-}
-
-}  // namespace
-
-namespace {
-
 // Batched solve; frame_data (optional) replaces each frame's own device data pointer for this call.
 fa_status align_batch_impl(fa_frame* const* frames, int n, const double* rigid_shifts, int max_iterations,
                            double* D_out, fa_align_stats* stats, const void* const* frame_data) {
@@ -1127,10 +990,12 @@ fa_status align_batch_impl(fa_frame* const* frames, int n, const double* rigid_s
   Job* jobs_dev;
   int* d_active;
   int* d_list;
+  int* d_prefix;
   int* h_active;
   FA_TRY(dalloc_t(ctx, (size_t)n, &jobs_dev, tmp));
   fa_status st = dalloc_t(ctx, 1, &d_active, tmp);
   if (st == FA_OK) st = dalloc_t(ctx, (size_t)n, &d_list, tmp);
+  if (st == FA_OK) st = dalloc_t(ctx, (size_t)n + 1, &d_prefix, tmp);
   if (st != FA_OK) {
     dfree_all(ctx, tmp);
     return st;
@@ -1149,10 +1014,14 @@ fa_status align_batch_impl(fa_frame* const* frames, int n, const double* rigid_s
   };
   if (cudaMemcpyAsync(jobs_dev, jobs.data(), n * sizeof(Job), cudaMemcpyHostToDevice, s) != cudaSuccess)
     return done(fail(FA_ERR_CUDA, "job upload failed"));
-  std::vector<int> all(n);
-  for (int i = 0; i < n; i++) all[i] = i;
+  std::vector<int> all(n), prefix(n + 1, 0);
+  for (int i = 0; i < n; i++) {
+    all[i] = i;
+    prefix[i + 1] = prefix[i] + frames[i]->ref->G.n_tiles;
+  }
   *h_active = n;
   if (cudaMemcpyAsync(d_list, all.data(), n * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(d_prefix, prefix.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess ||
       cudaMemcpyAsync(d_active, h_active, sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess)
     return done(fail(FA_ERR_CUDA, "active list upload failed"));
@@ -1166,15 +1035,13 @@ fa_status align_batch_impl(fa_frame* const* frames, int n, const double* rigid_s
   if (e == cudaSuccess) {
     for (int it = 0; it < kGraphIters && e == cudaSuccess; it++) {
       if (vec4)
-        e = fa::launch_eval4_active(jobs_dev, d_list, d_active, n, max_tiles, R0->n_dim, frames[0]->kind,
+        e = fa::launch_eval4_active(jobs_dev, d_list, d_active, d_prefix, prefix[n], R0->n_dim, frames[0]->kind,
                                     R0->prec == FA_PREC_MIXED, R0->host.tune_mb, R0->host.tune_grid_mult * sms, s);
       else
         e = fa::launch_eval(jobs_dev, n, max_tiles, R0->n_dim, frames[0]->kind, R0->prec == FA_PREC_MIXED, s, false);
       if (e == cudaSuccess) e = fa::launch_solve(jobs_dev, n, max_nD, R0->n_dim, s);
-      if (e == cudaSuccess) {
-        compact_active_kernel<<<1, 1024, 0, s>>>(jobs_dev, n, d_list, d_active);
-        e = cudaGetLastError();
-      }
+      if (e == cudaSuccess)
+        e = fa::launch_compact(jobs_dev, n, d_list, d_active, d_prefix, nullptr, nullptr, nullptr, s);
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(h_active, d_active, sizeof(int), cudaMemcpyDeviceToHost, s);
     cudaError_t e2 = cudaStreamEndCapture(s, &graph);
@@ -1237,6 +1104,10 @@ fa_status correlator_reserve(fa_correlator* C, int n) {
 
 // Window, D2Z, cross-power normalisation, Z2D and first-maximum argmax for n volumes (device
 // pointers, FP32 or raw uint16) in batches of C->cap; peak indices to C->d_idx[0..n).
+}  // namespace
+
+namespace fa_rt {
+
 fa_status correlator_enqueue(fa_correlator* C, const void* const* vols, int in_kind, int n) {
   FA_TRY(correlator_reserve(C, n));
   for (int i = 0; i < n; i++) C->h_ptrs[i] = vols[i];
@@ -1258,6 +1129,10 @@ fa_status correlator_enqueue(fa_correlator* C, const void* const* vols, int in_k
   return FA_OK;
 }
 
+}  // namespace fa_rt
+
+namespace fa_rt {
+
 // Peak index -> signed integer shift (VolumePhaseCorrelator.cpp:94-103).
 void unravel_shift(const fa_correlator* C, long long idx, double* shift) {
   long long x = idx % C->nx;
@@ -1270,6 +1145,10 @@ void unravel_shift(const fa_correlator* C, long long idx, double* shift) {
   shift[1] = (double)y;
   shift[2] = (double)z;
 }
+
+}  // namespace fa_rt
+
+namespace {
 
 fa_status correlator_read(fa_correlator* C, int n, double* shifts) {
   FA_CU(cudaMemcpyAsync(C->h_idx, C->d_idx, (size_t)n * sizeof(long long), cudaMemcpyDeviceToHost, C->stream));
@@ -1454,27 +1333,6 @@ extern "C" fa_status fa_test_tr_subproblem(fa_context* ctx, int nD, int n_dim, c
 
 // ================================================================== aligner =======================
 
-struct fa_aligner {
-  fa_context* ctx = nullptr;
-  fa_aligner_params prm{};
-  fa_reference* ref = nullptr;
-  fa_correlator* corr = nullptr;
-  int nz = 0, ny = 0, nx = 0, nD = 0;
-  int dz = 0, dy = 0, dx = 0;  // downsampled dims
-  cudaStream_t stream = nullptr;
-  std::vector<fa_frame*> slots;
-  int slot_kind = -1;
-  void* staging = nullptr;     // raw frames copied from the host when they need a conversion pass
-  size_t staging_bytes = 0;
-  float* vols = nullptr;       // downsampled frames for the correlator (spatial_binning > 1)
-  size_t vols_count = 0;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  double last_ms = 0;
-  std::vector<Alloc> allocs;   // staging / vols
-  std::vector<Alloc> ref_allocs;
-  std::mutex mu;
-};
-
 namespace {
 
 void aligner_release_reference(fa_aligner* A) {
@@ -1488,7 +1346,15 @@ void aligner_release_reference(fa_aligner* A) {
   dfree_all(A->ctx, A->ref_allocs);
 }
 
+}  // namespace
+
+namespace fa_rt {
+
 size_t dtype_size(fa_dtype t) { return t == FA_F32 ? 4 : 2; }
+
+}  // namespace fa_rt
+
+namespace fa_rt {
 
 // Slot storage for a batch: raw uint16 counts (the kernels add the +1) when the input is uint16
 // and the reference is mixed precision; otherwise FP16 / FP32 values with the +1 applied.
@@ -1496,6 +1362,10 @@ int slot_kind_for(const fa_aligner* A, fa_dtype dtype) {
   if (A->prm.precision == FA_PREC_MIXED) return dtype == FA_U16 ? fa::kFrameRawU16 : fa::kFrameF16;
   return fa::kFrameF32;
 }
+
+}  // namespace fa_rt
+
+namespace {
 
 fa_status aligner_grow(fa_aligner* A, int n, int kind, size_t staging_need) {
   if (A->slot_kind != kind) {

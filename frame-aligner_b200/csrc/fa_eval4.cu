@@ -364,18 +364,29 @@ __global__ void __launch_bounds__(kEvalThreads, MB) eval4_kernel(const Job* __re
 }
 
 // Persistent form for batched solves: a fixed grid walks the (active frame, tile) items of the
-// compacted active list, so frames that have converged cost nothing.
+// compacted active list, item = tile_prefix[a] + tile, so frames that have converged cost nothing and
+// frames of different sizes share the launch. Each CTA's items increase, so its frame index only
+// moves forward (binary search over the remaining prefix).
 template <int NDIM, typename FT, typename RT, int MB>
 __global__ void __launch_bounds__(kEvalThreads, MB) eval4_active_kernel(const Job* __restrict__ jobs,
                                                                      const int* __restrict__ active,
-                                                                     const int* __restrict__ n_active, int max_tiles) {
-  const long long n_items = (long long)(*n_active) * max_tiles;
-  for (long long item = blockIdx.x; item < n_items; item += gridDim.x) {
-    const int a = (int)(item / max_tiles);
-    const int tile = (int)(item - (long long)a * max_tiles);
+                                                                     const int* __restrict__ n_active,
+                                                                     const int* __restrict__ tile_prefix) {
+  const int na = *n_active;
+  const int n_items = tile_prefix[na];
+  int a = 0;
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    int hi = na - 1;
+    while (a < hi) {  // last a with tile_prefix[a] <= item
+      const int mid = (a + hi + 1) >> 1;
+      if (tile_prefix[mid] <= item)
+        a = mid;
+      else
+        hi = mid - 1;
+    }
+    const int tile = item - tile_prefix[a];
     const Job& job = jobs[active[a]];
     const RefDev& R = *job.ref;
-    if (tile >= R.n_tiles) continue;
     eval4_tile<NDIM, FT, RT>(job, R, tile);
     __syncthreads();  // the next item reuses the shared-memory window
   }
@@ -400,15 +411,15 @@ cudaError_t launch_eval4(const Job* jobs_dev, int n_jobs, int max_tiles, int n_d
   });
 }
 
-cudaError_t launch_eval4_active(const Job* jobs_dev, const int* active, const int* n_active, int n_jobs, int max_tiles,
-                                int n_dim, int frame_kind, bool ref_bf16, int mb, int grid, cudaStream_t s) {
-  const long long most = (long long)n_jobs * max_tiles;
-  const int g = (int)(most < grid ? most : grid);
+cudaError_t launch_eval4_active(const Job* jobs_dev, const int* active, const int* n_active, const int* tile_prefix,
+                                long long most_items, int n_dim, int frame_kind, bool ref_bf16, int mb, int grid,
+                                cudaStream_t s) {
+  const int g = (int)(most_items < grid ? (most_items < 1 ? 1 : most_items) : grid);
   return dispatch_cfg(n_dim, frame_kind, ref_bf16, [&](auto c) {
     using C = decltype(c);
     return dispatch_mb(mb, [&](auto m) {
       eval4_active_kernel<C::nd, typename C::F, typename C::R, decltype(m)::value>
-          <<<g, kEvalThreads, 0, s>>>(jobs_dev, active, n_active, max_tiles);
+          <<<g, kEvalThreads, 0, s>>>(jobs_dev, active, n_active, tile_prefix);
       return cudaGetLastError();
     });
   });

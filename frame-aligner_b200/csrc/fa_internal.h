@@ -45,7 +45,8 @@ enum Phase : int {
   kPhaseStartZero = 0,   // trial = zero displacement
   kPhaseStartRigid = 1,  // trial = rigid shift
   kPhaseTrial = 2,       // trial = x + p
-  kPhaseDone = 3
+  kPhaseDone = 3,
+  kPhaseStartLast = 4    // trial = the previous frame's solution (warm start)
 };
 
 struct FrameState {
@@ -62,7 +63,15 @@ struct FrameState {
   int max_iter;
   int hit_max;
   double rigid[3];
+  int use_warm;    // *warm holds a fourth starting point
+  int pad_;
+  double* warm;    // P doubles or null: read by kPhaseStartLast when use_warm; the solution is
+                   // written here when the solve finishes
 };
+
+// Where a finished frame's solve is reported (host-mapped memory): the final FrameState, then the
+// P accepted parameters.
+constexpr int kReportHeaderBytes = (int)sizeof(FrameState);
 
 // Everything a kernel needs about one reference (device-resident copy).
 struct RefDev {
@@ -114,6 +123,17 @@ struct Job {
   double* gt;             // P: gradient at the trial point
   double* work;           // solve scratch (band Cholesky etc.)
   double* result;         // [f, g(P)] of the last pass (bare evaluation)
+  void* report;           // host-mapped FrameState + P doubles written when the solve finishes, or null
+};
+
+// A frame entering a batched solve (written by the host, applied on the device by launch_activate).
+struct Activation {
+  int job;       // index in the job table
+  int use_warm;  // 1: *warm is a starting point
+  int max_iter;
+  int pad_;
+  double rigid[3];
+  double* warm;  // FrameState::warm (null: none)
 };
 
 }  // namespace fa

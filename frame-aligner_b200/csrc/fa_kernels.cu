@@ -516,4 +516,118 @@ cudaError_t launch_hessian(const RefDev* ref_dev, const RefDev& R, const double*
   return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------ batched-solve bookkeeping ----
+
+// One block of 1024 threads scans the job table in chunks: ballots give each warp's active / done
+// counts, a shuffle scan the tile prefix inside a warp, and thread 0 the per-warp offsets.
+__global__ void __launch_bounds__(1024) compact_kernel(const Job* __restrict__ jobs, int n, int* __restrict__ active,
+                                                       int* __restrict__ n_active, int* __restrict__ tile_prefix,
+                                                       int* __restrict__ busy, int* __restrict__ done_list,
+                                                       int* __restrict__ n_done) {
+  __shared__ int s_act[32], s_tiles[32], s_done[32];
+  __shared__ int base_a, base_t, base_d, tot_a, tot_t, tot_d;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (threadIdx.x == 0) {
+    base_a = 0;
+    base_t = 0;
+    base_d = busy != nullptr ? *n_done : 0;
+  }
+  __syncthreads();
+  const unsigned lt = (1u << lane) - 1u;
+  for (int c = 0; c < n; c += blockDim.x) {
+    const int i = c + threadIdx.x;
+    const int phase = i < n ? jobs[i].state->phase : (int)kPhaseDone;
+    const bool act = i < n && phase != kPhaseDone;
+    const bool fin = i < n && busy != nullptr && phase == kPhaseDone && busy[i] != 0;
+    const int tiles = act ? jobs[i].ref->n_tiles : 0;
+    int incl = tiles;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const unsigned ma = __ballot_sync(0xffffffffu, act), md = __ballot_sync(0xffffffffu, fin);
+    if (lane == 31) s_tiles[w] = incl;
+    if (lane == 0) {
+      s_act[w] = __popc(ma);
+      s_done[w] = __popc(md);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int a = 0, t = 0, d = 0;
+      for (int k = 0; k < nw; k++) {
+        const int va = s_act[k], vt = s_tiles[k], vd = s_done[k];
+        s_act[k] = a;
+        s_tiles[k] = t;
+        s_done[k] = d;
+        a += va;
+        t += vt;
+        d += vd;
+      }
+      tot_a = a;
+      tot_t = t;
+      tot_d = d;
+    }
+    __syncthreads();
+    if (act) {
+      const int pos = base_a + s_act[w] + __popc(ma & lt);
+      active[pos] = i;
+      tile_prefix[pos] = base_t + s_tiles[w] + incl - tiles;
+    }
+    if (fin) {
+      done_list[base_d + s_done[w] + __popc(md & lt)] = i;
+      busy[i] = 0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      base_a += tot_a;
+      base_t += tot_t;
+      base_d += tot_d;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    *n_active = base_a;
+    tile_prefix[base_a] = base_t;
+    if (busy != nullptr) *n_done = base_d;
+  }
+}
+
+cudaError_t launch_compact(const Job* jobs_dev, int n_jobs, int* active, int* n_active, int* tile_prefix, int* busy,
+                           int* done_list, int* n_done, cudaStream_t s) {
+  compact_kernel<<<1, 1024, 0, s>>>(jobs_dev, n_jobs, active, n_active, tile_prefix, busy, done_list, n_done);
+  return cudaGetLastError();
+}
+
+// Zero start of a batched solve (the host-side init of the single-frame driver, on the device).
+__global__ void activate_kernel(const Job* __restrict__ jobs, const Activation* __restrict__ recs, int* busy) {
+  const Activation r = recs[blockIdx.x];
+  const Job& j = jobs[r.job];
+  const RefDev& R = *j.ref;
+  for (int i = threadIdx.x; i < R.P; i += blockDim.x) {
+    j.x[i] = 0.0;
+    j.g[i] = 0.0;
+    j.p[i] = 0.0;
+    j.gt[i] = 0.0;
+  }
+  for (int i = threadIdx.x; i < R.nD * kDParamF4; i += blockDim.x) j.dparams[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (threadIdx.x == 0) {
+    FrameState S{};
+    S.phase = kPhaseStartZero;
+    S.max_iter = r.max_iter > 0 ? r.max_iter : 100;
+    S.warm = r.warm;
+    S.use_warm = (r.use_warm != 0 && r.warm != nullptr) ? 1 : 0;
+    for (int c = 0; c < 3; c++) S.rigid[c] = r.rigid[c];
+    if (R.n_dim == 2) S.rigid[2] = 0.0;
+    *j.state = S;
+    busy[r.job] = 1;
+  }
+}
+
+cudaError_t launch_activate(const Job* jobs_dev, const Activation* recs, int n, int* busy, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  activate_kernel<<<n, 128, 0, s>>>(jobs_dev, recs, busy);
+  return cudaGetLastError();
+}
+
 }  // namespace fa

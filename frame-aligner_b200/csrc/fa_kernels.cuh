@@ -40,10 +40,21 @@ cudaError_t launch_downsample(const void* in, fa_dtype in_type, int nz, int ny, 
 cudaError_t launch_eval(const Job* jobs_dev, int n_jobs, int max_tiles, int n_dim, int frame_kind, bool ref_bf16,
                         cudaStream_t s, bool rows_multiple_of_4, int mb = 2);
 
-// Persistent fused pass over the compacted active list: grid CTAs walk the (active[a], tile) items
-// for a < *n_active (rows must be multiples of 4).
-cudaError_t launch_eval4_active(const Job* jobs_dev, const int* active, const int* n_active, int n_jobs, int max_tiles,
-                                int n_dim, int frame_kind, bool ref_bf16, int mb, int grid, cudaStream_t s);
+// Persistent fused pass over the compacted active list: grid CTAs walk the (active[a], tile) items,
+// item = tile_prefix[a] + tile for a < *n_active, so frames of different sizes share one launch
+// (rows must be multiples of 4). most_items bounds the grid.
+cudaError_t launch_eval4_active(const Job* jobs_dev, const int* active, const int* n_active, const int* tile_prefix,
+                                long long most_items, int n_dim, int frame_kind, bool ref_bf16, int mb, int grid,
+                                cudaStream_t s);
+
+// Rebuilds the active list of a job table (frames not done, ascending index), the exclusive prefix
+// sum of their tile counts (tile_prefix[*n_active] = items of the next fused pass), and, when busy is
+// non-null, appends frames that are done and still busy to done_list[*n_done...] and clears busy.
+cudaError_t launch_compact(const Job* jobs_dev, int n_jobs, int* active, int* n_active, int* tile_prefix, int* busy,
+                           int* done_list, int* n_done, cudaStream_t s);
+
+// Initialises the solve state of n frames (zero start, optional rigid and warm starts) and marks them busy.
+cudaError_t launch_activate(const Job* jobs_dev, const Activation* recs, int n, int* busy, cudaStream_t s);
 
 // Reduces one job's tile partials into result = [f, g(P)] (deterministic order).
 cudaError_t launch_reduce(const Job* job_dev, const RefDev& ref_host, cudaStream_t s);
@@ -54,9 +65,11 @@ cudaError_t launch_warp(const RefDev* ref_dev, const RefDev& ref_host, const voi
                         const float4* dparams, float invalid_value, float* out, cudaStream_t s);
 
 // One trust-region step for each job (grid = n_jobs): reduce partials, advance the state machine,
-// solve the next subproblem, write the next trial point's dparams.
-// max_nD / n_dim size the shared-memory staging (frames above about 200 KB work in global memory).
-cudaError_t launch_solve(const Job* jobs_dev, int n_jobs, int max_nD, int n_dim, cudaStream_t s);
+// solve the next subproblem, write the next trial point's dparams. With an active list, block b
+// serves jobs[active[b]] for b < *n_active. max_nD / n_dim size the shared-memory staging (frames
+// above about 200 KB work in global memory).
+cudaError_t launch_solve(const Job* jobs_dev, int n_jobs, int max_nD, int n_dim, cudaStream_t s,
+                         const int* active = nullptr, const int* n_active = nullptr);
 
 // Test hook: the device trust-region subproblem on given dense H (P x P) and g.
 cudaError_t launch_test_subproblem(const double* Hd, const double* Hl, int nD, int nd, const double* g,

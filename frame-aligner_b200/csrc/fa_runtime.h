@@ -1,0 +1,177 @@
+// fa_runtime.h -- host runtime state shared by the C ABI translation units (fa_api.cu, fa_server.cu):
+// the opaque handle types of include/fa_b200.h, device allocation under the context budget, error
+// reporting, and the helpers the serving loop reuses from the single-aligner path.
+#pragma once
+
+#include <cufft.h>
+
+#include <atomic>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "fa_kernels.cuh"
+
+namespace fa_rt {
+
+// Last error message of the calling thread (fa_last_error) and the count of this library's kernel
+// launches (fa_kernel_launches).
+extern thread_local std::string g_err;
+extern std::atomic<long long> g_launches;
+
+// Records msg as the calling thread's last error and returns s.
+fa_status fail(fa_status s, const std::string& msg);
+
+#define FA_CU(call)                                                                                       \
+  do {                                                                                                    \
+    cudaError_t e_ = (call);                                                                              \
+    if (e_ != cudaSuccess) return fa_rt::fail(FA_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define FA_TRY(call)            \
+  do {                          \
+    fa_status s_ = (call);      \
+    if (s_ != FA_OK) return s_; \
+  } while (0)
+
+struct Alloc {
+  void* p;
+  size_t n;
+};
+
+// Exact scan geometry, computed on the host in double with the reference's expressions
+// (FrameWarper.cpp:252-283), without per-voxel tables.
+struct Geometry {
+  int nz, ny, nx, nD, n_rows;
+  long long N;
+  std::vector<long long> scan_begin;  // first scan index of interval k (k = 0..nD-2)
+  std::vector<int> begin, end;        // storage D_range
+  std::vector<fa::RowDesc> rows;
+  float dq;
+  long long lmin;
+  int tile_rows, n_tiles;
+  std::vector<int> tile_c0;
+  std::vector<int2> ctrl_tiles;
+};
+
+}  // namespace fa_rt
+
+struct fa_context {
+  int device = 0;
+  int autotune = 0;
+  size_t budget = 0;
+  std::atomic<size_t> used{0};
+  std::mutex mu;
+};
+
+struct fa_reference {
+  fa_context* ctx = nullptr;
+  int nz = 0, ny = 0, nx = 0, nD = 0, n_dim = 0, P = 0;
+  long long N = 0;
+  fa_precision prec = FA_PREC_F32;
+  fa_scan_params scan{};
+  fa_rt::Geometry G;
+  int* tile_c0_dev = nullptr;
+  int2* ctrl_dev = nullptr;
+  std::vector<double> hd, hl;  // host copies of the Hessian blocks (diagonal, sub-diagonal)
+  fa::RefDev host{};
+  fa::RefDev* dev = nullptr;
+  cudaStream_t stream = nullptr;
+  std::vector<fa_rt::Alloc> allocs;
+  std::atomic<int> n_frames{0};
+};
+
+struct fa_frame {
+  fa_reference* ref = nullptr;
+  void* data = nullptr;
+  int kind = fa::kFrameF32;
+  cudaStream_t stream = nullptr;
+  fa::Job job{};
+  fa::Job* job_dev = nullptr;
+  fa::FrameState* state = nullptr;
+  double* h_result = nullptr;  // pinned: [f, g(P)]
+  float4* h_dparams = nullptr;  // pinned: nD * 3
+  double* h_x = nullptr;        // pinned: P
+  fa::FrameState* h_state = nullptr;  // pinned
+  float* warp_out = nullptr;
+  std::vector<double> lastD;
+  std::vector<double> last_g;
+  double last_f = 0;
+  bool have_last = false;
+  std::mutex mu;
+  std::vector<fa_rt::Alloc> allocs;
+};
+
+struct fa_correlator {
+  fa_context* ctx = nullptr;
+  int nz = 0, ny = 0, nx = 0;
+  long long n_el = 0, n_complex = 0;
+  int cap = 0;                          // frames per batched FFT
+  cufftHandle fwd = 0, inv = 0;         // batch of cap frames
+  cufftHandle fwd1 = 0, inv1 = 0;       // single frame
+  cudaStream_t stream = nullptr;
+  double* wy = nullptr;                 // square-root Hann window along y
+  double* wx = nullptr;                 // ... and along x (1 along z)
+  double* real = nullptr;               // cap * n_el
+  double2* spec = nullptr;              // cap * n_complex
+  double2* ref_conj = nullptr;          // n_complex
+  float* vol = nullptr;                 // one host-uploaded volume
+  const void** d_ptrs = nullptr;        // device array of input pointers
+  const void** h_ptrs = nullptr;        // pinned staging of the same
+  int ptr_cap = 0;
+  double* bval = nullptr;
+  long long* bidx = nullptr;
+  long long* d_idx = nullptr;           // one peak index per frame (ptr_cap)
+  long long* h_idx = nullptr;
+  int n_blocks = 0;                     // argmax blocks per frame
+  std::mutex mu;
+  std::vector<fa_rt::Alloc> allocs;
+  std::vector<fa_rt::Alloc> ptr_allocs;
+};
+
+struct fa_aligner {
+  fa_context* ctx = nullptr;
+  fa_aligner_params prm{};
+  fa_reference* ref = nullptr;
+  fa_correlator* corr = nullptr;
+  int nz = 0, ny = 0, nx = 0, nD = 0;
+  int dz = 0, dy = 0, dx = 0;  // downsampled dims
+  cudaStream_t stream = nullptr;
+  std::vector<fa_frame*> slots;
+  int slot_kind = -1;
+  void* staging = nullptr;     // raw frames copied from the host when they need a conversion pass
+  size_t staging_bytes = 0;
+  float* vols = nullptr;       // downsampled frames for the correlator (spatial_binning > 1)
+  size_t vols_count = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double last_ms = 0;
+  std::vector<fa_rt::Alloc> allocs;   // staging / vols
+  std::vector<fa_rt::Alloc> ref_allocs;
+  std::mutex mu;
+};
+
+namespace fa_rt {
+
+// cudaMalloc of bytes charged to the context's budget; the block is recorded in owner.
+fa_status dalloc(fa_context* ctx, size_t bytes, void** out, std::vector<Alloc>& owner);
+template <typename T>
+fa_status dalloc_t(fa_context* ctx, size_t count, T** out, std::vector<Alloc>& owner) {
+  void* p = nullptr;
+  FA_TRY(dalloc(ctx, count * sizeof(T), &p, owner));
+  *out = static_cast<T*>(p);
+  return FA_OK;
+}
+// Frees every block in owner and returns its bytes to the budget.
+void dfree_all(fa_context* ctx, std::vector<Alloc>& owner);
+
+size_t dtype_size(fa_dtype t);
+// Frame slot (zero-halo storage of the given FrameKind + solve buffers + stream) for reference R.
+fa_status frame_alloc(fa_reference* R, int kind, fa_frame** out);
+// Slot storage the aligner uses for frames of dtype (raw uint16 counts + 1, FP16 or FP32 values + 1).
+int slot_kind_for(const fa_aligner* A, fa_dtype dtype);
+// Window, D2Z, normalisation, Z2D and argmax for n device volumes; peak indices to C->d_idx[0..n).
+fa_status correlator_enqueue(fa_correlator* C, const void* const* vols, int in_kind, int n);
+// Peak index -> signed integer shift (x, y, z).
+void unravel_shift(const fa_correlator* C, long long idx, double* shift);
+
+}  // namespace fa_rt

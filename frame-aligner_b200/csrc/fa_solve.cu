@@ -296,7 +296,12 @@ __device__ void state_step(const Job& job, FrameState* S, const RefDev& R, const
         next = kPhaseStartRigid;
       } else {
         S->f = ft;
-        go_top = true;
+        if (S->use_warm && S->warm != nullptr) {
+          for (int i = 0; i < P; i++) p[i] = S->warm[i] - x[i];
+          next = kPhaseStartLast;
+        } else {
+          go_top = true;
+        }
       }
       break;
     }
@@ -311,6 +316,25 @@ __device__ void state_step(const Job& job, FrameState* S, const RefDev& R, const
         S->f = ft;
       } else {
         S->f = S->f_start;
+      }
+      if (S->use_warm && S->warm != nullptr) {
+        for (int i = 0; i < P; i++) p[i] = S->warm[i] - x[i];
+        next = kPhaseStartLast;
+      } else {
+        go_top = true;
+      }
+      break;
+    }
+    case kPhaseStartLast: {
+      // Warm start: the previous frame's solution as a fourth starting point after {0, 0, rigid};
+      // only a strictly smaller value replaces the current start (first minimum kept). The trial
+      // point was x + (warm - x), and that is the point taken.
+      if (ft < S->f) {
+        for (int i = 0; i < P; i++) {
+          x[i] = x[i] + p[i];
+          g[i] = gt[i];
+        }
+        S->f = ft;
       }
       go_top = true;
       break;
@@ -360,9 +384,12 @@ __device__ void state_step(const Job& job, FrameState* S, const RefDev& R, const
   S->phase = done ? kPhaseDone : next;
   }
 
-__global__ void __launch_bounds__(kSolveThreads, 1) solve_kernel(const Job* __restrict__ jobs, int smem_cap_doubles) {
+__global__ void __launch_bounds__(kSolveThreads, 1) solve_kernel(const Job* __restrict__ jobs, int smem_cap_doubles,
+                                                                 const int* __restrict__ active,
+                                                                 const int* __restrict__ n_active) {
   extern __shared__ double s_dyn[];
-  const Job& job = jobs[blockIdx.x];
+  if (active != nullptr && (int)blockIdx.x >= *n_active) return;
+  const Job& job = jobs[active != nullptr ? active[blockIdx.x] : blockIdx.x];
   FrameState* S = job.state;
   if (S->phase == kPhaseDone) return;
   const RefDev& R = *job.ref;
@@ -412,7 +439,17 @@ __global__ void __launch_bounds__(kSolveThreads, 1) solve_kernel(const Job* __re
     }
     __syncthreads();
   }
-  if (S->phase == kPhaseDone) return;
+  if (S->phase == kPhaseDone) {
+    // Finished in this step: report the state and parameters, and keep them as the warm start.
+    if (job.report != nullptr) {
+      if (threadIdx.x == 0) *static_cast<FrameState*>(job.report) = *S;
+      double* xr = reinterpret_cast<double*>(static_cast<char*>(job.report) + kReportHeaderBytes);
+      for (int i = threadIdx.x; i < P; i += blockDim.x) xr[i] = job.x[i];
+    }
+    if (S->warm != nullptr)
+      for (int i = threadIdx.x; i < P; i += blockDim.x) S->warm[i] = job.x[i];
+    return;
+  }
   // Next trial point D = x + p, as the fused pass's control-point parameters.
   for (int k = threadIdx.x; k < R.nD; k += blockDim.x) {
     double d[3], dn[3];
@@ -431,7 +468,8 @@ __global__ void __launch_bounds__(kSolveThreads, 1) solve_kernel(const Job* __re
   }
 }
 
-cudaError_t launch_solve(const Job* jobs_dev, int n_jobs, int max_nD, int n_dim, cudaStream_t s) {
+cudaError_t launch_solve(const Job* jobs_dev, int n_jobs, int max_nD, int n_dim, cudaStream_t s, const int* active,
+                         const int* n_active) {
   constexpr long long kCapBytes = 200 * 1024;
   long long need = solve_smem_doubles(max_nD, n_dim) * (long long)sizeof(double);
   int smem = need <= kCapBytes ? (int)need : 0;
@@ -439,7 +477,7 @@ cudaError_t launch_solve(const Job* jobs_dev, int n_jobs, int max_nD, int n_dim,
     cudaError_t e = cudaFuncSetAttribute(solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
   }
-  solve_kernel<<<n_jobs, kSolveThreads, smem, s>>>(jobs_dev, smem / (int)sizeof(double));
+  solve_kernel<<<n_jobs, kSolveThreads, smem, s>>>(jobs_dev, smem / (int)sizeof(double), active, n_active);
   return cudaGetLastError();
 }
 

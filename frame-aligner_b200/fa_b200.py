@@ -24,6 +24,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libfa_b200.so")
 
 FA_OK = 0
+(FA_ERR_BAD_ARG, FA_ERR_OOM, FA_ERR_CUDA, FA_ERR_TIMEOUT, FA_ERR_UNSUPPORTED, FA_ERR_NOT_FOUND, FA_ERR_STATE,
+ FA_ERR_BUSY) = range(1, 9)
 STATUS = {0: "ok", 1: "bad argument", 2: "out of memory", 3: "CUDA error", 4: "timeout", 5: "unsupported",
           6: "not found", 7: "bad state", 8: "busy"}
 F32, F16, BF16, U16 = 0, 1, 2, 3
@@ -67,6 +69,25 @@ class AlignerParams(C.Structure):
         ("precision", C.c_int),
         ("max_iterations", C.c_int),
     ]
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("memory_budget", C.c_size_t), ("max_in_flight", C.c_int), ("iterations_per_launch", C.c_int),
+                ("warm_start", C.c_int)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_longlong), ("completed", C.c_longlong), ("failed", C.c_longlong),
+        ("in_flight", C.c_longlong), ("peak_in_flight", C.c_longlong),
+        ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("max_ms", C.c_double),
+        ("frames_per_s", C.c_double),
+        ("slot_bytes", C.c_size_t), ("peak_slot_bytes", C.c_size_t),
+        ("graph_launches", C.c_longlong),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class AlignStats(C.Structure):
@@ -128,6 +149,15 @@ SIGNATURES = {
     "fa_aligner_info": [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)],
     "fa_aligner_add_frames": [_vp, _vp, C.c_int, C.c_int, _f64p, _vp],
     "fa_aligner_add_frames_device": [_vp, _vp, C.c_int, C.c_int, _f64p, _vp],
+    "fa_server_create": [_vp, C.POINTER(ServerConfig), C.POINTER(_vp)],
+    "fa_server_destroy": [_vp],
+    "fa_server_add_acquisition": [_vp, C.POINTER(AlignerParams), _vp, C.c_int, C.c_int, C.c_int, C.c_int,
+                                  C.POINTER(ScanParams), C.c_int, C.POINTER(C.c_int)],
+    "fa_server_acquisition_info": [_vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)],
+    "fa_server_submit": [_vp, C.c_int, _vp, C.c_int, C.POINTER(C.c_ulonglong)],
+    "fa_server_wait": [_vp, C.c_ulonglong, C.c_double, _vp, _vp, C.POINTER(C.c_double)],
+    "fa_server_get_stats": [_vp, C.POINTER(ServerStats)],
+    "fa_server_reset_stats": [_vp],
     "fa_get_error_jacobian_static": [_vp, _vp, C.c_int, _f64p, C.POINTER(C.c_double), _f64p],
     "fa_kernel_launches": [],
     "fa_aligner_last_device_ms": [_vp, C.POINTER(C.c_double)],
@@ -412,6 +442,86 @@ class Aligner:
         if getattr(self, "_h", None) and self._h.value:
             lib().fa_aligner_destroy(self._h)
             self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """The serving loop (fa_server_*): several acquisitions, frames submitted asynchronously and
+    solved with continuous batching on the device."""
+
+    def __init__(self, ctx: Context, memory_budget=0, max_in_flight=0, iterations_per_launch=0, warm_start=True):
+        self.ctx = ctx
+        self._h = _vp()
+        lag = int(warm_start)  # True -> 1 (the previous frame), False -> 0, d -> frame k - d
+        cfg = ServerConfig(memory_budget, max_in_flight, iterations_per_launch, lag)
+        check(lib().fa_server_create(ctx._h, C.byref(cfg), C.byref(self._h)))
+        self.acqs = {}
+        self._keep = {}  # host frames referenced by outstanding tickets
+
+    def add_acquisition(self, reference, scan: ScanParams, frame_dtype=np.uint16, spatial_binning=1, nD=0,
+                        n_resampling_points=30, precision=PREC_MIXED, max_iterations=100):
+        ref = np.ascontiguousarray(reference)
+        if ref.dtype not in (np.float32, np.uint16):
+            ref = ref.astype(np.float32)
+        if ref.ndim == 2:
+            ref = ref[None]
+        prm = AlignerParams(spatial_binning, n_resampling_points, nD, 0.0, precision, max_iterations)
+        a = C.c_int()
+        check(lib().fa_server_add_acquisition(self._h, C.byref(prm), ref.ctypes.data, _DTYPES[ref.dtype], *ref.shape,
+                                              C.byref(scan), _DTYPES[np.dtype(frame_dtype)], C.byref(a)))
+        nD_, nd = C.c_int(), C.c_int()
+        check(lib().fa_server_acquisition_info(self._h, a.value, C.byref(nD_), C.byref(nd)))
+        self.acqs[a.value] = {"dims": ref.shape, "nD": nD_.value, "n_dim": nd.value,
+                              "dtype": np.dtype(frame_dtype)}
+        return a.value
+
+    def submit(self, acquisition, frame):
+        """Queues a host frame (kept referenced until its result is collected); returns the ticket."""
+        info = self.acqs[acquisition]
+        arr = np.ascontiguousarray(frame, dtype=info["dtype"])
+        if arr.size != int(np.prod(info["dims"])):
+            raise ValueError(f"frame has {arr.size} elements, the acquisition's volume {info['dims']}")
+        t = C.c_ulonglong()
+        check(lib().fa_server_submit(self._h, acquisition, arr.ctypes.data, 0, C.byref(t)))
+        self._keep[t.value] = (acquisition, arr)
+        return t.value
+
+    def submit_ptr(self, acquisition, ptr, on_device):
+        """Queues a frame at a raw address (device memory when on_device); the caller keeps it valid."""
+        t = C.c_ulonglong()
+        check(lib().fa_server_submit(self._h, acquisition, ptr, 1 if on_device else 0, C.byref(t)))
+        self._keep[t.value] = (acquisition, None)
+        return t.value
+
+    def wait(self, ticket, timeout_s=-1.0):
+        """Returns (D (nD x 3), stats dict, latency ms) of a ticket."""
+        acq, _ = self._keep[ticket]
+        D = np.empty((self.acqs[acq]["nD"], 3), np.float64)
+        st = AlignStats()
+        lat = C.c_double()
+        check(lib().fa_server_wait(self._h, ticket, timeout_s, D.ctypes.data, C.cast(C.byref(st), _vp),
+                                   C.byref(lat)))
+        del self._keep[ticket]
+        return D, st.as_dict(), lat.value
+
+    def stats(self):
+        s = ServerStats()
+        check(lib().fa_server_get_stats(self._h, C.byref(s)))
+        return s.as_dict()
+
+    def reset_stats(self):
+        check(lib().fa_server_reset_stats(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().fa_server_destroy(self._h)
+            self._h = _vp()
+            self._keep.clear()
 
     def __del__(self):
         try:

@@ -167,6 +167,32 @@ def config2_acquisitions(n_per_size=64, seed=2000):
     return out
 
 
+# Served stream: eight concurrent acquisitions of different sizes.
+CONFIG3_SHAPES = [(1, 256, 256), (1, 512, 512), (8, 512, 512), (16, 512, 512), (1, 1024, 1024), (32, 256, 256),
+                  (32, 512, 512), (4, 1024, 1024)]
+
+
+def config3_nD(shape):
+    """Control points scale with the lines of a plane (16 per 256 lines), at least 2 per plane of a
+    stack (so that processScanParameters keeps the inter-plane gap), at most 64."""
+    nz, ny, _ = shape
+    return int(min(64, max(16 * ny // 256, 2 * nz if nz > 1 else 0)))
+
+
+def config3_acquisitions(n_frames=8, seed=3000, shapes=None):
+    """The served-stream acquisitions: each its own blob reference; the displacement walk continues
+    across consecutive frames (the case a warm start from the previous solution serves)."""
+    out = []
+    for j, shape in enumerate(shapes or CONFIG3_SHAPES):
+        nz, ny, nx = shape
+        nblobs = int(200 * ny * nx / 65536 * (1 if nz == 1 else max(1, nz // 4)))
+        out.append(make_acquisition(shape, config3_nD(shape), n_frames,
+                                    BlobSpec(nblobs, (2.0, 6.0), (1.0, 2.0) if nz > 1 else (1.0, 1.0), mean=20.0),
+                                    WalkSpec(1.0, 8.0, 0.3 if nz > 1 else 0.0, 2.0 if nz > 1 else 0.0),
+                                    seed=seed + j, continue_walk=True))
+    return out
+
+
 def make_config(cfg: dict, n_frames=None, shape=None, **kw) -> Acquisition:
     c = dict(cfg)
     if n_frames is not None:

@@ -226,6 +226,61 @@ fa_status fa_aligner_add_frames(fa_aligner* a, const void* const* frames, fa_dty
 fa_status fa_aligner_add_frames_device(fa_aligner* a, const void* const* frames, fa_dtype dtype, int n,
                                        double* D_out, fa_align_stats* stats);
 
+/* ---------------------------------------------------------------- serving ---------------------- */
+
+/* A device-resident request loop over several concurrent acquisitions (no single counterpart in the
+   reference: each acquisition is one FrameWarpAligner, FrameAligner/FrameWarpAligner.cpp:77-251,
+   whose addFrame calls the MEX pool issues from many threads, FrameAlignerMex.cpp:120). Each
+   acquisition keeps its reference, gradient, Hessian, correlator and last solution on the device.
+   Frames submitted from any thread are admitted into device slots as slot count and memory budget
+   allow, uploaded and phase-correlated on the acquisition's stream, and then solved together with
+   every other admitted frame of the same dimensionality and storage, one CUDA graph of
+   iterations_per_launch x (fused pass, trust-region step) per launch, while later frames upload and
+   correlate. A frame's result does not depend on which other frames share its launches. */
+typedef struct fa_server fa_server;
+
+typedef struct {
+  size_t memory_budget;       /* device bytes frame slots may hold (0: 40 GiB) */
+  int max_in_flight;          /* frames admitted and not finished, all acquisitions (0: 256) */
+  int iterations_per_launch;  /* trust-region iterations per graph launch (0: 2) */
+  int warm_start;             /* lag d >= 1: frame k's starting points are {0, 0, rigid, the solution of
+                                 frame k - d of the same acquisition} (d = 1: the previous frame), and
+                                 frame k starts its solve after frame k - d finished, so at most d frames
+                                 of an acquisition solve at once; 0: no warm start (at most 64) */
+} fa_server_config;
+
+typedef struct {
+  long long submitted, completed, failed;
+  long long in_flight, peak_in_flight;
+  double p50_ms, p99_ms, mean_ms, max_ms;  /* per-frame latency: submission -> result on the host */
+  double frames_per_s;                     /* completed / (last completion - first submission) */
+  size_t slot_bytes, peak_slot_bytes;      /* device bytes held by frame slots */
+  long long graph_launches;
+} fa_server_stats;
+
+fa_status fa_server_create(fa_context* ctx, const fa_server_config* cfg, fa_server** out);
+/* Finishes every submitted frame, then releases the server and its acquisitions. */
+fa_status fa_server_destroy(fa_server* s);
+/* FrameWarpAligner::setReference for a new acquisition (reference: host memory, nz*ny*nx elements of
+   reference_dtype, FA_F32 or FA_U16); its frames will be frame_dtype (FA_F32 or FA_U16). */
+fa_status fa_server_add_acquisition(fa_server* s, const fa_aligner_params* params, const void* reference,
+                                    fa_dtype reference_dtype, int nz, int ny, int nx, const fa_scan_params* scan,
+                                    fa_dtype frame_dtype, int* acquisition);
+fa_status fa_server_acquisition_info(fa_server* s, int acquisition, int* nD, int* n_dim);
+/* FrameWarpAligner::addFrame, asynchronous: queues one raw frame (host memory, or device memory when
+   frame_on_device) and returns its ticket. The frame's memory must stay valid and unchanged until its
+   result has been collected; page-locked host memory lets the upload overlap other work. */
+fa_status fa_server_submit(fa_server* s, int acquisition, const void* frame, int frame_on_device,
+                           unsigned long long* ticket);
+/* Waits up to timeout_s seconds (< 0: no limit) for a ticket's result and collects it: D_out nD*3
+   doubles, stats and latency_ms may be NULL. FA_ERR_TIMEOUT leaves the result to a later call;
+   FA_ERR_NOT_FOUND means the ticket is unknown or already collected. */
+fa_status fa_server_wait(fa_server* s, unsigned long long ticket, double timeout_s, double* D_out,
+                         fa_align_stats* stats, double* latency_ms);
+fa_status fa_server_get_stats(fa_server* s, fa_server_stats* out);
+/* Clears the latency record and counters (not the acquisitions or their warm starts). */
+fa_status fa_server_reset_stats(fa_server* s);
+
 /* ---------------------------------------------------------------- static-scratch evaluation --- */
 
 /* No counterpart in the reference. For callers that cannot call cudaMalloc when they evaluate a

@@ -536,6 +536,11 @@ static void model_g(void* ctx, const double* x, double* g) {
 
 int or_align_frame(const or_warper* w, const float* frame, const double* rigid_shift, int max_iter, double* D_out,
                    or_tr_stats* st) {
+  return or_align_frame_warm(w, frame, rigid_shift, NULL, max_iter, D_out, st);
+}
+
+int or_align_frame_warm(const or_warper* w, const float* frame, const double* rigid_shift, const double* warm_D,
+                        int max_iter, double* D_out, or_tr_stats* st) {
   int nd = w->n_dim, nD = w->nD, P = nD * nd;
   or_model m;
   memset(&m, 0, sizeof(m));
@@ -556,6 +561,19 @@ int or_align_frame(const or_warper* w, const float* frame, const double* rigid_s
     if (fe[s] < fe[best]) best = s;
   double* x = (double*)malloc(sizeof(double) * (size_t)P);
   memcpy(x, start[best], sizeof(double) * (size_t)P);
+  if (warm_D) {
+    /* Warm start (the serving loop's extension): the previous frame's solution is a fourth
+       candidate, reached as x + (warm - x) from the chosen start and kept only if strictly better. */
+    double* t = (double*)malloc(sizeof(double) * (size_t)P);
+    for (int k = 0; k < nD; k++)
+      for (int c = 0; c < nd; c++) {
+        int i = k * nd + c;
+        double p = warm_D[3 * k + c] - x[i];
+        t[i] = x[i] + p;
+      }
+    if (model_f(&m, t) < fe[best]) memcpy(x, t, sizeof(double) * (size_t)P);
+    free(t);
+  }
   or_tr_stats local;
   if (!st) st = &local;
   int rc = or_trust_region(P, w->H, x, 40.0, 1e-8, max_iter, model_f, model_g, &m, st);

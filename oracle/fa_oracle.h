@@ -98,6 +98,11 @@ int or_tr_subproblem(int P, const double* H, const double* g, double radius, dou
    D_out = nD x 3 doubles. */
 int or_align_frame(const or_warper* w, const float* frame, const double* rigid_shift, int max_iter, double* D_out,
                    or_tr_stats* st);
+/* or_align_frame plus the serving loop's warm start: warm_D (nD x 3, or NULL) is a fourth starting
+   point after {0, 0, rigid}, reached as x + (warm - x) from the chosen start and taken only if its
+   value is strictly smaller. */
+int or_align_frame_warm(const or_warper* w, const float* frame, const double* rigid_shift, const double* warm_D,
+                        int max_iter, double* D_out, or_tr_stats* st);
 /* The reference's threading model: frames spread over n_threads workers, one frame per worker
    at a time. frames = n_frames * N floats; D_out = n_frames * nD * 3. Returns 0 on success. */
 int or_align_frames_mt(const or_warper* w, const float* frames, int n_frames, const double* rigid_shifts,

@@ -83,6 +83,7 @@ def lib():
         L.or_correlation.argtypes = [_f32p, _f32p, _u8p, C.c_long]
         L.or_tr_subproblem.argtypes = [C.c_int, _f64p, _f64p, C.c_double, C.c_double, C.c_int, _f64p]
         L.or_align_frame.argtypes = [C.c_void_p, _f32p, _f64p, C.c_int, _f64p, C.POINTER(OrStats)]
+        L.or_align_frame_warm.argtypes = [C.c_void_p, _f32p, _f64p, C.c_void_p, C.c_int, _f64p, C.POINTER(OrStats)]
         L.or_align_frames_mt.argtypes = [C.c_void_p, _f32p, C.c_int, _f64p, C.c_int, C.c_int, _f64p, _i32p]
         _lib = L
     return _lib
@@ -212,10 +213,16 @@ class OracleWarper:
         lib().or_warp_point(self._h, _c64(D).ravel(), x, y, z, spatial_binning, out)
         return out
 
-    def align_frame(self, frame, rigid_shift=(0.0, 0.0, 0.0), max_iter=100):
+    def align_frame(self, frame, rigid_shift=(0.0, 0.0, 0.0), max_iter=100, warm=None):
+        """or_align_frame; warm (nD x 3) adds the previous frame's solution as a fourth start."""
         D = np.empty((self.nD, 3), np.float64)
         st = OrStats()
-        lib().or_align_frame(self._h, _c32(frame).ravel(), _c64(rigid_shift), max_iter, D, C.byref(st))
+        if warm is None:
+            lib().or_align_frame(self._h, _c32(frame).ravel(), _c64(rigid_shift), max_iter, D, C.byref(st))
+        else:
+            w = _c64(warm).ravel()
+            lib().or_align_frame_warm(self._h, _c32(frame).ravel(), _c64(rigid_shift), w.ctypes.data, max_iter, D,
+                                      C.byref(st))
         return D, st
 
     def align_frames_mt(self, frames, rigid_shifts, n_threads, max_iter=100):

@@ -122,3 +122,24 @@ def test_live_against_reference_build(seed):
     assert np.array_equal(ow.get_jacobian(fr, D), rw.get_jacobian(D))
     assert np.array_equal(ow.hessian(), rw.hessian())
     assert np.array_equal(ow.warp_interpolated(fr, D, 0), rw.warp_interpolated(D, 0))
+
+
+def test_warm_start_candidate():
+    """The serving loop's fourth starting point: a candidate worse than {0, 0, rigid} is not taken
+    (the solve is then bit-identical to the cold one); the frame's own solution as the candidate is
+    taken and the solve stays there (within the 1e-8 stop rule's reach)."""
+    import fa_synth as S
+
+    acq = S.make_acquisition((1, 96, 96), 8, 1, S.BlobSpec(40, (2.0, 6.0), (1.0, 1.0), mean=20.0),
+                             S.WalkSpec(1.0, 3.0), seed=5)
+    nz, ny, nx = acq.reference.shape
+    line, il, ifr = acq.scan
+    ow = O.OracleWarper(acq.reference + 1, acq.nD, O.scan_init(line, il, ifr, nx, ny, nz))
+    frame = acq.frames[0] + 1
+    shift = O.phase_shift(acq.reference, acq.frames[0])
+    cold, st_cold = ow.align_frame(frame, shift, 100)
+    far, _ = ow.align_frame(frame, shift, 100, warm=cold + 40.0)
+    assert np.array_equal(far, cold)
+    again, st_again = ow.align_frame(frame, shift, 100, warm=cold)
+    assert np.sqrt(((again - cold)[:, :2] ** 2).sum(-1).mean()) <= 1e-3
+    assert st_again.iterations <= st_cold.iterations
