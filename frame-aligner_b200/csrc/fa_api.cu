@@ -533,6 +533,9 @@ fa_status reference_setup(fa_reference* R, const float* src, bool src_device) {
   FA_CU(cudaMemcpyAsync(R->hd.data(), Hd, R->hd.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
   FA_CU(cudaMemcpyAsync(R->hl.data(), Hl, R->hl.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
   FA_CU(cudaStreamSynchronize(s));
+  fa::band_bounds(R->hd.data(), R->hl.data(), R->nD, R->n_dim, &h.h_inf, &h.h_mindiag);
+  FA_CU(cudaMemcpyAsync(R->dev, &h, sizeof(RefDev), cudaMemcpyHostToDevice, s));
+  FA_CU(cudaStreamSynchronize(s));
   dfree_all(ctx, tmp);
   if (ctx->autotune && R->nx % 4 == 0) FA_TRY(autotune(R));
   return FA_OK;
@@ -1324,7 +1327,9 @@ extern "C" fa_status fa_test_tr_subproblem(fa_context* ctx, int nD, int n_dim, c
   cudaError_t e = cudaMemcpy(dHd, hd.data(), hd.size() * sizeof(double), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(dHl, hl.data(), hl.size() * sizeof(double), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(dg, g, (size_t)P * sizeof(double), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = fa::launch_test_subproblem(dHd, dHl, nD, n_dim, dg, radius, dp, db, work, 0);
+  double hinf, mindiag;
+  fa::band_bounds(hd.data(), hl.data(), nD, n_dim, &hinf, &mindiag);
+  if (e == cudaSuccess) e = fa::launch_test_subproblem(dHd, dHl, nD, n_dim, hinf, mindiag, dg, radius, dp, db, work, 0);
   if (e == cudaSuccess) e = cudaMemcpy(p, dp, (size_t)P * sizeof(double), cudaMemcpyDeviceToHost);
   if (e == cudaSuccess) e = cudaMemcpy(on_boundary, db, sizeof(int), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return done(fail(FA_ERR_CUDA, std::string("subproblem: ") + cudaGetErrorString(e)));

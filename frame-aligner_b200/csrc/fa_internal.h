@@ -98,7 +98,37 @@ struct RefDev {
   const __nv_bfloat16* gz16;
   const double* Hd;  // nD blocks of n_dim x n_dim (diagonal), row-major
   const double* Hl;  // nD blocks (block k couples k and k-1; block 0 unused)
+  double h_inf;      // max_i sum_j |H_ij| (ascending j), the subproblem's bracket bound
+  double h_mindiag;  // min_i H_ii
 };
+
+// h_inf and h_mindiag of a block-tridiagonal H from its blocks (host), summing |H_ij| over ascending
+// j within the band like the dense loop over all j (whose other terms are exact zeros).
+inline void band_bounds(const double* Hd, const double* Hl, int nD, int nd, double* h_inf, double* h_mindiag) {
+  const int P = nD * nd, nn = nd * nd;
+  double hinf = 0.0, mind = Hd[0];
+  for (int i = 0; i < P; i++) {
+    const int b = i / nd, a = i % nd;
+    const int j0 = b > 0 ? (b - 1) * nd : 0, j1 = (b + 2) * nd < P ? (b + 2) * nd : P;
+    double r = 0.0;
+    for (int j = j0; j < j1; j++) {
+      const int bj = j / nd, c = j % nd;
+      double v;
+      if (bj == b)
+        v = Hd[b * nn + a * nd + c];
+      else if (bj + 1 == b)
+        v = Hl[b * nn + a * nd + c];
+      else
+        v = Hl[bj * nn + c * nd + a];
+      r += v < 0 ? -v : v;
+    }
+    if (r > hinf) hinf = r;
+    const double d = Hd[b * nn + a * nd + a];
+    if (d < mind) mind = d;
+  }
+  *h_inf = hinf;
+  *h_mindiag = mind;
+}
 
 // One frame in a fused pass / solve launch.
 // Zero halo around every frame slot: taps that leave the volume read these zeros, which is the

@@ -72,8 +72,9 @@ cudaError_t launch_solve(const Job* jobs_dev, int n_jobs, int max_nD, int n_dim,
                          const int* active = nullptr, const int* n_active = nullptr);
 
 // Test hook: the device trust-region subproblem on given dense H (P x P) and g.
-cudaError_t launch_test_subproblem(const double* Hd, const double* Hl, int nD, int nd, const double* g,
-                                   double radius, double* p_out, int* boundary_out, double* work, cudaStream_t s);
+cudaError_t launch_test_subproblem(const double* Hd, const double* Hl, int nD, int nd, double hinf, double mindiag,
+                                   const double* g, double radius, double* p_out, int* boundary_out, double* work,
+                                   cudaStream_t s);
 
 // Phase correlation kernels (fa_phase.cu), each over a batch of frames.
 cudaError_t launch_phase_window(const void* const* vols, int in_kind, const double* wy, const double* wx, int ny,

@@ -30,19 +30,8 @@ struct Band {
   const double* Hd;
   const double* Hl;
   int nD, P;
+  double hinf, mindiag;  // band_bounds of H
 };
-
-// Element (i, j) of the dense Hessian.
-template <int ND>
-__device__ __forceinline__ double hval(const Band<ND>& B, int i, int j) {
-  const int bi = i / B.nd, bj = j / B.nd;
-  const int a = i - bi * B.nd, b = j - bj * B.nd;
-  const int nn = B.nd * B.nd;
-  if (bi == bj) return B.Hd[bi * nn + a * B.nd + b];
-  if (bi == bj + 1) return B.Hl[bi * nn + a * B.nd + b];
-  if (bj == bi + 1) return B.Hl[bj * nn + b * B.nd + a];
-  return 0.0;
-}
 
 // Band factor storage: row i of block b holds 2*n_dim entries, the columns of block b-1 then those of
 // block b.
@@ -170,17 +159,7 @@ __device__ int subproblem(const Band<ND>& B, const double* g, double radius, dou
     for (int i = 0; i < P; i++) p[i] = 0.0;
     return 0;
   }
-  double hinf = 0, mindiag = hval(B, 0, 0);
-  for (int i = 0; i < P; i++) {
-    double r = 0;
-    int j0 = (i / B.nd - 1) * B.nd, j1 = (i / B.nd + 2) * B.nd;
-    if (j0 < 0) j0 = 0;
-    if (j1 > P) j1 = P;
-    for (int j = j0; j < j1; j++) r += fabs(hval(B, i, j));
-    if (r > hinf) hinf = r;
-    const double d = hval(B, i, i);
-    if (d < mindiag) mindiag = d;
-  }
+  const double hinf = B.hinf, mindiag = B.mindiag;
   double lam_hi = gnorm / radius + hinf;
   double lam_lo = gnorm / radius - hinf;
   if (-mindiag > lam_lo) lam_lo = -mindiag;
@@ -231,18 +210,33 @@ __device__ int subproblem(const Band<ND>& B, const double* g, double radius, dou
   return boundary;
 }
 
-// Predicted reduction -(g.p + 0.5 p.H.p) with the dense algorithm's summation order.
+// Predicted reduction -(g.p + 0.5 p.H.p) with the dense algorithm's summation order: row i of H p
+// sums over ascending j within the band (blocks b-1, b, b+1 of row block b).
 template <int ND>
 __device__ double predicted(const Band<ND>& B, const double* g, const double* p) {
+  constexpr int NN = ND * ND;
   double gp = 0, pHp = 0;
-  for (int i = 0; i < B.P; i++) {
-    double s = 0;
-    int j0 = (i / B.nd - 1) * B.nd, j1 = (i / B.nd + 2) * B.nd;
-    if (j0 < 0) j0 = 0;
-    if (j1 > B.P) j1 = B.P;
-    for (int j = j0; j < j1; j++) s += hval(B, i, j) * p[j];
-    gp += g[i] * p[i];
-    pHp += p[i] * s;
+  for (int b = 0; b < B.nD; b++) {
+    const double* hl0 = B.Hl + b * NN;        // block (b, b-1)
+    const double* hd = B.Hd + b * NN;         // block (b, b)
+    const double* hl1 = B.Hl + (b + 1) * NN;  // block (b+1, b), read transposed
+#pragma unroll
+    for (int a = 0; a < ND; a++) {
+      const int i = b * ND + a;
+      double s = 0;
+      if (b > 0) {
+#pragma unroll
+        for (int c = 0; c < ND; c++) s += hl0[a * ND + c] * p[(b - 1) * ND + c];
+      }
+#pragma unroll
+      for (int c = 0; c < ND; c++) s += hd[a * ND + c] * p[b * ND + c];
+      if (b + 1 < B.nD) {
+#pragma unroll
+        for (int c = 0; c < ND; c++) s += hl1[c * ND + a] * p[(b + 1) * ND + c];
+      }
+      gp += g[i] * p[i];
+      pHp += p[i] * s;
+    }
   }
   return -(gp + 0.5 * pHp);
 }
@@ -276,7 +270,7 @@ template <int ND>
 __device__ void state_step(const Job& job, FrameState* S, const RefDev& R, const double* Hd, const double* Hl,
                            double* gv, double* pv, double* work, double ft) {
   const int P = R.P, nd = ND;
-  Band<ND> B{Hd, Hl, R.nD, P};
+  Band<ND> B{Hd, Hl, R.nD, P, R.h_inf, R.h_mindiag};
   double* x = job.x;
   double* g = gv;
   double* p = pv;
@@ -481,22 +475,24 @@ cudaError_t launch_solve(const Job* jobs_dev, int n_jobs, int max_nD, int n_dim,
   return cudaGetLastError();
 }
 
-__global__ void test_subproblem_kernel(const double* Hd, const double* Hl, int nD, int nd, const double* g,
-                                       double radius, double* p, int* boundary, double* work) {
+__global__ void test_subproblem_kernel(const double* Hd, const double* Hl, int nD, int nd, double hinf,
+                                       double mindiag, const double* g, double radius, double* p, int* boundary,
+                                       double* work) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   // work: P*(2*nd) + 3*P doubles
   if (nd == 3) {
-    Band<3> B{Hd, Hl, nD, nD * 3};
+    Band<3> B{Hd, Hl, nD, nD * 3, hinf, mindiag};
     *boundary = subproblem(B, g, radius, 0.1, 20, p, work);
   } else {
-    Band<2> B{Hd, Hl, nD, nD * 2};
+    Band<2> B{Hd, Hl, nD, nD * 2, hinf, mindiag};
     *boundary = subproblem(B, g, radius, 0.1, 20, p, work);
   }
 }
 
-cudaError_t launch_test_subproblem(const double* Hd, const double* Hl, int nD, int nd, const double* g,
-                                   double radius, double* p_out, int* boundary_out, double* work, cudaStream_t s) {
-  test_subproblem_kernel<<<1, 32, 0, s>>>(Hd, Hl, nD, nd, g, radius, p_out, boundary_out, work);
+cudaError_t launch_test_subproblem(const double* Hd, const double* Hl, int nD, int nd, double hinf, double mindiag,
+                                   const double* g, double radius, double* p_out, int* boundary_out, double* work,
+                                   cudaStream_t s) {
+  test_subproblem_kernel<<<1, 32, 0, s>>>(Hd, Hl, nD, nd, hinf, mindiag, g, radius, p_out, boundary_out, work);
   return cudaGetLastError();
 }
 
