@@ -57,6 +57,7 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="length of the Poisson arrival stream")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="total arrivals per second")
     ap.add_argument("--serve-pool", type=int, default=6, help="distinct frames per served acquisition")
+    ap.add_argument("--serve-slots", type=int, default=24, help="frame slots reserved per served acquisition")
     ap.add_argument("--serve-lags", type=int, nargs="+", default=[1, 4],
                     help="warm-start lags to serve with (1 = the previous frame's solution)")
     return ap.parse_args()
@@ -231,7 +232,9 @@ def measure_serving(fa, ctx, args, acqs, pools, lag):
         ids.append(srv.add_acquisition(a.reference, fa.scan_params(line, il, ifr, nx, ny, nz), frame_dtype=np.uint16,
                                        nD=a.nD, precision=fa.PREC_MIXED))
     n_acq = len(acqs)
-    # warm-up: every acquisition's pool once (graphs, slots, cuFFT plans)
+    for i in ids:  # frame slots created before the stream (each admitted frame holds one)
+        srv.reserve(i, args.serve_slots)
+    # warm-up: every acquisition's pool once (graphs, cuFFT plans)
     warm = [srv.submit_ptr(ids[j], pools[j][k].data_ptr(), False) for k in range(args.serve_pool)
             for j in range(n_acq)]
     for t in warm:

@@ -60,6 +60,15 @@ struct SrvResult {
 struct SrvClass;
 struct SrvAcq;
 
+// fa_server_reserve's request to the worker.
+struct SrvReserve {
+  int acq = -1;
+  int n = 0;
+  bool done = false;
+  fa_status status = FA_OK;
+  std::string error;
+};
+
 struct SrvSlot {
   SrvAcq* acq = nullptr;
   fa_frame* F = nullptr;      // zero-halo frame storage + solve buffers
@@ -84,6 +93,7 @@ struct SrvAcq {
   std::deque<SrvRequest> pending;
   std::vector<SrvSlot*> idle;
   int n_busy = 0;            // admitted, not finished
+  int n_slots = 0;           // slots that exist (busy or idle)
   long long next_seq = 0;
   std::unordered_set<long long> finished;  // warm start: finished frames whose successor has not started
   std::map<long long, SrvSlot*> ready;      // correlated, waiting to start (by sequence number)
@@ -136,6 +146,7 @@ struct fa_server {
   bool wake = false;
   bool stop = false;
   std::deque<SrvRequest> inbox;
+  std::deque<SrvReserve*> reserves;
   std::vector<std::unique_ptr<SrvAcq>> acqs;
   std::unordered_map<unsigned long long, SrvResult> results;
   std::unordered_set<unsigned long long> outstanding;
@@ -257,6 +268,7 @@ fa_status attach(fa_server* S, SrvAcq* q) {
   SrvClass* C = nullptr;
   for (auto& c : S->classes)
     if (c->n_dim == R->n_dim && c->kind == q->kind && c->bf16 == bf16 && c->vec4 == vec4) C = c.get();
+  if (!S->cfg.shared_launches) C = nullptr;  // one launch group per acquisition
   if (!C) FA_TRY(class_create(S, R->n_dim, q->kind, bf16, vec4, &C));
   q->cls = C;
   C->acqs.push_back(q);
@@ -331,6 +343,7 @@ fa_status slot_destroy(fa_server* S, SrvSlot* sl) {
   dfree_all(S->ctx, sl->allocs);
   if (sl->report) cudaFreeHost(sl->report);
   S->slot_bytes -= sl->bytes;
+  if (sl->bytes) sl->acq->n_slots--;
   for (auto it = S->slots.begin(); it != S->slots.end(); ++it)
     if (it->get() == sl) {
       S->slots.erase(it);
@@ -373,6 +386,7 @@ fa_status slot_create(fa_server* S, SrvAcq* q, SrvSlot** out) {
   for (const Alloc& a : sl->allocs) bytes += a.n;
   sl->bytes = bytes;
   S->slot_bytes += bytes;
+  q->n_slots++;
   sl->index = C->free_idx.back();
   C->free_idx.pop_back();
   C->owner[sl->index] = sl;
@@ -637,6 +651,54 @@ bool worker_idle(const fa_server* S) {
   return true;
 }
 
+// Creates the idle slots fa_server_reserve asked for (within the budget; no eviction).
+fa_status serve_reserves(fa_server* S) {
+  std::deque<SrvReserve*> todo;
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    // requests for acquisitions this pass has not attached yet wait for the next pass
+    std::deque<SrvReserve*> later;
+    for (SrvReserve* r : S->reserves) {
+      if (r->acq < (int)S->wacqs.size() && S->wacqs[r->acq]->cls)
+        todo.push_back(r);
+      else
+        later.push_back(r);
+    }
+    S->reserves.swap(later);
+    if (!S->reserves.empty()) S->wake = true;
+  }
+  for (SrvReserve* r : todo) {
+    SrvAcq* q = S->wacqs[r->acq];
+    fa_status st = FA_OK;
+    std::string err;
+    while (q->n_slots < r->n) {
+      if (S->slot_bytes + slot_estimate(q) > S->cfg.memory_budget || q->cls->free_idx.empty()) {
+        st = FA_ERR_OOM;
+        err = "the server's memory budget or job table holds no more slots for this acquisition";
+        break;
+      }
+      SrvSlot* sl = nullptr;
+      st = slot_create(S, q, &sl);
+      if (st != FA_OK) {
+        err = g_err;
+        break;
+      }
+      q->idle.push_back(sl);
+    }
+    const bool device_error = st == FA_ERR_CUDA;
+    {
+      std::lock_guard<std::mutex> lk(S->mu);
+      r->status = st;
+      r->error = err;
+      r->done = true;
+      S->peak_slot_bytes = std::max(S->peak_slot_bytes, S->slot_bytes.load());
+      S->cv_done.notify_all();
+    }
+    if (device_error) return fail(st, err);
+  }
+  return FA_OK;
+}
+
 // Longest a shutdown waits for submitted frames before failing the rest.
 constexpr double kStopDeadlineS = 120.0;
 
@@ -661,6 +723,7 @@ void worker_main(fa_server* S) {
     fa_status st = FA_OK;
     for (SrvAcq* q : S->wacqs)
       if (!q->cls && st == FA_OK) st = attach(S, q);
+    if (st == FA_OK) st = serve_reserves(S);
     for (SrvRequest& r : incoming) S->wacqs[r.acq]->pending.push_back(r);
     bool progress = true;
     while (st == FA_OK && progress) st = worker_pass(S, &progress);
@@ -772,6 +835,32 @@ extern "C" fa_status fa_server_add_acquisition(fa_server* S, const fa_aligner_pa
   *acquisition = q->id;
   S->acqs.push_back(std::move(q));
   S->cv_work.notify_one();
+  return FA_OK;
+}
+
+extern "C" fa_status fa_server_reserve(fa_server* S, int acquisition, int n_slots) {
+  if (!S) return fail(FA_ERR_BAD_ARG, "NULL server");
+  if (n_slots < 0 || n_slots > S->cfg.max_in_flight)
+    return fail(FA_ERR_BAD_ARG, "n_slots must be in 0..max_in_flight");
+  SrvReserve r;
+  r.acq = acquisition;
+  r.n = n_slots;
+  std::unique_lock<std::mutex> lk(S->mu);
+  if (acquisition < 0 || acquisition >= (int)S->acqs.size()) return fail(FA_ERR_NOT_FOUND, "unknown acquisition");
+  if (S->fatal != FA_OK) return fail(S->fatal, "server stopped after an error: " + S->fatal_msg);
+  if (S->stop) return fail(FA_ERR_STATE, "server is shutting down");
+  S->reserves.push_back(&r);
+  S->cv_work.notify_one();
+  S->cv_done.wait(lk, [&] { return r.done || S->fatal != FA_OK; });
+  if (!r.done) {  // the worker stopped: withdraw the request
+    for (auto it = S->reserves.begin(); it != S->reserves.end(); ++it)
+      if (*it == &r) {
+        S->reserves.erase(it);
+        break;
+      }
+    return fail(S->fatal, "server stopped after an error: " + S->fatal_msg);
+  }
+  if (r.status != FA_OK) return fail(r.status, r.error);
   return FA_OK;
 }
 

@@ -73,7 +73,7 @@ class AlignerParams(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("memory_budget", C.c_size_t), ("max_in_flight", C.c_int), ("iterations_per_launch", C.c_int),
-                ("warm_start", C.c_int)]
+                ("warm_start", C.c_int), ("shared_launches", C.c_int)]
 
 
 class ServerStats(C.Structure):
@@ -154,6 +154,7 @@ SIGNATURES = {
     "fa_server_add_acquisition": [_vp, C.POINTER(AlignerParams), _vp, C.c_int, C.c_int, C.c_int, C.c_int,
                                   C.POINTER(ScanParams), C.c_int, C.POINTER(C.c_int)],
     "fa_server_acquisition_info": [_vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)],
+    "fa_server_reserve": [_vp, C.c_int, C.c_int],
     "fa_server_submit": [_vp, C.c_int, _vp, C.c_int, C.POINTER(C.c_ulonglong)],
     "fa_server_wait": [_vp, C.c_ulonglong, C.c_double, _vp, _vp, C.POINTER(C.c_double)],
     "fa_server_get_stats": [_vp, C.POINTER(ServerStats)],
@@ -454,11 +455,12 @@ class Server:
     """The serving loop (fa_server_*): several acquisitions, frames submitted asynchronously and
     solved with continuous batching on the device."""
 
-    def __init__(self, ctx: Context, memory_budget=0, max_in_flight=0, iterations_per_launch=0, warm_start=True):
+    def __init__(self, ctx: Context, memory_budget=0, max_in_flight=0, iterations_per_launch=0, warm_start=True,
+                 shared_launches=False):
         self.ctx = ctx
         self._h = _vp()
         lag = int(warm_start)  # True -> 1 (the previous frame), False -> 0, d -> frame k - d
-        cfg = ServerConfig(memory_budget, max_in_flight, iterations_per_launch, lag)
+        cfg = ServerConfig(memory_budget, max_in_flight, iterations_per_launch, lag, 1 if shared_launches else 0)
         check(lib().fa_server_create(ctx._h, C.byref(cfg), C.byref(self._h)))
         self.acqs = {}
         self._keep = {}  # host frames referenced by outstanding tickets
@@ -479,6 +481,10 @@ class Server:
         self.acqs[a.value] = {"dims": ref.shape, "nD": nD_.value, "n_dim": nd.value,
                               "dtype": np.dtype(frame_dtype)}
         return a.value
+
+    def reserve(self, acquisition, n_slots):
+        """fa_server_reserve: pre-creates frame slots for an acquisition."""
+        check(lib().fa_server_reserve(self._h, acquisition, n_slots))
 
     def submit(self, acquisition, frame):
         """Queues a host frame (kept referenced until its result is collected); returns the ticket."""

@@ -247,6 +247,10 @@ typedef struct {
                                  frame k - d of the same acquisition} (d = 1: the previous frame), and
                                  frame k starts its solve after frame k - d finished, so at most d frames
                                  of an acquisition solve at once; 0: no warm start (at most 64) */
+  int shared_launches;        /* 0: each acquisition's frames have their own job table, graph and stream,
+                                 and acquisitions overlap on the device; 1: acquisitions whose frames
+                                 can share a kernel (same dimensionality, storage and precision) share
+                                 the launches */
 } fa_server_config;
 
 typedef struct {
@@ -267,6 +271,11 @@ fa_status fa_server_add_acquisition(fa_server* s, const fa_aligner_params* param
                                     fa_dtype reference_dtype, int nz, int ny, int nx, const fa_scan_params* scan,
                                     fa_dtype frame_dtype, int* acquisition);
 fa_status fa_server_acquisition_info(fa_server* s, int acquisition, int* nD, int* n_dim);
+/* Creates idle frame slots for an acquisition until it holds n_slots (device memory for frames and
+   their solve state, within the memory budget), so that the first frames of a stream do not wait
+   for allocations. FA_ERR_OOM when the budget or job table cannot hold them (the slots created so
+   far stay). */
+fa_status fa_server_reserve(fa_server* s, int acquisition, int n_slots);
 /* FrameWarpAligner::addFrame, asynchronous: queues one raw frame (host memory, or device memory when
    frame_on_device) and returns its ticket. The frame's memory must stay valid and unchanged until its
    result has been collected; page-locked host memory lets the upload overlap other work. */

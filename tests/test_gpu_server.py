@@ -74,9 +74,10 @@ def _run_sequence(srv, acq_id, frames):
     return [srv.wait(t, 120.0) for t in tickets]
 
 
-def test_served_equals_aligner_without_warm_start(ctx, acqs):
+@pytest.mark.parametrize("shared", [False, True])
+def test_served_equals_aligner_without_warm_start(ctx, acqs, shared):
     names = ["stack", "plane", "odd"]
-    srv, ids = _server(ctx, acqs, names, warm_start=False)
+    srv, ids = _server(ctx, acqs, names, warm_start=False, shared_launches=shared)
     tickets = {n: [] for n in names}
     for k in range(6):  # interleaved submissions: the acquisitions share launches
         for n in names:
@@ -94,16 +95,16 @@ def test_served_equals_aligner_without_warm_start(ctx, acqs):
         assert np.max(np.abs(served[n] - D)) <= 1e-9, (n, np.max(np.abs(served[n] - D)))
 
 
-@pytest.mark.parametrize("lag", [1, 3])
-def test_alone_equals_mix_with_warm_start(ctx, acqs, lag):
+@pytest.mark.parametrize("lag,shared", [(1, False), (1, True), (3, True)])
+def test_alone_equals_mix_with_warm_start(ctx, acqs, lag, shared):
     names = ["stack", "plane", "odd"]
     alone = {}
-    srv, ids = _server(ctx, acqs, names, warm_start=lag)
+    srv, ids = _server(ctx, acqs, names, warm_start=lag, shared_launches=shared)
     for n in names:  # one acquisition at a time
         alone[n] = np.array([r[0] for r in _run_sequence(srv, ids[n], _raw(acqs[n]))])
     srv.close()
 
-    srv, ids = _server(ctx, acqs, names, warm_start=lag)
+    srv, ids = _server(ctx, acqs, names, warm_start=lag, shared_launches=shared)
     out, errors = {}, []
 
     def feed(n):
@@ -195,4 +196,28 @@ def test_server_errors(ctx, acqs):
     with pytest.raises(fa.FaError) as e:
         fa.check(fa.lib().fa_server_wait(srv._h, 12345, 0.0, None, None, None))
     assert e.value.status == fa.FA_ERR_NOT_FOUND
+    srv.close()
+
+
+def test_reserve_slots(ctx, acqs):
+    """fa_server_reserve creates the slots up front (results unchanged); a budget that cannot hold
+    them is reported."""
+    a = acqs["stack"]
+    srv, ids = _server(ctx, acqs, ["stack"], warm_start=False)
+    ref = _run_sequence(srv, ids["stack"], _raw(a))
+    per_slot = srv.stats()["peak_slot_bytes"] / 6
+    srv.close()
+    srv, ids = _server(ctx, acqs, ["stack"], warm_start=False)
+    srv.reserve(ids["stack"], 4)
+    held = srv.stats()["slot_bytes"]
+    assert abs(held - 4 * per_slot) <= 1e-6 * held
+    got = _run_sequence(srv, ids["stack"], _raw(a))
+    srv.close()
+    for r, g in zip(ref, got):
+        assert np.array_equal(r[0], g[0])
+    srv, ids = _server(ctx, acqs, ["stack"], warm_start=False, memory_budget=int(2.5 * per_slot))
+    with pytest.raises(fa.FaError) as e:
+        srv.reserve(ids["stack"], 4)
+    assert e.value.status == fa.FA_ERR_OOM
+    assert srv.stats()["slot_bytes"] <= 2.5 * per_slot
     srv.close()
