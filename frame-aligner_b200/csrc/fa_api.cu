@@ -324,10 +324,11 @@ struct TuneResult {
 std::mutex g_tune_mu;
 std::map<std::string, TuneResult> g_tune_cache;
 
-// The project's autotuner for the fused pass: times each (tile size, CTAs per SM) candidate on a
-// batch of 8 synthetic frames (the reference itself, slightly displaced) with the persistent kernel
-// the batched solver uses, keeps the fastest, and caches the choice per volume shape, control-point
-// count and precision for the life of the process.
+// The project's autotuner for the fused pass: times each (tile size, CTAs per SM) candidate with the
+// persistent kernel the batched solver uses, on a launch of 8 synthetic frames (the reference itself,
+// slightly displaced) and on a launch of one, keeps the lowest sum of per-frame times, and caches the
+// choice per volume shape, control-point count and precision for the life of the process. Register
+// budgets under which the kernel spills are skipped (the largest budget is always a candidate).
 fa_status autotune(fa_reference* R) {
   char keyb[128];
   std::snprintf(keyb, sizeof(keyb), "%d,%d,%d,%d,%d,%d", R->nz, R->ny, R->nx, R->nD, (int)R->prec,
@@ -398,7 +399,7 @@ fa_status autotune(fa_reference* R) {
     jobs[i] = j;
     all[i] = i;
   }
-  const int kcount = K;
+  const int kcount = K, kone = 1;
   if (e == cudaSuccess) e = cudaMemcpyAsync(dp, hdp.data(), hdp.size() * sizeof(float4), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(jobs_dev, jobs.data(), K * sizeof(Job), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(list, all.data(), K * sizeof(int), cudaMemcpyHostToDevice, s);
@@ -410,8 +411,8 @@ fa_status autotune(fa_reference* R) {
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  TuneResult best{8192, 2, 2, 1e30};
-  const int targets[] = {2048, 4096, 8192, 16384, 32768};
+  TuneResult best{4096, 2, 2, 1e30};
+  const int targets[] = {1024, 2048, 4096, 8192, 16384};
   const int mbs[] = {2, 3, 4};
   std::vector<int> hprefix(K + 1);
   for (int target : targets) {
@@ -422,20 +423,30 @@ fa_status autotune(fa_reference* R) {
     if (e != cudaSuccess) break;
     for (int mb : mbs) {
       const bool mixed = R->prec == FA_PREC_MIXED;
+      // register budgets that make the kernel spill to local memory are not candidates
+      if (mb != mbs[0] && fa::eval4_active_local_bytes(R->n_dim, kind, mixed, mb) > 0) continue;
       auto launch = [&]() {
         return fa::launch_eval4_active(jobs_dev, list, cnt, prefix, (long long)K * R->G.n_tiles, R->n_dim, kind, mixed,
                                        mb, mb * sms, s);
       };
-      e = launch();
-      if (e == cudaSuccess) e = cudaEventRecord(e0, s);
-      for (int r = 0; r < 3 && e == cudaSuccess; r++) e = launch();
-      if (e == cudaSuccess) e = cudaEventRecord(e1, s);
-      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
-      float ms = 0;
-      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
-      g_launches += 4;
+      // Score: per-frame time of a K-frame launch plus that of a one-frame launch, so that the
+      // choice also serves the late iterations of a batch and the few-frame launches of serving.
+      double score = 0;
+      for (int count : {K, 1}) {
+        e = cudaMemcpyAsync(cnt, count == K ? &kcount : &kone, sizeof(int), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = launch();
+        if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+        for (int r = 0; r < 3 && e == cudaSuccess; r++) e = launch();
+        if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float ms = 0;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        g_launches += 4;
+        if (e != cudaSuccess) break;
+        score += ms / count;
+      }
       if (e != cudaSuccess) break;
-      if (ms < best.ms) best = TuneResult{target, mb, mb, ms};
+      if (score < best.ms) best = TuneResult{target, mb, mb, score};
     }
     if (e != cudaSuccess) break;
   }
@@ -557,7 +568,7 @@ fa_status set_reference_impl(fa_context* ctx, const float* src, bool src_device,
   R->N = (long long)nz * ny * nx;
   R->prec = precision;
   R->scan = *scan;
-  fa_status st = build_geometry(*scan, nz, ny, nx, nD, 8192, R->G);
+  fa_status st = build_geometry(*scan, nz, ny, nx, nD, 4096, R->G);
   if (st == FA_OK) st = reference_setup(R, src, src_device);
   if (st != FA_OK) {
     std::string keep = g_err;

@@ -98,9 +98,11 @@ __device__ __forceinline__ void masked5(const FT* row, bool row_valid, int ix, i
 
 }  // namespace
 
-// One tile of one frame: the whole CTA cooperates; all threads must call it together.
+// One tile of one frame, processed by one warp on its own: its control-point window sD (the warp's
+// slice of shared memory), its row segments, and its partial sums. No CTA barrier is involved, so
+// the warps of a CTA drift apart and hide each other's load latency.
 template <int NDIM, typename FT, typename RT>
-__device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, const int tile) {
+__device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, const int tile, float4* sD) {
   const int nx = R.nx, ny = R.ny, nz = R.nz;
   const int row_begin = tile * R.tile_rows;
   const int row_end = min(row_begin + R.tile_rows, R.n_rows);
@@ -108,14 +110,14 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
   const int cw = max(c0 - 1, 0);
   const bool bidir = R.bidir != 0;
   const float dq = R.dq;
+  const int lane = threadIdx.x & 31;
 
-  __shared__ float4 sD[kWin * kDParamF4];
-  __shared__ float sred[kEvalWarps][1 + 3 * NDIM];
-  for (int i = threadIdx.x; i < kWin * kDParamF4; i += blockDim.x) {
-    const int k = cw + i / kDParamF4;
-    sD[i] = (k < R.nD) ? job.dparams[k * kDParamF4 + i % kDParamF4] : make_float4(0.f, 0.f, 0.f, 0.f);
+  __syncwarp();  // the previous tile's readers of sD are done
+  if (lane < kWin * kDParamF4) {
+    const int k = cw + lane / kDParamF4;
+    sD[lane] = (k < R.nD) ? job.dparams[k * kDParamF4 + lane % kDParamF4] : make_float4(0.f, 0.f, 0.f, 0.f);
   }
-  __syncthreads();
+  __syncwarp();
 
   const FT* __restrict__ fr = static_cast<const FT*>(job.frame);
   const RT* __restrict__ tref;
@@ -139,185 +141,180 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
 #pragma unroll
     for (int k = 0; k < NDIM; k++) ag[s][k] = 0.0f;
 
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // 128-voxel segments of the tile's rows, one per step of the warp
   const int segs = (nx + 127) >> 7;
-  const int rows_here = row_end - row_begin;
-  // When the number of 128-voxel segments per row divides the warp count (row lengths 128, 256,
-  // 512, 1024), each warp keeps one segment and steps over rows; otherwise items are enumerated.
-  const bool fixed_seg = (kEvalWarps % segs) == 0;
-  const int row_step = fixed_seg ? kEvalWarps / segs : 0;
-  const int n_items = fixed_seg ? (warp / segs < rows_here ? (rows_here - warp / segs + row_step - 1) / row_step : 0)
-                                : (rows_here * segs - warp + kEvalWarps - 1) / kEvalWarps;
+  const int n_items = (row_end - row_begin) * segs;
   const long long plane = job.fplane;
   const int pitch = job.fpitch;
   const bool padded = job.fpad != 0;
+  int row = row_begin, seg = 0;
   for (int item = 0; item < n_items; item++) {
-    int row, x0;
-    if (fixed_seg) {
-      row = row_begin + warp / segs + item * row_step;
-      x0 = (warp % segs) * 128 + lane * 4;
-    } else {
-      const int it = warp + item * kEvalWarps;
-      const int rr = it / segs;
-      row = row_begin + rr;
-      x0 = (it - rr * segs) * 128 + lane * 4;
+    const int x0 = seg * 128 + lane * 4;
+    const int row_here = row;
+    if (++seg == segs) {
+      seg = 0;
+      ++row;
     }
-    if (x0 >= nx) continue;
-    const RowDesc rd = R.rows[row];
-    const int z = rd.z;
-    const int y = rd.y;
-    const bool flip = bidir && (y & 1);
-    const long long p0 = (long long)row * nx + x0;
-    float t4[4], g4[NDIM][4];
-    load4(tref + p0, t4);
-#pragma unroll
-    for (int k = 0; k < NDIM; k++) load4(tg[k] + p0, g4[k]);
+    if (x0 < nx) {
+      const RowDesc rd = R.rows[row_here];
+      const int z = rd.z;
+      const int y = rd.y;
+      const bool flip = bidir && (y & 1);
+      const long long p0 = (long long)row_here * nx + x0;
+      float t4[4], g4[NDIM][4];
+      load4(tref + p0, t4);
+  #pragma unroll
+      for (int k = 0; k < NDIM; k++) load4(tg[k] + p0, g4[k]);
 
-    // Do the four voxels share interval, storage range and integer tap offsets, away from edges?
-    const int xs0 = flip ? nx - 1 - x0 : x0;
-    const int xs3 = flip ? xs0 - 3 : xs0 + 3;
-    const int di = rd.di0 + (xs0 >= rd.xdi ? 1 : 0);
-    const int di3 = rd.di0 + (xs3 >= rd.xdi ? 1 : 0);
-    const int r = bidir ? rd.r0 + (x0 >= rd.xr ? 1 : 0) : di;
-    const int r3 = bidir ? rd.r0 + (x0 + 3 >= rd.xr ? 1 : 0) : di3;
-    bool fast = (di == di3) && (r == r3) && (rd.xlast < x0 || rd.xlast > x0 + 3);
-    const float4* P = sD + min(max(di - cw, 0), kWin - 2) * kDParamF4;
-    const float f0 = fmaf((float)xs0, dq, rd.qbase) - (float)(di - rd.di0);
-    const float fs = flip ? -dq : dq;
-    const float4 n = P[0], ph = P[1], dd = P[2];
-    const float t0x = fmaf(f0, dd.x, ph.x), t0y = fmaf(f0, dd.y, ph.y);
-    const float sx = fs * dd.x, sy = fs * dd.y;
-    const float flx = floorf(t0x), fly = floorf(t0y);
-    fast = fast && floorf(fmaf(3.0f, sx, t0x)) == flx && floorf(fmaf(3.0f, sy, t0y)) == fly;
-    const int ix = x0 + (int)n.x + (int)flx;
-    const int iy = y + (int)n.y + (int)fly;
-    bool inside = ix >= 0 && ix + 4 <= nx - 1 && iy >= 0 && iy + 1 <= ny - 1;
-    float t0z = 0.f, sz = 0.f, flz = 0.f;
-    int iz = 0;
-    if (NDIM == 3) {
-      t0z = fmaf(f0, dd.z, ph.z);
-      sz = fs * dd.z;
-      flz = floorf(t0z);
-      fast = fast && floorf(fmaf(3.0f, sz, t0z)) == flz;
-      iz = z + (int)n.z + (int)flz;
-      inside = inside && iz >= 0 && iz + 1 <= nz - 1;
-    }
+      // Do the four voxels share interval, storage range and integer tap offsets, away from edges?
+      const int xs0 = flip ? nx - 1 - x0 : x0;
+      const int xs3 = flip ? xs0 - 3 : xs0 + 3;
+      const int di = rd.di0 + (xs0 >= rd.xdi ? 1 : 0);
+      const int di3 = rd.di0 + (xs3 >= rd.xdi ? 1 : 0);
+      const int r = bidir ? rd.r0 + (x0 >= rd.xr ? 1 : 0) : di;
+      const int r3 = bidir ? rd.r0 + (x0 + 3 >= rd.xr ? 1 : 0) : di3;
+      bool fast = (di == di3) && (r == r3) && (rd.xlast < x0 || rd.xlast > x0 + 3);
+      const float4* P = sD + min(max(di - cw, 0), kWin - 2) * kDParamF4;
+      const float f0 = fmaf((float)xs0, dq, rd.qbase) - (float)(di - rd.di0);
+      const float fs = flip ? -dq : dq;
+      const float4 n = P[0], ph = P[1], dd = P[2];
+      const float t0x = fmaf(f0, dd.x, ph.x), t0y = fmaf(f0, dd.y, ph.y);
+      const float sx = fs * dd.x, sy = fs * dd.y;
+      const float flx = floorf(t0x), fly = floorf(t0y);
+      fast = fast && floorf(fmaf(3.0f, sx, t0x)) == flx && floorf(fmaf(3.0f, sy, t0y)) == fly;
+      const int ix = x0 + (int)n.x + (int)flx;
+      const int iy = y + (int)n.y + (int)fly;
+      bool inside = ix >= 0 && ix + 4 <= nx - 1 && iy >= 0 && iy + 1 <= ny - 1;
+      float t0z = 0.f, sz = 0.f, flz = 0.f;
+      int iz = 0;
+      if (NDIM == 3) {
+        t0z = fmaf(f0, dd.z, ph.z);
+        sz = fs * dd.z;
+        flz = floorf(t0z);
+        fast = fast && floorf(fmaf(3.0f, sz, t0z)) == flz;
+        iz = z + (int)n.z + (int)flz;
+        inside = inside && iz >= 0 && iz + 1 <= nz - 1;
+      }
 
-    float acc0[NDIM], acc1[NDIM];  // J^T e of controls r and r+1 for this lane's voxels
-#pragma unroll
-    for (int k = 0; k < NDIM; k++) acc0[k] = acc1[k] = 0.0f;
+      float acc0[NDIM], acc1[NDIM];  // J^T e of controls r and r+1 for this lane's voxels
+  #pragma unroll
+      for (int k = 0; k < NDIM; k++) acc0[k] = acc1[k] = 0.0f;
 
-    if (fast) {
-      float v[NDIM == 3 ? 4 : 2][5];
-      if (padded) {
-        // Clamp into the zero halo: a window that would lie wholly outside the volume along an
-        // axis reads halo zeros instead, exactly as the unclamped taps would read zero padding.
-        const int cx = min(max(ix, -kHaloX), nx + kHaloX - 5);
-        const int cy = min(max(iy, -kHaloY), ny + kHaloY - 2);
-        const int cz = NDIM == 3 ? min(max(iz, -kHaloZ), nz + kHaloZ - 2) : 0;
-        const int a = cx & ~3, s = cx - a;
-        const long long rb = (long long)cz * plane + (long long)cy * pitch + a;
-        window5(fr + rb, s, v[0]);
-        window5(fr + rb + pitch, s, v[1]);
-        if (NDIM == 3) {
-          window5(fr + rb + plane, s, v[NDIM == 3 ? 2 : 0]);
-          window5(fr + rb + plane + pitch, s, v[NDIM == 3 ? 3 : 1]);
+      if (fast) {
+        float v[NDIM == 3 ? 4 : 2][5];
+        if (padded) {
+          // Clamp into the zero halo: a window that would lie wholly outside the volume along an
+          // axis reads halo zeros instead, exactly as the unclamped taps would read zero padding.
+          const int cx = min(max(ix, -kHaloX), nx + kHaloX - 5);
+          const int cy = min(max(iy, -kHaloY), ny + kHaloY - 2);
+          const int cz = NDIM == 3 ? min(max(iz, -kHaloZ), nz + kHaloZ - 2) : 0;
+          const int a = cx & ~3, s = cx - a;
+          const long long rb = (long long)cz * plane + (long long)cy * pitch + a;
+          window5(fr + rb, s, v[0]);
+          window5(fr + rb + pitch, s, v[1]);
+          if (NDIM == 3) {
+            window5(fr + rb + plane, s, v[NDIM == 3 ? 2 : 0]);
+            window5(fr + rb + plane + pitch, s, v[NDIM == 3 ? 3 : 1]);
+          }
+        } else if (inside) {
+          const int a = ix & ~3, s = ix & 3;
+          const long long rb = (long long)iz * plane + (long long)iy * pitch + a;
+          window5(fr + rb, s, v[0]);
+          window5(fr + rb + pitch, s, v[1]);
+          if (NDIM == 3) {
+            window5(fr + rb + plane, s, v[NDIM == 3 ? 2 : 0]);
+            window5(fr + rb + plane + pitch, s, v[NDIM == 3 ? 3 : 1]);
+          }
+        } else {
+          // tap rows (y, z), (y+1, z), (y, z+1), (y+1, z+1); rows outside the volume read zeros
+          const bool y0v = (unsigned)iy < (unsigned)ny, y1v = (unsigned)(iy + 1) < (unsigned)ny;
+          const bool z0v = NDIM == 2 || (unsigned)iz < (unsigned)nz;
+          const bool z1v = NDIM == 2 || (unsigned)(iz + 1) < (unsigned)nz;
+          const long long rb = (long long)iz * plane + (long long)iy * pitch;
+          masked5(fr + rb, y0v && z0v, ix, nx, v[0]);
+          masked5(fr + rb + pitch, y1v && z0v, ix, nx, v[1]);
+          if (NDIM == 3) {
+            masked5(fr + rb + plane, y0v && z1v, ix, nx, v[NDIM == 3 ? 2 : 0]);
+            masked5(fr + rb + plane + pitch, y1v && z1v, ix, nx, v[NDIM == 3 ? 3 : 1]);
+          }
         }
-      } else if (inside) {
-        const int a = ix & ~3, s = ix & 3;
-        const long long rb = (long long)iz * plane + (long long)iy * pitch + a;
-        window5(fr + rb, s, v[0]);
-        window5(fr + rb + pitch, s, v[1]);
-        if (NDIM == 3) {
-          window5(fr + rb + plane, s, v[NDIM == 3 ? 2 : 0]);
-          window5(fr + rb + plane + pitch, s, v[NDIM == 3 ? 3 : 1]);
+        const float wx0 = t0x - flx, wy0 = t0y - fly, wz0 = t0z - flz;
+  #pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const float wx = fmaf((float)j, sx, wx0), wy = fmaf((float)j, sy, wy0);
+          const float c00 = fmaf(wx, v[0][j + 1] - v[0][j], v[0][j]);
+          const float c01 = fmaf(wx, v[1][j + 1] - v[1][j], v[1][j]);
+          float val = fmaf(wy, c01 - c00, c00);
+          if (NDIM == 3) {
+            const float wz = fmaf((float)j, sz, wz0);
+            const float c10 = fmaf(wx, v[NDIM == 3 ? 2 : 0][j + 1] - v[NDIM == 3 ? 2 : 0][j], v[NDIM == 3 ? 2 : 0][j]);
+            const float c11 = fmaf(wx, v[NDIM == 3 ? 3 : 1][j + 1] - v[NDIM == 3 ? 3 : 1][j], v[NDIM == 3 ? 3 : 1][j]);
+            const float c1 = fmaf(wy, c11 - c10, c10);
+            val = fmaf(wz, c1 - val, val);
+          }
+          const float e = (val > 0.0f) ? val - t4[j] : 0.0f;
+          af = fmaf(e, e, af);
+          const float fj = fmaf((float)j, fs, f0);
+          const float e1 = e * fj;
+          const float e0 = e - e1;
+  #pragma unroll
+          for (int k = 0; k < NDIM; k++) {
+            acc0[k] = fmaf(g4[k][j], e0, acc0[k]);
+            acc1[k] = fmaf(g4[k][j], e1, acc1[k]);
+          }
         }
       } else {
-        // tap rows (y, z), (y+1, z), (y, z+1), (y+1, z+1); rows outside the volume read zeros
-        const bool y0v = (unsigned)iy < (unsigned)ny, y1v = (unsigned)(iy + 1) < (unsigned)ny;
-        const bool z0v = NDIM == 2 || (unsigned)iz < (unsigned)nz;
-        const bool z1v = NDIM == 2 || (unsigned)(iz + 1) < (unsigned)nz;
-        const long long rb = (long long)iz * plane + (long long)iy * pitch;
-        masked5(fr + rb, y0v && z0v, ix, nx, v[0]);
-        masked5(fr + rb + pitch, y1v && z0v, ix, nx, v[1]);
-        if (NDIM == 3) {
-          masked5(fr + rb + plane, y0v && z1v, ix, nx, v[NDIM == 3 ? 2 : 0]);
-          masked5(fr + rb + plane + pitch, y1v && z1v, ix, nx, v[NDIM == 3 ? 3 : 1]);
-        }
-      }
-      const float wx0 = t0x - flx, wy0 = t0y - fly, wz0 = t0z - flz;
-#pragma unroll
-      for (int j = 0; j < 4; j++) {
-        const float wx = fmaf((float)j, sx, wx0), wy = fmaf((float)j, sy, wy0);
-        const float c00 = fmaf(wx, v[0][j + 1] - v[0][j], v[0][j]);
-        const float c01 = fmaf(wx, v[1][j + 1] - v[1][j], v[1][j]);
-        float val = fmaf(wy, c01 - c00, c00);
-        if (NDIM == 3) {
-          const float wz = fmaf((float)j, sz, wz0);
-          const float c10 = fmaf(wx, v[NDIM == 3 ? 2 : 0][j + 1] - v[NDIM == 3 ? 2 : 0][j], v[NDIM == 3 ? 2 : 0][j]);
-          const float c11 = fmaf(wx, v[NDIM == 3 ? 3 : 1][j + 1] - v[NDIM == 3 ? 3 : 1][j], v[NDIM == 3 ? 3 : 1][j]);
-          const float c1 = fmaf(wy, c11 - c10, c10);
-          val = fmaf(wz, c1 - val, val);
-        }
-        const float e = (val > 0.0f) ? val - t4[j] : 0.0f;
-        af = fmaf(e, e, af);
-        const float fj = fmaf((float)j, fs, f0);
-        const float e1 = e * fj;
-        const float e0 = e - e1;
-#pragma unroll
-        for (int k = 0; k < NDIM; k++) {
-          acc0[k] = fmaf(g4[k][j], e0, acc0[k]);
-          acc1[k] = fmaf(g4[k][j], e1, acc1[k]);
-        }
-      }
-    } else {
-#pragma unroll
-      for (int j = 0; j < 4; j++) {
-        const int x = x0 + j;
-        const VoxelModel vm = voxel_model(rd, x, nx, flip, bidir, dq);
-        const int wi = min(max(vm.di - cw, 0), kWin - 2);
-        const float val = sample<NDIM, FT>(fr, plane, pitch, sD + wi * kDParamF4, vm.f, x, y, z, nx, ny, nz);
-        const float e = (val > 0.0f) ? val - t4[j] : 0.0f;
-        af = fmaf(e, e, af);
-        if (!vm.last) {
-          const float e1 = e * vm.f;
-          const float e0 = e * (1.0f - vm.f);
-          if (vm.r == r) {
-#pragma unroll
-            for (int k = 0; k < NDIM; k++) {
-              acc0[k] = fmaf(g4[k][j], e0, acc0[k]);
-              acc1[k] = fmaf(g4[k][j], e1, acc1[k]);
-            }
-          } else {
-            // voxel in the following range: controls r+1 and r+2
-            const int s2 = vm.r - c0;
-#pragma unroll
-            for (int k = 0; k < NDIM; k++) {
-              if (s2 == 1) {
-                ag[1][k] = fmaf(g4[k][j], e0, ag[1][k]);
-                ag[2][k] = fmaf(g4[k][j], e1, ag[2][k]);
-              } else {
-                ag[0][k] = fmaf(g4[k][j], e0, ag[0][k]);
-                ag[1][k] = fmaf(g4[k][j], e1, ag[1][k]);
+  #pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const int x = x0 + j;
+          const VoxelModel vm = voxel_model(rd, x, nx, flip, bidir, dq);
+          const int wi = min(max(vm.di - cw, 0), kWin - 2);
+          const float val = sample<NDIM, FT>(fr, plane, pitch, sD + wi * kDParamF4, vm.f, x, y, z, nx, ny, nz);
+          const float e = (val > 0.0f) ? val - t4[j] : 0.0f;
+          af = fmaf(e, e, af);
+          if (!vm.last) {
+            const float e1 = e * vm.f;
+            const float e0 = e * (1.0f - vm.f);
+            if (vm.r == r) {
+  #pragma unroll
+              for (int k = 0; k < NDIM; k++) {
+                acc0[k] = fmaf(g4[k][j], e0, acc0[k]);
+                acc1[k] = fmaf(g4[k][j], e1, acc1[k]);
+              }
+            } else {
+              // voxel in the following range: controls r+1 and r+2
+              const int s2 = vm.r - c0;
+  #pragma unroll
+              for (int k = 0; k < NDIM; k++) {
+                if (s2 == 1) {
+                  ag[1][k] = fmaf(g4[k][j], e0, ag[1][k]);
+                  ag[2][k] = fmaf(g4[k][j], e1, ag[2][k]);
+                } else {
+                  ag[0][k] = fmaf(g4[k][j], e0, ag[0][k]);
+                  ag[1][k] = fmaf(g4[k][j], e1, ag[1][k]);
+                }
               }
             }
           }
         }
       }
-    }
-    if (r == c0) {
-#pragma unroll
-      for (int k = 0; k < NDIM; k++) {
-        ag[0][k] += acc0[k];
-        ag[1][k] += acc1[k];
+      if (r == c0) {
+  #pragma unroll
+        for (int k = 0; k < NDIM; k++) {
+          ag[0][k] += acc0[k];
+          ag[1][k] += acc1[k];
+        }
+      } else {
+  #pragma unroll
+        for (int k = 0; k < NDIM; k++) {
+          ag[1][k] += acc0[k];
+          ag[2][k] += acc1[k];
+        }
       }
-    } else {
-#pragma unroll
-      for (int k = 0; k < NDIM; k++) {
-        ag[1][k] += acc0[k];
-        ag[2][k] += acc1[k];
-      }
     }
+    // Explicit reconvergence point: the per-lane fast / per-voxel branches above must not leave
+    // the warp split into groups that then run the rest of the loop one after the other.
+    __syncwarp();
   }
 
 #pragma unroll
@@ -328,54 +325,47 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
 #pragma unroll
       for (int k = 0; k < NDIM; k++) ag[s][k] += __shfl_xor_sync(0xffffffffu, ag[s][k], o);
   }
-  if (lane == 0) {
-    sred[warp][0] = af;
+  // Lane i < 11 writes entry i of the tile's partial sums [f, c0, g(3 x 3)] (every lane holds the
+  // totals; the value is picked with selects so that the warp does not branch).
+  float pick = af;
 #pragma unroll
-    for (int s = 0; s < 3; s++)
+  for (int s = 0; s < 3; s++)
 #pragma unroll
-      for (int k = 0; k < NDIM; k++) sred[warp][1 + s * NDIM + k] = ag[s][k];
-  }
-  __syncthreads();
+    for (int k = 0; k < 3; k++) pick = (lane == 2 + s * 3 + k) ? (k < NDIM ? ag[s][k < NDIM ? k : 0] : 0.0f) : pick;
   double* out = job.partials + (long long)tile * kPartialDoubles;
-  if (threadIdx.x < 1 + 3 * NDIM) {
-    double acc = 0.0;
-    for (int w = 0; w < kEvalWarps; w++) acc += (double)sred[w][threadIdx.x];
-    const int i = threadIdx.x;
-    if (i == 0) {
-      out[0] = acc;
-    } else {
-      const int s = (i - 1) / NDIM, k = (i - 1) % NDIM;
-      out[2 + s * 3 + k] = acc;
-    }
-  } else if (threadIdx.x == 1 + 3 * NDIM) {
-    out[1] = (double)c0;
-    if (NDIM == 2) out[2 + 0 * 3 + 2] = out[2 + 1 * 3 + 2] = out[2 + 2 * 3 + 2] = 0.0;
-  }
+  if (lane < 11) out[lane] = lane == 1 ? (double)c0 : (double)pick;
+  __syncwarp();
 }
 
+// One grid per launch: CTA x of job y covers tiles 8x .. 8x+7, one per warp.
 template <int NDIM, typename FT, typename RT, int MB>
 __global__ void __launch_bounds__(kEvalThreads, MB) eval4_kernel(const Job* __restrict__ jobs) {
+  __shared__ float4 sD[kEvalWarps][kWin * kDParamF4];
   const Job& job = jobs[blockIdx.y];
   if (job.state != nullptr && job.state->phase == kPhaseDone) return;
   const RefDev& R = *job.ref;
-  const int tile = blockIdx.x;
+  const int warp = threadIdx.x >> 5;
+  const int tile = blockIdx.x * kEvalWarps + warp;
   if (tile >= R.n_tiles) return;
-  eval4_tile<NDIM, FT, RT>(job, R, tile);
+  eval4_tile<NDIM, FT, RT>(job, R, tile, sD[warp]);
 }
 
-// Persistent form for batched solves: a fixed grid walks the (active frame, tile) items of the
+// Persistent form for batched solves: the grid's warps walk the (active frame, tile) items of the
 // compacted active list, item = tile_prefix[a] + tile, so frames that have converged cost nothing and
-// frames of different sizes share the launch. Each CTA's items increase, so its frame index only
+// frames of different sizes share the launch. Each warp's items increase, so its frame index only
 // moves forward (binary search over the remaining prefix).
 template <int NDIM, typename FT, typename RT, int MB>
 __global__ void __launch_bounds__(kEvalThreads, MB) eval4_active_kernel(const Job* __restrict__ jobs,
                                                                      const int* __restrict__ active,
                                                                      const int* __restrict__ n_active,
                                                                      const int* __restrict__ tile_prefix) {
+  __shared__ float4 sD[kEvalWarps][kWin * kDParamF4];
   const int na = *n_active;
   const int n_items = tile_prefix[na];
+  const int warp = threadIdx.x >> 5;
+  const int stride = gridDim.x * kEvalWarps;
   int a = 0;
-  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+  for (int item = blockIdx.x * kEvalWarps + warp; item < n_items; item += stride) {
     int hi = na - 1;
     while (a < hi) {  // last a with tile_prefix[a] <= item
       const int mid = (a + hi + 1) >> 1;
@@ -386,9 +376,7 @@ __global__ void __launch_bounds__(kEvalThreads, MB) eval4_active_kernel(const Jo
     }
     const int tile = item - tile_prefix[a];
     const Job& job = jobs[active[a]];
-    const RefDev& R = *job.ref;
-    eval4_tile<NDIM, FT, RT>(job, R, tile);
-    __syncthreads();  // the next item reuses the shared-memory window
+    eval4_tile<NDIM, FT, RT>(job, *job.ref, tile, sD[warp]);
   }
 }
 
@@ -401,7 +389,7 @@ inline cudaError_t dispatch_mb(int mb, Fn&& f) {
 
 cudaError_t launch_eval4(const Job* jobs_dev, int n_jobs, int max_tiles, int n_dim, int frame_kind, bool ref_bf16,
                          int mb, cudaStream_t s) {
-  const dim3 grid(max_tiles, n_jobs);
+  const dim3 grid((max_tiles + kEvalWarps - 1) / kEvalWarps, n_jobs);
   return dispatch_cfg(n_dim, frame_kind, ref_bf16, [&](auto c) {
     using C = decltype(c);
     return dispatch_mb(mb, [&](auto m) {
@@ -411,10 +399,26 @@ cudaError_t launch_eval4(const Job* jobs_dev, int n_jobs, int max_tiles, int n_d
   });
 }
 
+size_t eval4_active_local_bytes(int n_dim, int frame_kind, bool ref_bf16, int mb) {
+  size_t bytes = 0;
+  dispatch_cfg(n_dim, frame_kind, ref_bf16, [&](auto c) {
+    using C = decltype(c);
+    return dispatch_mb(mb, [&](auto m) {
+      cudaFuncAttributes a{};
+      const cudaError_t e =
+          cudaFuncGetAttributes(&a, eval4_active_kernel<C::nd, typename C::F, typename C::R, decltype(m)::value>);
+      bytes = e == cudaSuccess ? a.localSizeBytes : 0;
+      return e;
+    });
+  });
+  return bytes;
+}
+
 cudaError_t launch_eval4_active(const Job* jobs_dev, const int* active, const int* n_active, const int* tile_prefix,
                                 long long most_items, int n_dim, int frame_kind, bool ref_bf16, int mb, int grid,
                                 cudaStream_t s) {
-  const int g = (int)(most_items < grid ? (most_items < 1 ? 1 : most_items) : grid);
+  const long long most_ctas = (most_items + kEvalWarps - 1) / kEvalWarps;
+  const int g = (int)(most_ctas < grid ? (most_ctas < 1 ? 1 : most_ctas) : grid);
   return dispatch_cfg(n_dim, frame_kind, ref_bf16, [&](auto c) {
     using C = decltype(c);
     return dispatch_mb(mb, [&](auto m) {
