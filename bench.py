@@ -386,13 +386,17 @@ def run_ours(args, rank, world, local):
         algo_bytes = n * N * 2 + N * (2 + 3 * 2)
         achieved = algo_bytes / (ms / 1000.0) / 1e9
         peak, peak_kind = load_peaks()
+        # DRAM bytes per launch from the ncu capture summarised in profiles/ (8- and 16-frame launches,
+        # fitted per frame and shared, scaled to n frames), or null without it
         traffic = None
         tp = os.path.join(ROOT, "profiles", "eval_traffic.json")
         if os.path.exists(tp):
             t = json.load(open(tp))
-            traffic = t.get("dram_bytes_per_frame_eval", 0) * n or None
+            traffic = t["dram_bytes_shared"] + n * t["dram_bytes_per_frame"]
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                    "traffic": traffic, "kernel": "eval_kernel<3, half, bf16> (fused warp+error+J^T e)",
+                    "traffic": traffic, "traffic_unit": "bytes per launch",
+                    "kernel": "eval4_kernel<3, half, bf16> (fused warp + error + J^T e, grid form of the tile body "
+                              "the aligner's persistent kernel runs)",
                     "algorithmic_bytes_per_launch": algo_bytes, "ms_per_launch": ms,
                     "bytes_per_unit": "2 B per voxel per frame + 8 B per voxel of the shared reference",
                     "tuning": {"tile_voxels": tile_voxels, "ctas_per_sm": ctas_per_sm},
