@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--cpu-frames", type=int, default=0, help="CPU baseline sample size (0 = one per thread)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--only", choices=["roofline"], default=None,
+                    help="roofline: only the fused-pass probe on --frames FP16 frames (for ncu captures)")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="length of the Poisson arrival stream")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="total arrivals per second")
     ap.add_argument("--serve-pool", type=int, default=6, help="distinct frames per served acquisition")
@@ -74,10 +76,23 @@ def config_dict(n_frames, world):
             "l2": "inputs exceed L2: %d frames x 8.4 MB fp16 + 33.6 MB reference/gradient per step" % n_frames}
 
 
-def make_data(n_frames, rank):
-    cfg = dict(S.CONFIG1)
-    cfg["seed"] = S.CONFIG1["seed"] + 7919 * rank
-    return S.make_config(cfg, n_frames=n_frames)
+def make_data(n_frames, rank, cfg=None):
+    """Rank `rank`'s frames: its own seeded acquisition of the workload (weak scaling: every rank
+    aligns n_frames of its own; no frame is shared, so the data path needs no collective)."""
+    c = dict(cfg or S.CONFIG1)
+    c["seed"] = c["seed"] + 7919 * rank
+    return S.make_config(c, n_frames=n_frames)
+
+
+def max_over_ranks(x, dist=None, device="cpu"):
+    """The slowest rank's value (timings are reported as the max over ranks)."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def load_peaks():
@@ -295,8 +310,28 @@ def run_reference(args, rank, world):
     return 0
 
 
+def run_roofline_probe(args, local):
+    """The fused-pass probe alone: one mixed-precision reference, args.frames FP16 frames, two timed
+    launches of eval4_kernel (the command the DRAM-traffic captures in profiles/ run)."""
+    import fa_b200 as fa
+
+    acq = make_data(args.frames, 0)
+    nz, ny, nx = acq.reference.shape
+    line, il, ifr = acq.scan
+    ctx = fa.Context(device=local, autotune=True)
+    ref = fa.Reference(ctx, acq.reference + 1, acq.nD, fa.scan_params(line, il, ifr, nx, ny, nz), fa.PREC_MIXED)
+    frs = [fa.Frame(ref, (acq.frames[k] + 1).astype(np.float16)) for k in range(args.frames)]
+    ms = fa.profile_eval(frs, acq.D_true[0], 2)
+    print(json.dumps({"probe": "eval4_kernel<3, half, bf16>", "frames": args.frames, "ms_per_launch": ms,
+                      "tuning": list(ref.tuning())}))
+    return 0
+
+
 def run_ours(args, rank, world, local):
     import fa_b200 as fa
+
+    if args.only == "roofline":
+        return run_roofline_probe(args, local)
 
     pg = None
     if world > 1:
@@ -330,13 +365,6 @@ def run_ours(args, rank, world, local):
         if pg:
             pg.barrier()
 
-    def max_over_ranks(x):
-        if not pg:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
-
     # warm-up (untimed)
     for _ in range(args.warmup):
         D, stats = al.add_frames_device(ptrs, fa.U16, n)
@@ -349,7 +377,7 @@ def run_ours(args, rank, world, local):
             dev_ms += al.last_device_ms()
         barrier()
     launches = fa.kernel_launches() - launches0
-    dev_ms = max_over_ranks(dev_ms)
+    dev_ms = max_over_ranks(dev_ms, pg, f"cuda:{local}")
     value = n * world * args.steps / (dev_ms / 1000.0)
     iters = [s["iterations"] for s in stats]
 
@@ -369,7 +397,7 @@ def run_ours(args, rank, world, local):
     for _ in range(args.steps):
         fa.check(fa.lib().fa_aligner_add_frames(al._h, C.cast(arr, C.c_void_p), fa.U16, n, Dh, C.cast(st, C.c_void_p)))
     barrier()
-    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, pg, f"cuda:{local}")
     e2e = {"value": n * world * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(n * N * 2),
            "d2h_bytes_per_step": int(n * acq.nD * 3 * 8 + n * C.sizeof(fa.AlignStats))}
 
