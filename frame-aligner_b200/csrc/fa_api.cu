@@ -55,7 +55,7 @@ void dfree_all(fa_context* ctx, std::vector<Alloc>& owner) {
 
 }  // namespace fa_rt
 
-namespace {
+namespace fa_rt {
 
 // ImageScanParameters fields after AbstractFrameWarper::processScanParameters
 // (FrameWarper.cpp:223-236).
@@ -68,6 +68,11 @@ fa_scan_params process_scan(const fa_scan_params& in, int nz, int nD) {
   }
   return out;
 }
+
+}  // namespace fa_rt
+
+namespace {
+
 
 struct ScanEval {
   fa_scan_params p;
@@ -192,6 +197,10 @@ fa_status build_geometry(const fa_scan_params& scan, int nz, int ny, int nx, int
   return FA_OK;
 }
 
+}  // namespace
+
+namespace fa_rt {
+
 // Control-point parameters of the fused pass from a host displacement set (see kDParamF4).
 void make_dparams(const double* D, int nD, int n_dim, float4* out) {
   for (int k = 0; k < nD; k++) {
@@ -207,11 +216,25 @@ void make_dparams(const double* D, int nD, int n_dim, float4* out) {
   }
 }
 
+}  // namespace fa_rt
+
+namespace {
+
+
+}  // namespace
+
+namespace fa_rt {
+
 bool finite_all(const double* v, size_t n) {
   for (size_t i = 0; i < n; i++)
     if (!std::isfinite(v[i])) return false;
   return true;
 }
+
+}  // namespace fa_rt
+
+namespace {
+
 
 }  // namespace
 
@@ -1352,6 +1375,7 @@ extern "C" fa_status fa_test_tr_subproblem(fa_context* ctx, int nD, int n_dim, c
 namespace {
 
 void aligner_release_reference(fa_aligner* A) {
+  aligner_release_results(A);
   for (fa_frame* f : A->slots) fa_deregister_frame(f);
   A->slots.clear();
   A->slot_kind = -1;

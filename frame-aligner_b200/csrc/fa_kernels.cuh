@@ -79,6 +79,19 @@ cudaError_t launch_test_subproblem(const double* Hd, const double* Hl, int nD, i
                                    const double* g, double radius, double* p_out, int* boundary_out, double* work,
                                    cudaStream_t s);
 
+// Outputs after the solve (fa_output.cu). scan4 = processed {pixel, interline, interframe, stack}.
+// Forward splat of a dense raw frame (FA_F32 / FA_U16) by D (device, nD x 3): coverage always, the
+// intensity-preserving image when wimg is set (both zeroed first).
+cudaError_t launch_splat(const RefDev* ref_dev, const RefDev& ref_host, const double* scan4, const void* img,
+                         int img_kind, const double* D_dev, float* wimg, float* cov, cudaStream_t s);
+// Masked sums for the correlations of the warped frame and of the unaligned frame (raw + 1) against
+// the reference over cov > 0: totals[0..7) = count, sum w, sum r, sum ww, sum rr, sum f, sum ff;
+// totals[8..10) = the centred cross sums. parts: 296 x 8 doubles of scratch.
+cudaError_t launch_metrics(const float* cov, const float* warped, const float* ref, const void* raw, int raw_kind,
+                           long long n, double* parts, double* totals, cudaStream_t s);
+// convertTo(CV_16U) of num (or num / den).
+cudaError_t launch_to_u16(const float* num, const float* den, long long n, unsigned short* out, cudaStream_t s);
+
 // Phase correlation kernels (fa_phase.cu), each over a batch of frames.
 cudaError_t launch_phase_window(const void* const* vols, int in_kind, const double* wy, const double* wx, int ny,
                                 int nx, long long n_el, int batch, double* out, cudaStream_t s);

@@ -145,6 +145,16 @@ struct fa_aligner {
   size_t vols_count = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = 0;
+  // per-frame outputs and metrics (fa_aligner_results): an FP32 frame slot and work buffers
+  fa_frame* res_slot = nullptr;
+  void* res_raw = nullptr;
+  float* res_wimg = nullptr;
+  float* res_cov = nullptr;
+  float* res_warp = nullptr;
+  unsigned short* res_u16 = nullptr;
+  double* res_D = nullptr;
+  double* res_parts = nullptr;
+  std::vector<fa_rt::Alloc> res_allocs;
   std::vector<fa_rt::Alloc> allocs;   // staging / vols
   std::vector<fa_rt::Alloc> ref_allocs;
   std::mutex mu;
@@ -165,6 +175,13 @@ fa_status dalloc_t(fa_context* ctx, size_t count, T** out, std::vector<Alloc>& o
 void dfree_all(fa_context* ctx, std::vector<Alloc>& owner);
 
 size_t dtype_size(fa_dtype t);
+// ImageScanParameters after AbstractFrameWarper::processScanParameters.
+fa_scan_params process_scan(const fa_scan_params& in, int nz, int nD);
+// Control-point parameters of the fused pass (3 float4 per control point) from D (nD x 3 doubles).
+void make_dparams(const double* D, int nD, int n_dim, float4* out);
+bool finite_all(const double* v, size_t n);
+// Frees the buffers of fa_aligner_results (with the aligner's reference).
+void aligner_release_results(fa_aligner* A);
 // Frame slot (zero-halo storage of the given FrameKind + solve buffers + stream) for reference R.
 fa_status frame_alloc(fa_reference* R, int kind, fa_frame** out);
 // Slot storage the aligner uses for frames of dtype (raw uint16 counts + 1, FP16 or FP32 values + 1).

@@ -68,6 +68,8 @@ class AlignerParams(C.Structure):
         ("smoothing", C.c_double),
         ("precision", C.c_int),
         ("max_iterations", C.c_int),
+        ("correlation_threshold", C.c_double),
+        ("coverage_threshold", C.c_double),
     ]
 
 
@@ -85,6 +87,14 @@ class ServerStats(C.Structure):
         ("slot_bytes", C.c_size_t), ("peak_slot_bytes", C.c_size_t),
         ("graph_launches", C.c_longlong),
     ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class FrameResult(C.Structure):
+    _fields_ = [("correlation", C.c_double), ("unaligned_correlation", C.c_double), ("coverage", C.c_double),
+                ("use_frame", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -149,6 +159,8 @@ SIGNATURES = {
     "fa_aligner_info": [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)],
     "fa_aligner_add_frames": [_vp, _vp, C.c_int, C.c_int, _f64p, _vp],
     "fa_aligner_add_frames_device": [_vp, _vp, C.c_int, C.c_int, _f64p, _vp],
+    "fa_warp_image": [_vp, _f32p, _f64p, _vp, _f32p],
+    "fa_aligner_results": [_vp, _vp, C.c_int, C.c_int, _f64p, _vp, _vp, _vp, _vp],
     "fa_server_create": [_vp, C.POINTER(ServerConfig), C.POINTER(_vp)],
     "fa_server_destroy": [_vp],
     "fa_server_add_acquisition": [_vp, C.POINTER(AlignerParams), _vp, C.c_int, C.c_int, C.c_int, C.c_int,
@@ -270,6 +282,15 @@ class Reference:
 
     def retune(self, tile_voxels, ctas_per_sm):
         check(lib().fa_reference_retune(self._h, tile_voxels, ctas_per_sm))
+
+    def warp_image(self, frame, D, want_image=True):
+        """fa_warp_image: forward intensity-preserving splat and coverage (AbstractFrameWarper::warpImage)."""
+        fr = np.ascontiguousarray(frame, dtype=np.float32).reshape(self.dims)
+        cov = np.empty(self.dims, np.float32)
+        wimg = np.empty(self.dims, np.float32) if want_image else None
+        check(lib().fa_warp_image(self._h, fr, np.ascontiguousarray(D, dtype=np.float64).reshape(-1, 3),
+                                  wimg.ctypes.data if want_image else None, cov))
+        return wimg, cov
 
     def ranges(self):
         r = np.empty(2 * self.nD, np.int32)
@@ -431,6 +452,30 @@ class Aligner:
         ms = C.c_double()
         check(lib().fa_aligner_last_device_ms(self._h, C.byref(ms)))
         return ms.value
+
+    def results(self, frames, D, images=False):
+        """fa_aligner_results: per frame the metrics dict, and with images=True also the realigned and
+        intensity-preserving realigned uint16 images and the coverage mask."""
+        arrs = [np.ascontiguousarray(f) for f in frames]
+        dt = arrs[0].dtype
+        if dt not in (np.float32, np.uint16):
+            arrs = [a.astype(np.float32) for a in arrs]
+            dt = np.dtype(np.float32)
+        n = len(arrs)
+        ptrs = (_vp * n)(*[a.ctypes.data for a in arrs])
+        D = np.ascontiguousarray(D, dtype=np.float64).reshape(n, self.nD, 3)
+        res = (FrameResult * n)()
+        if images:
+            out = {k: [np.empty(self.dims, t) for _ in range(n)]
+                   for k, t in (("realigned", np.uint16), ("realigned_preserving", np.uint16), ("mask", np.float32))}
+            pa = {k: (_vp * n)(*[o.ctypes.data for o in v]) for k, v in out.items()}
+            check(lib().fa_aligner_results(self._h, C.cast(ptrs, _vp), _DTYPES[dt], n, D, C.cast(res, _vp),
+                                           C.cast(pa["realigned"], _vp), C.cast(pa["realigned_preserving"], _vp),
+                                           C.cast(pa["mask"], _vp)))
+            return [r.as_dict() for r in res], out
+        check(lib().fa_aligner_results(self._h, C.cast(ptrs, _vp), _DTYPES[dt], n, D, C.cast(res, _vp), None, None,
+                                       None))
+        return [r.as_dict() for r in res]
 
     def add_frames_device(self, ptrs, dtype, n):
         arr = (_vp * n)(*ptrs)

@@ -153,6 +153,12 @@ fa_status fa_get_jacobian(fa_frame* frame, const double* D, double* jac);
    nz*ny*nx floats. */
 fa_status fa_warp(fa_frame* frame, const double* D, float invalid_value, float* out);
 
+/* AbstractFrameWarper::warpImage (FrameAligner/FrameWarper.cpp:71-136): the forward,
+   intensity-preserving splat of a frame (host, nz*ny*nx floats) by D into wimg (may be NULL) and the
+   sum of splat weights per voxel into coverage; host outputs. Sums agree with the reference to float
+   rounding (contributions are added in arbitrary order). */
+fa_status fa_warp_image(fa_reference* ref, const float* frame, const double* D, float* wimg, float* coverage);
+
 /* ---------------------------------------------------------------- alignment ------------------- */
 
 typedef struct {
@@ -208,7 +214,17 @@ typedef struct {
   double smoothing;          /* must be 0: the Gaussian pre-smoothing (FrameWarpAligner.cpp:46-64) is not built */
   fa_precision precision;
   int max_iterations;        /* <= 0: 100 */
+  double correlation_threshold;  /* RealignmentParameters::correlation_threshold (RealignmentResult::useFrame) */
+  double coverage_threshold;     /* RealignmentParameters::coverage_threshold */
 } fa_aligner_params;
+
+/* RealignmentResult's metrics (FrameAligner/AbstractFrameAligner.h:51-66). */
+typedef struct {
+  double correlation;            /* correlation(warped, reference) over coverage > 0 (FrameWarpAligner.cpp:240) */
+  double unaligned_correlation;  /* correlation(frame, reference) over the same mask (:241) */
+  double coverage;               /* fraction of voxels with coverage > 0 (:243) */
+  int use_frame;                 /* RealignmentResult::useFrame with the aligner's thresholds */
+} fa_frame_result;
 
 fa_status fa_aligner_create(fa_context* ctx, const fa_aligner_params* params, fa_aligner** out);
 fa_status fa_aligner_destroy(fa_aligner* a);
@@ -225,6 +241,17 @@ fa_status fa_aligner_add_frames(fa_aligner* a, const void* const* frames, fa_dty
 /* Same, frames already in device memory (frames[i] device pointers). */
 fa_status fa_aligner_add_frames_device(fa_aligner* a, const void* const* frames, fa_dtype dtype, int n,
                                        double* D_out, fa_align_stats* stats);
+
+/* The end of FrameWarpAligner::addFrame (FrameAligner/FrameWarpAligner.cpp:221-247) and its cached
+   outputs, for n frames already aligned (D: n*nD*3, e.g. from fa_aligner_add_frames): the forward
+   splat's coverage, the correlations and coverage fraction (results, may be NULL), and optionally
+   per frame (arrays of n host pointers, or NULL; an entry may be NULL) the realigned image
+   (getInterpolatedWarpedFrame :328-338, uint16), the intensity-preserving realigned image
+   (getWarpedFrame :317-326, uint16) and the mask (getMask :340-346, the coverage, float).
+   frames: raw frames in host memory (dtype FA_F32 or FA_U16). */
+fa_status fa_aligner_results(fa_aligner* a, const void* const* frames, fa_dtype dtype, int n, const double* D,
+                             fa_frame_result* results, uint16_t* const* realigned,
+                             uint16_t* const* realigned_preserving, float* const* mask);
 
 /* ---------------------------------------------------------------- serving ---------------------- */
 
