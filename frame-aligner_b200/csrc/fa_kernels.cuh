@@ -89,6 +89,9 @@ cudaError_t launch_splat(const RefDev* ref_dev, const RefDev& ref_host, const do
 // totals[8..10) = the centred cross sums. parts: 296 x 8 doubles of scratch.
 cudaError_t launch_metrics(const float* cov, const float* warped, const float* ref, const void* raw, int raw_kind,
                            long long n, double* parts, double* totals, cudaStream_t s);
+// FrameWarpAligner::shiftPixel for n points (device arrays, in place).
+cudaError_t launch_shift_points(const RefDev* ref_dev, const double* scan4, const double* D_dev, long long n, double* x,
+                                double* y, double* z, cudaStream_t s);
 // convertTo(CV_16U) of num (or num / den).
 cudaError_t launch_to_u16(const float* num, const float* den, long long n, unsigned short* out, cudaStream_t s);
 

@@ -16,6 +16,7 @@
 // blocks in order), so they are deterministic.
 #include <cmath>
 #include <cstring>
+#include <fstream>
 
 #include "fa_runtime.h"
 
@@ -185,7 +186,44 @@ __global__ void to_u16_kernel(const float* __restrict__ num, const float* __rest
   }
 }
 
+// FrameWarpAligner::shiftPixel (FrameWarpAligner.cpp:253-266) for n points: warpPoint
+// (FrameWarper.cpp:397-419) is called with the coordinates converted to int (truncation), and points
+// outside the volume are not moved.
+__global__ void shift_points_kernel(const RefDev* __restrict__ Rp, ScanD sc, const double* __restrict__ D, long long n,
+                                    double* __restrict__ px, double* __restrict__ py, double* __restrict__ pz) {
+  const RefDev& R = *Rp;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const double x = px[k], y = py[k], z = pz[k];
+    // int conversion of coordinates that fit in an int; others are outside the volume anyway
+    const bool fits = fabs(x) < 2147483647.0 && fabs(y) < 2147483647.0 && fabs(z) < 2147483647.0;
+    if (!fits) continue;
+    const int xi = (int)x, yi = (int)y, zi = (int)z;
+    if (xi < 0 || xi >= R.nx || yi < 0 || yi >= R.ny || zi < 0 || zi >= R.nz) continue;
+    int i;
+    double f;
+    exact_interval(R, sc, xi, yi, zi, &i, &f);
+    const double g = __dsub_rn(1.0, f);
+    const int nd = R.n_dim;
+    double d[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      d[c] = c < nd ? __dadd_rn(__dmul_rn(f, D[3 * (i + 1) + c]), __dmul_rn(g, D[3 * i + c])) : 0.0;
+    px[k] = __dsub_rn(x, d[0]);
+    py[k] = __dsub_rn(y, d[1]);
+    pz[k] = __dsub_rn(z, d[2]);
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_shift_points(const RefDev* ref_dev, const double* scan4, const double* D_dev, long long n, double* x,
+                                double* y, double* z, cudaStream_t s) {
+  const ScanD sc{scan4[0], scan4[1], scan4[2], scan4[3]};
+  long long blocks = (n + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  shift_points_kernel<<<(int)(blocks < 1 ? 1 : blocks), 256, 0, s>>>(ref_dev, sc, D_dev, n, x, y, z);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_splat(const RefDev* ref_dev, const RefDev& R, const double* scan4, const void* img, int img_kind,
                          const double* D_dev, float* wimg, float* cov, cudaStream_t s) {
@@ -381,5 +419,72 @@ extern "C" fa_status fa_aligner_results(fa_aligner* A, const void* const* frames
       r.use_frame = (r.correlation >= A->prm.correlation_threshold && r.coverage >= A->prm.coverage_threshold) ? 1 : 0;
     }
   }
+  return FA_OK;
+}
+
+extern "C" fa_status fa_shift_pixels(fa_reference* R, const double* D, long long n, double* x, double* y, double* z) {
+  if (!R || !D || n < 0 || (n > 0 && (!x || !y || !z))) return fail(FA_ERR_BAD_ARG, "bad arguments");
+  if (n == 0) return FA_OK;
+  if (!finite_all(D, (size_t)R->nD * 3)) return fail(FA_ERR_BAD_ARG, "D has non-finite entries");
+  FA_CU(cudaSetDevice(R->ctx->device));
+  std::vector<Alloc> tmp;
+  double *dx, *dy, *dz, *Dd;
+  auto done = [&](fa_status st) {
+    std::string keep = g_err;
+    cudaStreamSynchronize(R->stream);
+    dfree_all(R->ctx, tmp);
+    g_err = keep;
+    return st;
+  };
+  fa_status st;
+  if ((st = dalloc_t(R->ctx, (size_t)n, &dx, tmp)) != FA_OK) return done(st);
+  if ((st = dalloc_t(R->ctx, (size_t)n, &dy, tmp)) != FA_OK) return done(st);
+  if ((st = dalloc_t(R->ctx, (size_t)n, &dz, tmp)) != FA_OK) return done(st);
+  if ((st = dalloc_t(R->ctx, (size_t)R->nD * 3, &Dd, tmp)) != FA_OK) return done(st);
+  double scan4[4];
+  scan4_of(R, scan4);
+  cudaStream_t s = R->stream;
+  const size_t b = (size_t)n * sizeof(double);
+  cudaError_t e = cudaMemcpyAsync(dx, x, b, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dy, y, b, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dz, z, b, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(Dd, D, (size_t)R->nD * 3 * sizeof(double), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = fa::launch_shift_points(R->dev, scan4, Dd, n, dx, dy, dz, s);
+  g_launches += 1;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(x, dx, b, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(y, dy, b, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(z, dz, b, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return done(fail(FA_ERR_CUDA, std::string("shift pixels: ") + cudaGetErrorString(e)));
+  return done(FA_OK);
+}
+
+extern "C" fa_status fa_write_realignment_info(const char* filename, const fa_scan_params* image_params, int n_frames,
+                                               int nD, const double* D, const fa_frame_result* results) {
+  if (!filename || !image_params || n_frames < 0 || nD < 1 || (n_frames > 0 && (!D || !results)))
+    return fail(FA_ERR_BAD_ARG, "bad arguments");
+  if (n_frames == 0) return FA_OK;  // the reference writes nothing without frames
+  std::ofstream os(filename);
+  if (!os) return fail(FA_ERR_BAD_ARG, std::string("cannot open ") + filename);
+  // FrameWarpAligner::writeRealignmentInfo (FrameWarpAligner.cpp:288-314), default stream formatting
+  os << "Realignment Information Version, 2\n";
+  os << "Line Duration," << image_params->line_duration << "\n";
+  os << "Interline Duration," << image_params->interline_duration << "\n";
+  os << "Frame Duration," << image_params->frame_duration << "\n";
+  os << "Interframe Duration," << image_params->interframe_duration << "\n";
+  os << "Lines," << image_params->n_y << "\n";
+  os << "Frames Per Stack," << image_params->n_z << "\n";
+  os << "Frame, UnalignedCorrelation, Correlation, Coverage";
+  for (int j = 0; j < nD; j++) os << ", dx_" << j << ", dy_" << j << ", dz_" << j;
+  os << "\n";
+  for (int i = 0; i < n_frames; i++) {
+    os << i << "," << results[i].unaligned_correlation << "," << results[i].correlation << ", " << results[i].coverage;
+    for (int j = 0; j < nD; j++) {
+      const double* d = D + ((size_t)i * nD + j) * 3;
+      os << ", " << d[0] << ", " << d[1] << ", " << d[2];
+    }
+    os << "\n";
+  }
+  if (!os) return fail(FA_ERR_CUDA, "write failed");
   return FA_OK;
 }

@@ -161,6 +161,8 @@ SIGNATURES = {
     "fa_aligner_add_frames_device": [_vp, _vp, C.c_int, C.c_int, _f64p, _vp],
     "fa_warp_image": [_vp, _f32p, _f64p, _vp, _f32p],
     "fa_aligner_results": [_vp, _vp, C.c_int, C.c_int, _f64p, _vp, _vp, _vp, _vp],
+    "fa_shift_pixels": [_vp, _f64p, C.c_longlong, _f64p, _f64p, _f64p],
+    "fa_write_realignment_info": [C.c_char_p, C.POINTER(ScanParams), C.c_int, C.c_int, _f64p, _vp],
     "fa_server_create": [_vp, C.POINTER(ServerConfig), C.POINTER(_vp)],
     "fa_server_destroy": [_vp],
     "fa_server_add_acquisition": [_vp, C.POINTER(AlignerParams), _vp, C.c_int, C.c_int, C.c_int, C.c_int,
@@ -291,6 +293,13 @@ class Reference:
         check(lib().fa_warp_image(self._h, fr, np.ascontiguousarray(D, dtype=np.float64).reshape(-1, 3),
                                   wimg.ctypes.data if want_image else None, cov))
         return wimg, cov
+
+    def shift_pixels(self, D, x, y, z):
+        """fa_shift_pixels: FrameWarpAligner::shiftPixel for arrays of photon coordinates (copies)."""
+        xs, ys, zs = (np.array(v, dtype=np.float64).ravel() for v in (x, y, z))
+        check(lib().fa_shift_pixels(self._h, np.ascontiguousarray(D, dtype=np.float64).reshape(-1, 3), xs.size,
+                                    xs, ys, zs))
+        return xs, ys, zs
 
     def ranges(self):
         r = np.empty(2 * self.nD, np.int32)
@@ -648,3 +657,14 @@ class B200FrameWarper:
 
     def warpImageInterpolated(self, frame, D, invalid_value=0):
         return self._frame(frame).warp(D, invalid_value)
+
+
+def write_realignment_info(filename, scan: ScanParams, D, results):
+    """fa_write_realignment_info: D (n, nD, 3), results: list of FrameResult dicts."""
+    D = np.ascontiguousarray(D, dtype=np.float64)
+    n, nD = D.shape[0], D.shape[1]
+    res = (FrameResult * max(n, 1))()
+    for i, r in enumerate(results):
+        res[i] = FrameResult(r["correlation"], r["unaligned_correlation"], r["coverage"], r.get("use_frame", 1))
+    check(lib().fa_write_realignment_info(filename.encode(), C.byref(scan), n, nD, D.reshape(-1) if n else
+                                          np.zeros(3), C.cast(res, _vp)))

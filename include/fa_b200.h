@@ -253,6 +253,18 @@ fa_status fa_aligner_results(fa_aligner* a, const void* const* frames, fa_dtype 
                              fa_frame_result* results, uint16_t* const* realigned,
                              uint16_t* const* realigned_preserving, float* const* mask);
 
+/* FrameWarpAligner::shiftPixel (FrameAligner/FrameWarpAligner.cpp:253-266) for n photons: each
+   (x, y, z) moves by minus warpPoint(D, int(x), int(y), int(z)) (FrameWarper.cpp:397-419), the
+   displacement of the voxel it was recorded in; points outside the volume stay. Host arrays,
+   updated in place; D: nD*3 doubles of one frame. */
+fa_status fa_shift_pixels(fa_reference* ref, const double* D, long long n, double* x, double* y, double* z);
+
+/* FrameWarpAligner::writeRealignmentInfo (FrameAligner/FrameWarpAligner.cpp:288-314): the CSV of
+   the scan parameters (as given, not processed), per-frame metrics and D (n_frames*nD*3 doubles).
+   Host only; writes nothing when n_frames == 0. */
+fa_status fa_write_realignment_info(const char* filename, const fa_scan_params* image_params, int n_frames, int nD,
+                                    const double* D, const fa_frame_result* results);
+
 /* ---------------------------------------------------------------- serving ---------------------- */
 
 /* A device-resident request loop over several concurrent acquisitions (no single counterpart in the

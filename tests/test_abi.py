@@ -54,3 +54,28 @@ def test_gpu_support_reports_without_a_device():
     ok, msg = fa.gpu_support()
     if not ok:
         assert msg  # "No compatible GPU" / "Insufficient Driver" (GpuFrameWarper.cpp:16-44)
+
+
+def test_realignment_info_csv(tmp_path):
+    """fa_write_realignment_info writes FrameWarpAligner::writeRealignmentInfo's format
+    (FrameWarpAligner.cpp:288-314; C++ default stream formatting = printf %g)."""
+    import fa_b200 as fa
+
+    scan = fa.ScanParams()
+    fa.check(fa.lib().fa_scan_params_init(1.0, 1.01, 51.7, 32, 48, 3, 0, scan))
+    rng = np.random.default_rng(3)
+    D = rng.normal(0, 2, (2, 4, 3))
+    res = [{"correlation": 0.91234567, "unaligned_correlation": 0.5, "coverage": 1.0},
+           {"correlation": 1e-7, "unaligned_correlation": -0.25, "coverage": 0.875}]
+    f = tmp_path / "info.csv"
+    fa.write_realignment_info(str(f), scan, D, res)
+    g = lambda v: "%g" % v  # noqa: E731
+    want = ["Realignment Information Version, 2", "Line Duration," + g(scan.line_duration),
+            "Interline Duration," + g(scan.interline_duration), "Frame Duration," + g(scan.frame_duration),
+            "Interframe Duration," + g(scan.interframe_duration), "Lines,48", "Frames Per Stack,3",
+            "Frame, UnalignedCorrelation, Correlation, Coverage" + "".join(
+                ", dx_%d, dy_%d, dz_%d" % (j, j, j) for j in range(4))]
+    for i, r in enumerate(res):
+        want.append("%d,%s,%s, %s" % (i, g(r["unaligned_correlation"]), g(r["correlation"]), g(r["coverage"])) +
+                    "".join(", %s, %s, %s" % tuple(g(v) for v in D[i, j]) for j in range(4)))
+    assert f.read_text() == "\n".join(want) + "\n"

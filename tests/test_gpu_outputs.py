@@ -93,3 +93,30 @@ def test_aligner_results_against_oracle(ctx, shape, nD, precision):
         with np.errstate(invalid="ignore", divide="ignore"):
             assert _u16_ok(imgs["realigned_preserving"][k], wimg / cov)
         assert _u16_ok(imgs["realigned"][k], ow.warp_interpolated(frame, D[k], 0.0))
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_shift_pixels_against_oracle(ctx, name):
+    """FrameWarpAligner::shiftPixel: coordinates truncated to int for warpPoint, points outside the
+    volume unchanged; displacements from the oracle's warpPoint (pinned to the reference build)."""
+    g = load_golden(name)
+    nz, ny, nx = g["reference"].shape
+    line, il, ifr = g["scan"]
+    ref = fa.Reference(ctx, g["reference"], int(g["nD"]), _scan(g), fa.PREC_F32)
+    ow = O.OracleWarper(g["reference"], int(g["nD"]), O.scan_init(line, il, ifr, nx, ny, nz, bool(g["bidirectional"])))
+    rng = np.random.default_rng(5)
+    n = 500
+    x = rng.uniform(-1.5, nx + 0.5, n)
+    y = rng.uniform(-1.5, ny + 0.5, n)
+    z = rng.uniform(-0.9, nz + 0.5, n) if nz > 1 else np.zeros(n)
+    D = g["D_a"]
+    sx, sy, sz = ref.shift_pixels(D, x, y, z)
+    ref.close()
+    for k in range(n):
+        xi, yi, zi = int(x[k]), int(y[k]), int(z[k])  # C++ double -> int truncation
+        if 0 <= xi < nx and 0 <= yi < ny and 0 <= zi < nz:
+            d = ow.warp_point(D, xi, yi, zi)
+            want = (x[k] - d[0], y[k] - d[1], z[k] - d[2] if nz > 1 else z[k])
+        else:
+            want = (x[k], y[k], z[k])
+        assert (sx[k], sy[k], sz[k]) == want, (k, (sx[k], sy[k], sz[k]), want)
