@@ -351,7 +351,8 @@ std::map<std::string, TuneResult> g_tune_cache;
 // persistent kernel the batched solver uses, on a launch of 8 synthetic frames (the reference itself,
 // slightly displaced) and on a launch of one, keeps the lowest sum of per-frame times, and caches the
 // choice per volume shape, control-point count and precision for the life of the process. Register
-// budgets under which the kernel spills are skipped (the largest budget is always a candidate).
+// budgets under which the kernel spills more than 128 bytes are skipped (the largest budget is
+// always a candidate).
 fa_status autotune(fa_reference* R) {
   char keyb[128];
   std::snprintf(keyb, sizeof(keyb), "%d,%d,%d,%d,%d,%d", R->nz, R->ny, R->nx, R->nD, (int)R->prec,
@@ -446,8 +447,8 @@ fa_status autotune(fa_reference* R) {
     if (e != cudaSuccess) break;
     for (int mb : mbs) {
       const bool mixed = R->prec == FA_PREC_MIXED;
-      // register budgets that make the kernel spill to local memory are not candidates
-      if (mb != mbs[0] && fa::eval4_active_local_bytes(R->n_dim, kind, mixed, mb) > 0) continue;
+      // register budgets under which the kernel spills more than a few values are not candidates
+      if (mb != mbs[0] && fa::eval4_active_local_bytes(R->n_dim, kind, mixed, mb) > 128) continue;
       auto launch = [&]() {
         return fa::launch_eval4_active(jobs_dev, list, cnt, prefix, (long long)K * R->G.n_tiles, R->n_dim, kind, mixed,
                                        mb, mb * sms, s);

@@ -163,7 +163,7 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
       const long long p0 = (long long)row_here * nx + x0;
       float t4[4], g4[NDIM][4];
       load4(tref + p0, t4);
-  #pragma unroll
+#pragma unroll
       for (int k = 0; k < NDIM; k++) load4(tg[k] + p0, g4[k]);
 
       // Do the four voxels share interval, storage range and integer tap offsets, away from edges?
@@ -197,7 +197,7 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
       }
 
       float acc0[NDIM], acc1[NDIM];  // J^T e of controls r and r+1 for this lane's voxels
-  #pragma unroll
+#pragma unroll
       for (int k = 0; k < NDIM; k++) acc0[k] = acc1[k] = 0.0f;
 
       if (fast) {
@@ -239,7 +239,7 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
           }
         }
         const float wx0 = t0x - flx, wy0 = t0y - fly, wz0 = t0z - flz;
-  #pragma unroll
+#pragma unroll
         for (int j = 0; j < 4; j++) {
           const float wx = fmaf((float)j, sx, wx0), wy = fmaf((float)j, sy, wy0);
           const float c00 = fmaf(wx, v[0][j + 1] - v[0][j], v[0][j]);
@@ -257,14 +257,14 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
           const float fj = fmaf((float)j, fs, f0);
           const float e1 = e * fj;
           const float e0 = e - e1;
-  #pragma unroll
+#pragma unroll
           for (int k = 0; k < NDIM; k++) {
             acc0[k] = fmaf(g4[k][j], e0, acc0[k]);
             acc1[k] = fmaf(g4[k][j], e1, acc1[k]);
           }
         }
       } else {
-  #pragma unroll
+#pragma unroll
         for (int j = 0; j < 4; j++) {
           const int x = x0 + j;
           const VoxelModel vm = voxel_model(rd, x, nx, flip, bidir, dq);
@@ -276,7 +276,7 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
             const float e1 = e * vm.f;
             const float e0 = e * (1.0f - vm.f);
             if (vm.r == r) {
-  #pragma unroll
+#pragma unroll
               for (int k = 0; k < NDIM; k++) {
                 acc0[k] = fmaf(g4[k][j], e0, acc0[k]);
                 acc1[k] = fmaf(g4[k][j], e1, acc1[k]);
@@ -284,7 +284,7 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
             } else {
               // voxel in the following range: controls r+1 and r+2
               const int s2 = vm.r - c0;
-  #pragma unroll
+#pragma unroll
               for (int k = 0; k < NDIM; k++) {
                 if (s2 == 1) {
                   ag[1][k] = fmaf(g4[k][j], e0, ag[1][k]);
@@ -299,13 +299,13 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
         }
       }
       if (r == c0) {
-  #pragma unroll
+#pragma unroll
         for (int k = 0; k < NDIM; k++) {
           ag[0][k] += acc0[k];
           ag[1][k] += acc1[k];
         }
       } else {
-  #pragma unroll
+#pragma unroll
         for (int k = 0; k < NDIM; k++) {
           ag[1][k] += acc0[k];
           ag[2][k] += acc1[k];
