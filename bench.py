@@ -54,6 +54,12 @@ def parse():
     ap.add_argument("--cpu-frames", type=int, default=0, help="CPU baseline sample size (0 = one per thread)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-uneven", action="store_true")
+    ap.add_argument("--large", action="store_true", help="also run the 1024x1024x64 volume (minutes of data set-up)")
+    ap.add_argument("--large-frames", type=int, default=200)
+    ap.add_argument("--large-pool", type=int, default=2)
+    ap.add_argument("--large-cpu", type=int, default=2, help="frames of the large volume solved on the CPU")
+    ap.add_argument("--uneven-pool", type=int, default=4, help="distinct frames per size in the uneven batch")
     ap.add_argument("--only", choices=["roofline"], default=None,
                     help="roofline: only the fused-pass probe on --frames FP16 frames (for ncu captures)")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="length of the Poisson arrival stream")
@@ -287,6 +293,129 @@ def measure_serving(fa, ctx, args, acqs, pools, lag):
             "graph_launches": stats["graph_launches"], "iterations_mean": float(np.mean(iters))}
 
 
+def measure_uneven(fa, ctx, args):
+    """The batched uneven-size workload: four single-plane acquisitions (128^2, 256^2, 512^2, 1024^2
+    with nD 8 / 16 / 32 / 64), 64 frames each (drawn in order from args.uneven_pool distinct frames per
+    size), BF16 reference / gradient, raw uint16 frames, all 256 frames submitted at once to a server
+    whose acquisitions share one launch group: one persistent graph launch per iteration over frames
+    of every size. Then, per size, each reduction of the mixed-precision pass at the solved D against
+    the FP64 CPU statement (oracle): f, J^T e and the Hessian."""
+    import oracle_py as O
+    import torch
+
+    acqs = S.config2_acquisitions(n_per_size=args.uneven_pool)
+    pools = [torch.from_numpy(np.ascontiguousarray(a.frames.astype(np.uint16)).view(np.int16)).pin_memory()
+             for a in acqs]
+    srv = fa.Server(ctx, warm_start=False, shared_launches=True, max_in_flight=256)
+    ids = []
+    for a in acqs:
+        nz, ny, nx = a.reference.shape
+        line, il, ifr = a.scan
+        ids.append(srv.add_acquisition(a.reference, fa.scan_params(line, il, ifr, nx, ny, nz), frame_dtype=np.uint16,
+                                       nD=a.nD, precision=fa.PREC_MIXED))
+        srv.reserve(ids[-1], 64)
+    per = 64
+
+    def burst():
+        ts = [(j, k, srv.submit_ptr(ids[j], pools[j][k % args.uneven_pool].data_ptr(), False))
+              for k in range(per) for j in range(len(acqs))]
+        return [(j, k, srv.wait(t, 300.0)) for j, k, t in ts]
+
+    burst()  # warm-up: graphs, slots, cuFFT plans
+    srv.reset_stats()
+    t0 = time.perf_counter()
+    out = burst()
+    wall = time.perf_counter() - t0
+    stats = srv.stats()
+    srv.close()
+    errors = []
+    for j, a in enumerate(acqs):
+        nz, ny, nx = a.reference.shape
+        line, il, ifr = a.scan
+        D_sol = next(r[0] for jj, k, r in out if jj == j and k == 0)
+        D_zero = np.zeros_like(D_sol)
+        frame = a.frames[0] + 1
+        ref = fa.Reference(ctx, a.reference + 1, a.nD, fa.scan_params(line, il, ifr, nx, ny, nz), fa.PREC_MIXED)
+        fr = fa.Frame(ref, frame.astype(np.float16))
+        ow = O.OracleWarper(a.reference + 1, a.nD, O.scan_init(line, il, ifr, nx, ny, nz))
+        row = {"size": "%dx%d" % (ny, nx), "nD": a.nD}
+        # f at the zero start and at the solution; J^T e at the zero start, where it is far from zero
+        # (at the solution it is noise around zero and a relative error says nothing)
+        for tag, D in (("start", D_zero), ("solution", D_sol)):
+            f_gpu = fr.get_error(D)
+            f_cpu, e = ow.get_error(frame, D, want_image=True)
+            row["f_rel_" + tag] = abs(f_gpu - f_cpu) / abs(f_cpu)
+            if tag == "start":
+                g_gpu, g_cpu = fr.get_jacobian(D), ow.get_jacobian_from_error(e)
+                row["jte_rel_max_start"] = float(np.max(np.abs(g_gpu - g_cpu)) / np.max(np.abs(g_cpu)))
+        H_gpu, H_cpu = ref.hessian(), ow.hessian()
+        row["hessian_rel_max"] = float(np.max(np.abs(H_gpu - H_cpu)) / np.max(np.abs(H_cpu)))
+        fr.close()
+        ref.close()
+        errors.append(row)
+    return {"workload": "4 single-plane acquisitions 128^2 / 256^2 / 512^2 / 1024^2, nD 8 / 16 / 32 / 64, "
+                        "64 raw uint16 frames each (%d distinct per size), one shared launch group" % args.uneven_pool,
+            "frames": per * len(acqs), "wall_s": wall, "frames_per_s": per * len(acqs) / wall,
+            "graph_launches": stats["graph_launches"],
+            "reduction_error_vs_fp64_oracle": errors,
+            "note": "errors of the mixed-precision pass (BF16 reference/gradient, FP16 frame, FP32 sums over "
+                    "tiles of <= 2048 voxels, FP64 across tiles) against the FP64 CPU statement, each size's first "
+                    "frame: f at the zero start and at the solved D, J^T e (max error / max |J^T e|) at the zero "
+                    "start, the Hessian (FP64 from the FP32 gradient)"}
+
+
+def measure_large(fa, ctx, args, local):
+    """The large-volume workload: 1024x1024x64 reference (5000 blobs, mean 15 photons), nD = 64, three
+    displacement components; args.large_frames frames (cycled from args.large_pool distinct ones)
+    aligned through the full aligner pipeline -- 3-D FP64 phase correlation, then the batched solve --
+    in calls of 50 raw uint16 frames resident in HBM; the fused pass's unique-byte rate on 8 frames;
+    displacement RMS against the reference CPU solve of the first args.large_cpu frames."""
+    import torch
+
+    acq = S.make_config(S.CONFIG4, n_frames=args.large_pool)
+    nz, ny, nx = acq.reference.shape
+    N = nz * ny * nx
+    line, il, ifr = acq.scan
+    scan = fa.scan_params(line, il, ifr, nx, ny, nz)
+    al = fa.Aligner(ctx, nD=acq.nD, precision=fa.PREC_MIXED, max_iterations=100)
+    al.set_reference(acq.reference, scan)
+    dev = torch.from_numpy(np.ascontiguousarray(acq.frames.astype(np.uint16)).view(np.int16)).to(f"cuda:{local}")
+    batch = 50
+    ptrs = [dev[k % args.large_pool].data_ptr() for k in range(batch)]
+    D, _ = al.add_frames_device(ptrs, fa.U16, batch)  # warm-up
+    ms, iters = 0.0, []
+    done = 0
+    while done < args.large_frames:
+        m = min(batch, args.large_frames - done)
+        D, st = al.add_frames_device(ptrs[:m], fa.U16, m)
+        ms += al.last_device_ms()
+        iters += [x["iterations"] for x in st]
+        done += m
+    al.close()
+    del dev
+    torch.cuda.empty_cache()
+    ref = fa.Reference(ctx, acq.reference + 1, acq.nD, scan, fa.PREC_MIXED)
+    frs = [fa.Frame(ref, (acq.frames[k % args.large_pool] + 1).astype(np.float16)) for k in range(8)]
+    eval_ms = fa.profile_eval(frs, acq.D_true[0], 5)
+    for f in frs:
+        f.close()
+    ref.close()
+    algo = 8 * N * 2 + N * 8
+    peak, _ = load_peaks()
+    rms = None
+    if args.large_cpu > 0:
+        _, D_cpu, _ = cpu_baseline(acq, args.large_cpu, args.large_cpu)  # one thread per frame
+        rms = float(np.sqrt(((D[:args.large_cpu] - D_cpu) ** 2).sum(-1).mean()))
+    return {"workload": "1024x1024x64 reference, nD = 64, 3 components, %d frames (%d distinct), raw uint16 in HBM, "
+                        "calls of %d" % (args.large_frames, args.large_pool, batch),
+            "frames_per_s": args.large_frames / (ms / 1000.0), "device_ms": ms,
+            "iterations_mean": float(np.mean(iters)),
+            "fused_pass_8_frames": {"ms_per_launch": eval_ms, "unique_bytes": algo,
+                                    "achieved_gbs": algo / (eval_ms / 1000.0) / 1e9,
+                                    "frac_of_measured_hbm": algo / (eval_ms / 1000.0) / 1e9 / peak},
+            "displacement_rms_vs_cpu_px": rms, "cpu_frames": args.large_cpu}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
@@ -451,6 +580,10 @@ def run_ours(args, rank, world, local):
                        "frames_from": "pinned host memory (raw uint16), %d distinct frames per acquisition"
                                       % args.serve_pool,
                        "runs": [measure_serving(fa, ctx, args, sacqs, spools, lag) for lag in args.serve_lags]}
+        large = measure_large(fa, ctx, args, local) if args.large else None
+        uneven = None
+        if not args.no_uneven:
+            uneven = measure_uneven(fa, ctx, args)
         rms_vs_cpu = None
         if D_cpu is not None:
             k = D_cpu.shape[0]
@@ -465,6 +598,8 @@ def run_ours(args, rank, world, local):
                "batched_over_plain": value / world / plain["value"],
                "e2e_over_plain_e2e": e2e["value"] / world / plain["e2e"],
                "serving": serving,
+               "batched_uneven": uneven,
+               "large_volume": large,
                "displacement_rms_vs_cpu_px": rms_vs_cpu,
                "iterations": {"mean": float(np.mean(iters)), "max": int(np.max(iters))}}
     if pg:
