@@ -1574,6 +1574,13 @@ extern "C" fa_status fa_aligner_set_reference(fa_aligner* A, const void* referen
   return st;
 }
 
+extern "C" fa_status fa_aligner_reference(const fa_aligner* A, fa_reference** ref) {
+  if (!A || !ref) return fail(FA_ERR_BAD_ARG, "NULL argument");
+  if (!A->ref) return fail(FA_ERR_STATE, "Reference imaging not yet set");
+  *ref = A->ref;
+  return FA_OK;
+}
+
 extern "C" fa_status fa_aligner_info(const fa_aligner* A, int* nD, int* n_dim) {
   if (!A || !A->ref) return fail(FA_ERR_STATE, "Reference imaging not yet set");
   if (nD) *nD = A->ref->nD;

@@ -157,6 +157,7 @@ SIGNATURES = {
     "fa_aligner_destroy": [_vp],
     "fa_aligner_set_reference": [_vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(ScanParams)],
     "fa_aligner_info": [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)],
+    "fa_aligner_reference": [_vp, C.POINTER(_vp)],
     "fa_aligner_add_frames": [_vp, _vp, C.c_int, C.c_int, _f64p, _vp],
     "fa_aligner_add_frames_device": [_vp, _vp, C.c_int, C.c_int, _f64p, _vp],
     "fa_warp_image": [_vp, _f32p, _f64p, _vp, _f32p],

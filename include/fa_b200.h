@@ -234,6 +234,10 @@ fa_status fa_aligner_set_reference(fa_aligner* a, const void* reference, fa_dtyp
                                    const fa_scan_params* scan);
 /* The control-point count and parameter layout of the current reference. */
 fa_status fa_aligner_info(const fa_aligner* a, int* nD, int* n_dim);
+/* The aligner's warper (FrameWarpAligner::warper): the reference it aligns against, with the +1
+   offset, for the warper-level calls (fa_warp_image, fa_shift_pixels, fa_get_hessian ...). Owned by
+   the aligner; valid until its next fa_aligner_set_reference or fa_aligner_destroy. */
+fa_status fa_aligner_reference(const fa_aligner* a, fa_reference** ref);
 /* FrameWarpAligner::addFrame for n raw frames (host memory; frames[i] points at nz*ny*nx elements of
    dtype). D_out: n*nD*3 doubles, stats: n entries or NULL; host memory. */
 fa_status fa_aligner_add_frames(fa_aligner* a, const void* const* frames, fa_dtype dtype, int n, double* D_out,
