@@ -1377,6 +1377,9 @@ namespace {
 
 void aligner_release_reference(fa_aligner* A) {
   aligner_release_results(A);
+  dfree_all(A->ctx, A->smooth_allocs);
+  A->smooth_kx = A->smooth_ky = A->smooth_tmp = A->smooth_out = nullptr;
+  A->smooth_nkx = A->smooth_nky = 0;
   for (fa_frame* f : A->slots) fa_deregister_frame(f);
   A->slots.clear();
   A->slot_kind = -1;
@@ -1397,10 +1400,11 @@ size_t dtype_size(fa_dtype t) { return t == FA_F32 ? 4 : 2; }
 
 namespace fa_rt {
 
-// Slot storage for a batch: raw uint16 counts (the kernels add the +1) when the input is uint16
-// and the reference is mixed precision; otherwise FP16 / FP32 values with the +1 applied.
+// Slot storage for a batch: raw uint16 counts (the kernels add the +1) when the input is uint16,
+// unsmoothed and the reference is mixed precision; otherwise FP16 / FP32 values with the +1 applied.
 int slot_kind_for(const fa_aligner* A, fa_dtype dtype) {
-  if (A->prm.precision == FA_PREC_MIXED) return dtype == FA_U16 ? fa::kFrameRawU16 : fa::kFrameF16;
+  if (A->prm.precision == FA_PREC_MIXED)
+    return (dtype == FA_U16 && !(A->prm.smoothing > 0)) ? fa::kFrameRawU16 : fa::kFrameF16;
   return fa::kFrameF32;
 }
 
@@ -1469,7 +1473,14 @@ fa_status aligner_run(fa_aligner* A, const void* const* frames, fa_dtype dtype, 
       FA_CU(cudaMemcpyAsync(dst, frames[i], raw_bytes, cudaMemcpyHostToDevice, s));
       raw[i] = dst;
     }
-    FA_CU(fa::launch_to_slot(raw[i], dtype, F->data, kind, A->nz, A->ny, A->nx, F->job.fpitch, F->job.fplane, true, s));
+    if (A->prm.smoothing > 0) {  // smoothStack, then + 1 (FrameWarpAligner.cpp:139-142)
+      FA_TRY(aligner_smooth(A, raw[i], dtype, s));
+      FA_CU(fa::launch_to_slot(A->smooth_out, FA_F32, F->data, kind, A->nz, A->ny, A->nx, F->job.fpitch, F->job.fplane,
+                               true, s));
+    } else {
+      FA_CU(fa::launch_to_slot(raw[i], dtype, F->data, kind, A->nz, A->ny, A->nx, F->job.fpitch, F->job.fplane, true,
+                               s));
+    }
     g_launches += 1;
   }
   // Phase correlation on the raw frames (FrameWarpAligner.cpp:181-190), downsampled when binning.
@@ -1508,10 +1519,52 @@ fa_status aligner_run(fa_aligner* A, const void* const* frames, fa_dtype dtype, 
 
 }  // namespace
 
+namespace fa_rt {
+
+std::vector<float> gaussian_kernel(double sigma) {
+  // cv::getGaussianKernel for a float image: size cvRound(8 sigma + 1) | 1, weights exp(-x^2/(2 s^2))
+  // rounded to float, summed in double, scaled by the reciprocal of the sum
+  const int n = (int)std::nearbyint(sigma * 8 + 1) | 1;
+  if (n > 257) return {};
+  std::vector<float> k((size_t)n);
+  const double scale2 = -0.5 / (sigma * sigma);
+  double sum = 0;
+  for (int i = 0; i < n; i++) {
+    const double x = i - (n - 1) * 0.5;
+    k[i] = (float)std::exp(scale2 * x * x);
+    sum += k[i];
+  }
+  sum = 1.0 / sum;
+  for (int i = 0; i < n; i++) k[i] = (float)(k[i] * sum);
+  return k;
+}
+
+fa_status aligner_smooth(fa_aligner* A, const void* raw, fa_dtype dtype, cudaStream_t s) {
+  if (!(A->prm.smoothing > 0)) return FA_OK;
+  const size_t N = (size_t)A->nz * A->ny * A->nx;
+  if (!A->smooth_kx) {
+    const std::vector<float> kx = gaussian_kernel(A->prm.smoothing), ky = gaussian_kernel(1.0);
+    FA_TRY(dalloc_t(A->ctx, kx.size(), &A->smooth_kx, A->smooth_allocs));
+    FA_TRY(dalloc_t(A->ctx, ky.size(), &A->smooth_ky, A->smooth_allocs));
+    FA_TRY(dalloc_t(A->ctx, N, &A->smooth_tmp, A->smooth_allocs));
+    FA_TRY(dalloc_t(A->ctx, N, &A->smooth_out, A->smooth_allocs));
+    FA_CU(cudaMemcpy(A->smooth_kx, kx.data(), kx.size() * sizeof(float), cudaMemcpyHostToDevice));
+    FA_CU(cudaMemcpy(A->smooth_ky, ky.data(), ky.size() * sizeof(float), cudaMemcpyHostToDevice));
+    A->smooth_nkx = (int)kx.size();
+    A->smooth_nky = (int)ky.size();
+  }
+  FA_CU(fa::launch_smooth(raw, dtype, A->nz, A->ny, A->nx, A->smooth_kx, A->smooth_nkx, A->smooth_ky, A->smooth_nky,
+                          A->smooth_tmp, A->smooth_out, s));
+  g_launches += 2;
+  return FA_OK;
+}
+
+}  // namespace fa_rt
+
 extern "C" fa_status fa_aligner_create(fa_context* ctx, const fa_aligner_params* params, fa_aligner** out) {
   if (!ctx || !params || !out) return fail(FA_ERR_BAD_ARG, "NULL argument");
-  if (params->smoothing > 0.0)
-    return fail(FA_ERR_UNSUPPORTED, "Gaussian pre-smoothing (RealignmentParameters::smoothing > 0) is not built");
+  if (!(params->smoothing >= 0.0) || (params->smoothing > 0.0 && gaussian_kernel(params->smoothing).empty()))
+    return fail(FA_ERR_BAD_ARG, "smoothing must be >= 0 and at most 32 (a kernel of at most 257 taps)");
   if (params->spatial_binning < 1) return fail(FA_ERR_BAD_ARG, "spatial_binning must be >= 1");
   if (params->precision != FA_PREC_F32 && params->precision != FA_PREC_MIXED)
     return fail(FA_ERR_BAD_ARG, "unknown precision");
@@ -1556,8 +1609,14 @@ extern "C" fa_status fa_aligner_set_reference(fa_aligner* A, const void* referen
   FA_TRY(dalloc(A->ctx, (size_t)N * sizeof(float), &plus1, A->ref_allocs));
   FA_TRY(dalloc(A->ctx, (size_t)A->dz * A->dy * A->dx * sizeof(float), &down, A->ref_allocs));
   FA_CU(cudaMemcpyAsync(raw, reference, (size_t)N * dtype_size(dtype), cudaMemcpyHostToDevice, A->stream));
-  // smoothed_reference = reference + 1 (smoothing 0), FrameWarpAligner.cpp:86-90
-  FA_CU(fa::launch_offset_convert(raw, dtype, plus1, FA_F32, N, A->stream));
+  // smoothed_reference = smoothStack(reference) + 1, FrameWarpAligner.cpp:86-90
+  if (A->prm.smoothing > 0) {
+    fa_status sst = aligner_smooth(A, raw, dtype, A->stream);
+    if (sst != FA_OK) return sst;
+    FA_CU(fa::launch_offset_convert(A->smooth_out, FA_F32, plus1, FA_F32, N, A->stream));
+  } else {
+    FA_CU(fa::launch_offset_convert(raw, dtype, plus1, FA_F32, N, A->stream));
+  }
   FA_CU(fa::launch_downsample(raw, dtype, nz, ny, nx, b, static_cast<float*>(down), A->stream));
   FA_CU(cudaStreamSynchronize(A->stream));
   // Frames go through the correlator in batches of up to 16 (one batched cuFFT plan).

@@ -630,4 +630,58 @@ cudaError_t launch_activate(const Job* jobs_dev, const Activation* recs, int n, 
   return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------ smoothStack ------------------
+
+// FrameWarpAligner::smoothStack (FrameWarpAligner.cpp:46-64): per plane, cv::GaussianBlur with sigma
+// along x and 1 along y, BORDER_REFLECT_101, float arithmetic (products and sums rounded one by one):
+// a row pass summing taps in kernel order, then a column pass in the symmetric form.
+__device__ __forceinline__ int reflect101(int p, int n) {
+  if (n == 1) return 0;
+  while (p < 0 || p >= n) {
+    if (p < 0) p = -p;
+    if (p >= n) p = 2 * n - 2 - p;
+  }
+  return p;
+}
+
+__global__ void smooth_rows_kernel(const void* __restrict__ in, int in_t, int ny, int nx, long long n,
+                                   const float* __restrict__ k, int nk, float* __restrict__ out) {
+  const int r = nk / 2;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % nx);
+    const long long row = i - x;
+    float s = __fmul_rn(k[0], load_any(in, in_t, row + reflect101(x - r, nx)));
+    for (int t = 1; t < nk; t++) s = __fadd_rn(s, __fmul_rn(k[t], load_any(in, in_t, row + reflect101(x + t - r, nx))));
+    out[i] = s;
+  }
+}
+
+__global__ void smooth_cols_kernel(const float* __restrict__ in, int ny, int nx, long long n,
+                                   const float* __restrict__ k, int nk, float* __restrict__ out) {
+  const int r = nk / 2;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % nx);
+    const long long py = i / nx;
+    const int y = (int)(py % ny);
+    const long long plane = (py - y) * nx;
+    float s = __fmul_rn(k[r], in[i]);
+    for (int t = 1; t <= r; t++) {
+      const float a = in[plane + (long long)reflect101(y - t, ny) * nx + x];
+      const float b = in[plane + (long long)reflect101(y + t, ny) * nx + x];
+      s = __fadd_rn(s, __fmul_rn(k[r + t], __fadd_rn(a, b)));
+    }
+    out[i] = s;
+  }
+}
+
+cudaError_t launch_smooth(const void* in, fa_dtype in_type, int nz, int ny, int nx, const float* kx, int nkx,
+                          const float* ky, int nky, float* tmp, float* out, cudaStream_t s) {
+  const long long n = (long long)nz * ny * nx;
+  long long blocks = (n + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  smooth_rows_kernel<<<(int)blocks, 256, 0, s>>>(in, (int)in_type, ny, nx, n, kx, nkx, tmp);
+  smooth_cols_kernel<<<(int)blocks, 256, 0, s>>>(tmp, ny, nx, n, ky, nky, out);
+  return cudaGetLastError();
+}
+
 }  // namespace fa

@@ -34,6 +34,11 @@ cudaError_t launch_offset_convert(const void* in, fa_dtype in_type, void* out, f
 cudaError_t launch_downsample(const void* in, fa_dtype in_type, int nz, int ny, int nx, int b, float* out,
                               cudaStream_t s);
 
+// smoothStack: per-plane Gaussian of a dense frame (kx: nkx weights along x, ky: nky along y; tmp and
+// out: nz*ny*nx floats).
+cudaError_t launch_smooth(const void* in, fa_dtype in_type, int nz, int ny, int nx, const float* kx, int nkx,
+                          const float* ky, int nky, float* tmp, float* out, cudaStream_t s);
+
 // Fused warp + error + J^T e over all tiles of n_jobs frames (grid.y = job). frame_kind is a
 // FrameKind, ref_bf16 selects the BF16 reference/gradient copies, rows_multiple_of_4 the
 // four-voxels-per-lane kernel (every job's nx % 4 == 0).

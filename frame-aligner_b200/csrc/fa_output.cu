@@ -383,12 +383,20 @@ extern "C" fa_status fa_aligner_results(fa_aligner* A, const void* const* frames
     const bool want_wimg = realigned_preserving && realigned_preserving[k];
     FA_CU(fa::launch_splat(R->dev, R->host, scan4, A->res_raw, dtype, A->res_D, want_wimg ? A->res_wimg : nullptr,
                            A->res_cov, s));
-    // warped_smoothed: warpImageInterpolated of the frame + 1, invalid value 0 (:223)
-    FA_CU(fa::launch_to_slot(A->res_raw, dtype, F->data, fa::kFrameF32, R->nz, R->ny, R->nx, F->job.fpitch,
-                             F->job.fplane, true, s));
+    // warped_smoothed: warpImageInterpolated of the (smoothed) frame + 1, invalid value 0 (:223);
+    // the unaligned correlation uses the same frame
+    const void* fsm = A->res_raw;
+    fa_dtype fsm_type = dtype;
+    if (A->prm.smoothing > 0) {
+      FA_TRY(aligner_smooth(A, A->res_raw, dtype, s));
+      fsm = A->smooth_out;
+      fsm_type = FA_F32;
+    }
+    FA_CU(fa::launch_to_slot(fsm, fsm_type, F->data, fa::kFrameF32, R->nz, R->ny, R->nx, F->job.fpitch, F->job.fplane,
+                             true, s));
     FA_CU(fa::launch_warp(R->dev, R->host, F->data, F->job.fplane, F->job.fpitch, fa::kFrameF32, F->job.dparams,
                           0.0f, A->res_warp, s));
-    FA_CU(fa::launch_metrics(A->res_cov, A->res_warp, R->host.ref32, A->res_raw, dtype, N, A->res_parts,
+    FA_CU(fa::launch_metrics(A->res_cov, A->res_warp, R->host.ref32, fsm, fsm_type, N, A->res_parts,
                              A->res_parts + 296 * 8, s));
     g_launches += 7;
     if (results) FA_CU(cudaMemcpyAsync(totals, A->res_parts + 296 * 8, 16 * sizeof(double), cudaMemcpyDeviceToHost, s));

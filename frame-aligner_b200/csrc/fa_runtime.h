@@ -145,6 +145,14 @@ struct fa_aligner {
   size_t vols_count = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = 0;
+  // smoothStack (smoothing > 0): Gaussian weights along x and y, and two frame-sized work buffers
+  // used one frame at a time in stream order
+  float* smooth_kx = nullptr;
+  float* smooth_ky = nullptr;
+  int smooth_nkx = 0, smooth_nky = 0;
+  float* smooth_tmp = nullptr;
+  float* smooth_out = nullptr;
+  std::vector<fa_rt::Alloc> smooth_allocs;
   // per-frame outputs and metrics (fa_aligner_results): an FP32 frame slot and work buffers
   fa_frame* res_slot = nullptr;
   void* res_raw = nullptr;
@@ -182,6 +190,11 @@ void make_dparams(const double* D, int nD, int n_dim, float4* out);
 bool finite_all(const double* v, size_t n);
 // Frees the buffers of fa_aligner_results (with the aligner's reference).
 void aligner_release_results(fa_aligner* A);
+// cv::GaussianBlur's float kernel for sigma (the size rule and weights of smoothStack's blur); empty
+// when it would exceed 257 taps.
+std::vector<float> gaussian_kernel(double sigma);
+// smoothStack of one dense raw frame (device) into A->smooth_out on stream s (no-op without smoothing).
+fa_status aligner_smooth(fa_aligner* A, const void* raw, fa_dtype dtype, cudaStream_t s);
 // Frame slot (zero-halo storage of the given FrameKind + solve buffers + stream) for reference R.
 fa_status frame_alloc(fa_reference* R, int kind, fa_frame** out);
 // Slot storage the aligner uses for frames of dtype (raw uint16 counts + 1, FP16 or FP32 values + 1).

@@ -502,8 +502,14 @@ fa_status intake(fa_server* S, SrvAcq* q, std::vector<SrvSlot*>& batch) {
       FA_CU(cudaMemcpyAsync(sl->raw, src, q->raw_bytes, cudaMemcpyHostToDevice, s));
       src = sl->raw;
     }
-    FA_CU(fa::launch_to_slot(src, q->dtype, F->data, q->kind, A->nz, A->ny, A->nx, F->job.fpitch, F->job.fplane,
-                             true, s));
+    if (A->prm.smoothing > 0) {  // smoothStack, then + 1; the correlator keeps the raw frame
+      FA_TRY(aligner_smooth(A, src, q->dtype, s));
+      FA_CU(fa::launch_to_slot(A->smooth_out, FA_F32, F->data, q->kind, A->nz, A->ny, A->nx, F->job.fpitch,
+                               F->job.fplane, true, s));
+    } else {
+      FA_CU(fa::launch_to_slot(src, q->dtype, F->data, q->kind, A->nz, A->ny, A->nx, F->job.fpitch, F->job.fplane,
+                               true, s));
+    }
     g_launches += 1;
     if (A->prm.spatial_binning > 1) {
       FA_CU(fa::launch_downsample(src, q->dtype, A->nz, A->ny, A->nx, A->prm.spatial_binning, sl->vol, s));

@@ -463,6 +463,14 @@ class Aligner:
         check(lib().fa_aligner_last_device_ms(self._h, C.byref(ms)))
         return ms.value
 
+    def reference_gradient(self):
+        """The Sobel gradient of the aligner's warper reference (its smoothed reference + 1)."""
+        r = _vp()
+        check(lib().fa_aligner_reference(self._h, C.byref(r)))
+        g = [np.empty(self.dims, np.float32) for _ in range(3)]
+        check(lib().fa_get_gradient(r, *[x.ctypes.data for x in g]))
+        return g
+
     def results(self, frames, D, images=False):
         """fa_aligner_results: per frame the metrics dict, and with images=True also the realigned and
         intensity-preserving realigned uint16 images and the coverage mask."""
@@ -521,13 +529,13 @@ class Server:
         self._keep = {}  # host frames referenced by outstanding tickets
 
     def add_acquisition(self, reference, scan: ScanParams, frame_dtype=np.uint16, spatial_binning=1, nD=0,
-                        n_resampling_points=30, precision=PREC_MIXED, max_iterations=100):
+                        n_resampling_points=30, precision=PREC_MIXED, max_iterations=100, smoothing=0.0):
         ref = np.ascontiguousarray(reference)
         if ref.dtype not in (np.float32, np.uint16):
             ref = ref.astype(np.float32)
         if ref.ndim == 2:
             ref = ref[None]
-        prm = AlignerParams(spatial_binning, n_resampling_points, nD, 0.0, precision, max_iterations)
+        prm = AlignerParams(spatial_binning, n_resampling_points, nD, smoothing, precision, max_iterations)
         a = C.c_int()
         check(lib().fa_server_add_acquisition(self._h, C.byref(prm), ref.ctypes.data, _DTYPES[ref.dtype], *ref.shape,
                                               C.byref(scan), _DTYPES[np.dtype(frame_dtype)], C.byref(a)))

@@ -211,7 +211,8 @@ typedef struct {
   int spatial_binning;       /* RealignmentParameters::spatial_binning: phase-correlation downsampling */
   int n_resampling_points;   /* nD = n_resampling_points * n_z + 1 (FrameWarpAligner.cpp:100) ... */
   int nD;                    /* ... unless nD > 0, which sets the control-point count directly */
-  double smoothing;          /* must be 0: the Gaussian pre-smoothing (FrameWarpAligner.cpp:46-64) is not built */
+  double smoothing;          /* smoothStack (FrameWarpAligner.cpp:46-64): sigma along x of the per-plane Gaussian
+                                (sigma 1 along y, as the reference); 0: none; at most 32 */
   fa_precision precision;
   int max_iterations;        /* <= 0: 100 */
   double correlation_threshold;  /* RealignmentParameters::correlation_threshold (RealignmentResult::useFrame) */

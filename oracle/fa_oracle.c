@@ -469,6 +469,63 @@ void or_downsample(const float* in, int nz, int ny, int nx, int factor, float* o
         out[((long)z * nh + y / factor) * nw + x / factor] += in[((long)z * ny + y) * nx + x];
 }
 
+/* smoothStack, FrameWarpAligner.cpp:46-64: per plane cv::GaussianBlur(plane, Size(0, 0), sigma, 1)
+   on float data. OpenCV is not part of this build, so this states its documented algorithm (parity
+   with OpenCV itself is unpinned): kernel size cvRound(8 s + 1) | 1 for float images; weights
+   exp(-x^2 / (2 s^2)) at x = i - (n - 1) / 2, rounded to float, summed in double and scaled by the
+   reciprocal of the sum (rounded to float again); a row pass summing taps in kernel order, then a
+   column pass in the symmetric form k_c T[y] + sum_k k_{c+k} (T[y-k] + T[y+k]); BORDER_REFLECT_101
+   at the edges; float arithmetic with every product and sum rounded. */
+int or_gaussian_kernel(double sigma, float* k, int max_n) {
+  int n = (int)nearbyint(sigma * 8 + 1) | 1;
+  if (n > max_n) return -1;
+  double scale2 = -0.5 / (sigma * sigma), sum = 0;
+  for (int i = 0; i < n; i++) {
+    double x = i - (n - 1) * 0.5;
+    k[i] = (float)exp(scale2 * x * x);
+    sum += k[i];
+  }
+  sum = 1.0 / sum;
+  for (int i = 0; i < n; i++) k[i] = (float)(k[i] * sum);
+  return n;
+}
+
+static int reflect101(int p, int n) {
+  if (n == 1) return 0;
+  while (p < 0 || p >= n) {
+    if (p < 0) p = -p;
+    if (p >= n) p = 2 * n - 2 - p;
+  }
+  return p;
+}
+
+int or_smooth_stack(const float* in, int nz, int ny, int nx, double sigma, float* out) {
+  float kx[257], ky[257];
+  int nkx = or_gaussian_kernel(sigma, kx, 257), nky = or_gaussian_kernel(1.0, ky, 257);
+  if (nkx < 0 || nky < 0) return -1;
+  int rx = nkx / 2, ry = nky / 2;
+  float* t = (float*)malloc(sizeof(float) * (size_t)ny * nx);
+  for (int z = 0; z < nz; z++) {
+    const float* src = in + (size_t)z * ny * nx;
+    float* dst = out + (size_t)z * ny * nx;
+    for (int y = 0; y < ny; y++)
+      for (int x = 0; x < nx; x++) {
+        float s = kx[0] * src[(size_t)y * nx + reflect101(x - rx, nx)];
+        for (int i = 1; i < nkx; i++) s += kx[i] * src[(size_t)y * nx + reflect101(x + i - rx, nx)];
+        t[(size_t)y * nx + x] = s;
+      }
+    for (int y = 0; y < ny; y++)
+      for (int x = 0; x < nx; x++) {
+        float s = ky[ry] * t[(size_t)y * nx + x];
+        for (int k = 1; k <= ry; k++)
+          s += ky[ry + k] * (t[(size_t)reflect101(y - k, ny) * nx + x] + t[(size_t)reflect101(y + k, ny) * nx + x]);
+        dst[(size_t)y * nx + x] = s;
+      }
+  }
+  free(t);
+  return 0;
+}
+
 /* correlation, Cv3dUtils.cpp:57-81: covariance over the mask divided by the product of the
    population standard deviations over the mask. */
 double or_correlation(const float* a, const float* b, const uint8_t* mask, long n) {

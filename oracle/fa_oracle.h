@@ -18,6 +18,7 @@
  *   or_warp_image           FrameAligner/FrameWarper.cpp:71-136 (intensity-preserving splat)
  *   or_warp_point           FrameAligner/FrameWarper.cpp:397-419
  *   or_downsample           FrameAligner/AbstractFrameAligner.cpp:37-56
+ *   or_smooth_stack         FrameAligner/FrameWarpAligner.cpp:46-64 (cv::GaussianBlur stated, unpinned)
  *   or_correlation          FrameAligner/Cv3dUtils.cpp:57-81 (masked Pearson)
  *   or_trust_region         the project's trust-region algorithm (dlib find_min_trust_region is
  *                           called at FrameAligner/FrameWarpAligner.cpp:205-209 but its source is
@@ -72,6 +73,11 @@ void or_warp_point(const or_warper* w, const double* D, int x, int y, int z, int
 
 void or_sobel3d(const float* m, int nz, int ny, int nx, float* gx, float* gy, float* gz);
 void or_downsample(const float* in, int nz, int ny, int nx, int factor, float* out);
+/* smoothStack (FrameWarpAligner.cpp:46-64): per-plane Gaussian blur, sigma along x and 1 along y.
+   Returns -1 if a kernel would exceed 257 taps. or_gaussian_kernel writes the n float weights and
+   returns n. */
+int or_smooth_stack(const float* in, int nz, int ny, int nx, double sigma, float* out);
+int or_gaussian_kernel(double sigma, float* k, int max_n);
 double or_correlation(const float* a, const float* b, const uint8_t* mask, long n);
 
 typedef struct {

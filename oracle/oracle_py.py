@@ -79,6 +79,8 @@ def lib():
         L.or_warp_point.argtypes = [C.c_void_p, _f64p, C.c_int, C.c_int, C.c_int, C.c_int, _f64p]
         L.or_sobel3d.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, _f32p, _f32p, _f32p]
         L.or_downsample.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, _f32p]
+        L.or_smooth_stack.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_double, _f32p]
+        L.or_gaussian_kernel.argtypes = [C.c_double, _f32p, C.c_int]
         L.or_correlation.restype = C.c_double
         L.or_correlation.argtypes = [_f32p, _f32p, _u8p, C.c_long]
         L.or_tr_subproblem.argtypes = [C.c_int, _f64p, _f64p, C.c_double, C.c_double, C.c_int, _f64p]
@@ -417,3 +419,20 @@ def phase_shift(ref, vol):
     if z > nz // 2:
         z -= nz
     return np.array([x, y, z], np.float64)
+
+
+def smooth_stack(vol, sigma):
+    """or_smooth_stack: smoothStack's per-plane Gaussian (sigma along x, 1 along y)."""
+    v = _c32(vol)
+    if v.ndim == 2:
+        v = v[None]
+    out = np.empty_like(v)
+    if lib().or_smooth_stack(v.ravel(), v.shape[0], v.shape[1], v.shape[2], float(sigma), out.ravel()) != 0:
+        raise ValueError("kernel too large")
+    return out
+
+
+def gaussian_kernel(sigma):
+    k = np.empty(257, np.float32)
+    n = lib().or_gaussian_kernel(float(sigma), k, 257)
+    return k[:n]

@@ -143,3 +143,13 @@ def test_warm_start_candidate():
     again, st_again = ow.align_frame(frame, shift, 100, warm=cold)
     assert np.sqrt(((again - cold)[:, :2] ** 2).sum(-1).mean()) <= 1e-3
     assert st_again.iterations <= st_cold.iterations
+
+
+def test_smoothing_statement():
+    """smoothStack's kernel size rule cvRound(8 s + 1) | 1, symmetric weights summing to 1, and a
+    constant plane staying constant (to float rounding)."""
+    for sigma, n in [(0.5, 5), (1.0, 9), (1.5, 13), (2.6, 23), (3.0, 25)]:
+        k = O.gaussian_kernel(sigma)
+        assert len(k) == n and np.array_equal(k, k[::-1]) and abs(float(k.sum()) - 1) < 1e-6
+    c = np.full((2, 17, 23), 7.0, np.float32)
+    assert np.allclose(O.smooth_stack(c, 1.7), 7.0, rtol=1e-6, atol=0)
