@@ -66,6 +66,7 @@ def parse():
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="total arrivals per second")
     ap.add_argument("--serve-pool", type=int, default=6, help="distinct frames per served acquisition")
     ap.add_argument("--serve-slots", type=int, default=24, help="frame slots reserved per served acquisition")
+    ap.add_argument("--serve-iters", type=int, default=2, help="trust-region iterations per serving graph launch")
     ap.add_argument("--serve-lags", type=int, nargs="+", default=[1, 4],
                     help="warm-start lags to serve with (1 = the previous frame's solution)")
     return ap.parse_args()
@@ -245,7 +246,7 @@ def measure_serving(fa, ctx, args, acqs, pools, lag):
     pool of args.serve_pool frames (raw uint16 in pinned host memory); warm start from the solution of
     the frame `lag` positions earlier in the same acquisition; 40 GB admission budget.
     Latency = submission -> result on the host."""
-    srv = fa.Server(ctx, memory_budget=40 << 30, warm_start=lag)
+    srv = fa.Server(ctx, memory_budget=40 << 30, warm_start=lag, iterations_per_launch=args.serve_iters)
     ids = []
     for a in acqs:
         nz, ny, nx = a.reference.shape
@@ -286,7 +287,7 @@ def measure_serving(fa, ctx, args, acqs, pools, lag):
         iters.append(st["iterations"])
     stats = srv.stats()
     srv.close()
-    return {"warm_start_lag": lag, "arrival_rate": args.serve_rate, "arrival_rate_achieved": n / t_sub,
+    return {"warm_start_lag": lag, "iterations_per_launch": args.serve_iters, "arrival_rate": args.serve_rate, "arrival_rate_achieved": n / t_sub,
             "frames": n, "p50_ms": stats["p50_ms"], "p99_ms": stats["p99_ms"], "mean_ms": stats["mean_ms"],
             "max_ms": stats["max_ms"], "frames_per_s": stats["frames_per_s"],
             "peak_in_flight": stats["peak_in_flight"], "peak_slot_gb": stats["peak_slot_bytes"] / 1e9,

@@ -152,4 +152,22 @@ __device__ __forceinline__ void reduce_partials(const RefDev& R, const double* _
   __syncthreads();
 }
 
+// Control-point parameters (kDParamF4 float4 per control point) of the trial point D = x + p, from
+// job.x and job.p; control points k = t0, t0 + stride, ...
+__device__ __forceinline__ void write_trial_dparams(const Job& job, const RefDev& R, int t0, int stride) {
+  const int nd = R.n_dim;
+  for (int k = t0; k < R.nD; k += stride) {
+    double d[3], dn[3];
+    for (int c = 0; c < 3; c++) {
+      d[c] = c < nd ? job.x[k * nd + c] + job.p[k * nd + c] : 0.0;
+      dn[c] = (c < nd && k + 1 < R.nD) ? job.x[(k + 1) * nd + c] + job.p[(k + 1) * nd + c] : d[c];
+    }
+    const double f0 = floor(d[0]), f1 = floor(d[1]), f2 = floor(d[2]);
+    job.dparams[k * kDParamF4 + 0] = make_float4((float)f0, (float)f1, (float)f2, 0.f);
+    job.dparams[k * kDParamF4 + 1] = make_float4((float)(d[0] - f0), (float)(d[1] - f1), (float)(d[2] - f2), 0.f);
+    job.dparams[k * kDParamF4 + 2] =
+        make_float4((float)(dn[0] - d[0]), (float)(dn[1] - d[1]), (float)(dn[2] - d[2]), 0.f);
+  }
+}
+
 }  // namespace fa

@@ -342,7 +342,7 @@ template <int NDIM, typename FT, typename RT, int MB>
 __global__ void __launch_bounds__(kEvalThreads, MB) eval4_kernel(const Job* __restrict__ jobs) {
   __shared__ float4 sD[kEvalWarps][kWin * kDParamF4];
   const Job& job = jobs[blockIdx.y];
-  if (job.state != nullptr && job.state->phase == kPhaseDone) return;
+  if (job.state != nullptr && (job.state->phase == kPhaseDone || job.state->phase == kPhaseWaitWarm)) return;
   const RefDev& R = *job.ref;
   const int warp = threadIdx.x >> 5;
   const int tile = blockIdx.x * kEvalWarps + warp;

@@ -46,7 +46,9 @@ enum Phase : int {
   kPhaseStartRigid = 1,  // trial = rigid shift
   kPhaseTrial = 2,       // trial = x + p
   kPhaseDone = 3,
-  kPhaseStartLast = 4    // trial = the previous frame's solution (warm start)
+  kPhaseStartLast = 4,   // trial = an earlier frame's solution (warm start)
+  kPhaseWaitWarm = 5     // cold starting points done; out of the passes until the warm-start vector
+                         // has been written (resumed by the compact pass)
 };
 
 struct FrameState {
@@ -67,6 +69,9 @@ struct FrameState {
   int pad_;
   double* warm;    // P doubles or null: read by kPhaseStartLast when use_warm; the solution is
                    // written here when the solve finishes
+  long long* warm_seq;  // sequence number of the frame whose solution *warm holds (null: no warm start)
+  long long warm_need;  // the writer this frame's warm start must come from
+  long long seq;        // this frame's sequence number, stored to *warm_seq with its solution
 };
 
 // Where a finished frame's solve is reported (host-mapped memory): the final FrameState, then the
@@ -163,7 +168,10 @@ struct Activation {
   int max_iter;
   int pad_;
   double rigid[3];
-  double* warm;  // FrameState::warm (null: none)
+  double* warm;          // FrameState::warm (null: none)
+  long long* warm_seq;   // FrameState::warm_seq
+  long long warm_need;   // FrameState::warm_need
+  long long seq;         // FrameState::seq
 };
 
 }  // namespace fa

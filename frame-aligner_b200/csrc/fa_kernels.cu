@@ -194,7 +194,7 @@ cudaError_t launch_downsample(const void* in, fa_dtype in_type, int nz, int ny, 
 template <int NDIM, typename FT, typename RT>
 __global__ void __launch_bounds__(kEvalThreads) eval_kernel(const Job* __restrict__ jobs) {
   const Job& job = jobs[blockIdx.y];
-  if (job.state != nullptr && job.state->phase == kPhaseDone) return;
+  if (job.state != nullptr && (job.state->phase == kPhaseDone || job.state->phase == kPhaseWaitWarm)) return;
   const RefDev& R = *job.ref;
   const int tile = blockIdx.x;
   if (tile >= R.n_tiles) return;
@@ -536,8 +536,21 @@ __global__ void __launch_bounds__(1024) compact_kernel(const Job* __restrict__ j
   const unsigned lt = (1u << lane) - 1u;
   for (int c = 0; c < n; c += blockDim.x) {
     const int i = c + threadIdx.x;
-    const int phase = i < n ? jobs[i].state->phase : (int)kPhaseDone;
-    const bool act = i < n && phase != kPhaseDone;
+    int phase = i < n ? jobs[i].state->phase : (int)kPhaseDone;
+    if (phase == kPhaseWaitWarm) {
+      // Resume a frame waiting for its warm start once the earlier frame's solution is written (by a
+      // finished solve launch): the fourth starting point x + (warm - x).
+      const Job& j = jobs[i];
+      FrameState* S = j.state;
+      if (*S->warm_seq == S->warm_need) {
+        const RefDev& R = *j.ref;
+        for (int q = 0; q < R.P; q++) j.p[q] = S->warm[q] - j.x[q];
+        write_trial_dparams(j, R, 0, 1);
+        S->phase = kPhaseStartLast;
+        phase = kPhaseStartLast;
+      }
+    }
+    const bool act = i < n && phase != kPhaseDone && phase != kPhaseWaitWarm;
     const bool fin = i < n && busy != nullptr && phase == kPhaseDone && busy[i] != 0;
     const int tiles = act ? jobs[i].ref->n_tiles : 0;
     int incl = tiles;
@@ -616,7 +629,10 @@ __global__ void activate_kernel(const Job* __restrict__ jobs, const Activation* 
     S.phase = kPhaseStartZero;
     S.max_iter = r.max_iter > 0 ? r.max_iter : 100;
     S.warm = r.warm;
-    S.use_warm = (r.use_warm != 0 && r.warm != nullptr) ? 1 : 0;
+    S.warm_seq = r.warm_seq;
+    S.warm_need = r.warm_need;
+    S.seq = r.seq;
+    S.use_warm = (r.use_warm != 0 && r.warm != nullptr && r.warm_seq != nullptr) ? 1 : 0;
     for (int c = 0; c < 3; c++) S.rigid[c] = r.rigid[c];
     if (R.n_dim == 2) S.rigid[2] = 0.0;
     *j.state = S;

@@ -14,9 +14,10 @@
 //
 // Determinism: a frame's fused passes and steps use only its own tiles, partial sums and state, so
 // its result is the same whichever frames share its launches. With a warm-start lag d, frame k of an
-// acquisition starts its solve only after frame k-d finished (that solution is its fourth starting
-// point), so results do not depend on arrival timing either; up to d frames of one acquisition solve
-// at the same time.
+// acquisition evaluates its cold starting points (zero, rigid) as soon as it is correlated, then waits
+// on the device (out of the passes) until frame k-d has written its solution to the warm-start ring
+// entry stamped with k-d's sequence number, and continues from that fourth starting point; results
+// therefore do not depend on arrival timing either.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -95,13 +96,13 @@ struct SrvAcq {
   int n_busy = 0;            // admitted, not finished
   int n_slots = 0;           // slots that exist (busy or idle)
   long long next_seq = 0;
-  std::unordered_set<long long> finished;  // warm start: finished frames whose successor has not started
   std::map<long long, SrvSlot*> ready;      // correlated, waiting to start (by sequence number)
   bool corr_busy = false;
   std::vector<SrvSlot*> corr_slots;
   cudaEvent_t corr_ev = nullptr;
   long long* h_idx = nullptr;  // pinned: peak indices of the last correlator call
-  double* warm = nullptr;      // device, lag x P doubles: frame k reads and writes entry k % lag
+  double* warm = nullptr;        // device, lag x P doubles: frame k reads and writes entry k % lag
+  long long* warm_seq = nullptr; // device, lag: sequence number of the frame whose solution each entry holds
   std::vector<Alloc> allocs;
 };
 
@@ -456,7 +457,6 @@ void deliver(fa_server* S, SrvSlot* sl, double t) {
   res.latency_ms = (t - sl->req.t_submit) * 1e3;
   q->n_busy--;
   S->in_flight--;
-  if (S->cfg.warm_start > 0) q->finished.insert(sl->seq);
   q->idle.push_back(sl);
   q->cls->in_solve--;
   std::lock_guard<std::mutex> lk(S->mu);
@@ -536,13 +536,9 @@ fa_status class_launch(fa_server* S, SrvClass* C, bool* launched) {
   const long long lag = S->cfg.warm_start;
   for (SrvAcq* q : C->acqs) {
     for (auto it = q->ready.begin(); it != q->ready.end() && n_act < C->cap;) {
+      // every correlated frame starts; one with a warm start waits on the device for frame seq - lag
+      // (the first lag frames start cold)
       const long long seq = it->first;
-      // warm start: frame seq starts once frame seq - lag has finished (the first lag frames start cold)
-      if (lag > 0 && seq >= lag && !q->finished.count(seq - lag)) {
-        ++it;
-        continue;
-      }
-      if (lag > 0) q->finished.erase(seq - lag);
       SrvSlot* sl = it->second;
       it = q->ready.erase(it);
       fa::Activation& a = C->h_act[n_act++];
@@ -552,6 +548,9 @@ fa_status class_launch(fa_server* S, SrvClass* C, bool* launched) {
       a.pad_ = 0;
       for (int c = 0; c < 3; c++) a.rigid[c] = sl->rigid[c];
       a.warm = lag > 0 ? q->warm + (size_t)(seq % lag) * q->A->ref->P : nullptr;
+      a.warm_seq = lag > 0 ? q->warm_seq + seq % lag : nullptr;
+      a.warm_need = seq - lag;
+      a.seq = seq;
     }
   }
   if (n_act == 0 && C->in_solve == 0) return FA_OK;
@@ -829,7 +828,10 @@ extern "C" fa_status fa_server_add_acquisition(fa_server* S, const fa_aligner_pa
   if (S->cfg.warm_start > 0) {
     const size_t nw = (size_t)S->cfg.warm_start * A->ref->P;
     if ((st = dalloc_t(S->ctx, nw, &q->warm, q->allocs)) != FA_OK) return undo(st);
-    if (cudaMemset(q->warm, 0, nw * sizeof(double)) != cudaSuccess) return undo(fail(FA_ERR_CUDA, "cudaMemset failed"));
+    if ((st = dalloc_t(S->ctx, (size_t)S->cfg.warm_start, &q->warm_seq, q->allocs)) != FA_OK) return undo(st);
+    if (cudaMemset(q->warm, 0, nw * sizeof(double)) != cudaSuccess ||
+        cudaMemset(q->warm_seq, 0xff, (size_t)S->cfg.warm_start * sizeof(long long)) != cudaSuccess)  // -1: empty
+      return undo(fail(FA_ERR_CUDA, "cudaMemset failed"));
   }
   std::unique_lock<std::mutex> lk(S->mu);
   if (S->fatal != FA_OK) {

@@ -291,8 +291,7 @@ __device__ void state_step(const Job& job, FrameState* S, const RefDev& R, const
       } else {
         S->f = ft;
         if (S->use_warm && S->warm != nullptr) {
-          for (int i = 0; i < P; i++) p[i] = S->warm[i] - x[i];
-          next = kPhaseStartLast;
+          next = kPhaseWaitWarm;
         } else {
           go_top = true;
         }
@@ -312,8 +311,9 @@ __device__ void state_step(const Job& job, FrameState* S, const RefDev& R, const
         S->f = S->f_start;
       }
       if (S->use_warm && S->warm != nullptr) {
-        for (int i = 0; i < P; i++) p[i] = S->warm[i] - x[i];
-        next = kPhaseStartLast;
+        // the warm start waits (out of the passes) until the earlier frame's solution is written;
+        // the compact pass then sets p = warm - x and the trial point
+        next = kPhaseWaitWarm;
       } else {
         go_top = true;
       }
@@ -385,7 +385,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) solve_kernel(const Job* __re
   if (active != nullptr && (int)blockIdx.x >= *n_active) return;
   const Job& job = jobs[active != nullptr ? active[blockIdx.x] : blockIdx.x];
   FrameState* S = job.state;
-  if (S->phase == kPhaseDone) return;
+  if (S->phase == kPhaseDone || S->phase == kPhaseWaitWarm) return;
   const RefDev& R = *job.ref;
   __shared__ double s_f;
   reduce_partials(R, job.partials, &s_f, job.gt);
@@ -418,7 +418,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) solve_kernel(const Job* __re
     work = sp + R.P;
     __syncthreads();
   }
-  const int P = R.P, nd = R.n_dim;
+  const int P = R.P;
   if (threadIdx.x == 0) {
     if (R.n_dim == 3)
       state_step<3>(job, S, R, Hd, Hl, gv, pv, work, s_f);
@@ -440,26 +440,15 @@ __global__ void __launch_bounds__(kSolveThreads, 1) solve_kernel(const Job* __re
       double* xr = reinterpret_cast<double*>(static_cast<char*>(job.report) + kReportHeaderBytes);
       for (int i = threadIdx.x; i < P; i += blockDim.x) xr[i] = job.x[i];
     }
-    if (S->warm != nullptr)
+    if (S->warm != nullptr) {
       for (int i = threadIdx.x; i < P; i += blockDim.x) S->warm[i] = job.x[i];
+      if (threadIdx.x == 0 && S->warm_seq != nullptr) *S->warm_seq = S->seq;  // read by later launches
+    }
     return;
   }
+  if (S->phase == kPhaseWaitWarm) return;
   // Next trial point D = x + p, as the fused pass's control-point parameters.
-  for (int k = threadIdx.x; k < R.nD; k += blockDim.x) {
-    double d[3], dn[3];
-    for (int c = 0; c < 3; c++) {
-      d[c] = c < nd ? job.x[k * nd + c] + job.p[k * nd + c] : 0.0;
-      dn[c] = (c < nd && k + 1 < R.nD) ? job.x[(k + 1) * nd + c] + job.p[(k + 1) * nd + c] : d[c];
-    }
-    float4 a, b, e;
-    const double f0 = floor(d[0]), f1 = floor(d[1]), f2 = floor(d[2]);
-    a = make_float4((float)f0, (float)f1, (float)f2, 0.f);
-    b = make_float4((float)(d[0] - f0), (float)(d[1] - f1), (float)(d[2] - f2), 0.f);
-    e = make_float4((float)(dn[0] - d[0]), (float)(dn[1] - d[1]), (float)(dn[2] - d[2]), 0.f);
-    job.dparams[k * kDParamF4 + 0] = a;
-    job.dparams[k * kDParamF4 + 1] = b;
-    job.dparams[k * kDParamF4 + 2] = e;
-  }
+  write_trial_dparams(job, R, threadIdx.x, blockDim.x);
 }
 
 cudaError_t launch_solve(const Job* jobs_dev, int n_jobs, int max_nD, int n_dim, cudaStream_t s, const int* active,

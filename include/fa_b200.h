@@ -288,9 +288,9 @@ typedef struct {
   int max_in_flight;          /* frames admitted and not finished, all acquisitions (0: 256) */
   int iterations_per_launch;  /* trust-region iterations per graph launch (0: 2) */
   int warm_start;             /* lag d >= 1: frame k's starting points are {0, 0, rigid, the solution of
-                                 frame k - d of the same acquisition} (d = 1: the previous frame), and
-                                 frame k starts its solve after frame k - d finished, so at most d frames
-                                 of an acquisition solve at once; 0: no warm start (at most 64) */
+                                 frame k - d of the same acquisition} (d = 1: the previous frame); frame k
+                                 evaluates the first three at once and waits on the device for frame
+                                 k - d's solution before the fourth; 0: no warm start (at most 64) */
   int shared_launches;        /* 0: each acquisition's frames have their own job table, graph and stream,
                                  and acquisitions overlap on the device; 1: acquisitions whose frames
                                  can share a kernel (same dimensionality, storage and precision) share
