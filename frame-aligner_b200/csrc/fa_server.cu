@@ -757,7 +757,7 @@ extern "C" fa_status fa_server_create(fa_context* ctx, const fa_server_config* c
   if (cfg) c = *cfg;
   if (c.memory_budget == 0) c.memory_budget = (size_t)40 << 30;
   if (c.max_in_flight <= 0) c.max_in_flight = 256;
-  if (c.iterations_per_launch <= 0) c.iterations_per_launch = 2;
+  if (c.iterations_per_launch <= 0) c.iterations_per_launch = 4;
   if (c.max_in_flight > 4096 || c.iterations_per_launch > 64 || c.warm_start < 0 || c.warm_start > 64)
     return fail(FA_ERR_BAD_ARG, "need max_in_flight <= 4096, iterations_per_launch <= 64, 0 <= warm_start <= 64");
   FA_CU(cudaSetDevice(ctx->device));

@@ -286,7 +286,7 @@ typedef struct fa_server fa_server;
 typedef struct {
   size_t memory_budget;       /* device bytes frame slots may hold (0: 40 GiB) */
   int max_in_flight;          /* frames admitted and not finished, all acquisitions (0: 256) */
-  int iterations_per_launch;  /* trust-region iterations per graph launch (0: 2) */
+  int iterations_per_launch;  /* trust-region iterations per graph launch (0: 4) */
   int warm_start;             /* lag d >= 1: frame k's starting points are {0, 0, rigid, the solution of
                                  frame k - d of the same acquisition} (d = 1: the previous frame); frame k
                                  evaluates the first three at once and waits on the device for frame
