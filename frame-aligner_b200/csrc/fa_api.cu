@@ -1151,9 +1151,10 @@ fa_status correlator_enqueue(fa_correlator* C, const void* const* vols, int in_k
   for (int i = 0; i < n; i++) C->h_ptrs[i] = vols[i];
   FA_CU(cudaMemcpyAsync(C->d_ptrs, C->h_ptrs, (size_t)n * sizeof(void*), cudaMemcpyHostToDevice, C->stream));
   for (int c0 = 0; c0 < n;) {
-    const int m = (n - c0 >= C->cap) ? C->cap : 1;
-    cufftHandle fwd = (m == C->cap) ? C->fwd : C->fwd1;
-    cufftHandle inv = (m == C->cap) ? C->inv : C->inv1;
+    int m = C->cap;  // the largest power-of-two batch that fits the rest
+    while (m > n - c0) m >>= 1;
+    cufftHandle fwd, inv;
+    FA_TRY(correlator_plans(C, m, &fwd, &inv));
     FA_CU(fa::launch_phase_window(C->d_ptrs + c0, in_kind, C->wy, C->wx, C->ny, C->nx, C->n_el, m, C->real, C->stream));
     if (cufftExecD2Z(fwd, C->real, reinterpret_cast<cufftDoubleComplex*>(C->spec)) != CUFFT_SUCCESS)
       return fail(FA_ERR_CUDA, "cufftExecD2Z failed");
@@ -1195,7 +1196,17 @@ fa_status correlator_read(fa_correlator* C, int n, double* shifts) {
   return FA_OK;
 }
 
-fa_status correlator_plan(fa_correlator* C, int batch, cufftHandle* fwd, cufftHandle* inv) {
+}  // namespace
+
+namespace fa_rt {
+
+fa_status correlator_plans(fa_correlator* C, int batch, cufftHandle* fwd, cufftHandle* inv) {
+  auto it = C->plans.find(batch);
+  if (it != C->plans.end()) {
+    *fwd = it->second.first;
+    *inv = it->second.second;
+    return FA_OK;
+  }
   int dims[3] = {C->nz, C->ny, C->nx};
   int rank = 3;
   int* d = dims;
@@ -1208,13 +1219,42 @@ fa_status correlator_plan(fa_correlator* C, int batch, cufftHandle* fwd, cufftHa
     }
   }
   // Basic layout: batches contiguous, n_el reals apart on the real side, n_complex on the complex side.
-  if (cufftPlanMany(fwd, rank, d, nullptr, 1, 0, nullptr, 1, 0, CUFFT_D2Z, batch) != CUFFT_SUCCESS ||
-      cufftPlanMany(inv, rank, d, nullptr, 1, 0, nullptr, 1, 0, CUFFT_Z2D, batch) != CUFFT_SUCCESS)
-    return fail(FA_ERR_CUDA, "cufftPlanMany failed");
-  cufftSetStream(*fwd, C->stream);
-  cufftSetStream(*inv, C->stream);
+  cufftHandle f = 0, v = 0;
+  size_t wf = 0, wv = 0;
+  if (cufftCreate(&f) != CUFFT_SUCCESS || cufftCreate(&v) != CUFFT_SUCCESS || cufftSetAutoAllocation(f, 0) ||
+      cufftSetAutoAllocation(v, 0) ||
+      cufftMakePlanMany(f, rank, d, nullptr, 1, 0, nullptr, 1, 0, CUFFT_D2Z, batch, &wf) != CUFFT_SUCCESS ||
+      cufftMakePlanMany(v, rank, d, nullptr, 1, 0, nullptr, 1, 0, CUFFT_Z2D, batch, &wv) != CUFFT_SUCCESS) {
+    if (f) cufftDestroy(f);
+    if (v) cufftDestroy(v);
+    return fail(FA_ERR_CUDA, "cufftMakePlanMany failed");
+  }
+  C->plans[batch] = {f, v};
+  const size_t need = std::max(wf, wv);
+  if (need > C->work_bytes) {  // a larger shared work area, given to every plan
+    FA_CU(cudaStreamSynchronize(C->stream));
+    dfree_all(C->ctx, C->work_allocs);
+    C->work = nullptr;
+    C->work_bytes = 0;
+    FA_TRY(dalloc(C->ctx, need, &C->work, C->work_allocs));
+    C->work_bytes = need;
+    for (auto& pl : C->plans)
+      if (cufftSetWorkArea(pl.second.first, C->work) != CUFFT_SUCCESS ||
+          cufftSetWorkArea(pl.second.second, C->work) != CUFFT_SUCCESS)
+        return fail(FA_ERR_CUDA, "cufftSetWorkArea failed");
+  } else if (cufftSetWorkArea(f, C->work) != CUFFT_SUCCESS || cufftSetWorkArea(v, C->work) != CUFFT_SUCCESS) {
+    return fail(FA_ERR_CUDA, "cufftSetWorkArea failed");
+  }
+  cufftSetStream(f, C->stream);
+  cufftSetStream(v, C->stream);
+  *fwd = f;
+  *inv = v;
   return FA_OK;
 }
+
+}  // namespace fa_rt
+
+namespace {
 
 fa_status correlator_create_impl(fa_context* ctx, const void* reference, bool ref_device, int nz, int ny, int nx,
                                  int cap, fa_correlator** out) {
@@ -1227,7 +1267,14 @@ fa_status correlator_create_impl(fa_context* ctx, const void* reference, bool re
   C->nx = nx;
   C->n_el = (long long)nz * ny * nx;
   C->n_complex = (long long)nz * ny * (nx / 2 + 1);
-  C->cap = cap < 1 ? 1 : cap;
+  // batch cap: a power of two, at most the requested cap and what 4 GiB of FP64 buffers hold
+  {
+    const long long per = C->n_el * 8 + C->n_complex * 16;
+    const long long fit = std::max<long long>(1, (4LL << 30) / per);
+    int c = 1;
+    while (c * 2 <= cap && c * 2 <= fit) c *= 2;
+    C->cap = c;
+  }
   auto cleanup = [&](fa_status st) {
     std::string keep = g_err;
     fa_correlator_destroy(C);
@@ -1260,13 +1307,8 @@ fa_status correlator_create_impl(fa_context* ctx, const void* reference, bool re
   if (cudaMemcpy(C->wy, wy.data(), wy.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(C->wx, wx.data(), wx.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
     return cleanup(fail(FA_ERR_CUDA, "window upload"));
-  if ((st = correlator_plan(C, C->cap, &C->fwd, &C->inv)) != FA_OK) return cleanup(st);
-  if (C->cap > 1) {
-    if ((st = correlator_plan(C, 1, &C->fwd1, &C->inv1)) != FA_OK) return cleanup(st);
-  } else {
-    C->fwd1 = C->fwd;
-    C->inv1 = C->inv;
-  }
+  cufftHandle fwd1, inv1;
+  if ((st = correlator_plans(C, 1, &fwd1, &inv1)) != FA_OK) return cleanup(st);
   if (cudaMemcpyAsync(C->vol, reference, (size_t)C->n_el * sizeof(float),
                       ref_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, C->stream) != cudaSuccess)
     return cleanup(fail(FA_ERR_CUDA, "reference upload"));
@@ -1276,7 +1318,7 @@ fa_status correlator_create_impl(fa_context* ctx, const void* reference, bool re
       fa::launch_phase_window(C->d_ptrs, FA_F32, C->wy, C->wx, ny, nx, C->n_el, 1, C->real, C->stream) !=
           cudaSuccess)
     return cleanup(fail(FA_ERR_CUDA, "window kernel"));
-  if (cufftExecD2Z(C->fwd1, C->real, reinterpret_cast<cufftDoubleComplex*>(C->spec)) != CUFFT_SUCCESS)
+  if (cufftExecD2Z(fwd1, C->real, reinterpret_cast<cufftDoubleComplex*>(C->spec)) != CUFFT_SUCCESS)
     return cleanup(fail(FA_ERR_CUDA, "cufftExecD2Z failed"));
   if (fa::launch_phase_conj(C->spec, C->ref_conj, C->n_complex, C->stream) != cudaSuccess)
     return cleanup(fail(FA_ERR_CUDA, "conj kernel"));
@@ -1296,10 +1338,12 @@ extern "C" fa_status fa_correlator_destroy(fa_correlator* C) {
   if (!C) return fail(FA_ERR_BAD_ARG, "NULL correlator");
   cudaSetDevice(C->ctx->device);
   if (C->stream) cudaStreamSynchronize(C->stream);
-  if (C->fwd1 && C->fwd1 != C->fwd) cufftDestroy(C->fwd1);
-  if (C->inv1 && C->inv1 != C->inv) cufftDestroy(C->inv1);
-  if (C->fwd) cufftDestroy(C->fwd);
-  if (C->inv) cufftDestroy(C->inv);
+  for (auto& pl : C->plans) {
+    cufftDestroy(pl.second.first);
+    cufftDestroy(pl.second.second);
+  }
+  C->plans.clear();
+  dfree_all(C->ctx, C->work_allocs);
   if (C->h_ptrs) cudaFreeHost(C->h_ptrs);
   if (C->h_idx) cudaFreeHost(C->h_idx);
   if (C->stream) cudaStreamDestroy(C->stream);
@@ -1619,8 +1663,8 @@ extern "C" fa_status fa_aligner_set_reference(fa_aligner* A, const void* referen
   }
   FA_CU(fa::launch_downsample(raw, dtype, nz, ny, nx, b, static_cast<float*>(down), A->stream));
   FA_CU(cudaStreamSynchronize(A->stream));
-  // Frames go through the correlator in batches of up to 16 (one batched cuFFT plan).
-  fa_status st = correlator_create_impl(A->ctx, down, true, A->dz, A->dy, A->dx, 16, &A->corr);
+  // Frames go through the correlator in batched cuFFT plans of up to 64 frames (less for large volumes).
+  fa_status st = correlator_create_impl(A->ctx, down, true, A->dz, A->dy, A->dx, 64, &A->corr);
   if (st == FA_OK)
     st = fa_set_reference_device(A->ctx, static_cast<const float*>(plus1), nz, ny, nx, A->nD, scan, A->prm.precision,
                                  &A->ref);

@@ -6,6 +6,7 @@
 #include <cufft.h>
 
 #include <atomic>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -106,9 +107,13 @@ struct fa_correlator {
   fa_context* ctx = nullptr;
   int nz = 0, ny = 0, nx = 0;
   long long n_el = 0, n_complex = 0;
-  int cap = 0;                          // frames per batched FFT
-  cufftHandle fwd = 0, inv = 0;         // batch of cap frames
-  cufftHandle fwd1 = 0, inv1 = 0;       // single frame
+  int cap = 0;                          // most frames per batched FFT (a power of two)
+  // D2Z / Z2D plans per batch size (powers of two up to cap), made on first use; they share one work
+  // area (they run one after another on the correlator's stream)
+  std::map<int, std::pair<cufftHandle, cufftHandle>> plans;
+  void* work = nullptr;
+  size_t work_bytes = 0;
+  std::vector<fa_rt::Alloc> work_allocs;
   cudaStream_t stream = nullptr;
   double* wy = nullptr;                 // square-root Hann window along y
   double* wx = nullptr;                 // ... and along x (1 along z)
@@ -199,6 +204,8 @@ fa_status aligner_smooth(fa_aligner* A, const void* raw, fa_dtype dtype, cudaStr
 fa_status frame_alloc(fa_reference* R, int kind, fa_frame** out);
 // Slot storage the aligner uses for frames of dtype (raw uint16 counts + 1, FP16 or FP32 values + 1).
 int slot_kind_for(const fa_aligner* A, fa_dtype dtype);
+// The correlator's D2Z / Z2D plans for a batch size (made and cached on first use).
+fa_status correlator_plans(fa_correlator* C, int batch, cufftHandle* fwd, cufftHandle* inv);
 // Window, D2Z, normalisation, Z2D and argmax for n device volumes; peak indices to C->d_idx[0..n).
 fa_status correlator_enqueue(fa_correlator* C, const void* const* vols, int in_kind, int n);
 // Peak index -> signed integer shift (x, y, z).
