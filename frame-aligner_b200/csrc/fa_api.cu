@@ -1146,23 +1146,50 @@ fa_status correlator_reserve(fa_correlator* C, int n) {
 
 namespace fa_rt {
 
-fa_status correlator_enqueue(fa_correlator* C, const void* const* vols, int in_kind, int n) {
+fa_status correlator_enqueue(fa_correlator* C, const void* const* vols, int in_kind, int n, double* surface,
+                             bool planes) {
   FA_TRY(correlator_reserve(C, n));
-  for (int i = 0; i < n; i++) C->h_ptrs[i] = vols[i];
+  // the fused passes stage frames in 16-byte chunks: 16-byte aligned frames only
+  for (int i = 0; i < n; i++) {
+    C->h_ptrs[i] = vols[i];
+    if (reinterpret_cast<uintptr_t>(vols[i]) % 16) planes = false;
+  }
+  planes = planes && C->planes;
   FA_CU(cudaMemcpyAsync(C->d_ptrs, C->h_ptrs, (size_t)n * sizeof(void*), cudaMemcpyHostToDevice, C->stream));
+  if (!planes && C->planes && !C->ref_conj_rows) {  // a plane-path correlator falling back to cuFFT
+    FA_CU(cudaStreamSynchronize(C->stream));
+    FA_TRY(dalloc_t(C->ctx, (size_t)C->n_el * C->cap, &C->real, C->allocs));
+    FA_TRY(dalloc_t(C->ctx, (size_t)C->n_complex, &C->ref_conj_rows, C->allocs));
+    FA_CU(fa::launch_plane_to_rows(C->pd, C->ref_conj, C->ref_conj_rows, C->stream));
+  }
+  const double2* ref_rows = C->planes ? C->ref_conj_rows : C->ref_conj;
   for (int c0 = 0; c0 < n;) {
     int m = C->cap;  // the largest power-of-two batch that fits the rest
     while (m > n - c0) m >>= 1;
-    cufftHandle fwd, inv;
-    FA_TRY(correlator_plans(C, m, &fwd, &inv));
-    FA_CU(fa::launch_phase_window(C->d_ptrs + c0, in_kind, C->wy, C->wx, C->ny, C->nx, C->n_el, m, C->real, C->stream));
-    if (cufftExecD2Z(fwd, C->real, reinterpret_cast<cufftDoubleComplex*>(C->spec)) != CUFFT_SUCCESS)
-      return fail(FA_ERR_CUDA, "cufftExecD2Z failed");
-    FA_CU(fa::launch_phase_normalise(C->spec, C->ref_conj, C->n_complex, m, C->stream));
-    if (cufftExecZ2D(inv, reinterpret_cast<cufftDoubleComplex*>(C->spec), C->real) != CUFFT_SUCCESS)
-      return fail(FA_ERR_CUDA, "cufftExecZ2D failed");
-    FA_CU(fa::launch_phase_argmax(C->real, C->n_el, m, C->bval, C->bidx, C->n_blocks, C->d_idx + c0, C->stream));
-    g_launches += 4;  // window, normalise, two argmax stages (the FFTs are cuFFT's)
+    double* surf = surface ? surface + (size_t)c0 * C->n_el : nullptr;
+    if (planes) {
+      const int nb = fa::plane_blocks_per_frame(C->pd);
+      FA_CU(fa::launch_plane_rows_fwd(C->pd, C->d_ptrs + c0, in_kind, m, C->wy, C->wx, C->tw_x, C->spec, C->stream));
+      FA_CU(fa::launch_plane_yz(C->pd, C->spec, C->spec, C->ref_conj, C->tw_y, m, false, C->stream));
+      FA_CU(fa::launch_plane_rows_inv_argmax(C->pd, C->spec, m, C->tw_x, C->bval, C->bidx, surf, C->stream));
+      FA_CU(fa::launch_phase_argmax_final(C->bval, C->bidx, nb, m, C->d_idx + c0, C->stream));
+      g_launches += 4;
+    } else {
+      cufftHandle fwd, inv;
+      FA_TRY(correlator_plans(C, m, &fwd, &inv));
+      FA_CU(fa::launch_phase_window(C->d_ptrs + c0, in_kind, C->wy, C->wx, C->ny, C->nx, C->n_el, m, C->real,
+                                    C->stream));
+      if (cufftExecD2Z(fwd, C->real, reinterpret_cast<cufftDoubleComplex*>(C->spec)) != CUFFT_SUCCESS)
+        return fail(FA_ERR_CUDA, "cufftExecD2Z failed");
+      FA_CU(fa::launch_phase_normalise(C->spec, ref_rows, C->n_complex, m, C->stream));
+      if (cufftExecZ2D(inv, reinterpret_cast<cufftDoubleComplex*>(C->spec), C->real) != CUFFT_SUCCESS)
+        return fail(FA_ERR_CUDA, "cufftExecZ2D failed");
+      FA_CU(fa::launch_phase_argmax(C->real, C->n_el, m, C->bval, C->bidx, C->n_blocks, C->d_idx + c0, C->stream));
+      if (surf)
+        FA_CU(cudaMemcpyAsync(surf, C->real, (size_t)m * C->n_el * sizeof(double), cudaMemcpyDeviceToDevice,
+                              C->stream));
+      g_launches += 4;  // window, normalise, two argmax stages (the FFTs are cuFFT's)
+    }
     c0 += m;
   }
   return FA_OK;
@@ -1286,13 +1313,18 @@ fa_status correlator_create_impl(fa_context* ctx, const void* reference, bool re
   fa_status st;
   if ((st = dalloc_t(ctx, (size_t)ny, &C->wy, C->allocs)) != FA_OK) return cleanup(st);
   if ((st = dalloc_t(ctx, (size_t)nx, &C->wx, C->allocs)) != FA_OK) return cleanup(st);
-  if ((st = dalloc_t(ctx, (size_t)C->n_el * C->cap, &C->real, C->allocs)) != FA_OK) return cleanup(st);
+  C->planes = fa::plane_dims(nz, ny, nx, &C->pd);
+  if (!C->planes)
+    if ((st = dalloc_t(ctx, (size_t)C->n_el * C->cap, &C->real, C->allocs)) != FA_OK) return cleanup(st);
   if ((st = dalloc_t(ctx, (size_t)C->n_complex * C->cap, &C->spec, C->allocs)) != FA_OK) return cleanup(st);
   if ((st = dalloc_t(ctx, (size_t)C->n_complex, &C->ref_conj, C->allocs)) != FA_OK) return cleanup(st);
   if ((st = dalloc_t(ctx, (size_t)C->n_el, &C->vol, C->allocs)) != FA_OK) return cleanup(st);
   C->n_blocks = (int)std::min<long long>(std::max(1, 148 * 4 / C->cap), (C->n_el + 255) / 256);
-  if ((st = dalloc_t(ctx, (size_t)C->n_blocks * C->cap, &C->bval, C->allocs)) != FA_OK) return cleanup(st);
-  if ((st = dalloc_t(ctx, (size_t)C->n_blocks * C->cap, &C->bidx, C->allocs)) != FA_OK) return cleanup(st);
+  {
+    const int nb = std::max(C->n_blocks, C->planes ? fa::plane_blocks_per_frame(C->pd) : 0);
+    if ((st = dalloc_t(ctx, (size_t)nb * C->cap, &C->bval, C->allocs)) != FA_OK) return cleanup(st);
+    if ((st = dalloc_t(ctx, (size_t)nb * C->cap, &C->bidx, C->allocs)) != FA_OK) return cleanup(st);
+  }
   // Square-root Hann window in x and y, 1 along z (VolumePhaseCorrelator.cpp:141-166).
   auto hann = [](int n) {
     std::vector<double> w(n, 1.0);
@@ -1307,22 +1339,53 @@ fa_status correlator_create_impl(fa_context* ctx, const void* reference, bool re
   if (cudaMemcpy(C->wy, wy.data(), wy.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(C->wx, wx.data(), wx.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
     return cleanup(fail(FA_ERR_CUDA, "window upload"));
-  cufftHandle fwd1, inv1;
-  if ((st = correlator_plans(C, 1, &fwd1, &inv1)) != FA_OK) return cleanup(st);
   if (cudaMemcpyAsync(C->vol, reference, (size_t)C->n_el * sizeof(float),
                       ref_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, C->stream) != cudaSuccess)
     return cleanup(fail(FA_ERR_CUDA, "reference upload"));
   if ((st = correlator_reserve(C, 1)) != FA_OK) return cleanup(st);
   C->h_ptrs[0] = C->vol;
-  if (cudaMemcpyAsync(C->d_ptrs, C->h_ptrs, sizeof(void*), cudaMemcpyHostToDevice, C->stream) != cudaSuccess ||
-      fa::launch_phase_window(C->d_ptrs, FA_F32, C->wy, C->wx, ny, nx, C->n_el, 1, C->real, C->stream) !=
-          cudaSuccess)
-    return cleanup(fail(FA_ERR_CUDA, "window kernel"));
-  if (cufftExecD2Z(fwd1, C->real, reinterpret_cast<cufftDoubleComplex*>(C->spec)) != CUFFT_SUCCESS)
-    return cleanup(fail(FA_ERR_CUDA, "cufftExecD2Z failed"));
-  if (fa::launch_phase_conj(C->spec, C->ref_conj, C->n_complex, C->stream) != cudaSuccess)
-    return cleanup(fail(FA_ERR_CUDA, "conj kernel"));
-  if (cudaStreamSynchronize(C->stream) != cudaSuccess) return cleanup(fail(FA_ERR_CUDA, "correlator set-up"));
+  if (cudaMemcpyAsync(C->d_ptrs, C->h_ptrs, sizeof(void*), cudaMemcpyHostToDevice, C->stream) != cudaSuccess)
+    return cleanup(fail(FA_ERR_CUDA, "pointer upload"));
+  if (C->planes) {
+    // W_L^m = exp(-2 pi i m / L), rounded from long double; exact at the quarter turns
+    auto twiddles = [](int L) {
+      std::vector<double2> t(L);
+      const long double two_pi = 6.283185307179586476925286766559L;
+      for (int m = 0; m < L; m++) {
+        const long double a = two_pi * m / L;
+        t[m] = make_double2((double)cosl(a), (double)-sinl(a));
+        if (4 * m == L) t[m] = make_double2(0.0, -1.0);
+        if (2 * m == L) t[m] = make_double2(-1.0, 0.0);
+        if (4 * m == 3 * L) t[m] = make_double2(0.0, 1.0);
+      }
+      return t;
+    };
+    const std::vector<double2> tx = twiddles(nx), ty = twiddles(ny);
+    if ((st = dalloc_t(ctx, tx.size(), &C->tw_x, C->allocs)) != FA_OK) return cleanup(st);
+    if ((st = dalloc_t(ctx, ty.size(), &C->tw_y, C->allocs)) != FA_OK) return cleanup(st);
+    if (cudaMemcpy(C->tw_x, tx.data(), tx.size() * sizeof(double2), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(C->tw_y, ty.data(), ty.size() * sizeof(double2), cudaMemcpyHostToDevice) != cudaSuccess)
+      return cleanup(fail(FA_ERR_CUDA, "twiddle upload"));
+    if (fa::launch_plane_rows_fwd(C->pd, C->d_ptrs, FA_F32, 1, C->wy, C->wx, C->tw_x, C->spec, C->stream) !=
+            cudaSuccess ||
+        fa::launch_plane_yz(C->pd, C->spec, C->ref_conj, nullptr, C->tw_y, 1, true, C->stream) != cudaSuccess)
+      return cleanup(fail(FA_ERR_CUDA, "reference spectrum"));
+  } else {
+    cufftHandle fwd1, inv1;
+    if ((st = correlator_plans(C, 1, &fwd1, &inv1)) != FA_OK) return cleanup(st);
+    if (fa::launch_phase_window(C->d_ptrs, FA_F32, C->wy, C->wx, ny, nx, C->n_el, 1, C->real, C->stream) !=
+        cudaSuccess)
+      return cleanup(fail(FA_ERR_CUDA, "window kernel"));
+    if (cufftExecD2Z(fwd1, C->real, reinterpret_cast<cufftDoubleComplex*>(C->spec)) != CUFFT_SUCCESS)
+      return cleanup(fail(FA_ERR_CUDA, "cufftExecD2Z failed"));
+    if (fa::launch_phase_conj(C->spec, C->ref_conj, C->n_complex, C->stream) != cudaSuccess)
+      return cleanup(fail(FA_ERR_CUDA, "conj kernel"));
+  }
+  {
+    const cudaError_t e = cudaStreamSynchronize(C->stream);
+    if (e != cudaSuccess)
+      return cleanup(fail(FA_ERR_CUDA, std::string("correlator set-up: ") + cudaGetErrorString(e)));
+  }
   *out = C;
   return FA_OK;
 }
@@ -1373,6 +1436,33 @@ extern "C" fa_status fa_correlator_shift_device(fa_correlator* C, const float* v
 }
 
 // ================================================================== test hooks ====================
+
+extern "C" fa_status fa_test_correlation_surface(fa_correlator* C, const float* volume, int use_planes,
+                                                 double* surface) {
+  if (!C || !volume || !surface) return fail(FA_ERR_BAD_ARG, "NULL argument");
+  if (use_planes && !C->planes) return fail(FA_ERR_UNSUPPORTED, "dimensions outside the fused plane passes");
+  std::lock_guard<std::mutex> lk(C->mu);
+  FA_CU(cudaSetDevice(C->ctx->device));
+  std::vector<Alloc> tmp;
+  double* d_surf = nullptr;
+  FA_TRY(dalloc_t(C->ctx, (size_t)C->n_el, &d_surf, tmp));
+  auto done = [&](fa_status r) {
+    cudaStreamSynchronize(C->stream);
+    dfree_all(C->ctx, tmp);
+    return r;
+  };
+  if (cudaMemcpyAsync(C->vol, volume, (size_t)C->n_el * sizeof(float), cudaMemcpyHostToDevice, C->stream) !=
+      cudaSuccess)
+    return done(fail(FA_ERR_CUDA, "volume upload"));
+  const void* v = C->vol;
+  fa_status st = correlator_enqueue(C, &v, FA_F32, 1, d_surf, use_planes != 0);
+  if (st != FA_OK) return done(st);
+  if (cudaMemcpyAsync(surface, d_surf, (size_t)C->n_el * sizeof(double), cudaMemcpyDeviceToHost, C->stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(C->stream) != cudaSuccess)
+    return done(fail(FA_ERR_CUDA, "surface read"));
+  return done(FA_OK);
+}
 
 extern "C" fa_status fa_test_tr_subproblem(fa_context* ctx, int nD, int n_dim, const double* H, const double* g,
                                            double radius, double* p, int* on_boundary) {

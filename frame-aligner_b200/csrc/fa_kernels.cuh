@@ -107,5 +107,36 @@ cudaError_t launch_phase_normalise(double2* spec, const double2* ref_conj, long 
 cudaError_t launch_phase_argmax(const double* surf, long long n, int batch, double* block_val, long long* block_idx,
                                 int blocks_per_frame, long long* out_idx, cudaStream_t s);
 cudaError_t launch_phase_conj(const double2* in, double2* out, long long n, cudaStream_t s);
+// Second argmax stage alone: the first maximum of nb (value, index) pairs per frame.
+cudaError_t launch_phase_argmax_final(const double* block_val, const long long* block_idx, int nb, int batch,
+                                      long long* out_idx, cudaStream_t s);
+
+// Phase correlation as three fused passes over kx planes (fa_plane_corr.cu), for power-of-two
+// volumes with nz <= 16, 8 <= ny <= 2048, 16 <= nx <= 4096 and nz * ny <= 8192 (plane_dims is false
+// otherwise). Half-spectra are stored as planes spec[kx][z][y], kx = 0..nx/2.
+struct PlaneDims {
+  int nz, ny, nx, rows;      // rows = nz * ny
+  int log2M, log2ny, log2G;  // M = nx / 2; G rows per row CTA
+  int PP;                    // planes per plane CTA
+  long long n_complex, n_el;
+};
+bool plane_dims(int nz, int ny, int nx, PlaneDims* d);
+// CTAs (argmax partials) per frame of the last pass.
+int plane_blocks_per_frame(const PlaneDims& d);
+// Window + real DFT along x of each frame (dense FP32 or uint16, in_kind an fa_dtype) into spec
+// (batch * n_complex).
+cudaError_t launch_plane_rows_fwd(const PlaneDims& d, const void* const* vols, int in_kind, int batch,
+                                  const double* wy, const double* wx, const double2* tw_x, double2* spec,
+                                  cudaStream_t s);
+// Per plane: forward DFT over (z, y), then either out = conj (reference) or, in place,
+// out = inverse DFT of the normalised cross-power spectrum with ref_conj.
+cudaError_t launch_plane_yz(const PlaneDims& d, const double2* in, double2* out, const double2* ref_conj,
+                            const double2* tw_y, int batch, bool reference, cudaStream_t s);
+// One frame's half-spectrum from planes spec[kx][z][y] to cuFFT's order [z][y][kx].
+cudaError_t launch_plane_to_rows(const PlaneDims& d, const double2* in, double2* out, cudaStream_t s);
+// Inverse real DFT along x and the per-CTA first maximum (bval / bidx: batch * plane_blocks_per_frame);
+// surface (batch * n_el doubles) receives the real surface when not null.
+cudaError_t launch_plane_rows_inv_argmax(const PlaneDims& d, const double2* spec, int batch, const double2* tw_x,
+                                         double* bval, long long* bidx, double* surface, cudaStream_t s);
 
 }  // namespace fa

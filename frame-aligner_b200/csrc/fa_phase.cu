@@ -147,6 +147,12 @@ __global__ void __launch_bounds__(256) phase_argmax_final(const double* __restri
   if (threadIdx.x == 0) out[blockIdx.x] = (si[0] == 0x7fffffffffffffffLL) ? 0 : si[0];
 }
 
+cudaError_t launch_phase_argmax_final(const double* block_val, const long long* block_idx, int nb, int batch,
+                                      long long* out_idx, cudaStream_t s) {
+  phase_argmax_final<<<batch, 256, 0, s>>>(block_val, block_idx, nb, out_idx);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_phase_argmax(const double* surf, long long n, int batch, double* block_val, long long* block_idx,
                                 int blocks_per_frame, long long* out_idx, cudaStream_t s) {
   phase_argmax_blocks<<<dim3(blocks_per_frame, batch), 256, 0, s>>>(surf, n, block_val, block_idx);

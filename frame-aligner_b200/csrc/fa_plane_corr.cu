@@ -1,0 +1,600 @@
+// fa_plane_corr.cu -- the phase correlator's FP64 transforms as three fused passes over a batch of
+// frames (power-of-two volumes with nz <= 16, 8 <= ny <= 2048, 16 <= nx <= 4096 and an (nz, ny) plane of at most
+// 8192 points), instead of window + cuFFT D2Z (three axis passes) + normalise + cuFFT Z2D (three
+// axis passes) + argmax. The computed quantity is the reference's
+// (VolumePhaseCorrelator.cpp:57-103): the windowed frame's 3-D DFT times the conjugate of the
+// reference's, divided by its modulus + DBL_MIN, transformed back, first maximum.
+//
+//   plane_rows_fwd_kernel   window (the reference's separately rounded FP64 products) and the real
+//                           DFT along x of G rows, as an nx/2-point complex DFT of the packed row
+//                           (even samples real, odd samples imaginary) and the split into the
+//                           nx/2 + 1 half-spectrum bins; written as planes spec[kx][z][y]
+//   plane_yz_kernel         per kx plane (nz x ny, on chip): DFT along y, DFT along z, times the
+//                           reference's conjugate spectrum, normalised, inverse along z and y; or,
+//                           for the reference itself, the conjugate of the forward plane
+//   plane_rows_inv_argmax   the inverse real DFT along x of G rows (the half-spectrum folded into
+//                           an nx/2-point complex inverse DFT) and the first maximum of the real
+//                           surface in flat (z, y, x) order, per CTA; then phase_argmax_final
+//
+// DFTs along a row are Stockham radix-8/4/2 stages in shared memory (line l, element i at
+// l * (L + 1) + (i ^ ((i >> 3) & 7)): conflict-free for the stride-R writes of every stage and for
+// column reads across lines); the z DFT (<= 16 points) runs in registers, one (kx, y) column per
+// thread. Twiddles W_L^m = exp(-2 pi i m / L) come from tables rounded from long double on the host.
+// The inverse transforms are unnormalised (a positive scale does not move the maximum).
+#include <float.h>
+
+#include <algorithm>
+
+#include "fa_kernels.cuh"
+
+namespace fa {
+
+namespace {
+
+__device__ __forceinline__ int swz(int i) { return i ^ ((i >> 3) & 7); }
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 w) {
+  return make_double2(fma(a.x, w.x, -a.y * w.y), fma(a.x, w.y, a.y * w.x));
+}
+// a * w (forward) or a * conj(w) (inverse)
+template <bool INV>
+__device__ __forceinline__ double2 cmul_tw(double2 a, double2 w) {
+  return INV ? make_double2(fma(a.x, w.x, a.y * w.y), fma(a.y, w.x, -a.x * w.y)) : cmul(a, w);
+}
+// a * (-i) (forward) or a * (+i) (inverse)
+template <bool INV>
+__device__ __forceinline__ double2 rot(double2 a) {
+  return INV ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+}
+
+constexpr double kS2 = 0.70710678118654752440;   // cos(pi/4)
+constexpr double kC8 = 0.92387953251128675613;   // cos(pi/8)
+constexpr double kS8 = 0.38268343236508977173;   // sin(pi/8)
+
+template <bool INV>
+__device__ __forceinline__ void dft2(double2& a0, double2& a1) {
+  const double2 t = a0;
+  a0 = cadd(t, a1);
+  a1 = csub(t, a1);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft4(double2& a0, double2& a1, double2& a2, double2& a3) {
+  const double2 t0 = cadd(a0, a2), t1 = csub(a0, a2), t2 = cadd(a1, a3), t3 = rot<INV>(csub(a1, a3));
+  a0 = cadd(t0, t2);
+  a2 = csub(t0, t2);
+  a1 = cadd(t1, t3);
+  a3 = csub(t1, t3);
+}
+
+// W_8^1 and W_8^3 (forward) or their conjugates (inverse)
+template <bool INV>
+__device__ __forceinline__ double2 w8_1(double2 a) {
+  return INV ? make_double2(kS2 * (a.x - a.y), kS2 * (a.x + a.y)) : make_double2(kS2 * (a.x + a.y), kS2 * (a.y - a.x));
+}
+template <bool INV>
+__device__ __forceinline__ double2 w8_3(double2 a) {
+  return INV ? make_double2(-kS2 * (a.x + a.y), kS2 * (a.x - a.y))
+             : make_double2(kS2 * (a.y - a.x), -kS2 * (a.x + a.y));
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft8(double2* a) {
+  double2 e0 = a[0], e1 = a[2], e2 = a[4], e3 = a[6];
+  double2 o0 = a[1], o1 = a[3], o2 = a[5], o3 = a[7];
+  dft4<INV>(e0, e1, e2, e3);
+  dft4<INV>(o0, o1, o2, o3);
+  o1 = w8_1<INV>(o1);
+  o2 = rot<INV>(o2);
+  o3 = w8_3<INV>(o3);
+  a[0] = cadd(e0, o0);
+  a[4] = csub(e0, o0);
+  a[1] = cadd(e1, o1);
+  a[5] = csub(e1, o1);
+  a[2] = cadd(e2, o2);
+  a[6] = csub(e2, o2);
+  a[3] = cadd(e3, o3);
+  a[7] = csub(e3, o3);
+}
+
+// W_16^e (forward) for the exponents a 4 x 4 split needs
+__device__ __forceinline__ double2 w16(int e) {
+  switch (e) {
+    case 1: return make_double2(kC8, -kS8);
+    case 2: return make_double2(kS2, -kS2);
+    case 3: return make_double2(kS8, -kC8);
+    case 4: return make_double2(0.0, -1.0);
+    case 6: return make_double2(-kS2, -kS2);
+    case 9: return make_double2(-kC8, kS8);
+    default: return make_double2(1.0, 0.0);
+  }
+}
+
+// 16 points as 4 x 4: X[k1 + 4 k2] = sum_n2 W_4^(n2 k2) W_16^(n2 k1) sum_n1 W_4^(n1 k1) a[4 n1 + n2]
+template <bool INV>
+__device__ __forceinline__ void dft16(double2* a) {
+  double2 b[4][4];
+#pragma unroll
+  for (int n2 = 0; n2 < 4; n2++) {
+    b[n2][0] = a[n2];
+    b[n2][1] = a[n2 + 4];
+    b[n2][2] = a[n2 + 8];
+    b[n2][3] = a[n2 + 12];
+    dft4<INV>(b[n2][0], b[n2][1], b[n2][2], b[n2][3]);
+#pragma unroll
+    for (int k1 = 1; k1 < 4; k1++)
+      if (n2 > 0) b[n2][k1] = cmul_tw<INV>(b[n2][k1], w16(n2 * k1));
+  }
+#pragma unroll
+  for (int k1 = 0; k1 < 4; k1++) {
+    double2 c0 = b[0][k1], c1 = b[1][k1], c2 = b[2][k1], c3 = b[3][k1];
+    dft4<INV>(c0, c1, c2, c3);
+    a[k1] = c0;
+    a[k1 + 4] = c1;
+    a[k1 + 8] = c2;
+    a[k1 + 12] = c3;
+  }
+}
+
+// In-register DFT of R points (natural order in and out).
+template <int R, bool INV>
+__device__ __forceinline__ void dft(double2* a) {
+  if constexpr (R == 2) dft2<INV>(a[0], a[1]);
+  else if constexpr (R == 4) dft4<INV>(a[0], a[1], a[2], a[3]);
+  else if constexpr (R == 8) dft8<INV>(a);
+  else if constexpr (R == 16) dft16<INV>(a);
+}
+
+// One in-place Stockham radix-R stage over `lines` lines of L = 2^LOG2L points in shared memory
+// (line stride L + 1): every thread reads its butterflies into registers, the block synchronises,
+// then writes them back. Butterfly j of a line: a[r] = x[j + r L/R], twiddled by W_(Ns R)^(r k)
+// with k = j mod Ns, R-point DFT, stored at ((j - k) R + k) + r Ns. NB bounds the butterflies per
+// thread; tw (W_L'^m with L' = L << TWS) is in shared memory, so it is read with plain loads. The
+// sizes are template constants, so the swizzled addresses reduce to a few integer operations.
+template <int R, int NB, bool INV, int LOG2L, int LOG2NS, int TWS, int T>
+__device__ __forceinline__ void stockham_stage(double2* sm, int lines, const double2* tw) {
+  constexpr int log2R = R == 8 ? 3 : (R == 4 ? 2 : 1);
+  constexpr int log2q = LOG2L - log2R;
+  constexpr int q = 1 << log2q;
+  constexpr int Ns = 1 << LOG2NS;
+  constexpr int S = (1 << LOG2L) + 1;
+  constexpr int twsh = LOG2L - LOG2NS - log2R + TWS;
+  const int nb = lines << log2q;
+  double2 a[NB][R];
+#pragma unroll
+  for (int u = 0; u < NB; u++) {
+    const int b = threadIdx.x + u * T;
+    if (b < nb) {
+      const int l = b >> log2q, j = b & (q - 1);
+      const double2* line = sm + l * S;
+#pragma unroll
+      for (int r = 0; r < R; r++) a[u][r] = line[swz(j + (r << log2q))];
+      if (Ns > 1) {
+        const int k = j & (Ns - 1);
+#pragma unroll
+        for (int r = 1; r < R; r++) a[u][r] = cmul_tw<INV>(a[u][r], tw[(r * k) << twsh]);
+      }
+      dft<R, INV>(a[u]);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < NB; u++) {
+    const int b = threadIdx.x + u * T;
+    if (b < nb) {
+      const int l = b >> log2q, j = b & (q - 1);
+      const int k = j & (Ns - 1);
+      const int o = ((j - k) << log2R) + k;
+      double2* line = sm + l * S;
+#pragma unroll
+      for (int r = 0; r < R; r++) line[swz(o + (r << LOG2NS))] = a[u][r];
+    }
+  }
+  __syncthreads();
+}
+
+// Radix-8 stages, then one radix-4 or radix-2 stage.
+template <bool INV, int EPT, int LOG2L, int TWS, int T, int LOG2NS = 0>
+__device__ __forceinline__ void fft_rows_t(double2* sm, int lines, const double2* tw) {
+  if constexpr (LOG2L - LOG2NS >= 3) {
+    stockham_stage<8, EPT / 8, INV, LOG2L, LOG2NS, TWS, T>(sm, lines, tw);
+    fft_rows_t<INV, EPT, LOG2L, TWS, T, LOG2NS + 3>(sm, lines, tw);
+  } else if constexpr (LOG2L - LOG2NS == 2) {
+    stockham_stage<4, EPT / 4, INV, LOG2L, LOG2NS, TWS, T>(sm, lines, tw);
+  } else if constexpr (LOG2L - LOG2NS == 1) {
+    stockham_stage<2, EPT / 2, INV, LOG2L, LOG2NS, TWS, T>(sm, lines, tw);
+  }
+}
+
+// DFT of every line of 2^log2L points (3 <= log2L <= 11, line stride 2^log2L + 1) by a block of T
+// threads; starts with a barrier and ends with one. lines * 2^log2L <= EPT * T.
+template <bool INV, int EPT, int TWS, int T>
+__device__ __forceinline__ void fft_rows(double2* sm, int lines, int log2L, const double2* tw) {
+  __syncthreads();
+  switch (log2L) {
+    case 3: fft_rows_t<INV, EPT, 3, TWS, T>(sm, lines, tw); break;
+    case 4: fft_rows_t<INV, EPT, 4, TWS, T>(sm, lines, tw); break;
+    case 5: fft_rows_t<INV, EPT, 5, TWS, T>(sm, lines, tw); break;
+    case 6: fft_rows_t<INV, EPT, 6, TWS, T>(sm, lines, tw); break;
+    case 7: fft_rows_t<INV, EPT, 7, TWS, T>(sm, lines, tw); break;
+    case 8: fft_rows_t<INV, EPT, 8, TWS, T>(sm, lines, tw); break;
+    case 9: fft_rows_t<INV, EPT, 9, TWS, T>(sm, lines, tw); break;
+    case 10: fft_rows_t<INV, EPT, 10, TWS, T>(sm, lines, tw); break;
+    case 11: fft_rows_t<INV, EPT, 11, TWS, T>(sm, lines, tw); break;
+    default: break;
+  }
+}
+
+constexpr int kRowThreads = 256;
+constexpr int kRowEPT = 8;      // G * nx/2 <= 2048 points per row CTA
+constexpr int kPlaneThreads = 512;
+constexpr int kPlaneEPT = 16;   // PP * nz * ny <= 8192 points per plane CTA
+
+// Global -> shared staging in 16-byte chunks: chunk i is read from src_of(i) and written to
+// dst_of(i), with K loads of each thread in flight before the first store. Published by the
+// caller's next barrier.
+template <int K, class SrcOf, class DstOf>
+__device__ __forceinline__ void stage16(int n, SrcOf src_of, DstOf dst_of) {
+  for (int base = 0; base < n; base += K * (int)blockDim.x) {
+    uint4 v[K];
+#pragma unroll
+    for (int u = 0; u < K; u++) {
+      const int i = base + (int)threadIdx.x + u * (int)blockDim.x;
+      if (i < n) v[u] = __ldg(src_of(i));
+    }
+#pragma unroll
+    for (int u = 0; u < K; u++) {
+      const int i = base + (int)threadIdx.x + u * (int)blockDim.x;
+      if (i < n) *dst_of(i) = v[u];
+    }
+  }
+}
+
+// Row-pass shared memory: G lines of S = nx/2 + 1 points and the nx twiddles W_nx^m (double2), then
+// (forward pass) the nx window factors along x, G along y (8 slots) and the G raw rows.
+__host__ __device__ inline size_t rows_smem_bytes(const PlaneDims& d, int raw_bytes_per_el) {
+  const size_t G = (size_t)1 << d.log2G;
+  size_t b = (G * ((d.nx >> 1) + 1) + d.nx) * 16;
+  if (raw_bytes_per_el) b += (size_t)d.nx * 8 + 64 + G * d.nx * raw_bytes_per_el;
+  return b;
+}
+
+template <bool U16>
+__global__ void __launch_bounds__(kRowThreads) plane_rows_fwd_kernel(const void* const* __restrict__ vols,
+                                                                     const double* __restrict__ wy,
+                                                                     const double* __restrict__ wx,
+                                                                     const double2* __restrict__ tw_x, PlaneDims d,
+                                                                     double2* __restrict__ spec) {
+  extern __shared__ double2 sm[];
+  constexpr int kEsz = U16 ? 2 : 4;
+  const int M = d.nx >> 1, S = M + 1, G = 1 << d.log2G;
+  double2* tws = sm + G * S;
+  double* wxs = reinterpret_cast<double*>(tws + d.nx);
+  double* wys = wxs + d.nx;
+  unsigned char* raw = reinterpret_cast<unsigned char*>(wys + 8);
+  const int r0 = blockIdx.x << d.log2G;
+  {
+    // raw rows, then the twiddles, then the window factors along x (all 16-byte chunks)
+    const uint4* src = reinterpret_cast<const uint4*>(static_cast<const unsigned char*>(vols[blockIdx.y]) +
+                                                      (size_t)r0 * d.nx * kEsz);
+    const int n_raw = (G * d.nx * kEsz) >> 4, n_tw = d.nx, n_wx = d.nx >> 1;
+    const uint4* tsrc = reinterpret_cast<const uint4*>(tw_x);
+    const uint4* wsrc = reinterpret_cast<const uint4*>(wx);
+    uint4* rdst = reinterpret_cast<uint4*>(raw);
+    uint4* tdst = reinterpret_cast<uint4*>(tws);
+    uint4* wdst = reinterpret_cast<uint4*>(wxs);
+    stage16<4>(
+        n_raw + n_tw + n_wx,
+        [&](int i) { return i < n_raw ? src + i : (i < n_raw + n_tw ? tsrc + (i - n_raw) : wsrc + (i - n_raw - n_tw)); },
+        [&](int i) { return i < n_raw ? rdst + i : (i < n_raw + n_tw ? tdst + (i - n_raw) : wdst + (i - n_raw - n_tw)); });
+    if (threadIdx.x < G) wys[threadIdx.x] = __ldg(wy + (r0 & (d.ny - 1)) + threadIdx.x);
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < (G << d.log2M); idx += blockDim.x) {
+    const int g = idx >> d.log2M, m = idx & (M - 1);
+    const int x = 2 * (idx & (M - 1)) + (g << (d.log2M + 1));  // element of the staged rows
+    float v0, v1;
+    if (U16) {
+      const ushort2 q = reinterpret_cast<const ushort2*>(raw)[x >> 1];
+      v0 = (float)q.x;
+      v1 = (float)q.y;
+    } else {
+      const float2 f = reinterpret_cast<const float2*>(raw)[x >> 1];
+      v0 = f.x;
+      v1 = f.y;
+    }
+    // (double)v * ((1 * wy[y]) * wx[x]), each product rounded (VolumePhaseCorrelator.cpp:62-63)
+    const double wrow = __dmul_rn(1.0, wys[g]);
+    sm[g * S + swz(m)] = make_double2(__dmul_rn((double)v0, __dmul_rn(wrow, wxs[2 * m])),
+                                      __dmul_rn((double)v1, __dmul_rn(wrow, wxs[2 * m + 1])));
+  }
+  fft_rows<false, kRowEPT, 1, kRowThreads>(sm, G, d.log2M, tws);
+  // X[k] = (Z[k] + conj Z[M-k]) / 2 - i W_nx^k (Z[k] - conj Z[M-k]) / 2, k = 0..M, to plane k
+  double2* out = spec + (long long)blockIdx.y * d.n_complex;
+  for (int idx = threadIdx.x; idx < ((M + 1) << d.log2G); idx += blockDim.x) {
+    const int k = idx >> d.log2G, g = idx & (G - 1);
+    const double2 zk = sm[g * S + swz(k & (M - 1))];
+    const double2 zm = sm[g * S + swz((M - k) & (M - 1))];
+    const double2 e = make_double2(zk.x + zm.x, zk.y - zm.y);
+    const double2 wd = cmul(make_double2(zk.x - zm.x, zk.y + zm.y), tws[k]);
+    out[(long long)k * d.rows + r0 + g] = make_double2(0.5 * (e.x + wd.y), 0.5 * (e.y - wd.x));
+  }
+}
+
+// z / |z| of z = a * b (VolumePhaseCorrelator.cpp:70-75 divides by |z| + DBL_MIN, which only
+// matters for z = 0: zero stays zero here too). One reciprocal square root instead of a hypot and
+// two divisions: the result differs from the reference's rounding by a few ulp, well inside the
+// rounding differences of the transforms themselves.
+__device__ __forceinline__ double2 cross_power(double2 a, double2 b) {
+  const double re = fma(a.x, b.x, -a.y * b.y);
+  const double im = fma(a.x, b.y, a.y * b.x);
+  const double q = fma(re, re, im * im);
+  const double r = q > 0.0 ? rsqrt(q) : 0.0;
+  return make_double2(re * r, im * r);
+}
+
+// Planes p0 .. p0 + PP - 1 of the batch's plane array (frame-major, nx/2 + 1 planes per frame).
+// REF: out = conj(forward DFT over (z, y)); otherwise out = inverse(normalised forward * ref_conj).
+// Shared memory: PP * NZ lines of S = ny + 1 points, then the ny twiddles W_ny^m.
+template <int NZ, bool REF>
+__global__ void __launch_bounds__(kPlaneThreads, 1) plane_yz_kernel(const double2* in, double2* out,
+                                                                    const double2* __restrict__ ref_conj,
+                                                                    const double2* __restrict__ tw_y, PlaneDims d,
+                                                                    long long n_planes) {
+  extern __shared__ double2 sm[];
+  const int ny = d.ny, S = ny + 1;
+  const int plane = NZ * ny;
+  const long long p0 = (long long)blockIdx.x * d.PP;
+  const int pp = (int)min((long long)d.PP, n_planes - p0);
+  const int E = pp * plane;
+  double2* tws = sm + d.PP * NZ * S;
+  {
+    const double2* src = in + p0 * plane;
+    stage16<8>(
+        E + ny, [&](int i) { return reinterpret_cast<const uint4*>(i < E ? src + i : tw_y + (i - E)); },
+        [&](int i) {
+          return reinterpret_cast<uint4*>(i < E ? sm + (i >> d.log2ny) * S + swz(i & (ny - 1)) : tws + (i - E));
+        });
+  }
+  fft_rows<false, kPlaneEPT, 0, kPlaneThreads>(sm, pp * NZ, d.log2ny, tws);
+  const int M1 = (d.nx >> 1) + 1;
+  for (int c = threadIdx.x; c < pp * ny; c += blockDim.x) {
+    const int p = c >> d.log2ny, y = c & (ny - 1);
+    double2 a[NZ];
+    double2* col = sm + (p * NZ) * S + swz(y);
+    if (REF) {
+#pragma unroll
+      for (int z = 0; z < NZ; z++) a[z] = col[z * S];
+      dft<NZ, false>(a);
+#pragma unroll
+      for (int z = 0; z < NZ; z++) a[z].y = -a[z].y;
+    } else {
+      // the reference's spectrum in two halves: the first half's loads overlap the forward DFT
+      constexpr int kH = (NZ + 1) / 2;
+      const int k = (int)((p0 + p) % M1);
+      const double2* rc = ref_conj + (long long)k * plane + y;
+      double2 b[kH];
+#pragma unroll
+      for (int z = 0; z < kH; z++) b[z] = __ldg(rc + z * ny);
+#pragma unroll
+      for (int z = 0; z < NZ; z++) a[z] = col[z * S];
+      dft<NZ, false>(a);
+#pragma unroll
+      for (int z = 0; z < kH; z++) a[z] = cross_power(a[z], b[z]);
+#pragma unroll
+      for (int z = kH; z < NZ; z++) b[z - kH] = __ldg(rc + z * ny);
+#pragma unroll
+      for (int z = kH; z < NZ; z++) a[z] = cross_power(a[z], b[z - kH]);
+      dft<NZ, true>(a);
+    }
+#pragma unroll
+    for (int z = 0; z < NZ; z++) col[z * S] = a[z];
+  }
+  if (!REF) fft_rows<true, kPlaneEPT, 0, kPlaneThreads>(sm, pp * NZ, d.log2ny, tws);
+  __syncthreads();
+  double2* dst = out + p0 * plane;
+#pragma unroll
+  for (int u = 0; u < kPlaneEPT; u++) {
+    const int idx = threadIdx.x + u * kPlaneThreads;
+    if (idx < E) dst[idx] = sm[(idx >> d.log2ny) * S + swz(idx & (ny - 1))];
+  }
+}
+
+// (value, index), greater value then smaller index; NaN never wins (phase_argmax_blocks' rule).
+__device__ __forceinline__ void better(double& v, long long& i, double v2, long long i2) {
+  if (v2 > v || (v2 == v && i2 < i)) {
+    v = v2;
+    i = i2;
+  }
+}
+
+// Z[k] = (X[k] + conj X[M-k]) + i W_nx^-k (X[k] - conj X[M-k]): the nx/2-point inverse DFT of Z
+// holds the even samples of the real inverse in its real parts and the odd ones in its imaginary
+// parts.
+__device__ __forceinline__ double2 fold(double2 xa, double2 xb, double2 w) {
+  const double2 e = make_double2(xa.x + xb.x, xa.y - xb.y);
+  const double2 o = cmul_tw<true>(make_double2(xa.x - xb.x, xa.y + xb.y), w);
+  return make_double2(e.x - o.y, e.y + o.x);
+}
+
+// Shared memory as plane_rows_fwd_kernel's (bin M of line g at its unswizzled place M).
+__global__ void __launch_bounds__(kRowThreads) plane_rows_inv_argmax_kernel(const double2* __restrict__ spec,
+                                                                            const double2* __restrict__ tw_x,
+                                                                            PlaneDims d, double* __restrict__ bval,
+                                                                            long long* __restrict__ bidx,
+                                                                            double* __restrict__ surface) {
+  extern __shared__ double2 sm[];
+  const int M = d.nx >> 1, S = M + 1, G = 1 << d.log2G, H = M >> 1;
+  double2* tws = sm + G * S;
+  const int r0 = blockIdx.x << d.log2G;
+  const double2* in = spec + (long long)blockIdx.y * d.n_complex;
+  {
+    const int n_bins = (M + 1) << d.log2G;
+    stage16<8>(
+        n_bins + d.nx,
+        [&](int i) {
+          return reinterpret_cast<const uint4*>(
+              i < n_bins ? in + (long long)(i >> d.log2G) * d.rows + r0 + (i & (G - 1)) : tw_x + (i - n_bins));
+        },
+        [&](int i) {
+          const int k = i >> d.log2G;
+          return reinterpret_cast<uint4*>(i < n_bins ? sm + (i & (G - 1)) * S + (k < M ? swz(k) : M)
+                                                     : tws + (i - n_bins));
+        });
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < ((H + 1) << d.log2G); idx += blockDim.x) {
+    const int k = idx >> d.log2G, g = idx & (G - 1);
+    double2* line = sm + g * S;
+    const int ik = swz(k), im = k == 0 ? M : swz(M - k);
+    const double2 xk = line[ik], xm = line[im];
+    line[ik] = fold(xk, xm, tws[k]);
+    if (k > 0 && k < H) line[im] = fold(xm, xk, tws[M - k]);
+  }
+  fft_rows<true, kRowEPT, 1, kRowThreads>(sm, G, d.log2M, tws);
+  double v = -DBL_MAX;
+  long long best = 0x7fffffffffffffffLL;
+  for (int idx = threadIdx.x; idx < (G << d.log2M); idx += blockDim.x) {
+    const int g = idx >> d.log2M, m = idx & (M - 1);
+    const double2 z = sm[g * S + swz(m)];
+    const long long f = (long long)(r0 + g) * d.nx + 2 * m;
+    better(v, best, z.x, f);
+    better(v, best, z.y, f + 1);
+    if (surface) *reinterpret_cast<double2*>(surface + (long long)blockIdx.y * d.n_el + f) = z;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double v2 = __shfl_down_sync(0xffffffffu, v, o);
+    const long long i2 = __shfl_down_sync(0xffffffffu, best, o);
+    better(v, best, v2, i2);
+  }
+  __shared__ double wv[kRowThreads / 32];
+  __shared__ long long wi[kRowThreads / 32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+    wv[warp] = v;
+    wi[warp] = best;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) better(v, best, wv[w], wi[w]);
+    bval[(long long)blockIdx.y * gridDim.x + blockIdx.x] = v;
+    bidx[(long long)blockIdx.y * gridDim.x + blockIdx.x] = best;
+  }
+}
+
+// spec[kx][r] (planes) -> out[r][kx] (cuFFT's half-spectrum order), r = z * ny + y
+__global__ void plane_to_rows_kernel(const double2* __restrict__ in, double2* __restrict__ out, int rows, int M1,
+                                     long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const long long k = i / rows, r = i - k * rows;
+    out[r * M1 + k] = in[i];
+  }
+}
+
+template <typename K>
+cudaError_t allow_smem(K kernel, size_t bytes) {
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+int ilog2(long long v) {
+  int l = 0;
+  while ((1LL << l) < v) l++;
+  return l;
+}
+
+bool pow2(long long v) { return v > 0 && (v & (v - 1)) == 0; }
+
+}  // namespace
+
+bool plane_dims(int nz, int ny, int nx, PlaneDims* d) {
+  if (!pow2(nz) || !pow2(ny) || !pow2(nx) || nz > 16 || ny < 8 || ny > 2048 || nx < 16 || nx > 4096 ||
+      (long long)nz * ny > kPlaneThreads * kPlaneEPT)
+    return false;
+  d->nz = nz;
+  d->ny = ny;
+  d->nx = nx;
+  d->rows = nz * ny;
+  d->log2M = ilog2(nx / 2);
+  d->log2ny = ilog2(ny);
+  int G = 8;
+  while (G > 1 && ((long long)G * (nx / 2) > (long long)kRowThreads * kRowEPT || G > d->rows)) G >>= 1;
+  d->log2G = ilog2(G);
+  d->PP = std::max(1, (kPlaneThreads * kPlaneEPT) / (nz * ny));
+  d->n_complex = (long long)(nx / 2 + 1) * d->rows;
+  d->n_el = (long long)nx * d->rows;
+  return true;
+}
+
+int plane_blocks_per_frame(const PlaneDims& d) { return d.rows >> d.log2G; }
+
+cudaError_t launch_plane_rows_fwd(const PlaneDims& d, const void* const* vols, int in_kind, int batch,
+                                  const double* wy, const double* wx, const double2* tw_x, double2* spec,
+                                  cudaStream_t s) {
+  const size_t smem = rows_smem_bytes(d, in_kind == FA_U16 ? 2 : 4);
+  const dim3 grid(d.rows >> d.log2G, batch);
+  if (in_kind == FA_U16) {
+    cudaError_t e = allow_smem(plane_rows_fwd_kernel<true>, smem);
+    if (e != cudaSuccess) return e;
+    plane_rows_fwd_kernel<true><<<grid, kRowThreads, smem, s>>>(vols, wy, wx, tw_x, d, spec);
+  } else {
+    cudaError_t e = allow_smem(plane_rows_fwd_kernel<false>, smem);
+    if (e != cudaSuccess) return e;
+    plane_rows_fwd_kernel<false><<<grid, kRowThreads, smem, s>>>(vols, wy, wx, tw_x, d, spec);
+  }
+  return cudaGetLastError();
+}
+
+namespace {
+template <int NZ, bool REF>
+cudaError_t launch_yz(const PlaneDims& d, const double2* in, double2* out, const double2* ref_conj,
+                      const double2* tw_y, long long n_planes, cudaStream_t s) {
+  const size_t smem = ((size_t)d.PP * NZ * (d.ny + 1) + d.ny) * sizeof(double2);
+  cudaError_t e = allow_smem(plane_yz_kernel<NZ, REF>, smem);
+  if (e != cudaSuccess) return e;
+  const long long grid = (n_planes + d.PP - 1) / d.PP;
+  plane_yz_kernel<NZ, REF><<<(unsigned)grid, kPlaneThreads, smem, s>>>(in, out, ref_conj, tw_y, d, n_planes);
+  return cudaGetLastError();
+}
+
+template <bool REF>
+cudaError_t launch_yz_nz(const PlaneDims& d, const double2* in, double2* out, const double2* ref_conj,
+                         const double2* tw_y, long long n_planes, cudaStream_t s) {
+  switch (d.nz) {
+    case 1: return launch_yz<1, REF>(d, in, out, ref_conj, tw_y, n_planes, s);
+    case 2: return launch_yz<2, REF>(d, in, out, ref_conj, tw_y, n_planes, s);
+    case 4: return launch_yz<4, REF>(d, in, out, ref_conj, tw_y, n_planes, s);
+    case 8: return launch_yz<8, REF>(d, in, out, ref_conj, tw_y, n_planes, s);
+    case 16: return launch_yz<16, REF>(d, in, out, ref_conj, tw_y, n_planes, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+}  // namespace
+
+cudaError_t launch_plane_yz(const PlaneDims& d, const double2* in, double2* out, const double2* ref_conj,
+                            const double2* tw_y, int batch, bool reference, cudaStream_t s) {
+  const long long n_planes = (long long)batch * ((d.nx >> 1) + 1);
+  return reference ? launch_yz_nz<true>(d, in, out, nullptr, tw_y, n_planes, s)
+                   : launch_yz_nz<false>(d, in, out, ref_conj, tw_y, n_planes, s);
+}
+
+cudaError_t launch_plane_to_rows(const PlaneDims& d, const double2* in, double2* out, cudaStream_t s) {
+  const int blocks = (int)std::min<long long>((d.n_complex + 255) / 256, 148 * 8);
+  plane_to_rows_kernel<<<blocks, 256, 0, s>>>(in, out, d.rows, (d.nx >> 1) + 1, d.n_complex);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_plane_rows_inv_argmax(const PlaneDims& d, const double2* spec, int batch, const double2* tw_x,
+                                         double* bval, long long* bidx, double* surface, cudaStream_t s) {
+  const size_t smem = rows_smem_bytes(d, 0);
+  cudaError_t e = allow_smem(plane_rows_inv_argmax_kernel, smem);
+  if (e != cudaSuccess) return e;
+  plane_rows_inv_argmax_kernel<<<dim3(d.rows >> d.log2G, batch), kRowThreads, smem, s>>>(spec, tw_x, d, bval, bidx,
+                                                                                         surface);
+  return cudaGetLastError();
+}
+
+}  // namespace fa

@@ -114,12 +114,18 @@ struct fa_correlator {
   void* work = nullptr;
   size_t work_bytes = 0;
   std::vector<fa_rt::Alloc> work_allocs;
+  // fused kx-plane passes (fa_plane_corr.cu) when the dimensions allow them; cuFFT otherwise
+  bool planes = false;
+  fa::PlaneDims pd{};
+  double2* tw_x = nullptr;              // W_nx^m, m < nx
+  double2* tw_y = nullptr;              // W_ny^m, m < ny
   cudaStream_t stream = nullptr;
   double* wy = nullptr;                 // square-root Hann window along y
   double* wx = nullptr;                 // ... and along x (1 along z)
-  double* real = nullptr;               // cap * n_el
+  double* real = nullptr;               // cap * n_el (cuFFT path only)
   double2* spec = nullptr;              // cap * n_complex
-  double2* ref_conj = nullptr;          // n_complex
+  double2* ref_conj = nullptr;          // n_complex (planes [kx][z][y] when `planes`, else cuFFT's order)
+  double2* ref_conj_rows = nullptr;     // cuFFT's order, made when a plane-path correlator falls back
   float* vol = nullptr;                 // one host-uploaded volume
   const void** d_ptrs = nullptr;        // device array of input pointers
   const void** h_ptrs = nullptr;        // pinned staging of the same
@@ -128,7 +134,7 @@ struct fa_correlator {
   long long* bidx = nullptr;
   long long* d_idx = nullptr;           // one peak index per frame (ptr_cap)
   long long* h_idx = nullptr;
-  int n_blocks = 0;                     // argmax blocks per frame
+  int n_blocks = 0;                     // argmax blocks per frame (cuFFT path)
   std::mutex mu;
   std::vector<fa_rt::Alloc> allocs;
   std::vector<fa_rt::Alloc> ptr_allocs;
@@ -206,8 +212,11 @@ fa_status frame_alloc(fa_reference* R, int kind, fa_frame** out);
 int slot_kind_for(const fa_aligner* A, fa_dtype dtype);
 // The correlator's D2Z / Z2D plans for a batch size (made and cached on first use).
 fa_status correlator_plans(fa_correlator* C, int batch, cufftHandle* fwd, cufftHandle* inv);
-// Window, D2Z, normalisation, Z2D and argmax for n device volumes; peak indices to C->d_idx[0..n).
-fa_status correlator_enqueue(fa_correlator* C, const void* const* vols, int in_kind, int n);
+// Window, forward DFT, normalisation, inverse DFT and argmax for n device volumes; peak indices to
+// C->d_idx[0..n). surface (n * n_el doubles, optional) receives the correlation surfaces; planes
+// selects the fused kx-plane passes (when C->planes) or cuFFT.
+fa_status correlator_enqueue(fa_correlator* C, const void* const* vols, int in_kind, int n,
+                             double* surface = nullptr, bool planes = true);
 // Peak index -> signed integer shift (x, y, z).
 void unravel_shift(const fa_correlator* C, long long idx, double* shift);
 

@@ -179,6 +179,7 @@ SIGNATURES = {
     "fa_aligner_last_device_ms": [_vp, C.POINTER(C.c_double)],
     "fa_profile_eval": [_vp, C.c_int, _f64p, C.c_int, C.POINTER(C.c_double)],
     "fa_test_tr_subproblem": [_vp, C.c_int, C.c_int, _f64p, _f64p, C.c_double, _f64p, C.POINTER(C.c_int)],
+    "fa_test_correlation_surface": [_vp, _f32p, C.c_int, _f64p],
 }
 
 
@@ -409,6 +410,13 @@ class Correlator:
         s = np.empty(3, np.float64)
         check(lib().fa_correlator_shift_device(self._h, ptr, s))
         return s
+
+    def surface(self, volume, planes=True):
+        """Correlation surface of one volume (test hook): fused kx-plane passes or cuFFT."""
+        out = np.empty(self.dims, np.float64)
+        vol = np.ascontiguousarray(volume, dtype=np.float32).reshape(self.dims)
+        check(lib().fa_test_correlation_surface(self._h, vol, 1 if planes else 0, out))
+        return out
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:

@@ -373,6 +373,13 @@ fa_status fa_profile_eval(fa_frame* const* frames, int n, const double* D, int l
 fa_status fa_test_tr_subproblem(fa_context* ctx, int nD, int n_dim, const double* H, const double* g, double radius,
                                 double* p, int* on_boundary);
 
+/* Test hook (no reference counterpart): the phase-correlation surface of one FP32 volume (host
+   memory, nz*ny*nx) against the correlator's reference -- the unnormalised inverse DFT of the
+   normalised cross-power spectrum, nz*ny*nx doubles into host memory -- computed by the fused
+   kx-plane passes (use_planes = 1; FA_ERR_UNSUPPORTED when the dimensions are outside them) or by
+   cuFFT (use_planes = 0). Lets tests compare both with a CPU DFT. */
+fa_status fa_test_correlation_surface(fa_correlator* c, const float* volume, int use_planes, double* surface);
+
 #ifdef __cplusplus
 }
 #endif
