@@ -1347,20 +1347,8 @@ fa_status correlator_create_impl(fa_context* ctx, const void* reference, bool re
   if (cudaMemcpyAsync(C->d_ptrs, C->h_ptrs, sizeof(void*), cudaMemcpyHostToDevice, C->stream) != cudaSuccess)
     return cleanup(fail(FA_ERR_CUDA, "pointer upload"));
   if (C->planes) {
-    // W_L^m = exp(-2 pi i m / L), rounded from long double; exact at the quarter turns
-    auto twiddles = [](int L) {
-      std::vector<double2> t(L);
-      const long double two_pi = 6.283185307179586476925286766559L;
-      for (int m = 0; m < L; m++) {
-        const long double a = two_pi * m / L;
-        t[m] = make_double2((double)cosl(a), (double)-sinl(a));
-        if (4 * m == L) t[m] = make_double2(0.0, -1.0);
-        if (2 * m == L) t[m] = make_double2(-1.0, 0.0);
-        if (4 * m == 3 * L) t[m] = make_double2(0.0, 1.0);
-      }
-      return t;
-    };
-    const std::vector<double2> tx = twiddles(nx), ty = twiddles(ny);
+    std::vector<double2> tx, ty;
+    fa::plane_twiddles(C->pd, &tx, &ty);
     if ((st = dalloc_t(ctx, tx.size(), &C->tw_x, C->allocs)) != FA_OK) return cleanup(st);
     if ((st = dalloc_t(ctx, ty.size(), &C->tw_y, C->allocs)) != FA_OK) return cleanup(st);
     if (cudaMemcpy(C->tw_x, tx.data(), tx.size() * sizeof(double2), cudaMemcpyHostToDevice) != cudaSuccess ||

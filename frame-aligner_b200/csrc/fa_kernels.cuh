@@ -1,6 +1,8 @@
 // fa_kernels.cuh -- kernel launch declarations (implemented in fa_kernels.cu, fa_solve.cu).
 #pragma once
 
+#include <vector>
+
 #include "fa_internal.h"
 
 namespace fa {
@@ -118,9 +120,13 @@ struct PlaneDims {
   int nz, ny, nx, rows;      // rows = nz * ny
   int log2M, log2ny, log2G;  // M = nx / 2; G rows per row CTA
   int PP;                    // planes per plane CTA
+  int n_twx, tw_x_post;      // x twiddles: stage table of the nx/2-point DFT, then W_nx^k (k <= nx/2)
+  int n_twy;                 // y twiddles: stage table of the ny-point DFT
   long long n_complex, n_el;
 };
 bool plane_dims(int nz, int ny, int nx, PlaneDims* d);
+// The twiddle tables the passes read (tw_x: d.n_twx entries, tw_y: d.n_twy), computed in long double.
+void plane_twiddles(const PlaneDims& d, std::vector<double2>* tw_x, std::vector<double2>* tw_y);
 // CTAs (argmax partials) per frame of the last pass.
 int plane_blocks_per_frame(const PlaneDims& d);
 // Window + real DFT along x of each frame (dense FP32 or uint16, in_kind an fa_dtype) into spec

@@ -24,6 +24,8 @@
 #include <float.h>
 
 #include <algorithm>
+#include <cmath>
+#include <vector>
 
 #include "fa_kernels.cuh"
 
@@ -151,16 +153,16 @@ __device__ __forceinline__ void dft(double2* a) {
 // (line stride L + 1): every thread reads its butterflies into registers, the block synchronises,
 // then writes them back. Butterfly j of a line: a[r] = x[j + r L/R], twiddled by W_(Ns R)^(r k)
 // with k = j mod Ns, R-point DFT, stored at ((j - k) R + k) + r Ns. NB bounds the butterflies per
-// thread; tw (W_L'^m with L' = L << TWS) is in shared memory, so it is read with plain loads. The
-// sizes are template constants, so the swizzled addresses reduce to a few integer operations.
-template <int R, int NB, bool INV, int LOG2L, int LOG2NS, int TWS, int T>
+// thread. The stage's twiddles sit at tw[OFF + (r - 1) Ns + k] in shared memory (contiguous in k, so
+// the lanes of a warp read distinct banks; plain loads). The sizes are template constants, so the
+// swizzled addresses reduce to a few integer operations.
+template <int R, int NB, bool INV, int LOG2L, int LOG2NS, int OFF, int T>
 __device__ __forceinline__ void stockham_stage(double2* sm, int lines, const double2* tw) {
   constexpr int log2R = R == 8 ? 3 : (R == 4 ? 2 : 1);
   constexpr int log2q = LOG2L - log2R;
   constexpr int q = 1 << log2q;
   constexpr int Ns = 1 << LOG2NS;
   constexpr int S = (1 << LOG2L) + 1;
-  constexpr int twsh = LOG2L - LOG2NS - log2R + TWS;
   const int nb = lines << log2q;
   double2 a[NB][R];
 #pragma unroll
@@ -174,7 +176,7 @@ __device__ __forceinline__ void stockham_stage(double2* sm, int lines, const dou
       if (Ns > 1) {
         const int k = j & (Ns - 1);
 #pragma unroll
-        for (int r = 1; r < R; r++) a[u][r] = cmul_tw<INV>(a[u][r], tw[(r * k) << twsh]);
+        for (int r = 1; r < R; r++) a[u][r] = cmul_tw<INV>(a[u][r], tw[OFF + (r - 1) * Ns + k]);
       }
       dft<R, INV>(a[u]);
     }
@@ -195,34 +197,36 @@ __device__ __forceinline__ void stockham_stage(double2* sm, int lines, const dou
   __syncthreads();
 }
 
-// Radix-8 stages, then one radix-4 or radix-2 stage.
-template <bool INV, int EPT, int LOG2L, int TWS, int T, int LOG2NS = 0>
+// Radix-8 stages, then one radix-4 or radix-2 stage; OFF advances by the (R - 1) Ns twiddles of
+// every stage after the first (stage_table on the host lays them out in the same order).
+template <bool INV, int EPT, int LOG2L, int T, int LOG2NS = 0, int OFF = 0>
 __device__ __forceinline__ void fft_rows_t(double2* sm, int lines, const double2* tw) {
   if constexpr (LOG2L - LOG2NS >= 3) {
-    stockham_stage<8, EPT / 8, INV, LOG2L, LOG2NS, TWS, T>(sm, lines, tw);
-    fft_rows_t<INV, EPT, LOG2L, TWS, T, LOG2NS + 3>(sm, lines, tw);
+    stockham_stage<8, EPT / 8, INV, LOG2L, LOG2NS, OFF, T>(sm, lines, tw);
+    fft_rows_t<INV, EPT, LOG2L, T, LOG2NS + 3, OFF + (LOG2NS > 0 ? 7 << LOG2NS : 0)>(sm, lines, tw);
   } else if constexpr (LOG2L - LOG2NS == 2) {
-    stockham_stage<4, EPT / 4, INV, LOG2L, LOG2NS, TWS, T>(sm, lines, tw);
+    stockham_stage<4, EPT / 4, INV, LOG2L, LOG2NS, OFF, T>(sm, lines, tw);
   } else if constexpr (LOG2L - LOG2NS == 1) {
-    stockham_stage<2, EPT / 2, INV, LOG2L, LOG2NS, TWS, T>(sm, lines, tw);
+    stockham_stage<2, EPT / 2, INV, LOG2L, LOG2NS, OFF, T>(sm, lines, tw);
   }
 }
 
 // DFT of every line of 2^log2L points (3 <= log2L <= 11, line stride 2^log2L + 1) by a block of T
-// threads; starts with a barrier and ends with one. lines * 2^log2L <= EPT * T.
-template <bool INV, int EPT, int TWS, int T>
+// threads, with the stage twiddles of stage_table(2^log2L) at tw; starts with a barrier and ends
+// with one. lines * 2^log2L <= EPT * T.
+template <bool INV, int EPT, int T>
 __device__ __forceinline__ void fft_rows(double2* sm, int lines, int log2L, const double2* tw) {
   __syncthreads();
   switch (log2L) {
-    case 3: fft_rows_t<INV, EPT, 3, TWS, T>(sm, lines, tw); break;
-    case 4: fft_rows_t<INV, EPT, 4, TWS, T>(sm, lines, tw); break;
-    case 5: fft_rows_t<INV, EPT, 5, TWS, T>(sm, lines, tw); break;
-    case 6: fft_rows_t<INV, EPT, 6, TWS, T>(sm, lines, tw); break;
-    case 7: fft_rows_t<INV, EPT, 7, TWS, T>(sm, lines, tw); break;
-    case 8: fft_rows_t<INV, EPT, 8, TWS, T>(sm, lines, tw); break;
-    case 9: fft_rows_t<INV, EPT, 9, TWS, T>(sm, lines, tw); break;
-    case 10: fft_rows_t<INV, EPT, 10, TWS, T>(sm, lines, tw); break;
-    case 11: fft_rows_t<INV, EPT, 11, TWS, T>(sm, lines, tw); break;
+    case 3: fft_rows_t<INV, EPT, 3, T>(sm, lines, tw); break;
+    case 4: fft_rows_t<INV, EPT, 4, T>(sm, lines, tw); break;
+    case 5: fft_rows_t<INV, EPT, 5, T>(sm, lines, tw); break;
+    case 6: fft_rows_t<INV, EPT, 6, T>(sm, lines, tw); break;
+    case 7: fft_rows_t<INV, EPT, 7, T>(sm, lines, tw); break;
+    case 8: fft_rows_t<INV, EPT, 8, T>(sm, lines, tw); break;
+    case 9: fft_rows_t<INV, EPT, 9, T>(sm, lines, tw); break;
+    case 10: fft_rows_t<INV, EPT, 10, T>(sm, lines, tw); break;
+    case 11: fft_rows_t<INV, EPT, 11, T>(sm, lines, tw); break;
     default: break;
   }
 }
@@ -279,7 +283,7 @@ __global__ void __launch_bounds__(kRowThreads) plane_rows_fwd_kernel(const void*
     // raw rows, then the twiddles, then the window factors along x (all 16-byte chunks)
     const uint4* src = reinterpret_cast<const uint4*>(static_cast<const unsigned char*>(vols[blockIdx.y]) +
                                                       (size_t)r0 * d.nx * kEsz);
-    const int n_raw = (G * d.nx * kEsz) >> 4, n_tw = d.nx, n_wx = d.nx >> 1;
+    const int n_raw = (G * d.nx * kEsz) >> 4, n_tw = d.n_twx, n_wx = d.nx >> 1;
     const uint4* tsrc = reinterpret_cast<const uint4*>(tw_x);
     const uint4* wsrc = reinterpret_cast<const uint4*>(wx);
     uint4* rdst = reinterpret_cast<uint4*>(raw);
@@ -307,10 +311,11 @@ __global__ void __launch_bounds__(kRowThreads) plane_rows_fwd_kernel(const void*
     }
     // (double)v * ((1 * wy[y]) * wx[x]), each product rounded (VolumePhaseCorrelator.cpp:62-63)
     const double wrow = __dmul_rn(1.0, wys[g]);
-    sm[g * S + swz(m)] = make_double2(__dmul_rn((double)v0, __dmul_rn(wrow, wxs[2 * m])),
-                                      __dmul_rn((double)v1, __dmul_rn(wrow, wxs[2 * m + 1])));
+    const double2 w = reinterpret_cast<const double2*>(wxs)[m];
+    sm[g * S + swz(m)] = make_double2(__dmul_rn((double)v0, __dmul_rn(wrow, w.x)),
+                                      __dmul_rn((double)v1, __dmul_rn(wrow, w.y)));
   }
-  fft_rows<false, kRowEPT, 1, kRowThreads>(sm, G, d.log2M, tws);
+  fft_rows<false, kRowEPT, kRowThreads>(sm, G, d.log2M, tws);
   // X[k] = (Z[k] + conj Z[M-k]) / 2 - i W_nx^k (Z[k] - conj Z[M-k]) / 2, k = 0..M, to plane k
   double2* out = spec + (long long)blockIdx.y * d.n_complex;
   for (int idx = threadIdx.x; idx < ((M + 1) << d.log2G); idx += blockDim.x) {
@@ -318,7 +323,7 @@ __global__ void __launch_bounds__(kRowThreads) plane_rows_fwd_kernel(const void*
     const double2 zk = sm[g * S + swz(k & (M - 1))];
     const double2 zm = sm[g * S + swz((M - k) & (M - 1))];
     const double2 e = make_double2(zk.x + zm.x, zk.y - zm.y);
-    const double2 wd = cmul(make_double2(zk.x - zm.x, zk.y + zm.y), tws[k]);
+    const double2 wd = cmul(make_double2(zk.x - zm.x, zk.y + zm.y), tws[d.tw_x_post + k]);
     out[(long long)k * d.rows + r0 + g] = make_double2(0.5 * (e.x + wd.y), 0.5 * (e.y - wd.x));
   }
 }
@@ -353,12 +358,12 @@ __global__ void __launch_bounds__(kPlaneThreads, 1) plane_yz_kernel(const double
   {
     const double2* src = in + p0 * plane;
     stage16<8>(
-        E + ny, [&](int i) { return reinterpret_cast<const uint4*>(i < E ? src + i : tw_y + (i - E)); },
+        E + d.n_twy, [&](int i) { return reinterpret_cast<const uint4*>(i < E ? src + i : tw_y + (i - E)); },
         [&](int i) {
           return reinterpret_cast<uint4*>(i < E ? sm + (i >> d.log2ny) * S + swz(i & (ny - 1)) : tws + (i - E));
         });
   }
-  fft_rows<false, kPlaneEPT, 0, kPlaneThreads>(sm, pp * NZ, d.log2ny, tws);
+  fft_rows<false, kPlaneEPT, kPlaneThreads>(sm, pp * NZ, d.log2ny, tws);
   const int M1 = (d.nx >> 1) + 1;
   for (int c = threadIdx.x; c < pp * ny; c += blockDim.x) {
     const int p = c >> d.log2ny, y = c & (ny - 1);
@@ -392,7 +397,7 @@ __global__ void __launch_bounds__(kPlaneThreads, 1) plane_yz_kernel(const double
 #pragma unroll
     for (int z = 0; z < NZ; z++) col[z * S] = a[z];
   }
-  if (!REF) fft_rows<true, kPlaneEPT, 0, kPlaneThreads>(sm, pp * NZ, d.log2ny, tws);
+  if (!REF) fft_rows<true, kPlaneEPT, kPlaneThreads>(sm, pp * NZ, d.log2ny, tws);
   __syncthreads();
   double2* dst = out + p0 * plane;
 #pragma unroll
@@ -433,7 +438,7 @@ __global__ void __launch_bounds__(kRowThreads) plane_rows_inv_argmax_kernel(cons
   {
     const int n_bins = (M + 1) << d.log2G;
     stage16<8>(
-        n_bins + d.nx,
+        n_bins + d.n_twx,
         [&](int i) {
           return reinterpret_cast<const uint4*>(
               i < n_bins ? in + (long long)(i >> d.log2G) * d.rows + r0 + (i & (G - 1)) : tw_x + (i - n_bins));
@@ -450,10 +455,10 @@ __global__ void __launch_bounds__(kRowThreads) plane_rows_inv_argmax_kernel(cons
     double2* line = sm + g * S;
     const int ik = swz(k), im = k == 0 ? M : swz(M - k);
     const double2 xk = line[ik], xm = line[im];
-    line[ik] = fold(xk, xm, tws[k]);
-    if (k > 0 && k < H) line[im] = fold(xm, xk, tws[M - k]);
+    line[ik] = fold(xk, xm, tws[d.tw_x_post + k]);
+    if (k > 0 && k < H) line[im] = fold(xm, xk, tws[d.tw_x_post + M - k]);
   }
-  fft_rows<true, kRowEPT, 1, kRowThreads>(sm, G, d.log2M, tws);
+  fft_rows<true, kRowEPT, kRowThreads>(sm, G, d.log2M, tws);
   double v = -DBL_MAX;
   long long best = 0x7fffffffffffffffLL;
   for (int idx = threadIdx.x; idx < (G << d.log2M); idx += blockDim.x) {
@@ -510,6 +515,49 @@ bool pow2(long long v) { return v > 0 && (v & (v - 1)) == 0; }
 
 }  // namespace
 
+namespace {
+
+// exp(-2 pi i m / n), rounded from long double; exact at the quarter turns.
+double2 unit_root(long long m, long long n) {
+  m %= n;
+  if (m == 0) return make_double2(1.0, 0.0);
+  if (4 * m == n) return make_double2(0.0, -1.0);
+  if (2 * m == n) return make_double2(-1.0, 0.0);
+  if (4 * m == 3 * n) return make_double2(0.0, 1.0);
+  const long double a = 6.283185307179586476925286766559L * (long double)m / (long double)n;
+  return make_double2((double)cosl(a), (double)-sinl(a));
+}
+
+// Stage twiddles of an L-point transform in fft_rows_t's order: for every stage after the first
+// (Ns > 1, radix R), W_(Ns R)^(r k) at (r - 1) Ns + k, r = 1..R-1, k = 0..Ns-1.
+void stage_table(int L, std::vector<double2>* t) {
+  const int log2L = ilog2(L);
+  for (int log2Ns = 0; log2Ns < log2L;) {
+    const int log2R = std::min(3, log2L - log2Ns);
+    const int R = 1 << log2R, Ns = 1 << log2Ns;
+    if (Ns > 1)
+      for (int r = 1; r < R; r++)
+        for (int k = 0; k < Ns; k++) t->push_back(unit_root((long long)r * k, (long long)Ns * R));
+    log2Ns += log2R;
+  }
+}
+
+int stage_count(int L) {
+  std::vector<double2> t;
+  stage_table(L, &t);
+  return (int)t.size();
+}
+
+}  // namespace
+
+void plane_twiddles(const PlaneDims& d, std::vector<double2>* tw_x, std::vector<double2>* tw_y) {
+  tw_x->clear();
+  tw_y->clear();
+  stage_table(d.nx / 2, tw_x);
+  for (int k = 0; k <= d.nx / 2; k++) tw_x->push_back(unit_root(k, d.nx));  // W_nx^k, k = 0..nx/2
+  stage_table(d.ny, tw_y);
+}
+
 bool plane_dims(int nz, int ny, int nx, PlaneDims* d) {
   if (!pow2(nz) || !pow2(ny) || !pow2(nx) || nz > 16 || ny < 8 || ny > 2048 || nx < 16 || nx > 4096 ||
       (long long)nz * ny > kPlaneThreads * kPlaneEPT)
@@ -526,6 +574,9 @@ bool plane_dims(int nz, int ny, int nx, PlaneDims* d) {
   d->PP = std::max(1, (kPlaneThreads * kPlaneEPT) / (nz * ny));
   d->n_complex = (long long)(nx / 2 + 1) * d->rows;
   d->n_el = (long long)nx * d->rows;
+  d->tw_x_post = stage_count(nx / 2);
+  d->n_twx = d->tw_x_post + nx / 2 + 1;  // <= nx: the twiddle slots of the row passes
+  d->n_twy = stage_count(ny);            // <  ny
   return true;
 }
 
