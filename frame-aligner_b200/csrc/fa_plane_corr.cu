@@ -149,20 +149,20 @@ __device__ __forceinline__ void dft(double2* a) {
   else if constexpr (R == 16) dft16<INV>(a);
 }
 
-// One in-place Stockham radix-R stage over `lines` lines of L = 2^LOG2L points in shared memory
-// (line stride L + 1): every thread reads its butterflies into registers, the block synchronises,
-// then writes them back. Butterfly j of a line: a[r] = x[j + r L/R], twiddled by W_(Ns R)^(r k)
-// with k = j mod Ns, R-point DFT, stored at ((j - k) R + k) + r Ns. NB bounds the butterflies per
-// thread. The stage's twiddles sit at tw[OFF + (r - 1) Ns + k] in shared memory (contiguous in k, so
-// the lanes of a warp read distinct banks; plain loads). The sizes are template constants, so the
-// swizzled addresses reduce to a few integer operations.
-template <int R, int NB, bool INV, int LOG2L, int LOG2NS, int OFF, int T>
-__device__ __forceinline__ void stockham_stage(double2* sm, int lines, const double2* tw) {
+// One Stockham radix-R stage over `lines` lines of L = 2^LOG2L points. Butterfly j of line l reads
+// x[j + r L/R] (load(l, i)), twiddles them by W_(Ns R)^(r k) with k = j mod Ns, takes the R-point
+// DFT and writes y[((j - k) R + k) + r Ns] (store(l, i, v)). Every thread first loads all of its
+// butterflies (NB at most), so global loads are in flight together. In place in shared memory the
+// block synchronises between the reads and the writes (SYNC_MID) and after the writes (SYNC_END).
+// The stage's twiddles sit at tw[OFF + (r - 1) Ns + k] in shared memory (contiguous in k, so the
+// lanes of a warp read distinct banks). The sizes are template constants.
+template <int R, int NB, bool INV, int LOG2L, int LOG2NS, int OFF, int T, bool SYNC_MID, bool SYNC_END, class Load,
+          class Store>
+__device__ __forceinline__ void stockham_stage(int lines, const double2* tw, Load load, Store store) {
   constexpr int log2R = R == 8 ? 3 : (R == 4 ? 2 : 1);
   constexpr int log2q = LOG2L - log2R;
   constexpr int q = 1 << log2q;
   constexpr int Ns = 1 << LOG2NS;
-  constexpr int S = (1 << LOG2L) + 1;
   const int nb = lines << log2q;
   double2 a[NB][R];
 #pragma unroll
@@ -170,18 +170,23 @@ __device__ __forceinline__ void stockham_stage(double2* sm, int lines, const dou
     const int b = threadIdx.x + u * T;
     if (b < nb) {
       const int l = b >> log2q, j = b & (q - 1);
-      const double2* line = sm + l * S;
 #pragma unroll
-      for (int r = 0; r < R; r++) a[u][r] = line[swz(j + (r << log2q))];
+      for (int r = 0; r < R; r++) a[u][r] = load(l, j + (r << log2q));
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < NB; u++) {
+    const int b = threadIdx.x + u * T;
+    if (b < nb) {
       if (Ns > 1) {
-        const int k = j & (Ns - 1);
+        const int k = b & (Ns - 1);  // j mod Ns (Ns <= q)
 #pragma unroll
         for (int r = 1; r < R; r++) a[u][r] = cmul_tw<INV>(a[u][r], tw[OFF + (r - 1) * Ns + k]);
       }
       dft<R, INV>(a[u]);
     }
   }
-  __syncthreads();
+  if (SYNC_MID) __syncthreads();
 #pragma unroll
   for (int u = 0; u < NB; u++) {
     const int b = threadIdx.x + u * T;
@@ -189,47 +194,70 @@ __device__ __forceinline__ void stockham_stage(double2* sm, int lines, const dou
       const int l = b >> log2q, j = b & (q - 1);
       const int k = j & (Ns - 1);
       const int o = ((j - k) << log2R) + k;
-      double2* line = sm + l * S;
 #pragma unroll
-      for (int r = 0; r < R; r++) line[swz(o + (r << LOG2NS))] = a[u][r];
+      for (int r = 0; r < R; r++) store(l, o + (r << LOG2NS), a[u][r]);
     }
   }
-  __syncthreads();
+  if (SYNC_END) __syncthreads();
 }
 
-// Radix-8 stages, then one radix-4 or radix-2 stage; OFF advances by the (R - 1) Ns twiddles of
-// every stage after the first (stage_table on the host lays them out in the same order).
-template <bool INV, int EPT, int LOG2L, int T, int LOG2NS = 0, int OFF = 0>
-__device__ __forceinline__ void fft_rows_t(double2* sm, int lines, const double2* tw) {
-  if constexpr (LOG2L - LOG2NS >= 3) {
-    stockham_stage<8, EPT / 8, INV, LOG2L, LOG2NS, OFF, T>(sm, lines, tw);
-    fft_rows_t<INV, EPT, LOG2L, T, LOG2NS + 3, OFF + (LOG2NS > 0 ? 7 << LOG2NS : 0)>(sm, lines, tw);
-  } else if constexpr (LOG2L - LOG2NS == 2) {
-    stockham_stage<4, EPT / 4, INV, LOG2L, LOG2NS, OFF, T>(sm, lines, tw);
-  } else if constexpr (LOG2L - LOG2NS == 1) {
-    stockham_stage<2, EPT / 2, INV, LOG2L, LOG2NS, OFF, T>(sm, lines, tw);
-  }
+// Radix-8 stages, then one radix-4 or radix-2 stage, over lines in shared memory (line stride
+// L + 1, element i at i ^ ((i >> 3) & 7)); OFF advances by the (R - 1) Ns twiddles of every stage
+// after the first (stage_table on the host lays them out in the same order). The first stage reads
+// through `first` unless FIRST_SMEM, the last writes through `last` unless LAST_SMEM; a stage that
+// writes shared memory ends with a barrier.
+template <bool INV, int EPT, int LOG2L, int T, bool FIRST_SMEM, bool LAST_SMEM, int LOG2NS = 0, int OFF = 0,
+          class First, class Last>
+__device__ __forceinline__ void fft_rows_t(double2* sm, int lines, const double2* tw, First first, Last last) {
+  constexpr int S = (1 << LOG2L) + 1;
+  constexpr int rem = LOG2L - LOG2NS;
+  constexpr int log2R = rem >= 3 ? 3 : rem;
+  constexpr int R = 1 << log2R;
+  constexpr bool is_first = LOG2NS == 0, is_last = LOG2NS + log2R == LOG2L;
+  constexpr bool in_smem = !is_first || FIRST_SMEM, out_smem = !is_last || LAST_SMEM;
+  auto load = [&](int l, int i) -> double2 {
+    if constexpr (in_smem) return sm[l * S + swz(i)];
+    else return first(l, i);
+  };
+  auto store = [&](int l, int i, double2 v) {
+    if constexpr (out_smem) sm[l * S + swz(i)] = v;
+    else last(l, i, v);
+  };
+  stockham_stage<R, EPT / R, INV, LOG2L, LOG2NS, OFF, T, in_smem && out_smem, out_smem>(lines, tw, load, store);
+  if constexpr (!is_last)
+    fft_rows_t<INV, EPT, LOG2L, T, FIRST_SMEM, LAST_SMEM, LOG2NS + log2R, OFF + (LOG2NS > 0 ? (R - 1) << LOG2NS : 0)>(
+        sm, lines, tw, first, last);
 }
 
-// DFT of every line of 2^log2L points (3 <= log2L <= 11, line stride 2^log2L + 1) by a block of T
-// threads, with the stage twiddles of stage_table(2^log2L) at tw; starts with a barrier and ends
-// with one. lines * 2^log2L <= EPT * T.
-template <bool INV, int EPT, int T>
-__device__ __forceinline__ void fft_rows(double2* sm, int lines, int log2L, const double2* tw) {
-  __syncthreads();
+// DFT of every line of 2^log2L points (3 <= log2L <= 11) by a block of T threads, with the stage
+// twiddles of stage_table(2^log2L) at tw. lines * 2^log2L <= EPT * T. The caller synchronises
+// before a first stage that reads shared memory.
+template <bool INV, int EPT, int T, bool FIRST_SMEM, bool LAST_SMEM, class First, class Last>
+__device__ __forceinline__ void fft_rows(double2* sm, int lines, int log2L, const double2* tw, First first,
+                                         Last last) {
   switch (log2L) {
-    case 3: fft_rows_t<INV, EPT, 3, T>(sm, lines, tw); break;
-    case 4: fft_rows_t<INV, EPT, 4, T>(sm, lines, tw); break;
-    case 5: fft_rows_t<INV, EPT, 5, T>(sm, lines, tw); break;
-    case 6: fft_rows_t<INV, EPT, 6, T>(sm, lines, tw); break;
-    case 7: fft_rows_t<INV, EPT, 7, T>(sm, lines, tw); break;
-    case 8: fft_rows_t<INV, EPT, 8, T>(sm, lines, tw); break;
-    case 9: fft_rows_t<INV, EPT, 9, T>(sm, lines, tw); break;
-    case 10: fft_rows_t<INV, EPT, 10, T>(sm, lines, tw); break;
-    case 11: fft_rows_t<INV, EPT, 11, T>(sm, lines, tw); break;
+    case 3: fft_rows_t<INV, EPT, 3, T, FIRST_SMEM, LAST_SMEM>(sm, lines, tw, first, last); break;
+    case 4: fft_rows_t<INV, EPT, 4, T, FIRST_SMEM, LAST_SMEM>(sm, lines, tw, first, last); break;
+    case 5: fft_rows_t<INV, EPT, 5, T, FIRST_SMEM, LAST_SMEM>(sm, lines, tw, first, last); break;
+    case 6: fft_rows_t<INV, EPT, 6, T, FIRST_SMEM, LAST_SMEM>(sm, lines, tw, first, last); break;
+    case 7: fft_rows_t<INV, EPT, 7, T, FIRST_SMEM, LAST_SMEM>(sm, lines, tw, first, last); break;
+    case 8: fft_rows_t<INV, EPT, 8, T, FIRST_SMEM, LAST_SMEM>(sm, lines, tw, first, last); break;
+    case 9: fft_rows_t<INV, EPT, 9, T, FIRST_SMEM, LAST_SMEM>(sm, lines, tw, first, last); break;
+    case 10: fft_rows_t<INV, EPT, 10, T, FIRST_SMEM, LAST_SMEM>(sm, lines, tw, first, last); break;
+    case 11: fft_rows_t<INV, EPT, 11, T, FIRST_SMEM, LAST_SMEM>(sm, lines, tw, first, last); break;
     default: break;
   }
 }
+
+}  // namespace
+
+// Neither: the first stage reads shared memory / the last writes it.
+struct NoIo {
+  __device__ double2 operator()(int, int) const { return make_double2(0.0, 0.0); }
+  __device__ void operator()(int, int, double2) const {}
+};
+
+namespace {
 
 constexpr int kRowThreads = 256;
 constexpr int kRowEPT = 8;      // G * nx/2 <= 2048 points per row CTA
@@ -256,13 +284,10 @@ __device__ __forceinline__ void stage16(int n, SrcOf src_of, DstOf dst_of) {
   }
 }
 
-// Row-pass shared memory: G lines of S = nx/2 + 1 points and the nx twiddles W_nx^m (double2), then
-// (forward pass) the nx window factors along x, G along y (8 slots) and the G raw rows.
-__host__ __device__ inline size_t rows_smem_bytes(const PlaneDims& d, int raw_bytes_per_el) {
+// Row-pass shared memory: G lines of S = nx/2 + 1 points, then the nx twiddle slots (double2).
+__host__ __device__ inline size_t rows_smem_bytes(const PlaneDims& d) {
   const size_t G = (size_t)1 << d.log2G;
-  size_t b = (G * ((d.nx >> 1) + 1) + d.nx) * 16;
-  if (raw_bytes_per_el) b += (size_t)d.nx * 8 + 64 + G * d.nx * raw_bytes_per_el;
-  return b;
+  return (G * ((d.nx >> 1) + 1) + d.nx) * 16;
 }
 
 template <bool U16>
@@ -272,50 +297,34 @@ __global__ void __launch_bounds__(kRowThreads) plane_rows_fwd_kernel(const void*
                                                                      const double2* __restrict__ tw_x, PlaneDims d,
                                                                      double2* __restrict__ spec) {
   extern __shared__ double2 sm[];
-  constexpr int kEsz = U16 ? 2 : 4;
   const int M = d.nx >> 1, S = M + 1, G = 1 << d.log2G;
   double2* tws = sm + G * S;
-  double* wxs = reinterpret_cast<double*>(tws + d.nx);
-  double* wys = wxs + d.nx;
-  unsigned char* raw = reinterpret_cast<unsigned char*>(wys + 8);
   const int r0 = blockIdx.x << d.log2G;
-  {
-    // raw rows, then the twiddles, then the window factors along x (all 16-byte chunks)
-    const uint4* src = reinterpret_cast<const uint4*>(static_cast<const unsigned char*>(vols[blockIdx.y]) +
-                                                      (size_t)r0 * d.nx * kEsz);
-    const int n_raw = (G * d.nx * kEsz) >> 4, n_tw = d.n_twx, n_wx = d.nx >> 1;
-    const uint4* tsrc = reinterpret_cast<const uint4*>(tw_x);
-    const uint4* wsrc = reinterpret_cast<const uint4*>(wx);
-    uint4* rdst = reinterpret_cast<uint4*>(raw);
-    uint4* tdst = reinterpret_cast<uint4*>(tws);
-    uint4* wdst = reinterpret_cast<uint4*>(wxs);
-    stage16<4>(
-        n_raw + n_tw + n_wx,
-        [&](int i) { return i < n_raw ? src + i : (i < n_raw + n_tw ? tsrc + (i - n_raw) : wsrc + (i - n_raw - n_tw)); },
-        [&](int i) { return i < n_raw ? rdst + i : (i < n_raw + n_tw ? tdst + (i - n_raw) : wdst + (i - n_raw - n_tw)); });
-    if (threadIdx.x < G) wys[threadIdx.x] = __ldg(wy + (r0 & (d.ny - 1)) + threadIdx.x);
-  }
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < (G << d.log2M); idx += blockDim.x) {
-    const int g = idx >> d.log2M, m = idx & (M - 1);
-    const int x = 2 * (idx & (M - 1)) + (g << (d.log2M + 1));  // element of the staged rows
+  const void* vol = vols[blockIdx.y];
+  // the twiddles (published by the first stage's closing barrier; the first stage needs none)
+  stage16<4>(
+      d.n_twx, [&](int i) { return reinterpret_cast<const uint4*>(tw_x) + i; },
+      [&](int i) { return reinterpret_cast<uint4*>(tws) + i; });
+  // the first stage reads the frame: point m of row g is (v[2m], v[2m + 1]), windowed as
+  // (double)v * ((1 * wy[y]) * wx[x]) with each product rounded (VolumePhaseCorrelator.cpp:62-63)
+  auto first = [&](int g, int m) -> double2 {
+    const int r = r0 + g;
+    const long long off = (long long)r * d.nx + 2 * m;
     float v0, v1;
     if (U16) {
-      const ushort2 q = reinterpret_cast<const ushort2*>(raw)[x >> 1];
+      const ushort2 q = __ldg(reinterpret_cast<const ushort2*>(static_cast<const unsigned short*>(vol) + off));
       v0 = (float)q.x;
       v1 = (float)q.y;
     } else {
-      const float2 f = reinterpret_cast<const float2*>(raw)[x >> 1];
+      const float2 f = __ldg(reinterpret_cast<const float2*>(static_cast<const float*>(vol) + off));
       v0 = f.x;
       v1 = f.y;
     }
-    // (double)v * ((1 * wy[y]) * wx[x]), each product rounded (VolumePhaseCorrelator.cpp:62-63)
-    const double wrow = __dmul_rn(1.0, wys[g]);
-    const double2 w = reinterpret_cast<const double2*>(wxs)[m];
-    sm[g * S + swz(m)] = make_double2(__dmul_rn((double)v0, __dmul_rn(wrow, w.x)),
-                                      __dmul_rn((double)v1, __dmul_rn(wrow, w.y)));
-  }
-  fft_rows<false, kRowEPT, kRowThreads>(sm, G, d.log2M, tws);
+    const double wrow = __dmul_rn(1.0, __ldg(wy + (r & (d.ny - 1))));
+    const double2 w = __ldg(reinterpret_cast<const double2*>(wx) + m);
+    return make_double2(__dmul_rn((double)v0, __dmul_rn(wrow, w.x)), __dmul_rn((double)v1, __dmul_rn(wrow, w.y)));
+  };
+  fft_rows<false, kRowEPT, kRowThreads, false, true>(sm, G, d.log2M, tws, first, NoIo{});
   // X[k] = (Z[k] + conj Z[M-k]) / 2 - i W_nx^k (Z[k] - conj Z[M-k]) / 2, k = 0..M, to plane k
   double2* out = spec + (long long)blockIdx.y * d.n_complex;
   for (int idx = threadIdx.x; idx < ((M + 1) << d.log2G); idx += blockDim.x) {
@@ -355,15 +364,14 @@ __global__ void __launch_bounds__(kPlaneThreads, 1) plane_yz_kernel(const double
   const int pp = (int)min((long long)d.PP, n_planes - p0);
   const int E = pp * plane;
   double2* tws = sm + d.PP * NZ * S;
-  {
-    const double2* src = in + p0 * plane;
-    stage16<8>(
-        E + d.n_twy, [&](int i) { return reinterpret_cast<const uint4*>(i < E ? src + i : tw_y + (i - E)); },
-        [&](int i) {
-          return reinterpret_cast<uint4*>(i < E ? sm + (i >> d.log2ny) * S + swz(i & (ny - 1)) : tws + (i - E));
-        });
-  }
-  fft_rows<false, kPlaneEPT, kPlaneThreads>(sm, pp * NZ, d.log2ny, tws);
+  const double2* src = in + p0 * plane;
+  stage16<4>(
+      d.n_twy, [&](int i) { return reinterpret_cast<const uint4*>(tw_y) + i; },
+      [&](int i) { return reinterpret_cast<uint4*>(tws) + i; });
+  // the first stage reads the planes (in may be out: each CTA reads its own planes before it
+  // writes them)
+  auto first = [&](int l, int i) -> double2 { return src[l * ny + i]; };
+  fft_rows<false, kPlaneEPT, kPlaneThreads, false, true>(sm, pp * NZ, d.log2ny, tws, first, NoIo{});
   const int M1 = (d.nx >> 1) + 1;
   for (int c = threadIdx.x; c < pp * ny; c += blockDim.x) {
     const int p = c >> d.log2ny, y = c & (ny - 1);
@@ -397,13 +405,18 @@ __global__ void __launch_bounds__(kPlaneThreads, 1) plane_yz_kernel(const double
 #pragma unroll
     for (int z = 0; z < NZ; z++) col[z * S] = a[z];
   }
-  if (!REF) fft_rows<true, kPlaneEPT, kPlaneThreads>(sm, pp * NZ, d.log2ny, tws);
   __syncthreads();
   double2* dst = out + p0 * plane;
+  if (!REF) {
+    // the last inverse stage writes the planes
+    auto last = [&](int l, int i, double2 v) { dst[l * ny + i] = v; };
+    fft_rows<true, kPlaneEPT, kPlaneThreads, true, false>(sm, pp * NZ, d.log2ny, tws, NoIo{}, last);
+  } else {
 #pragma unroll
-  for (int u = 0; u < kPlaneEPT; u++) {
-    const int idx = threadIdx.x + u * kPlaneThreads;
-    if (idx < E) dst[idx] = sm[(idx >> d.log2ny) * S + swz(idx & (ny - 1))];
+    for (int u = 0; u < kPlaneEPT; u++) {
+      const int idx = threadIdx.x + u * kPlaneThreads;
+      if (idx < E) dst[idx] = sm[(idx >> d.log2ny) * S + swz(idx & (ny - 1))];
+    }
   }
 }
 
@@ -458,17 +471,18 @@ __global__ void __launch_bounds__(kRowThreads) plane_rows_inv_argmax_kernel(cons
     line[ik] = fold(xk, xm, tws[d.tw_x_post + k]);
     if (k > 0 && k < H) line[im] = fold(xm, xk, tws[d.tw_x_post + M - k]);
   }
-  fft_rows<true, kRowEPT, kRowThreads>(sm, G, d.log2M, tws);
+  __syncthreads();
+  // the last inverse stage feeds the first-maximum search (and the optional surface)
   double v = -DBL_MAX;
   long long best = 0x7fffffffffffffffLL;
-  for (int idx = threadIdx.x; idx < (G << d.log2M); idx += blockDim.x) {
-    const int g = idx >> d.log2M, m = idx & (M - 1);
-    const double2 z = sm[g * S + swz(m)];
+  double* surf = surface ? surface + (long long)blockIdx.y * d.n_el : nullptr;
+  auto last = [&](int g, int m, double2 z) {
     const long long f = (long long)(r0 + g) * d.nx + 2 * m;
     better(v, best, z.x, f);
     better(v, best, z.y, f + 1);
-    if (surface) *reinterpret_cast<double2*>(surface + (long long)blockIdx.y * d.n_el + f) = z;
-  }
+    if (surf) *reinterpret_cast<double2*>(surf + f) = z;
+  };
+  fft_rows<true, kRowEPT, kRowThreads, true, false>(sm, G, d.log2M, tws, NoIo{}, last);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     const double v2 = __shfl_down_sync(0xffffffffu, v, o);
@@ -585,7 +599,7 @@ int plane_blocks_per_frame(const PlaneDims& d) { return d.rows >> d.log2G; }
 cudaError_t launch_plane_rows_fwd(const PlaneDims& d, const void* const* vols, int in_kind, int batch,
                                   const double* wy, const double* wx, const double2* tw_x, double2* spec,
                                   cudaStream_t s) {
-  const size_t smem = rows_smem_bytes(d, in_kind == FA_U16 ? 2 : 4);
+  const size_t smem = rows_smem_bytes(d);
   const dim3 grid(d.rows >> d.log2G, batch);
   if (in_kind == FA_U16) {
     cudaError_t e = allow_smem(plane_rows_fwd_kernel<true>, smem);
@@ -640,7 +654,7 @@ cudaError_t launch_plane_to_rows(const PlaneDims& d, const double2* in, double2*
 
 cudaError_t launch_plane_rows_inv_argmax(const PlaneDims& d, const double2* spec, int batch, const double2* tw_x,
                                          double* bval, long long* bidx, double* surface, cudaStream_t s) {
-  const size_t smem = rows_smem_bytes(d, 0);
+  const size_t smem = rows_smem_bytes(d);
   cudaError_t e = allow_smem(plane_rows_inv_argmax_kernel, smem);
   if (e != cudaSuccess) return e;
   plane_rows_inv_argmax_kernel<<<dim3(d.rows >> d.log2G, batch), kRowThreads, smem, s>>>(spec, tw_x, d, bval, bidx,
