@@ -1119,7 +1119,7 @@ extern "C" fa_status fa_align_batch(fa_frame* const* frames, int n, const double
 
 // ================================================================== phase correlation =============
 
-namespace {
+namespace fa_rt {
 
 // Pointer staging for a batch of n inputs (pinned host + device arrays), grown on demand.
 fa_status correlator_reserve(fa_correlator* C, int n) {
@@ -1140,22 +1140,22 @@ fa_status correlator_reserve(fa_correlator* C, int n) {
   return FA_OK;
 }
 
-// Window, D2Z, cross-power normalisation, Z2D and first-maximum argmax for n volumes (device
-// pointers, FP32 or raw uint16) in batches of C->cap; peak indices to C->d_idx[0..n).
-}  // namespace
-
-namespace fa_rt {
-
+// Window, forward DFT, cross-power normalisation, inverse DFT and first-maximum argmax for n volumes
+// (device pointers, FP32 or raw uint16) in batches of C->cap; peak indices to C->d_idx[first ..].
 fa_status correlator_enqueue(fa_correlator* C, const void* const* vols, int in_kind, int n, double* surface,
-                             bool planes) {
-  FA_TRY(correlator_reserve(C, n));
+                             bool planes, int first) {
+  if (first > 0 && first + n > C->ptr_cap) return fail(FA_ERR_STATE, "correlator slots not reserved");
+  FA_TRY(correlator_reserve(C, first + n));
   // the fused passes stage frames in 16-byte chunks: 16-byte aligned frames only
   for (int i = 0; i < n; i++) {
-    C->h_ptrs[i] = vols[i];
+    C->h_ptrs[first + i] = vols[i];
     if (reinterpret_cast<uintptr_t>(vols[i]) % 16) planes = false;
   }
   planes = planes && C->planes;
-  FA_CU(cudaMemcpyAsync(C->d_ptrs, C->h_ptrs, (size_t)n * sizeof(void*), cudaMemcpyHostToDevice, C->stream));
+  FA_CU(cudaMemcpyAsync(C->d_ptrs + first, C->h_ptrs + first, (size_t)n * sizeof(void*), cudaMemcpyHostToDevice,
+                        C->stream));
+  const void* const* d_ptrs = C->d_ptrs + first;
+  long long* d_idx = C->d_idx + first;
   if (!planes && C->planes && !C->ref_conj_rows) {  // a plane-path correlator falling back to cuFFT
     FA_CU(cudaStreamSynchronize(C->stream));
     FA_TRY(dalloc_t(C->ctx, (size_t)C->n_el * C->cap, &C->real, C->allocs));
@@ -1169,22 +1169,22 @@ fa_status correlator_enqueue(fa_correlator* C, const void* const* vols, int in_k
     double* surf = surface ? surface + (size_t)c0 * C->n_el : nullptr;
     if (planes) {
       const int nb = fa::plane_blocks_per_frame(C->pd);
-      FA_CU(fa::launch_plane_rows_fwd(C->pd, C->d_ptrs + c0, in_kind, m, C->wy, C->wx, C->tw_x, C->spec, C->stream));
+      FA_CU(fa::launch_plane_rows_fwd(C->pd, d_ptrs + c0, in_kind, m, C->wy, C->wx, C->tw_x, C->spec, C->stream));
       FA_CU(fa::launch_plane_yz(C->pd, C->spec, C->spec, C->ref_conj, C->tw_y, m, false, C->stream));
       FA_CU(fa::launch_plane_rows_inv_argmax(C->pd, C->spec, m, C->tw_x, C->bval, C->bidx, surf, C->stream));
-      FA_CU(fa::launch_phase_argmax_final(C->bval, C->bidx, nb, m, C->d_idx + c0, C->stream));
+      FA_CU(fa::launch_phase_argmax_final(C->bval, C->bidx, nb, m, d_idx + c0, C->stream));
       g_launches += 4;
     } else {
       cufftHandle fwd, inv;
       FA_TRY(correlator_plans(C, m, &fwd, &inv));
-      FA_CU(fa::launch_phase_window(C->d_ptrs + c0, in_kind, C->wy, C->wx, C->ny, C->nx, C->n_el, m, C->real,
+      FA_CU(fa::launch_phase_window(d_ptrs + c0, in_kind, C->wy, C->wx, C->ny, C->nx, C->n_el, m, C->real,
                                     C->stream));
       if (cufftExecD2Z(fwd, C->real, reinterpret_cast<cufftDoubleComplex*>(C->spec)) != CUFFT_SUCCESS)
         return fail(FA_ERR_CUDA, "cufftExecD2Z failed");
       FA_CU(fa::launch_phase_normalise(C->spec, ref_rows, C->n_complex, m, C->stream));
       if (cufftExecZ2D(inv, reinterpret_cast<cufftDoubleComplex*>(C->spec), C->real) != CUFFT_SUCCESS)
         return fail(FA_ERR_CUDA, "cufftExecZ2D failed");
-      FA_CU(fa::launch_phase_argmax(C->real, C->n_el, m, C->bval, C->bidx, C->n_blocks, C->d_idx + c0, C->stream));
+      FA_CU(fa::launch_phase_argmax(C->real, C->n_el, m, C->bval, C->bidx, C->n_blocks, d_idx + c0, C->stream));
       if (surf)
         FA_CU(cudaMemcpyAsync(surf, C->real, (size_t)m * C->n_el * sizeof(double), cudaMemcpyDeviceToDevice,
                               C->stream));
@@ -1585,52 +1585,92 @@ fa_status aligner_run(fa_aligner* A, const void* const* frames, fa_dtype dtype, 
     FA_CU(cudaEventCreate(&A->ev1));
   }
   FA_CU(cudaEventRecord(A->ev0, s));
-  std::vector<const void*> raw((size_t)n);
-  for (int i = 0; i < n; i++) {
-    fa_frame* F = A->slots[i];
-    if (device_src) {
-      raw[i] = frames[i];
-    } else {
-      void* dst = static_cast<char*>(A->staging) + (size_t)i * raw_bytes;
-      FA_CU(cudaMemcpyAsync(dst, frames[i], raw_bytes, cudaMemcpyHostToDevice, s));
-      raw[i] = dst;
+  // Host frames upload on a copy stream in chunks of kChunk; each chunk's conversion and phase
+  // correlation wait only for its own uploads, so they overlap the uploads of the chunks after it.
+  constexpr int kChunk = 8;
+  const int chunk = device_src ? n : kChunk;
+  if (!device_src) {
+    if (!A->copy_stream) FA_CU(cudaStreamCreateWithFlags(&A->copy_stream, cudaStreamNonBlocking));
+    while ((int)A->copy_ev.size() < (n + chunk - 1) / chunk) {
+      cudaEvent_t e;
+      FA_CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      A->copy_ev.push_back(e);
     }
-    if (A->prm.smoothing > 0) {  // smoothStack, then + 1 (FrameWarpAligner.cpp:139-142)
-      FA_TRY(aligner_smooth(A, raw[i], dtype, s));
-      FA_CU(fa::launch_to_slot(A->smooth_out, FA_F32, F->data, kind, A->nz, A->ny, A->nx, F->job.fpitch, F->job.fplane,
-                               true, s));
-    } else {
-      FA_CU(fa::launch_to_slot(raw[i], dtype, F->data, kind, A->nz, A->ny, A->nx, F->job.fpitch, F->job.fplane, true,
-                               s));
-    }
-    g_launches += 1;
+    // the copy stream starts after everything already queued on s (the previous call's readers of
+    // the staging buffer)
+    FA_CU(cudaEventRecord(A->ev1, s));
+    FA_CU(cudaStreamWaitEvent(A->copy_stream, A->ev1, 0));
   }
-  // Phase correlation on the raw frames (FrameWarpAligner.cpp:181-190), downsampled when binning.
-  std::vector<const void*> cin((size_t)n);
+  FA_TRY(correlator_reserve(A->corr, n));
+  // Host batches of 2 * kChunk frames or more are solved in two groups: the first group's solve
+  // runs while the second group uploads and correlates. Frames are independent, so the results do
+  // not depend on the grouping.
+  const int n_groups = (!device_src && n >= 2 * kChunk) ? 2 : 1;
+  const int g_split = n_groups == 2 ? ((n / 2 + kChunk - 1) / kChunk) * kChunk : n;
+  while ((int)A->group_ev.size() < n_groups) {
+    cudaEvent_t e;
+    FA_CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    A->group_ev.push_back(e);
+  }
+  fa_correlator* C = A->corr;
+  std::vector<const void*> raw((size_t)n), cin((size_t)n);
   int cin_kind = dtype;
-  if (A->prm.spatial_binning > 1) {
-    const long long nds = (long long)A->dz * A->dy * A->dx;
-    for (int i = 0; i < n; i++) {
-      float* vol = A->vols + (size_t)i * nds;
-      FA_CU(fa::launch_downsample(raw[i], dtype, A->nz, A->ny, A->nx, A->prm.spatial_binning, vol, s));
-      g_launches += 1;
-      cin[i] = vol;
+  for (int c0 = 0, ci = 0; c0 < n; c0 += chunk, ci++) {
+    const int m = std::min({chunk, n - c0, c0 < g_split ? g_split - c0 : n - c0});
+    if (!device_src) {
+      for (int i = c0; i < c0 + m; i++) {
+        void* dst = static_cast<char*>(A->staging) + (size_t)i * raw_bytes;
+        FA_CU(cudaMemcpyAsync(dst, frames[i], raw_bytes, cudaMemcpyHostToDevice, A->copy_stream));
+      }
+      FA_CU(cudaEventRecord(A->copy_ev[ci], A->copy_stream));
+      FA_CU(cudaStreamWaitEvent(s, A->copy_ev[ci], 0));
     }
-    cin_kind = FA_F32;
-  } else {
-    cin = raw;
-  }
-  FA_TRY(correlator_enqueue(A->corr, cin.data(), cin_kind, n));
-  std::vector<double> rigid((size_t)3 * n);
-  FA_TRY(correlator_read(A->corr, n, rigid.data()));
-  for (int i = 0; i < n; i++) {
-    // FrameWarpAligner.cpp:186-188: x and y scaled by the phase-correlation downsampling
-    rigid[(size_t)3 * i] *= A->prm.spatial_binning;
-    rigid[(size_t)3 * i + 1] *= A->prm.spatial_binning;
-    A->slots[i]->have_last = false;
+    for (int i = c0; i < c0 + m; i++) {
+      fa_frame* F = A->slots[i];
+      raw[i] = device_src ? frames[i] : static_cast<const char*>(A->staging) + (size_t)i * raw_bytes;
+      if (A->prm.smoothing > 0) {  // smoothStack, then + 1 (FrameWarpAligner.cpp:139-142)
+        FA_TRY(aligner_smooth(A, raw[i], dtype, s));
+        FA_CU(fa::launch_to_slot(A->smooth_out, FA_F32, F->data, kind, A->nz, A->ny, A->nx, F->job.fpitch,
+                                 F->job.fplane, true, s));
+      } else {
+        FA_CU(fa::launch_to_slot(raw[i], dtype, F->data, kind, A->nz, A->ny, A->nx, F->job.fpitch, F->job.fplane,
+                                 true, s));
+      }
+      g_launches += 1;
+      // Phase correlation on the raw frames (FrameWarpAligner.cpp:181-190), downsampled when binning.
+      if (A->prm.spatial_binning > 1) {
+        float* vol = A->vols + (size_t)i * A->dz * A->dy * A->dx;
+        FA_CU(fa::launch_downsample(raw[i], dtype, A->nz, A->ny, A->nx, A->prm.spatial_binning, vol, s));
+        g_launches += 1;
+        cin[i] = vol;
+        cin_kind = FA_F32;
+      } else {
+        cin[i] = raw[i];
+      }
+    }
+    FA_TRY(correlator_enqueue(C, cin.data() + c0, cin_kind, m, nullptr, true, c0));
+    if (c0 + m == g_split || c0 + m == n) {  // a group's peaks, read back without waiting for the rest
+      const int g0 = c0 + m == g_split ? 0 : g_split;
+      FA_CU(cudaMemcpyAsync(C->h_idx + g0, C->d_idx + g0, (size_t)(c0 + m - g0) * sizeof(long long),
+                            cudaMemcpyDeviceToHost, s));
+      FA_CU(cudaEventRecord(A->group_ev[g0 == 0 ? 0 : 1], s));
+    }
   }
   std::vector<fa_frame*> batch(A->slots.begin(), A->slots.begin() + n);
-  FA_TRY(align_batch_impl(batch.data(), n, rigid.data(), A->prm.max_iterations, D_out, stats, nullptr));
+  for (int g = 0; g < n_groups; g++) {
+    const int g0 = g == 0 ? 0 : g_split, g1 = g == 0 ? g_split : n;
+    FA_CU(cudaEventSynchronize(A->group_ev[g]));
+    std::vector<double> rigid((size_t)3 * (g1 - g0));
+    for (int i = g0; i < g1; i++) {
+      unravel_shift(C, C->h_idx[i], rigid.data() + (size_t)3 * (i - g0));
+      // FrameWarpAligner.cpp:186-188: x and y scaled by the phase-correlation downsampling
+      rigid[(size_t)3 * (i - g0)] *= A->prm.spatial_binning;
+      rigid[(size_t)3 * (i - g0) + 1] *= A->prm.spatial_binning;
+      A->slots[i]->have_last = false;
+    }
+    FA_TRY(align_batch_impl(batch.data() + g0, g1 - g0, rigid.data(), A->prm.max_iterations,
+                            D_out + (size_t)g0 * 3 * A->ref->nD, stats ? stats + g0 : nullptr, nullptr));
+  }
   FA_CU(cudaEventRecord(A->ev1, batch[0]->stream));
   FA_CU(cudaEventSynchronize(A->ev1));
   float ms = 0;
@@ -1705,6 +1745,9 @@ extern "C" fa_status fa_aligner_destroy(fa_aligner* A) {
   if (A->stream) cudaStreamDestroy(A->stream);
   if (A->ev0) cudaEventDestroy(A->ev0);
   if (A->ev1) cudaEventDestroy(A->ev1);
+  for (cudaEvent_t e : A->copy_ev) cudaEventDestroy(e);
+  for (cudaEvent_t e : A->group_ev) cudaEventDestroy(e);
+  if (A->copy_stream) cudaStreamDestroy(A->copy_stream);
   delete A;
   return FA_OK;
 }

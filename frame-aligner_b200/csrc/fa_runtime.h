@@ -156,6 +156,10 @@ struct fa_aligner {
   size_t vols_count = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = 0;
+  // host frames: uploads on their own stream, one event per chunk of frames
+  cudaStream_t copy_stream = nullptr;
+  std::vector<cudaEvent_t> copy_ev;
+  std::vector<cudaEvent_t> group_ev;  // peaks of a group of frames read back
   // smoothStack (smoothing > 0): Gaussian weights along x and y, and two frame-sized work buffers
   // used one frame at a time in stream order
   float* smooth_kx = nullptr;
@@ -213,10 +217,14 @@ int slot_kind_for(const fa_aligner* A, fa_dtype dtype);
 // The correlator's D2Z / Z2D plans for a batch size (made and cached on first use).
 fa_status correlator_plans(fa_correlator* C, int batch, cufftHandle* fwd, cufftHandle* inv);
 // Window, forward DFT, normalisation, inverse DFT and argmax for n device volumes; peak indices to
-// C->d_idx[0..n). surface (n * n_el doubles, optional) receives the correlation surfaces; planes
-// selects the fused kx-plane passes (when C->planes) or cuFFT.
+// C->d_idx[first .. first + n). surface (n * n_el doubles, optional) receives the correlation
+// surfaces; planes selects the fused kx-plane passes (when C->planes) or cuFFT. Calls with
+// first > 0 use pointer and result slots reserved before (correlator_reserve(C, first + n)), so
+// that consecutive calls queue on the stream without waiting for one another.
 fa_status correlator_enqueue(fa_correlator* C, const void* const* vols, int in_kind, int n,
-                             double* surface = nullptr, bool planes = true);
+                             double* surface = nullptr, bool planes = true, int first = 0);
+// Pointer staging and peak slots for n volumes (grows with a stream synchronisation).
+fa_status correlator_reserve(fa_correlator* C, int n);
 // Peak index -> signed integer shift (x, y, z).
 void unravel_shift(const fa_correlator* C, long long idx, double* shift);
 
