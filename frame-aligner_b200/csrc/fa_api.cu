@@ -935,12 +935,17 @@ fa_status init_solve(fa_frame* F, const double* rigid, int max_iterations) {
   return FA_OK;
 }
 
-fa_status finish_solve(fa_frame* F, double* D_out, fa_align_stats* stats) {
+// Queues the copies of a solved frame's x and state into its pinned buffers on stream s.
+fa_status finish_solve_enqueue(fa_frame* F, cudaStream_t s) {
+  FA_CU(cudaMemcpyAsync(F->h_x, F->job.x, (size_t)F->ref->P * sizeof(double), cudaMemcpyDeviceToHost, s));
+  FA_CU(cudaMemcpyAsync(F->h_state, F->state, sizeof(fa::FrameState), cudaMemcpyDeviceToHost, s));
+  return FA_OK;
+}
+
+// D (and the statistics) from the copies finish_solve_enqueue queued, once they completed.
+void finish_solve_read(fa_frame* F, double* D_out, fa_align_stats* stats) {
   fa_reference* R = F->ref;
   const int nd = R->n_dim;
-  FA_CU(cudaMemcpyAsync(F->h_x, F->job.x, (size_t)R->P * sizeof(double), cudaMemcpyDeviceToHost, F->stream));
-  FA_CU(cudaMemcpyAsync(F->h_state, F->state, sizeof(fa::FrameState), cudaMemcpyDeviceToHost, F->stream));
-  FA_CU(cudaStreamSynchronize(F->stream));
   for (int k = 0; k < R->nD; k++) {
     D_out[3 * k] = F->h_x[k * nd];
     D_out[3 * k + 1] = F->h_x[k * nd + 1];
@@ -955,6 +960,12 @@ fa_status finish_solve(fa_frame* F, double* D_out, fa_align_stats* stats) {
     stats->f_final = S.f;
     stats->radius_final = S.radius;
   }
+}
+
+fa_status finish_solve(fa_frame* F, double* D_out, fa_align_stats* stats) {
+  FA_TRY(finish_solve_enqueue(F, F->stream));
+  FA_CU(cudaStreamSynchronize(F->stream));
+  finish_solve_read(F, D_out, stats);
   return FA_OK;
 }
 
@@ -992,9 +1003,11 @@ extern "C" fa_status fa_align_frame(fa_frame* F, const double* rigid_shift, int 
 
 namespace {
 
-// Batched solve; frame_data (optional) replaces each frame's own device data pointer for this call.
+// Batched solve; frame_data (optional) replaces each frame's own device data pointer for this call;
+// cache (optional) keeps the buffers and the graph for the next call on the same frames.
 fa_status align_batch_impl(fa_frame* const* frames, int n, const double* rigid_shifts, int max_iterations,
-                           double* D_out, fa_align_stats* stats, const void* const* frame_data) {
+                           double* D_out, fa_align_stats* stats, const void* const* frame_data,
+                           BatchCache* cache = nullptr) {
   if (!frames || n <= 0 || !D_out) return fail(FA_ERR_BAD_ARG, "bad arguments");
   for (int i = 0; i < n; i++)
     if (!frames[i]) return fail(FA_ERR_BAD_ARG, "NULL frame");
@@ -1013,10 +1026,10 @@ fa_status align_batch_impl(fa_frame* const* frames, int n, const double* rigid_s
   int max_tiles = 0, max_nD = 0;
   bool vec4 = true;
   std::vector<Job> jobs(n);
+  // initial states on every frame's stream, then one wait per stream (the copies are done by then)
   for (int i = 0; i < n; i++) {
     fa_frame* F = frames[i];
     FA_TRY(init_solve(F, rigid_shifts ? rigid_shifts + 3 * i : nullptr, max_iterations));
-    FA_CU(cudaStreamSynchronize(F->stream));
     jobs[i] = F->job;
     jobs[i].state = F->state;
     if (frame_data) jobs[i].frame = frame_data[i];
@@ -1024,93 +1037,122 @@ fa_status align_batch_impl(fa_frame* const* frames, int n, const double* rigid_s
     vec4 = vec4 && (F->ref->nx % 4 == 0);
     max_nD = std::max(max_nD, F->ref->nD);
   }
-  std::vector<Alloc> tmp;
-  Job* jobs_dev;
-  int* d_active;
-  int* d_list;
-  int* d_prefix;
-  int* h_active;
-  FA_TRY(dalloc_t(ctx, (size_t)n, &jobs_dev, tmp));
-  fa_status st = dalloc_t(ctx, 1, &d_active, tmp);
-  if (st == FA_OK) st = dalloc_t(ctx, (size_t)n, &d_list, tmp);
-  if (st == FA_OK) st = dalloc_t(ctx, (size_t)n + 1, &d_prefix, tmp);
-  if (st != FA_OK) {
-    dfree_all(ctx, tmp);
-    return st;
-  }
-  if (cudaMallocHost(&h_active, sizeof(int)) != cudaSuccess) {
-    dfree_all(ctx, tmp);
-    return fail(FA_ERR_OOM, "cudaMallocHost failed");
-  }
-  auto done = [&](fa_status r) {
-    std::string keep = g_err;
-    cudaStreamSynchronize(s);
-    cudaFreeHost(h_active);
-    dfree_all(ctx, tmp);
-    g_err = keep;
-    return r;
-  };
-  if (cudaMemcpyAsync(jobs_dev, jobs.data(), n * sizeof(Job), cudaMemcpyHostToDevice, s) != cudaSuccess)
-    return done(fail(FA_ERR_CUDA, "job upload failed"));
+  for (int i = 0; i < n; i++) FA_CU(cudaStreamSynchronize(frames[i]->stream));
   std::vector<int> all(n), prefix(n + 1, 0);
   for (int i = 0; i < n; i++) {
     all[i] = i;
     prefix[i + 1] = prefix[i] + frames[i]->ref->G.n_tiles;
   }
-  *h_active = n;
-  if (cudaMemcpyAsync(d_list, all.data(), n * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess ||
-      cudaMemcpyAsync(d_prefix, prefix.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess ||
-      cudaMemcpyAsync(d_active, h_active, sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess ||
-      cudaStreamSynchronize(s) != cudaSuccess)
+  BatchCache local;
+  BatchCache* bc = cache ? cache : &local;
+  auto done = [&](fa_status r) {
+    std::string keep = g_err;
+    cudaStreamSynchronize(s);
+    if (bc == &local) batch_cache_release(ctx, &local);
+    g_err = keep;
+    return r;
+  };
+  if (bc->cap < n) {
+    FA_CU(cudaStreamSynchronize(s));
+    batch_cache_release(ctx, bc);
+    fa_status st = dalloc_t(ctx, (size_t)n, &bc->jobs_dev, bc->allocs);
+    if (st == FA_OK) st = dalloc_t(ctx, 1, &bc->d_active, bc->allocs);
+    if (st == FA_OK) st = dalloc_t(ctx, (size_t)n, &bc->d_list, bc->allocs);
+    if (st == FA_OK) st = dalloc_t(ctx, (size_t)n + 1, &bc->d_prefix, bc->allocs);
+    if (st == FA_OK && cudaMallocHost(&bc->h_active, sizeof(int)) != cudaSuccess) {
+      bc->h_active = nullptr;
+      st = fail(FA_ERR_OOM, "cudaMallocHost failed");
+    }
+    if (st != FA_OK) return done(st);
+    bc->cap = n;
+  }
+  *bc->h_active = n;
+  if (cudaMemcpyAsync(bc->jobs_dev, jobs.data(), n * sizeof(Job), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(bc->d_list, all.data(), n * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(bc->d_prefix, prefix.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(bc->d_active, bc->h_active, sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess)
     return done(fail(FA_ERR_CUDA, "active list upload failed"));
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
   // Iterations run as a CUDA graph of kGraphIters x (fused pass, solve), then one active count.
   constexpr int kGraphIters = 4;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
-  if (e == cudaSuccess) {
-    for (int it = 0; it < kGraphIters && e == cudaSuccess; it++) {
-      if (vec4)
-        e = fa::launch_eval4_active(jobs_dev, d_list, d_active, d_prefix, prefix[n], R0->n_dim, frames[0]->kind,
-                                    R0->prec == FA_PREC_MIXED, R0->host.tune_mb, R0->host.tune_grid_mult * sms, s);
-      else
-        e = fa::launch_eval(jobs_dev, n, max_tiles, R0->n_dim, frames[0]->kind, R0->prec == FA_PREC_MIXED, s, false);
-      if (e == cudaSuccess) e = fa::launch_solve(jobs_dev, n, max_nD, R0->n_dim, s);
-      if (e == cudaSuccess)
-        e = fa::launch_compact(jobs_dev, n, d_list, d_active, d_prefix, nullptr, nullptr, nullptr, s);
+  const long long key[6] = {n, prefix[n], max_nD, (vec4 ? 1 : 0) + 2 * frames[0]->kind, R0->host.tune_mb,
+                            R0->host.tune_grid_mult};
+  const bool reuse = bc->exec && bc->frames.size() == (size_t)n &&
+                     std::equal(bc->frames.begin(), bc->frames.end(), frames) && std::equal(key, key + 6, bc->key);
+  cudaError_t e = cudaSuccess;
+  if (!reuse) {
+    if (bc->exec) cudaGraphExecDestroy(bc->exec);
+    bc->exec = nullptr;
+    bc->frames.clear();
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      for (int it = 0; it < kGraphIters && e == cudaSuccess; it++) {
+        if (vec4)
+          e = fa::launch_eval4_active(bc->jobs_dev, bc->d_list, bc->d_active, bc->d_prefix, prefix[n], R0->n_dim,
+                                      frames[0]->kind, R0->prec == FA_PREC_MIXED, R0->host.tune_mb,
+                                      R0->host.tune_grid_mult * sms, s);
+        else
+          e = fa::launch_eval(bc->jobs_dev, n, max_tiles, R0->n_dim, frames[0]->kind, R0->prec == FA_PREC_MIXED, s,
+                              false);
+        if (e == cudaSuccess) e = fa::launch_solve(bc->jobs_dev, n, max_nD, R0->n_dim, s);
+        if (e == cudaSuccess)
+          e = fa::launch_compact(bc->jobs_dev, n, bc->d_list, bc->d_active, bc->d_prefix, nullptr, nullptr, nullptr, s);
+      }
+      if (e == cudaSuccess) e = cudaMemcpyAsync(bc->h_active, bc->d_active, sizeof(int), cudaMemcpyDeviceToHost, s);
+      cudaError_t e2 = cudaStreamEndCapture(s, &graph);
+      if (e == cudaSuccess) e = e2;
     }
-    if (e == cudaSuccess) e = cudaMemcpyAsync(h_active, d_active, sizeof(int), cudaMemcpyDeviceToHost, s);
-    cudaError_t e2 = cudaStreamEndCapture(s, &graph);
-    if (e == cudaSuccess) e = e2;
-  }
-  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
-  if (e != cudaSuccess) {
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&bc->exec, graph, 0);
     if (graph) cudaGraphDestroy(graph);
-    return done(fail(FA_ERR_CUDA, std::string("batch graph: ") + cudaGetErrorString(e)));
+    if (e != cudaSuccess) {
+      bc->exec = nullptr;
+      return done(fail(FA_ERR_CUDA, std::string("batch graph: ") + cudaGetErrorString(e)));
+    }
+    bc->frames.assign(frames, frames + n);
+    std::copy(key, key + 6, bc->key);
   }
   const int max_steps = (max_iterations > 0 ? max_iterations : 100) + 4;
   for (int step = 0; step < max_steps; step += kGraphIters) {
-    e = cudaGraphLaunch(exec, s);
+    e = cudaGraphLaunch(bc->exec, s);
     g_launches += 3 * kGraphIters;
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) break;
-    if (*h_active == 0) break;
+    if (*bc->h_active == 0) break;
   }
-  cudaGraphExecDestroy(exec);
-  cudaGraphDestroy(graph);
   if (e != cudaSuccess) return done(fail(FA_ERR_CUDA, std::string("batch solve: ") + cudaGetErrorString(e)));
+  // every frame's x and state in one batch of copies on the solve's stream
+  for (int i = 0; i < n; i++) {
+    fa_status r = finish_solve_enqueue(frames[i], s);
+    if (r != FA_OK) return done(r);
+  }
+  if (cudaStreamSynchronize(s) != cudaSuccess) return done(fail(FA_ERR_CUDA, "result read failed"));
   for (int i = 0; i < n; i++) {
     fa_frame* F = frames[i];
-    fa_status r = finish_solve(F, D_out + (size_t)i * 3 * F->ref->nD, stats ? stats + i : nullptr);
-    if (r != FA_OK) return done(r);
+    finish_solve_read(F, D_out + (size_t)i * 3 * F->ref->nD, stats ? stats + i : nullptr);
     F->have_last = false;
   }
   return done(FA_OK);
 }
 
 }  // namespace
+
+namespace fa_rt {
+
+void batch_cache_release(fa_context* ctx, BatchCache* c) {
+  if (c->exec) cudaGraphExecDestroy(c->exec);
+  c->exec = nullptr;
+  c->frames.clear();
+  if (c->h_active) cudaFreeHost(c->h_active);
+  c->h_active = nullptr;
+  dfree_all(ctx, c->allocs);
+  c->jobs_dev = nullptr;
+  c->d_active = c->d_list = c->d_prefix = nullptr;
+  c->cap = 0;
+}
+
+}  // namespace fa_rt
 
 extern "C" fa_status fa_align_batch(fa_frame* const* frames, int n, const double* rigid_shifts, int max_iterations,
                                     double* D_out, fa_align_stats* stats) {
@@ -1499,6 +1541,7 @@ namespace {
 
 void aligner_release_reference(fa_aligner* A) {
   aligner_release_results(A);
+  for (auto& c : A->batch_cache) batch_cache_release(A->ctx, &c);
   dfree_all(A->ctx, A->smooth_allocs);
   A->smooth_kx = A->smooth_ky = A->smooth_tmp = A->smooth_out = nullptr;
   A->smooth_nkx = A->smooth_nky = 0;
@@ -1670,7 +1713,8 @@ fa_status aligner_run(fa_aligner* A, const void* const* frames, fa_dtype dtype, 
       A->slots[i]->have_last = false;
     }
     FA_TRY(align_batch_impl(batch.data() + g0, g1 - g0, rigid.data(), A->prm.max_iterations,
-                            D_out + (size_t)g0 * 3 * A->ref->nD, stats ? stats + g0 : nullptr, nullptr));
+                            D_out + (size_t)g0 * 3 * A->ref->nD, stats ? stats + g0 : nullptr, nullptr,
+                            &A->batch_cache[g]));
   }
   FA_CU(cudaEventRecord(A->ev1, batch[0]->stream));
   FA_CU(cudaEventSynchronize(A->ev1));

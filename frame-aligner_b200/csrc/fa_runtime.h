@@ -140,6 +140,27 @@ struct fa_correlator {
   std::vector<fa_rt::Alloc> ptr_allocs;
 };
 
+namespace fa_rt {
+
+// Device buffers, a pinned active count and the instantiated graph of a batched solve, kept
+// between calls on the same frames (in the same order) with the same solve geometry.
+struct BatchCache {
+  std::vector<Alloc> allocs;
+  fa::Job* jobs_dev = nullptr;
+  int* d_active = nullptr;
+  int* d_list = nullptr;
+  int* d_prefix = nullptr;
+  int* h_active = nullptr;  // pinned
+  int cap = 0;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<fa_frame*> frames;  // the frames the graph was captured for
+  long long key[6] = {0, 0, 0, 0, 0, 0};
+};
+// Frees the cache's buffers and graph (after the caller's streams are idle).
+void batch_cache_release(fa_context* ctx, BatchCache* c);
+
+}  // namespace fa_rt
+
 struct fa_aligner {
   fa_context* ctx = nullptr;
   fa_aligner_params prm{};
@@ -160,6 +181,7 @@ struct fa_aligner {
   cudaStream_t copy_stream = nullptr;
   std::vector<cudaEvent_t> copy_ev;
   std::vector<cudaEvent_t> group_ev;  // peaks of a group of frames read back
+  fa_rt::BatchCache batch_cache[2];   // the batched solve's buffers and graph per solve group
   // smoothStack (smoothing > 0): Gaussian weights along x and y, and two frame-sized work buffers
   // used one frame at a time in stream order
   float* smooth_kx = nullptr;
