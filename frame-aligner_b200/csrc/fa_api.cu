@@ -1644,6 +1644,14 @@ fa_status aligner_run(fa_aligner* A, const void* const* frames, fa_dtype dtype, 
     FA_CU(cudaEventRecord(A->ev1, s));
     FA_CU(cudaStreamWaitEvent(A->copy_stream, A->ev1, 0));
   }
+  // Whatever the outcome, no upload from the caller's frames is left in flight when this returns
+  // (after success they are complete already: the conversions waited for every one of them).
+  struct DrainCopies {
+    cudaStream_t cs;
+    ~DrainCopies() {
+      if (cs) cudaStreamSynchronize(cs);
+    }
+  } drain{device_src ? nullptr : A->copy_stream};
   FA_TRY(correlator_reserve(A->corr, n));
   // Host batches of 2 * kChunk frames or more are solved in two groups: the first group's solve
   // runs while the second group uploads and correlates. Frames are independent, so the results do

@@ -240,7 +240,8 @@ fa_status fa_aligner_info(const fa_aligner* a, int* nD, int* n_dim);
    the aligner; valid until its next fa_aligner_set_reference or fa_aligner_destroy. */
 fa_status fa_aligner_reference(const fa_aligner* a, fa_reference** ref);
 /* FrameWarpAligner::addFrame for n raw frames (host memory; frames[i] points at nz*ny*nx elements of
-   dtype). D_out: n*nD*3 doubles, stats: n entries or NULL; host memory. */
+   dtype). D_out: n*nD*3 doubles, stats: n entries or NULL; host memory. Uploads overlap the device
+   work when the frames are in page-locked memory; none is in flight when the call returns. */
 fa_status fa_aligner_add_frames(fa_aligner* a, const void* const* frames, fa_dtype dtype, int n, double* D_out,
                                 fa_align_stats* stats);
 /* Same, frames already in device memory (frames[i] device pointers). */
