@@ -1467,6 +1467,32 @@ extern "C" fa_status fa_correlator_shift_device(fa_correlator* C, const float* v
 
 // ================================================================== test hooks ====================
 
+extern "C" fa_status fa_test_plane_tables(int nz, int ny, int nx, double* tw_x, int cap_x, int* n_x, int* x_post,
+                                          double* tw_y, int cap_y, int* n_y, int* rows_per_cta, int* planes_per_cta) {
+  if (!tw_x || !n_x || !x_post || !tw_y || !n_y || !rows_per_cta || !planes_per_cta)
+    return fail(FA_ERR_BAD_ARG, "NULL argument");
+  fa::PlaneDims d{};
+  if (!fa::plane_dims(nz, ny, nx, &d)) return fail(FA_ERR_UNSUPPORTED, "dimensions outside the fused plane passes");
+  std::vector<double2> tx, ty;
+  fa::plane_twiddles(d, &tx, &ty);
+  if ((int)tx.size() != d.n_twx || (int)ty.size() != d.n_twy) return fail(FA_ERR_STATE, "twiddle table size");
+  if ((int)tx.size() > cap_x || (int)ty.size() > cap_y) return fail(FA_ERR_BAD_ARG, "output arrays too small");
+  for (size_t i = 0; i < tx.size(); i++) {
+    tw_x[2 * i] = tx[i].x;
+    tw_x[2 * i + 1] = tx[i].y;
+  }
+  for (size_t i = 0; i < ty.size(); i++) {
+    tw_y[2 * i] = ty[i].x;
+    tw_y[2 * i + 1] = ty[i].y;
+  }
+  *n_x = d.n_twx;
+  *x_post = d.tw_x_post;
+  *n_y = d.n_twy;
+  *rows_per_cta = 1 << d.log2G;
+  *planes_per_cta = d.PP;
+  return FA_OK;
+}
+
 extern "C" fa_status fa_test_correlation_surface(fa_correlator* C, const float* volume, int use_planes,
                                                  double* surface) {
   if (!C || !volume || !surface) return fail(FA_ERR_BAD_ARG, "NULL argument");

@@ -180,6 +180,8 @@ SIGNATURES = {
     "fa_profile_eval": [_vp, C.c_int, _f64p, C.c_int, C.POINTER(C.c_double)],
     "fa_test_tr_subproblem": [_vp, C.c_int, C.c_int, _f64p, _f64p, C.c_double, _f64p, C.POINTER(C.c_int)],
     "fa_test_correlation_surface": [_vp, _f32p, C.c_int, _f64p],
+    "fa_test_plane_tables": [C.c_int, C.c_int, C.c_int, _f64p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                             _f64p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)],
 }
 
 
@@ -634,6 +636,19 @@ def test_tr_subproblem(ctx: Context, nD, n_dim, H, g, radius):
     b = C.c_int()
     check(lib().fa_test_tr_subproblem(ctx._h, nD, n_dim, _c64(H), _c64(g), radius, p, C.byref(b)))
     return p, bool(b.value)
+
+
+def plane_tables(nz, ny, nx):
+    """Host-only test hook: twiddle tables and launch shape of the fused phase-correlation passes
+    (fa_test_plane_tables). Raises FaError (FA_ERR_UNSUPPORTED) for dimensions that use cuFFT."""
+    tx = np.empty(2 * max(nx, 1), np.float64)
+    ty = np.empty(2 * max(ny, 1), np.float64)
+    n_x, x_post, n_y, g, pp = (C.c_int() for _ in range(5))
+    check(lib().fa_test_plane_tables(nz, ny, nx, tx, nx, C.byref(n_x), C.byref(x_post), ty, ny, C.byref(n_y),
+                                     C.byref(g), C.byref(pp)))
+    as_c = lambda a, n: a[: 2 * n].reshape(n, 2) @ np.array([1.0, 1.0j])
+    return {"tw_x": as_c(tx, n_x.value), "x_post": x_post.value, "tw_y": as_c(ty, n_y.value),
+            "rows_per_cta": g.value, "planes_per_cta": pp.value}
 
 
 class B200FrameWarper:

@@ -381,6 +381,16 @@ fa_status fa_test_tr_subproblem(fa_context* ctx, int nD, int n_dim, const double
    cuFFT (use_planes = 0). Lets tests compare both with a CPU DFT. */
 fa_status fa_test_correlation_surface(fa_correlator* c, const float* volume, int use_planes, double* surface);
 
+/* Test hook (no reference counterpart, host only: no device work): the tables and launch shape the
+   fused kx-plane passes would use for an nz x ny x nx volume. tw_x receives n_x complex twiddles
+   (interleaved re, im): the stage twiddles of the nx/2-point row DFT, then W_nx^k for k = 0..nx/2
+   from index x_post; tw_y the stage twiddles of the ny-point DFT (n_y). For every stage after the
+   first (Ns > 1, radix R: radix 8 while at least 3 octaves are left, then 4 or 2), the table holds
+   W_(Ns R)^(r k) at (r - 1) Ns + k, r = 1..R-1, k = 0..Ns-1. FA_ERR_UNSUPPORTED for dimensions that
+   take the cuFFT path. Lets CPU tests check the tables and the pass structure without a GPU. */
+fa_status fa_test_plane_tables(int nz, int ny, int nx, double* tw_x, int cap_x, int* n_x, int* x_post, double* tw_y,
+                               int cap_y, int* n_y, int* rows_per_cta, int* planes_per_cta);
+
 #ifdef __cplusplus
 }
 #endif
