@@ -55,10 +55,10 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-uneven", action="store_true")
-    ap.add_argument("--large", action="store_true", help="also run the 1024x1024x64 volume (minutes of data set-up)")
+    ap.add_argument("--no-large", action="store_true", help="skip the 1024x1024x64 volume")
     ap.add_argument("--large-frames", type=int, default=200)
     ap.add_argument("--large-pool", type=int, default=2)
-    ap.add_argument("--large-cpu", type=int, default=2, help="frames of the large volume solved on the CPU")
+    ap.add_argument("--large-cpu", type=int, default=1, help="frames of the large volume solved on the CPU")
     ap.add_argument("--uneven-pool", type=int, default=4, help="distinct frames per size in the uneven batch")
     ap.add_argument("--only", choices=["roofline"], default=None,
                     help="roofline: only the fused-pass probe on --frames FP16 frames (for ncu captures)")
@@ -163,32 +163,56 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
-def cpu_baseline(acq, n_threads, n_frames):
-    """The reference CPU warper (oracle/_ref, compiled from the reference's FrameWarper.cpp et al.)
-    driving the trust-region solve, one frame per worker thread (FrameAlignerMex.cpp:24-25,120);
-    falls back to the C restatement if the reference build is absent. Rigid shifts are computed
-    before the timed region (numpy FP64 FFT), so the sample times the non-rigid solve only."""
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+
+    return platform.processor() or "unknown"
+
+
+def cpu_baseline(acq, n_threads, n_frames, what="the 512x512x16 nD=32 workload"):
+    """The reference CPU warper (oracle/_ref, compiled from the reference's FrameWarper.cpp,
+    OptimisationModel.cpp et al.) driving the trust-region solve, one frame per worker thread
+    (FrameAlignerMex.cpp:24-25,120). The timing build uses the reference's own release flags
+    (-msse3 -O3 -ffast-math -ftree-vectorize, CMakeLists.txt:17-21); without it the parity build
+    (-O2), without either the C restatement. The trust region is the project's own statement of the
+    algorithm: dlib, whose find_min_trust_region the reference calls, is not in the reference tree.
+    Rigid shifts are computed before the timed region (numpy FP64 FFT), so the sample times the
+    non-rigid solve only."""
     import oracle_py as O
 
     nz, ny, nx = acq.reference.shape
     line, il, ifr = acq.scan
     frames = acq.frames[:n_frames] + 1
     shifts = np.array([O.phase_shift(acq.reference, acq.frames[k]) for k in range(n_frames)])
-    if O.ref_available():
-        pool = O.RefPool(acq.reference + 1, acq.nD, line, il, ifr, n_threads)
+    fast = O.ref_available(fast=True)
+    if fast or O.ref_available():
+        pool = O.RefPool(acq.reference + 1, acq.nD, line, il, ifr, n_threads, fast=fast)
         t0 = time.perf_counter()
         D, iters = pool.align(frames, shifts, 100)
         dt = time.perf_counter() - t0
         kind = "reference"
+        build = ("reference sources, reference release flags -msse3 -O3 -ffast-math -ftree-vectorize" if fast
+                 else "reference sources, -O2 parity build")
     else:
         ow = O.OracleWarper(acq.reference + 1, acq.nD, O.scan_init(line, il, ifr, nx, ny, nz))
         t0 = time.perf_counter()
         D, iters = ow.align_frames_mt(frames, shifts, n_threads, 100)
         dt = time.perf_counter() - t0
         kind = "port"
-    return {"value": n_frames / dt, "unit": UNIT, "cores": n_threads, "kind": kind,
-            "sample": "%d frames of the 512x512x16 nD=32 workload, non-rigid solve only (rigid shifts "
-                      "precomputed), %.1f s, %d threads" % (n_frames, dt, n_threads)}, D, shifts
+        build = "C restatement, -O2"
+    return {"value": n_frames / dt, "unit": UNIT, "cores": n_threads, "kind": kind, "cpu_model": cpu_model(),
+            "build": build,
+            "sample": "%d frames of %s, non-rigid solve only (rigid shifts precomputed), %.1f s, %d threads "
+                      "(one frame per thread); CpuFrameWarper + OptimisationModel from the reference's sources, "
+                      "trust region = the project's statement of the algorithm (dlib absent from the reference "
+                      "tree)" % (n_frames, what, dt, n_threads)}, D, shifts
 
 
 def measure_plain(fa, ctx, acq, scan, pf, local):
@@ -278,20 +302,30 @@ def measure_serving(fa, ctx, args, acqs, pools, lag):
             if d > 2e-4:
                 time.sleep(d - 1e-4)
         j = int(which[i])
-        tickets.append(srv.submit_ptr(ids[j], pools[j][nxt[j] % args.serve_pool].data_ptr(), False))
+        tickets.append((j, srv.submit_ptr(ids[j], pools[j][nxt[j] % args.serve_pool].data_ptr(), False)))
         nxt[j] += 1
     t_sub = time.perf_counter() - t0
     iters = []
-    for t in tickets:
-        _, st, _ = srv.wait(t, 300.0)
+    lat = [[] for _ in range(n_acq)]
+    for j, t in tickets:
+        _, st, ms = srv.wait(t, 300.0)
         iters.append(st["iterations"])
+        lat[j].append(ms)
     stats = srv.stats()
     srv.close()
+    per_acq = []
+    for j, a in enumerate(acqs):
+        nz, ny, nx = a.reference.shape
+        L = np.array(lat[j]) if lat[j] else np.zeros(1)
+        per_acq.append({"acquisition": "%dx%dx%d nD=%d" % (nx, ny, nz, a.nD), "frames": len(lat[j]),
+                        "p50_ms": float(np.percentile(L, 50)), "p99_ms": float(np.percentile(L, 99)),
+                        "max_ms": float(L.max())})
     return {"warm_start_lag": lag, "iterations_per_launch": args.serve_iters, "arrival_rate": args.serve_rate, "arrival_rate_achieved": n / t_sub,
             "frames": n, "p50_ms": stats["p50_ms"], "p99_ms": stats["p99_ms"], "mean_ms": stats["mean_ms"],
             "max_ms": stats["max_ms"], "frames_per_s": stats["frames_per_s"],
             "peak_in_flight": stats["peak_in_flight"], "peak_slot_gb": stats["peak_slot_bytes"] / 1e9,
-            "graph_launches": stats["graph_launches"], "iterations_mean": float(np.mean(iters))}
+            "graph_launches": stats["graph_launches"], "iterations_mean": float(np.mean(iters)),
+            "per_acquisition": per_acq}
 
 
 def measure_uneven(fa, ctx, args):
@@ -351,6 +385,9 @@ def measure_uneven(fa, ctx, args):
                 row["jte_rel_max_start"] = float(np.max(np.abs(g_gpu - g_cpu)) / np.max(np.abs(g_cpu)))
         H_gpu, H_cpu = ref.hessian(), ow.hessian()
         row["hessian_rel_max"] = float(np.max(np.abs(H_gpu - H_cpu)) / np.max(np.abs(H_cpu)))
+        # the served solve of frame 0 against the reference CPU solve of the same frame
+        _, D_cpu, _ = cpu_baseline(a, 1, 1, "%dx%d" % (ny, nx))
+        row["displacement_rms_vs_cpu_px"] = float(np.sqrt(((D_sol - D_cpu[0])[:, :2] ** 2).sum(-1).mean()))
         fr.close()
         ref.close()
         errors.append(row)
@@ -405,7 +442,7 @@ def measure_large(fa, ctx, args, local):
     peak, _ = load_peaks()
     rms = None
     if args.large_cpu > 0:
-        _, D_cpu, _ = cpu_baseline(acq, args.large_cpu, args.large_cpu)  # one thread per frame
+        _, D_cpu, _ = cpu_baseline(acq, args.large_cpu, args.large_cpu, "the 1024x1024x64 nD=64 volume")
         rms = float(np.sqrt(((D[:args.large_cpu] - D_cpu) ** 2).sum(-1).mean()))
     return {"workload": "1024x1024x64 reference, nD = 64, 3 components, %d frames (%d distinct), raw uint16 in HBM, "
                         "calls of %d" % (args.large_frames, args.large_pool, batch),
@@ -581,7 +618,7 @@ def run_ours(args, rank, world, local):
                        "frames_from": "pinned host memory (raw uint16), %d distinct frames per acquisition"
                                       % args.serve_pool,
                        "runs": [measure_serving(fa, ctx, args, sacqs, spools, lag) for lag in args.serve_lags]}
-        large = measure_large(fa, ctx, args, local) if args.large else None
+        large = None if args.no_large else measure_large(fa, ctx, args, local)
         uneven = None
         if not args.no_uneven:
             uneven = measure_uneven(fa, ctx, args)

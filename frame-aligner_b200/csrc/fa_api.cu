@@ -1520,6 +1520,33 @@ extern "C" fa_status fa_test_correlation_surface(fa_correlator* C, const float* 
   return done(FA_OK);
 }
 
+extern "C" fa_status fa_test_downsample(fa_context* ctx, const void* volume, fa_dtype dtype, int nz, int ny, int nx,
+                                        int factor, float* out) {
+  if (!ctx || !volume || !out || nz < 1 || ny < 1 || nx < 1 || factor < 1 || (dtype != FA_F32 && dtype != FA_U16))
+    return fail(FA_ERR_BAD_ARG, "bad arguments");
+  FA_CU(cudaSetDevice(ctx->device));
+  const size_t n_in = (size_t)nz * ny * nx;
+  const size_t n_out = (size_t)nz * ((ny + factor - 1) / factor) * ((nx + factor - 1) / factor);
+  std::vector<Alloc> tmp;
+  auto done = [&](fa_status st) {
+    std::string keep = g_err;
+    dfree_all(ctx, tmp);
+    g_err = keep;
+    return st;
+  };
+  void* d_in;
+  float* d_out;
+  fa_status st;
+  if ((st = dalloc(ctx, n_in * dtype_size(dtype), &d_in, tmp)) != FA_OK) return done(st);
+  if ((st = dalloc_t(ctx, n_out, &d_out, tmp)) != FA_OK) return done(st);
+  cudaError_t e = cudaMemcpy(d_in, volume, n_in * dtype_size(dtype), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = fa::launch_downsample(d_in, dtype, nz, ny, nx, factor, d_out, 0);
+  if (e == cudaSuccess) e = cudaMemcpy(out, d_out, n_out * sizeof(float), cudaMemcpyDeviceToHost);
+  g_launches += 1;
+  if (e != cudaSuccess) return done(fail(FA_ERR_CUDA, std::string("downsample: ") + cudaGetErrorString(e)));
+  return done(FA_OK);
+}
+
 extern "C" fa_status fa_test_tr_subproblem(fa_context* ctx, int nD, int n_dim, const double* H, const double* g,
                                            double radius, double* p, int* on_boundary) {
   if (!ctx || !H || !g || !p || !on_boundary || nD < 1 || (n_dim != 2 && n_dim != 3))
@@ -1962,9 +1989,10 @@ extern "C" fa_status fa_profile_eval(fa_frame* const* frames, int n, const doubl
 
 namespace fa {
 
-fa_status static_eval_prepare(const fa_reference* R, const RefDev** dev, const RefDev** host, int* nD, int* n_dim,
-                              bool* mixed) {
-  if (cudaSetDevice(R->ctx->device) != cudaSuccess) return fail(FA_ERR_CUDA, "cudaSetDevice failed");
+fa_status static_eval_prepare(const fa_reference* R, const double* D, const RefDev** dev, const RefDev** host, int* nD,
+                              int* n_dim, bool* mixed, int* device) {
+  if (!finite_all(D, (size_t)R->nD * 3)) return fail(FA_ERR_BAD_ARG, "D has non-finite entries");
+  *device = R->ctx->device;
   *dev = R->dev;
   *host = &R->host;
   *nD = R->nD;

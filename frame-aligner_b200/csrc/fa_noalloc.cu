@@ -35,8 +35,8 @@ size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
 
 // Internal accessors into fa_api.cu (the reference layout is private to the runtime).
 namespace fa {
-fa_status static_eval_prepare(const fa_reference* ref, const RefDev** dev, const RefDev** host, int* nD, int* n_dim,
-                              bool* mixed);
+fa_status static_eval_prepare(const fa_reference* ref, const double* D, const RefDev** dev, const RefDev** host, int* nD,
+                              int* n_dim, bool* mixed, int* device);
 fa_status static_eval_fail(fa_status s, const char* msg);
 void static_eval_dparams(const double* D, int nD, int n_dim, float4* out);
 void static_eval_count_launches(int n);
@@ -48,8 +48,9 @@ extern "C" fa_status fa_get_error_jacobian_static(const fa_reference* ref, const
   const fa::RefDev* host = nullptr;
   int nD = 0, n_dim = 0;
   bool mixed = false;
+  int device = 0;
   if (!ref || !frame_device || !D || !f || !jac) return fa::static_eval_fail(FA_ERR_BAD_ARG, "NULL argument");
-  fa_status st = fa::static_eval_prepare(ref, &dev, &host, &nD, &n_dim, &mixed);
+  fa_status st = fa::static_eval_prepare(ref, D, &dev, &host, &nD, &n_dim, &mixed, &device);
   if (st != FA_OK) return st;
   if (dtype != (mixed ? FA_F16 : FA_F32))
     return fa::static_eval_fail(FA_ERR_BAD_ARG, mixed ? "a mixed-precision reference needs FA_F16 frames"
@@ -66,9 +67,16 @@ extern "C" fa_status fa_get_error_jacobian_static(const fa_reference* ref, const
                   host->n_tiles, kStaticScratchBytes);
     return fa::static_eval_fail(FA_ERR_BAD_ARG, m);
   }
-  int device = 0;
-  if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kMaxDevices)
-    return fa::static_eval_fail(FA_ERR_CUDA, "cudaGetDevice failed");
+  if (device < 0 || device >= kMaxDevices) return fa::static_eval_fail(FA_ERR_BAD_ARG, "device ordinal out of range");
+  // The work runs with the reference's device current; the caller's current device is restored on
+  // every return.
+  int caller_device = -1;
+  if (cudaGetDevice(&caller_device) != cudaSuccess) return fa::static_eval_fail(FA_ERR_CUDA, "cudaGetDevice failed");
+  struct RestoreDevice {
+    int d;
+    ~RestoreDevice() { cudaSetDevice(d); }
+  } restore{caller_device};
+  if (cudaSetDevice(device) != cudaSuccess) return fa::static_eval_fail(FA_ERR_CUDA, "cudaSetDevice failed");
   char* base = nullptr;
   {
     std::lock_guard<std::mutex> lk(g_mu);
@@ -114,8 +122,12 @@ extern "C" fa_status fa_get_error_jacobian_static(const fa_reference* ref, const
                    cudaMemcpyHostToDevice);
   }
   const fa::Job* jd = reinterpret_cast<const fa::Job*>(base);
-  if (e == cudaSuccess) e = fa::launch_eval(jd, 1, host->n_tiles, n_dim, dtype == FA_F16 ? fa::kFrameF16 : fa::kFrameF32, mixed, 0,
-                           host->nx % 4 == 0 && (reinterpret_cast<uintptr_t>(frame_device) & 15u) == 0);
+  // The four-voxels-per-lane kernel needs rows of a multiple of 4 voxels and a 16-byte aligned frame;
+  // it runs with the register budget the reference's tile shape was tuned for.
+  const bool vec4 = host->nx % 4 == 0 && (reinterpret_cast<uintptr_t>(frame_device) & 15u) == 0;
+  if (e == cudaSuccess)
+    e = fa::launch_eval(jd, 1, host->n_tiles, n_dim, dtype == FA_F16 ? fa::kFrameF16 : fa::kFrameF32, mixed, 0, vec4,
+                        host->tune_mb);
   if (e == cudaSuccess) e = fa::launch_reduce(jd, *host, 0);
   if (e == cudaSuccess) e = cudaMemcpy(f, job.result, sizeof(double), cudaMemcpyDeviceToHost);
   if (e == cudaSuccess) e = cudaMemcpy(jac, job.result + 1, (size_t)P * sizeof(double), cudaMemcpyDeviceToHost);

@@ -180,6 +180,7 @@ SIGNATURES = {
     "fa_profile_eval": [_vp, C.c_int, _f64p, C.c_int, C.POINTER(C.c_double)],
     "fa_test_tr_subproblem": [_vp, C.c_int, C.c_int, _f64p, _f64p, C.c_double, _f64p, C.POINTER(C.c_int)],
     "fa_test_correlation_surface": [_vp, _f32p, C.c_int, _f64p],
+    "fa_test_downsample": [_vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _f32p],
     "fa_test_plane_tables": [C.c_int, C.c_int, C.c_int, _f64p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                              _f64p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)],
 }
@@ -636,6 +637,18 @@ def test_tr_subproblem(ctx: Context, nD, n_dim, H, g, radius):
     b = C.c_int()
     check(lib().fa_test_tr_subproblem(ctx._h, nD, n_dim, _c64(H), _c64(g), radius, p, C.byref(b)))
     return p, bool(b.value)
+
+
+def test_downsample(ctx: Context, volume, factor):
+    """fa_test_downsample: the device downsample (AbstractFrameAligner.cpp:37-56) of a float32 or
+    uint16 volume (nz, ny, nx)."""
+    v = np.ascontiguousarray(volume)
+    if v.dtype not in (np.float32, np.uint16):
+        v = v.astype(np.float32)
+    nz, ny, nx = v.shape
+    out = np.empty(nz * (-(-ny // factor)) * (-(-nx // factor)), np.float32)
+    check(lib().fa_test_downsample(ctx._h, v.ctypes.data, _DTYPES[v.dtype], nz, ny, nx, factor, out))
+    return out.reshape(nz, -(-ny // factor), -(-nx // factor))
 
 
 def plane_tables(nz, ny, nx):

@@ -346,10 +346,12 @@ fa_status fa_server_reset_stats(fa_server* s);
    library, which each GPU that loads the library holds until exit. The call allocates no device or
    host memory; it runs on the legacy default stream and returns when f (host double) and jac (P host
    doubles) are written. Volumes whose scratch would exceed 2 MiB (about 21,000 tiles of the fused
-   pass) are rejected with FA_ERR_BAD_ARG. The first call on each device looks up the array's device
-   address (cudaGetSymbolAddress) with that device current; make it before any stream capture. All
-   calls share the array, so calls that overlap on the GPU (other threads, other streams) race and
-   must be serialised by the caller. */
+   pass) are rejected with FA_ERR_BAD_ARG, and so is a D with a non-finite entry. The work runs on the
+   reference's device; the caller's current device is restored before the call returns. The first
+   call on each device looks up the array's device address (cudaGetSymbolAddress) with that device
+   current; make it before any stream capture (a cudaDeviceReset invalidates that address together
+   with every other handle of this library). All calls share the array, so calls that overlap on the
+   GPU (other threads, other streams) race and must be serialised by the caller. */
 fa_status fa_get_error_jacobian_static(const fa_reference* ref, const void* frame_device, fa_dtype dtype,
                                        const double* D, double* f, double* jac);
 
@@ -373,6 +375,15 @@ fa_status fa_profile_eval(fa_frame* const* frames, int n, const double* D, int l
    CPU statement of the same algorithm on identical inputs. */
 fa_status fa_test_tr_subproblem(fa_context* ctx, int nD, int n_dim, const double* H, const double* g, double radius,
                                 double* p, int* on_boundary);
+
+/* Test hook (no reference counterpart): the device form of downsample (FrameAligner/
+   AbstractFrameAligner.cpp:37-56) that the aligner applies before phase correlation when
+   spatial_binning > 1 -- each output voxel (z, y / factor, x / factor) is the float sum of its
+   factor x factor block, ceil-sized, the last block of a row or column ragged. volume: host memory,
+   nz*ny*nx elements of dtype (FA_F32 or FA_U16); out: host memory, nz*ceil(ny/factor)*ceil(nx/factor)
+   floats. Lets tests compare the kernel with the reference's loop bit for bit. */
+fa_status fa_test_downsample(fa_context* ctx, const void* volume, fa_dtype dtype, int nz, int ny, int nx, int factor,
+                             float* out);
 
 /* Test hook (no reference counterpart): the phase-correlation surface of one FP32 volume (host
    memory, nz*ny*nx) against the correlator's reference -- the unnormalised inverse DFT of the

@@ -51,7 +51,7 @@ class OrStats(C.Structure):
 
 
 _lib = None
-_ref = None
+_ref = {}
 
 
 def lib():
@@ -91,14 +91,19 @@ def lib():
     return _lib
 
 
-def ref_available() -> bool:
-    return os.path.exists(os.path.join(HERE, "_ref", "libfa_ref.so"))
+def _ref_path(fast=False):
+    return os.path.join(HERE, "_ref", "libfa_ref_fast.so" if fast else "libfa_ref.so")
 
 
-def reflib():
-    global _ref
-    if _ref is None:
-        path = os.path.join(HERE, "_ref", "libfa_ref.so")
+def ref_available(fast=False) -> bool:
+    """The reference build is present: the parity build (-O2, no fused multiply-add) or, with
+    fast=True, the timing build with the reference's release flags."""
+    return os.path.exists(_ref_path(fast))
+
+
+def reflib(fast=False):
+    if fast not in _ref:
+        path = _ref_path(fast)
         if not os.path.exists(path):
             raise RuntimeError(f"reference build missing: {path}")
         R = C.CDLL(path)
@@ -126,8 +131,8 @@ def reflib():
                                    C.c_int, C.c_int, C.c_char_p]
         R.fr_mt_destroy.argtypes = [C.c_void_p]
         R.fr_mt_align.argtypes = [C.c_void_p, _f32p, C.c_int, _f64p, C.c_int, _f64p, _i32p]
-        _ref = R
-    return _ref
+        _ref[fast] = R
+    return _ref[fast]
 
 
 def scan_init(line, interline, interframe, nx, ny, nz, bidirectional=False) -> OrScan:
@@ -309,21 +314,23 @@ class RefWarper:
 
 
 class RefPool:
-    """One reference warper per worker thread (fr_mt_create / fr_mt_align)."""
+    """One reference warper per worker thread (fr_mt_create / fr_mt_align); fast=True uses the timing
+    build (the reference's release flags)."""
 
-    def __init__(self, reference, nD, line, interline, interframe, n_threads, bidirectional=False):
+    def __init__(self, reference, nD, line, interline, interframe, n_threads, bidirectional=False, fast=False):
         ref = _c32(reference)
         self.dims = ref.shape
         self.nD = nD
+        self.fast = fast
         err = C.create_string_buffer(256)
-        self._h = reflib().fr_mt_create(ref, ref.shape[0], ref.shape[1], ref.shape[2], nD, line, interline,
-                                        interframe, int(bidirectional), n_threads, err)
+        self._h = reflib(fast).fr_mt_create(ref, ref.shape[0], ref.shape[1], ref.shape[2], nD, line, interline,
+                                            interframe, int(bidirectional), n_threads, err)
         if not self._h:
             raise RuntimeError(err.value.decode())
 
     def __del__(self):
         if getattr(self, "_h", None):
-            reflib().fr_mt_destroy(self._h)
+            reflib(self.fast).fr_mt_destroy(self._h)
             self._h = None
 
     def align(self, frames, rigid_shifts, max_iter=100):
@@ -331,7 +338,7 @@ class RefPool:
         n = frames.shape[0]
         D = np.empty((n, self.nD, 3), np.float64)
         iters = np.empty(n, np.int32)
-        reflib().fr_mt_align(self._h, frames.ravel(), n, _c64(rigid_shifts).ravel(), max_iter, D, iters)
+        reflib(self.fast).fr_mt_align(self._h, frames.ravel(), n, _c64(rigid_shifts).ravel(), max_iter, D, iters)
         return D, iters
 
 
@@ -369,6 +376,71 @@ def downsample(vol, factor):
 def correlation(a, b, mask):
     a = _c32(a).ravel()
     return lib().or_correlation(a, _c32(b).ravel(), np.ascontiguousarray(mask, np.uint8).ravel(), a.size)
+
+
+def round_bf16(a):
+    """float32 -> bfloat16 -> float32, round to nearest even (the conversion the device uses for the
+    mixed-precision reference and gradient copies); finite inputs only."""
+    b = np.ascontiguousarray(a, np.float32).view(np.uint32).astype(np.uint64)
+    r = ((b + 0x7FFF + ((b >> 16) & 1)) & 0xFFFF0000).astype(np.uint32)
+    return r.view(np.float32)
+
+
+def fp64_error_jacobian(ow, reference, gradient, frame, D):
+    """One evaluation of the warper's objective and gradient with every product and sum in double,
+    on explicitly given stored values (reference, gradient (gx, gy, gz) and frame, e.g. rounded to
+    BF16 / FP16), for measuring the error of a reduced-precision evaluation:
+
+      * d(x) = Df D[Di+1] + (1 - Df) D[Di] from the restated interval tables (warpPoint,
+        FrameWarper.cpp:397-419);
+      * the zero-padded trilinear (bilinear for one plane) sample at x + d (warpImageInterpolated,
+        FrameWarper.cpp:31-69; getZeroPadded, FrameWarper.h:39-47);
+      * e = sample - reference where the sample is positive, else 0 (computeErrorImage,
+        FrameWarper.cpp:4-29; the GPU mask v != 0, GpuFrameWarperKernels.cu:216-218); f = sum e^2;
+      * g[k] = sum over storage range k-1 of grad Df e + sum over range k of grad (1 - Df) e, each range
+        without its last voxel (computeSteepestDecentImages, FrameWarper.cpp:296-345, and
+        computeJacobian, FrameWarper.cpp:147-167).
+
+    Returns (f, g) with g in OptimisationModel's parameter order (P doubles)."""
+    nz, ny, nx = ow.dims
+    nd = ow.n_dim
+    Di, Df, rng = ow.precomp()
+    Di = Di.astype(np.int64).ravel()
+    Df = Df.astype(np.float64).ravel()
+    D = np.asarray(D, np.float64).reshape(ow.nD, 3)
+    d = Df[:, None] * D[Di + 1] + (1.0 - Df[:, None]) * D[Di]
+    z, y, x = (a.ravel() for a in np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij"))
+    lx, ly = x + d[:, 0], y + d[:, 1]
+    lz = z + d[:, 2] if nd == 3 else z.astype(np.float64)
+    x0, y0, z0 = np.floor(lx), np.floor(ly), np.floor(lz)
+    fx, fy, fz = lx - x0, ly - y0, lz - z0
+    x0, y0, z0 = x0.astype(np.int64), y0.astype(np.int64), z0.astype(np.int64)
+    img = np.asarray(frame, np.float64).reshape(nz, ny, nx)
+
+    def tap(zz, yy, xx):
+        ok = (xx >= 0) & (xx < nx) & (yy >= 0) & (yy < ny) & ((zz >= 0) & (zz < nz) if nd == 3 else True)
+        v = img[np.clip(zz, 0, nz - 1), np.clip(yy, 0, ny - 1), np.clip(xx, 0, nx - 1)]
+        return np.where(ok, v, 0.0)
+
+    def plane(zz):
+        return ((tap(zz, y0, x0) * (1 - fx) + tap(zz, y0, x0 + 1) * fx) * (1 - fy) +
+                (tap(zz, y0 + 1, x0) * (1 - fx) + tap(zz, y0 + 1, x0 + 1) * fx) * fy)
+
+    val = plane(z0) if nd == 2 else plane(z0) * (1 - fz) + plane(z0 + 1) * fz
+    e = np.where(val > 0, val - np.asarray(reference, np.float64).ravel(), 0.0)
+    f = float(np.sum(e * e))
+    grads = [np.asarray(g_, np.float64).ravel() for g_ in gradient[:nd]]
+    g = np.zeros(ow.nD * nd)
+    for k in range(ow.nD):
+        for kk, w in ((k - 1, Df), (k, 1.0 - Df)):
+            if kk < 0 or kk >= ow.nD - 1:
+                continue
+            b, en = int(rng[kk, 0]), int(rng[kk, 1])
+            sl = slice(b, en)
+            we = w[sl] * e[sl]
+            for c in range(nd):
+                g[k * nd + c] += float(np.dot(grads[c][sl], we))
+    return f, g
 
 
 def tr_subproblem(H, g, radius, eps=0.1, max_iter=20):

@@ -153,3 +153,32 @@ def test_smoothing_statement():
         assert len(k) == n and np.array_equal(k, k[::-1]) and abs(float(k.sum()) - 1) < 1e-6
     c = np.full((2, 17, 23), 7.0, np.float32)
     assert np.allclose(O.smooth_stack(c, 1.7), 7.0, rtol=1e-6, atol=0)
+
+
+@pytest.mark.parametrize("shape,nD", [((1, 64, 80), 8), ((4, 48, 64), 9)])
+def test_fp64_statement_matches_oracle(shape, nD):
+    """The FP64 statement of one evaluation (oracle_py.fp64_error_jacobian, the yardstick of the
+    mixed-precision reduction-error tests) agrees with the restated warper's float evaluation
+    (pinned bit for bit to the reference above) to float rounding: f 1e-6 relative, J^T e 1e-5 of
+    max|J^T e|."""
+    acq = S.make_acquisition(shape, nD, 1, S.BlobSpec(40, (2.0, 6.0), (1.0, 2.0)), S.WalkSpec(1.0, 3.0, 0.2, 0.8),
+                             seed=5)
+    nz, ny, nx = shape
+    line, il, ifr = acq.scan
+    ow = O.OracleWarper(acq.reference + 1, nD, O.scan_init(line, il, ifr, nx, ny, nz))
+    fr = (acq.frames[0] + 1).astype(np.float32)
+    for D in (np.zeros((nD, 3)), acq.D_true[0].copy()):
+        if nz == 1:
+            D[:, 2] = 0.0
+        f64, g64 = O.fp64_error_jacobian(ow, acq.reference + 1, ow.gradient(), fr, D)
+        f, e = ow.get_error(fr, D, want_image=True)
+        g = ow.get_jacobian_from_error(e)
+        assert abs(f64 - f) <= 1e-6 * f
+        assert np.max(np.abs(g64 - g)) <= 1e-5 * np.max(np.abs(g))
+
+
+def test_round_bf16():
+    """round_bf16: round to nearest, ties to even, on the 16 dropped bits."""
+    bits = np.array([0x3F800000, 0x3F808000, 0x3F818000, 0x3F807FFF, 0x3F808001, 0xBF80C000], np.uint32)
+    want = np.array([0x3F800000, 0x3F800000, 0x3F820000, 0x3F800000, 0x3F810000, 0xBF810000], np.uint32)
+    assert np.array_equal(O.round_bf16(bits.view(np.float32)).view(np.uint32), want)
