@@ -313,6 +313,88 @@ class RefWarper:
         return D, int(it[0])
 
 
+_adaptor = None
+
+
+def adaptor_available() -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "libfa_adaptor.so"))
+
+
+def adaptorlib():
+    """_ref/libfa_adaptor.so: the drop-in B200FrameWarper driven by the reference's own
+    FrameWarper.cpp / OptimisationModel.cpp (ref_adaptor.cpp)."""
+    global _adaptor
+    if _adaptor is None:
+        path = os.path.join(HERE, "_ref", "libfa_adaptor.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"adaptor build missing: {path}")
+        A = C.CDLL(path)
+        A.fa_adaptor_gpu_support.argtypes = [C.c_char_p, C.c_int]
+        A.fa_adaptor_create.restype = C.c_void_p
+        A.fa_adaptor_create.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                        C.c_double, C.c_int, C.c_int, C.c_char_p]
+        A.fa_adaptor_destroy.argtypes = [C.c_void_p]
+        A.fa_adaptor_n_dim.argtypes = [C.c_void_p]
+        A.fa_adaptor_set_frame.argtypes = [C.c_void_p, _f32p, C.c_char_p]
+        A.fa_adaptor_model.argtypes = [C.c_void_p, _f64p, C.POINTER(C.c_double), _f64p, _f64p, C.c_char_p]
+        A.fa_adaptor_warp.argtypes = [C.c_void_p, _f64p, C.c_int, _f32p, C.c_char_p]
+        A.fa_adaptor_align.argtypes = [C.c_void_p, _f64p, C.c_int, _f64p, C.POINTER(C.c_int), C.c_char_p]
+        _adaptor = A
+    return _adaptor
+
+
+class AdaptorWarper:
+    """B200FrameWarper (frame-aligner_b200/adaptor/B200FrameWarper.h) behind the reference's
+    AbstractFrameWarper::setReference and OptimisationModel."""
+
+    def __init__(self, reference, nD, line, interline, interframe, bidirectional=False, precision=0):
+        ref = _c32(reference)
+        self.dims = ref.shape
+        self.nD = nD
+        err = C.create_string_buffer(256)
+        self._h = adaptorlib().fa_adaptor_create(ref, ref.shape[0], ref.shape[1], ref.shape[2], nD, line, interline,
+                                                 interframe, int(bidirectional), int(precision), err)
+        if not self._h:
+            raise RuntimeError(err.value.decode())
+        self.n_dim = adaptorlib().fa_adaptor_n_dim(self._h)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            adaptorlib().fa_adaptor_destroy(self._h)
+            self._h = None
+
+    def _ok(self, rc, err):
+        if rc != 0:
+            raise RuntimeError(err.value.decode())
+
+    def set_frame(self, frame):
+        err = C.create_string_buffer(256)
+        self._ok(adaptorlib().fa_adaptor_set_frame(self._h, _c32(frame).ravel(), err), err)
+
+    def model(self, D):
+        """(f, der, hess) as OptimisationModel reads them through the adaptor."""
+        P = self.nD * self.n_dim
+        f = C.c_double()
+        der = np.empty(P, np.float64)
+        hess = np.empty((P, P), np.float64)
+        err = C.create_string_buffer(256)
+        self._ok(adaptorlib().fa_adaptor_model(self._h, _c64(D).ravel(), C.byref(f), der, hess, err), err)
+        return f.value, der, hess
+
+    def warp_interpolated(self, D, invalid_value=0):
+        out = np.empty(int(np.prod(self.dims)), np.float32)
+        err = C.create_string_buffer(256)
+        self._ok(adaptorlib().fa_adaptor_warp(self._h, _c64(D).ravel(), int(invalid_value), out, err), err)
+        return out.reshape(self.dims)
+
+    def align(self, rigid_shift=(0.0, 0.0, 0.0), max_iter=100):
+        D = np.zeros((self.nD, 3), np.float64)
+        it = C.c_int()
+        err = C.create_string_buffer(256)
+        self._ok(adaptorlib().fa_adaptor_align(self._h, _c64(rigid_shift), max_iter, D, C.byref(it), err), err)
+        return D, it.value
+
+
 class RefPool:
     """One reference warper per worker thread (fr_mt_create / fr_mt_align); fast=True uses the timing
     build (the reference's release flags)."""

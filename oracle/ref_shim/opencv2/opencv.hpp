@@ -123,6 +123,7 @@ class Mat {
   size_t elemSize() const { return elemSizeOf(type_); }
   size_t total() const { return total_; }
   bool empty() const { return data == nullptr || total_ == 0; }
+  bool isContinuous() const { return true; }  // this stand-in only holds dense storage
 
   Mat clone() const {
     Mat m;

@@ -8,10 +8,11 @@ Tolerances (stated per quantity):
   * reduction error of one evaluation, against an FP64 statement of the same evaluation
     (oracle_py.fp64_error_jacobian):
       - summation only (the FP64 statement fed the very values the device stores: BF16 reference and
-        gradient, FP16 frame): f relative 5e-6, J^T e 5e-5 of max|J^T e|. The device sums up to 64
-        voxel terms per lane in FP32 (fused multiply-add), then pairwise across the 32 lanes of a warp
-        (shuffle tree), then in FP64 across tiles: blocked pairwise summation, whose error grows with
-        the block length (64), not with the voxel count;
+        gradient, FP16 frame): f relative 5e-6, J^T e 5e-5 of max|J^T e|. The device sums the terms
+        of one lane of one tile in FP32 (fused multiply-add; tile voxels / 32 terms, 128 for the
+        default 4096-voxel tiles), then pairwise across the 32 lanes of a warp (shuffle tree), then
+        in FP64 across tiles: blocked pairwise summation, whose error grows with the block length,
+        not with the voxel count;
       - storage included (the FP64 statement on the FP32 reference, gradient and frame): f relative
         1e-3, J^T e 2e-3 of max|J^T e| (BF16 keeps 8 significant bits of each reference and gradient
         value);
