@@ -69,6 +69,9 @@ def parse():
     ap.add_argument("--serve-iters", type=int, default=4, help="trust-region iterations per serving graph launch")
     ap.add_argument("--serve-lags", type=int, nargs="+", default=[1, 4],
                     help="warm-start lags to serve with (1 = the previous frame's solution)")
+    ap.add_argument("--capacity-rates", type=float, nargs="*", default=[4000.0, 8000.0, 16000.0],
+                    help="offered rates of the saturation sweep (lag 4, --capacity-seconds each)")
+    ap.add_argument("--capacity-seconds", type=float, default=1.0)
     return ap.parse_args()
 
 
@@ -262,6 +265,25 @@ def serving_data(args):
     pools = [torch.from_numpy(np.ascontiguousarray(a.frames.astype(np.uint16)).view(np.int16)).pin_memory()
              for a in acqs]
     return acqs, pools
+
+
+def measure_capacity(fa, ctx, args, acqs, pools, lag=4):
+    """Saturation sweep of the served stream: the same eight acquisitions at rising offered rates;
+    the loop's capacity is the highest completed rate, reached where throughput stops tracking the
+    offered rate."""
+    import copy
+
+    rows = []
+    for rate in args.capacity_rates:
+        a = copy.copy(args)
+        a.serve_rate = rate
+        a.serve_seconds = args.capacity_seconds
+        r = measure_serving(fa, ctx, a, acqs, pools, lag)
+        rows.append({"offered": rate, "arrival_rate_achieved": r["arrival_rate_achieved"],
+                     "frames_per_s": r["frames_per_s"], "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"],
+                     "peak_in_flight": r["peak_in_flight"]})
+    return {"warm_start_lag": lag, "seconds_per_rate": args.capacity_seconds, "sweep": rows,
+            "capacity_frames_per_s": max(r["frames_per_s"] for r in rows) if rows else None}
 
 
 def measure_serving(fa, ctx, args, acqs, pools, lag):
@@ -617,7 +639,8 @@ def run_ours(args, rank, world, local):
                        "memory_budget_gb": 40 * 2 ** 30 / 1e9,
                        "frames_from": "pinned host memory (raw uint16), %d distinct frames per acquisition"
                                       % args.serve_pool,
-                       "runs": [measure_serving(fa, ctx, args, sacqs, spools, lag) for lag in args.serve_lags]}
+                       "runs": [measure_serving(fa, ctx, args, sacqs, spools, lag) for lag in args.serve_lags],
+                       "capacity": measure_capacity(fa, ctx, args, sacqs, spools) if args.capacity_rates else None}
         large = None if args.no_large else measure_large(fa, ctx, args, local)
         uneven = None
         if not args.no_uneven:

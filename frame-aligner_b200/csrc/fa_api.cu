@@ -545,19 +545,10 @@ fa_status reference_setup(fa_reference* R, const float* src, bool src_device) {
   h.Hd = Hd;
   h.Hl = Hl;
   if (R->prec == FA_PREC_MIXED) {
-    __nv_bfloat16 *r16, *x16, *y16, *z16;
-    FA_TRY(dalloc_t(ctx, (size_t)N, &r16, R->allocs));
-    FA_TRY(dalloc_t(ctx, (size_t)N, &x16, R->allocs));
-    FA_TRY(dalloc_t(ctx, (size_t)N, &y16, R->allocs));
-    FA_TRY(dalloc_t(ctx, (size_t)N, &z16, R->allocs));
-    FA_CU(fa::launch_to_bf16(ref32, r16, N, s));
-    FA_CU(fa::launch_to_bf16(gx, x16, N, s));
-    FA_CU(fa::launch_to_bf16(gy, y16, N, s));
-    FA_CU(fa::launch_to_bf16(gz, z16, N, s));
-    h.ref16 = r16;
-    h.gx16 = x16;
-    h.gy16 = y16;
-    h.gz16 = z16;
+    __nv_bfloat16* q16;
+    FA_TRY(dalloc_t(ctx, (size_t)((N + 3) / 4) * 16, &q16, R->allocs));
+    FA_CU(fa::launch_to_quad16(ref32, gx, gy, gz, N, q16, s));
+    h.q16 = q16;
   }
   FA_CU(cudaMemcpyAsync(R->dev, &h, sizeof(RefDev), cudaMemcpyHostToDevice, s));
   const fa_scan_params p = process_scan(R->scan, R->nz, R->nD);
@@ -1212,10 +1203,13 @@ fa_status correlator_enqueue(fa_correlator* C, const void* const* vols, int in_k
     if (planes) {
       const int nb = fa::plane_blocks_per_frame(C->pd);
       FA_CU(fa::launch_plane_rows_fwd(C->pd, d_ptrs + c0, in_kind, m, C->wy, C->wx, C->tw_x, C->spec, C->stream));
-      FA_CU(fa::launch_plane_yz(C->pd, C->spec, C->spec, C->ref_conj, C->tw_y, m, false, C->stream));
+      if (C->pd.split)
+        FA_CU(fa::launch_plane_yz_split(C->pd, C->spec, C->ref_conj, C->tw_y, C->tw_z, m, false, C->stream));
+      else
+        FA_CU(fa::launch_plane_yz(C->pd, C->spec, C->spec, C->ref_conj, C->tw_y, m, false, C->stream));
       FA_CU(fa::launch_plane_rows_inv_argmax(C->pd, C->spec, m, C->tw_x, C->bval, C->bidx, surf, C->stream));
       FA_CU(fa::launch_phase_argmax_final(C->bval, C->bidx, nb, m, d_idx + c0, C->stream));
-      g_launches += 4;
+      g_launches += C->pd.split ? 6 : 4;
     } else {
       cufftHandle fwd, inv;
       FA_TRY(correlator_plans(C, m, &fwd, &inv));
@@ -1389,17 +1383,24 @@ fa_status correlator_create_impl(fa_context* ctx, const void* reference, bool re
   if (cudaMemcpyAsync(C->d_ptrs, C->h_ptrs, sizeof(void*), cudaMemcpyHostToDevice, C->stream) != cudaSuccess)
     return cleanup(fail(FA_ERR_CUDA, "pointer upload"));
   if (C->planes) {
-    std::vector<double2> tx, ty;
-    fa::plane_twiddles(C->pd, &tx, &ty);
+    std::vector<double2> tx, ty, tz;
+    fa::plane_twiddles(C->pd, &tx, &ty, &tz);
     if ((st = dalloc_t(ctx, tx.size(), &C->tw_x, C->allocs)) != FA_OK) return cleanup(st);
     if ((st = dalloc_t(ctx, ty.size(), &C->tw_y, C->allocs)) != FA_OK) return cleanup(st);
+    if ((st = dalloc_t(ctx, std::max<size_t>(tz.size(), 1), &C->tw_z, C->allocs)) != FA_OK) return cleanup(st);
     if (cudaMemcpy(C->tw_x, tx.data(), tx.size() * sizeof(double2), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(C->tw_y, ty.data(), ty.size() * sizeof(double2), cudaMemcpyHostToDevice) != cudaSuccess)
+        cudaMemcpy(C->tw_y, ty.data(), ty.size() * sizeof(double2), cudaMemcpyHostToDevice) != cudaSuccess ||
+        (!tz.empty() &&
+         cudaMemcpy(C->tw_z, tz.data(), tz.size() * sizeof(double2), cudaMemcpyHostToDevice) != cudaSuccess))
       return cleanup(fail(FA_ERR_CUDA, "twiddle upload"));
-    if (fa::launch_plane_rows_fwd(C->pd, C->d_ptrs, FA_F32, 1, C->wy, C->wx, C->tw_x, C->spec, C->stream) !=
-            cudaSuccess ||
-        fa::launch_plane_yz(C->pd, C->spec, C->ref_conj, nullptr, C->tw_y, 1, true, C->stream) != cudaSuccess)
-      return cleanup(fail(FA_ERR_CUDA, "reference spectrum"));
+    const cudaError_t e_fwd =
+        fa::launch_plane_rows_fwd(C->pd, C->d_ptrs, FA_F32, 1, C->wy, C->wx, C->tw_x, C->spec, C->stream);
+    const cudaError_t e_yz =
+        e_fwd != cudaSuccess ? e_fwd
+        : C->pd.split
+            ? fa::launch_plane_yz_split(C->pd, C->spec, C->ref_conj, C->tw_y, C->tw_z, 1, true, C->stream)
+            : fa::launch_plane_yz(C->pd, C->spec, C->ref_conj, nullptr, C->tw_y, 1, true, C->stream);
+    if (e_yz != cudaSuccess) return cleanup(fail(FA_ERR_CUDA, "reference spectrum"));
   } else {
     cufftHandle fwd1, inv1;
     if ((st = correlator_plans(C, 1, &fwd1, &inv1)) != FA_OK) return cleanup(st);
@@ -1473,8 +1474,8 @@ extern "C" fa_status fa_test_plane_tables(int nz, int ny, int nx, double* tw_x, 
     return fail(FA_ERR_BAD_ARG, "NULL argument");
   fa::PlaneDims d{};
   if (!fa::plane_dims(nz, ny, nx, &d)) return fail(FA_ERR_UNSUPPORTED, "dimensions outside the fused plane passes");
-  std::vector<double2> tx, ty;
-  fa::plane_twiddles(d, &tx, &ty);
+  std::vector<double2> tx, ty, tz;
+  fa::plane_twiddles(d, &tx, &ty, &tz);
   if ((int)tx.size() != d.n_twx || (int)ty.size() != d.n_twy) return fail(FA_ERR_STATE, "twiddle table size");
   if ((int)tx.size() > cap_x || (int)ty.size() > cap_y) return fail(FA_ERR_BAD_ARG, "output arrays too small");
   for (size_t i = 0; i < tx.size(); i++) {

@@ -21,7 +21,7 @@ namespace fa {
 
 namespace {
 
-// Four consecutive reference / gradient values starting at a multiple of 4.
+// Four consecutive FP32 reference / gradient values starting at a multiple of 4.
 __device__ __forceinline__ void load4(const float* p, float* v) {
   const float4 a = __ldg(reinterpret_cast<const float4*>(p));
   v[0] = a.x;
@@ -29,13 +29,43 @@ __device__ __forceinline__ void load4(const float* p, float* v) {
   v[2] = a.z;
   v[3] = a.w;
 }
-__device__ __forceinline__ void load4(const __nv_bfloat16* p, float* v) {
-  const uint2 a = __ldg(reinterpret_cast<const uint2*>(p));
-  v[0] = __uint_as_float(a.x << 16);
-  v[1] = __uint_as_float(a.x & 0xffff0000u);
-  v[2] = __uint_as_float(a.y << 16);
-  v[3] = __uint_as_float(a.y & 0xffff0000u);
-}
+
+// The reference and gradient values of four consecutive voxels starting at a multiple of 4: four
+// FP32 planes, or the BF16 groups of RefDev::q16 (two 16-byte loads for all four quantities).
+template <typename RT>
+struct RefGradSrc;
+template <>
+struct RefGradSrc<float> {
+  const float* r;
+  const float* g[3];
+  __device__ explicit RefGradSrc(const RefDev& R) : r(R.ref32), g{R.gx32, R.gy32, R.gz32} {}
+  template <int NDIM>
+  __device__ __forceinline__ void load(long long p0, float* t4, float (*g4)[4]) const {
+    load4(r + p0, t4);
+#pragma unroll
+    for (int k = 0; k < NDIM; k++) load4(g[k] + p0, g4[k]);
+  }
+};
+template <>
+struct RefGradSrc<__nv_bfloat16> {
+  const __nv_bfloat16* q;
+  __device__ explicit RefGradSrc(const RefDev& R) : q(R.q16) {}
+  template <int NDIM>
+  __device__ __forceinline__ void load(long long p0, float* t4, float (*g4)[4]) const {
+    const uint4* b = reinterpret_cast<const uint4*>(q + (p0 >> 2) * 16);
+    const uint4 a = __ldg(b), c = __ldg(b + 1);
+    auto unpack = [](unsigned lo, unsigned hi, float* v) {
+      v[0] = __uint_as_float(lo << 16);
+      v[1] = __uint_as_float(lo & 0xffff0000u);
+      v[2] = __uint_as_float(hi << 16);
+      v[3] = __uint_as_float(hi & 0xffff0000u);
+    };
+    unpack(a.x, a.y, t4);
+    unpack(a.z, a.w, g4[0]);
+    unpack(c.x, c.y, g4[1]);
+    if (NDIM == 3) unpack(c.z, c.w, g4[NDIM == 3 ? 2 : 0]);
+  }
+};
 
 // Five consecutive frame values v[k] = p[s + k], k = 0..4, from the aligned 8-element window at p
 // (p is 8-element aligned in FP16 units or 4-element aligned in FP32 units; s in [0, 3]).
@@ -98,11 +128,289 @@ __device__ __forceinline__ void masked5(const FT* row, bool row_valid, int ix, i
 
 }  // namespace
 
+// Frame values v[k] = p[S + k], k = 0..4, from the aligned 8-element window at p, for an alignment
+// S that is the same for every lane of the warp (known at compile time: no shifts or selects).
+template <int S>
+__device__ __forceinline__ void window5s(const RawU16* p, float* v) {
+  const uint2 lo = __ldg(reinterpret_cast<const uint2*>(p));
+  const uint2 hi = __ldg(reinterpret_cast<const uint2*>(p + 4));
+  const unsigned w[4] = {lo.x, lo.y, hi.x, hi.y};
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    const int e = S + k;
+    v[k] = __uint_as_float(__byte_perm(w[e >> 1], 0x4B000000u, (e & 1) ? 0x7632 : 0x7610)) - 8388608.0f;
+  }
+}
+template <int S>
+__device__ __forceinline__ void window5s(const __half* p, float* v) {
+  const uint2 lo = __ldg(reinterpret_cast<const uint2*>(p));
+  const uint2 hi = __ldg(reinterpret_cast<const uint2*>(p + 4));
+  const unsigned w[4] = {lo.x, lo.y, hi.x, hi.y};
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    const int e = S + k;
+    const unsigned short h = (unsigned short)((e & 1) ? (w[e >> 1] >> 16) : (w[e >> 1] & 0xffffu));
+    v[k] = __half2float(__ushort_as_half(h));
+  }
+}
+template <int S>
+__device__ __forceinline__ void window5s(const float* p, float* v) {
+  const float4 a = __ldg(reinterpret_cast<const float4*>(p));
+  const float4 b = __ldg(reinterpret_cast<const float4*>(p + 4));
+  const float w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+  for (int k = 0; k < 5; k++) v[k] = w[S + k];
+}
+
+// Four voxels of a lane in a uniform row segment (see eval4_tile): the lane's window of each tap row
+// starts at wp (+ pitch for row y+1, + plane for plane z+1); weights of voxel j are w + j * s per
+// axis, its control-point fraction fl + j * fs.
+template <int NDIM, int S, typename FT>
+__device__ __forceinline__ void uniform4(const FT* __restrict__ wp, long long plane, int pitch, const float* t4,
+                                         const float (*g4)[4], float wxl, float sx, float wyl, float sy, float wzl,
+                                         float sz, float fl, float fs, float& af, float* acc0, float* acc1) {
+  float v[NDIM == 3 ? 4 : 2][5];
+  window5s<S>(wp, v[0]);
+  window5s<S>(wp + pitch, v[1]);
+  if (NDIM == 3) {
+    window5s<S>(wp + plane, v[NDIM == 3 ? 2 : 0]);
+    window5s<S>(wp + plane + pitch, v[NDIM == 3 ? 3 : 1]);
+  }
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const float wx = j ? fmaf((float)j, sx, wxl) : wxl;
+    const float wy = j ? fmaf((float)j, sy, wyl) : wyl;
+    const float c00 = fmaf(wx, v[0][j + 1] - v[0][j], v[0][j]);
+    const float c01 = fmaf(wx, v[1][j + 1] - v[1][j], v[1][j]);
+    float val = fmaf(wy, c01 - c00, c00);
+    if (NDIM == 3) {
+      const float wz = j ? fmaf((float)j, sz, wzl) : wzl;
+      const float c10 = fmaf(wx, v[NDIM == 3 ? 2 : 0][j + 1] - v[NDIM == 3 ? 2 : 0][j], v[NDIM == 3 ? 2 : 0][j]);
+      const float c11 = fmaf(wx, v[NDIM == 3 ? 3 : 1][j + 1] - v[NDIM == 3 ? 3 : 1][j], v[NDIM == 3 ? 3 : 1][j]);
+      const float c1 = fmaf(wy, c11 - c10, c10);
+      val = fmaf(wz, c1 - val, val);
+    }
+    const float e = (val > 0.0f) ? val - t4[j] : 0.0f;
+    af = fmaf(e, e, af);
+    const float fj = j ? fmaf((float)j, fs, fl) : fl;
+    const float e1 = e * fj;
+    const float e0 = e - e1;
+#pragma unroll
+    for (int k = 0; k < NDIM; k++) {
+      acc0[k] = fmaf(g4[k][j], e0, acc0[k]);
+      acc1[k] = fmaf(g4[k][j], e1, acc1[k]);
+    }
+  }
+}
+
+// The sums one lane adds for its four voxels on the per-lane path.
+template <int NDIM>
+struct LaneSums {
+  float f;
+  float g[3][NDIM];
+};
+
+// Per-lane path of eval4_tile for the four voxels x0 .. x0+3 of one image row (row descriptor rd):
+// the lane decides for itself whether they share interval, range and tap offsets (then one window
+// per tap row), else samples voxel by voxel. Kept out of line: it runs for a small share of the
+// segments, and inlined its registers would be reserved for the whole tile loop.
+template <int NDIM, typename FT, typename RT>
+__device__ __forceinline__ LaneSums<NDIM> lane_item(const FT* __restrict__ fr, long long plane, int pitch, bool padded,
+                                                    const RefGradSrc<RT> src, const RowDesc rd,
+                                                 int x0, int row_here, int nx, int ny, int nz, bool bidir, float dq,
+                                                 const float4* sD, int cw, int c0) {
+  LaneSums<NDIM> out;
+  float& af = out.f;
+  auto& ag = out.g;
+  af = 0.0f;
+#pragma unroll
+  for (int s = 0; s < 3; s++)
+#pragma unroll
+    for (int k = 0; k < NDIM; k++) ag[s][k] = 0.0f;
+  const int z = rd.z;
+  const int y = rd.y;
+  const bool flip = bidir && (y & 1);
+  const float fs = flip ? -dq : dq;
+  // ---- per-lane path: each lane classifies its own four voxels ----
+  const long long p0 = (long long)row_here * nx + x0;
+  float t4[4], g4[NDIM][4];
+  src.template load<NDIM>(p0, t4, g4);
+
+  // Do the four voxels share interval, storage range and integer tap offsets, away from edges?
+  const int xs0 = flip ? nx - 1 - x0 : x0;
+  const int xs3 = flip ? xs0 - 3 : xs0 + 3;
+  const int di = rd.di0 + (xs0 >= rd.xdi ? 1 : 0);
+  const int di3 = rd.di0 + (xs3 >= rd.xdi ? 1 : 0);
+  const int r = bidir ? rd.r0 + (x0 >= rd.xr ? 1 : 0) : di;
+  const int r3 = bidir ? rd.r0 + (x0 + 3 >= rd.xr ? 1 : 0) : di3;
+  bool fast = (di == di3) && (r == r3) && (rd.xlast < x0 || rd.xlast > x0 + 3);
+  const float4* P = sD + min(max(di - cw, 0), kWin - 2) * kDParamF4;
+  const float f0 = fmaf((float)xs0, dq, rd.qbase) - (float)(di - rd.di0);
+  const float4 n = P[0], ph = P[1], dd = P[2];
+  const float t0x = fmaf(f0, dd.x, ph.x), t0y = fmaf(f0, dd.y, ph.y);
+  const float sx = fs * dd.x, sy = fs * dd.y;
+  const float flx = floorf(t0x), fly = floorf(t0y);
+  fast = fast && floorf(fmaf(3.0f, sx, t0x)) == flx && floorf(fmaf(3.0f, sy, t0y)) == fly;
+  const int ix = x0 + (int)n.x + (int)flx;
+  const int iy = y + (int)n.y + (int)fly;
+  // the whole aligned 8-element window of each tap row inside the row
+  bool inside = ix >= 0 && (ix & ~3) + 7 <= nx - 1 && iy >= 0 && iy + 1 <= ny - 1;
+  float t0z = 0.f, sz = 0.f, flz = 0.f;
+  int iz = 0;
+  if (NDIM == 3) {
+    t0z = fmaf(f0, dd.z, ph.z);
+    sz = fs * dd.z;
+    flz = floorf(t0z);
+    fast = fast && floorf(fmaf(3.0f, sz, t0z)) == flz;
+    iz = z + (int)n.z + (int)flz;
+    inside = inside && iz >= 0 && iz + 1 <= nz - 1;
+  }
+
+  float acc0[NDIM], acc1[NDIM];  // J^T e of controls r and r+1 for this lane's voxels
+#pragma unroll
+  for (int k = 0; k < NDIM; k++) acc0[k] = acc1[k] = 0.0f;
+
+  if (fast) {
+    float v[NDIM == 3 ? 4 : 2][5];
+    if (padded) {
+      // Clamp into the zero halo: a window that would lie wholly outside the volume along an
+      // axis reads halo zeros instead, exactly as the unclamped taps would read zero padding.
+      const int cx = min(max(ix, -kHaloX), nx + kHaloX - 5);
+      const int cy = min(max(iy, -kHaloY), ny + kHaloY - 2);
+      const int cz = NDIM == 3 ? min(max(iz, -kHaloZ), nz + kHaloZ - 2) : 0;
+      const int a = cx & ~3, s = cx - a;
+      const long long rb = (long long)cz * plane + (long long)cy * pitch + a;
+      window5(fr + rb, s, v[0]);
+      window5(fr + rb + pitch, s, v[1]);
+      if (NDIM == 3) {
+        window5(fr + rb + plane, s, v[NDIM == 3 ? 2 : 0]);
+        window5(fr + rb + plane + pitch, s, v[NDIM == 3 ? 3 : 1]);
+      }
+    } else if (inside) {
+      const int a = ix & ~3, s = ix & 3;
+      const long long rb = (long long)iz * plane + (long long)iy * pitch + a;
+      window5(fr + rb, s, v[0]);
+      window5(fr + rb + pitch, s, v[1]);
+      if (NDIM == 3) {
+        window5(fr + rb + plane, s, v[NDIM == 3 ? 2 : 0]);
+        window5(fr + rb + plane + pitch, s, v[NDIM == 3 ? 3 : 1]);
+      }
+    } else {
+      // tap rows (y, z), (y+1, z), (y, z+1), (y+1, z+1); rows outside the volume read zeros
+      const bool y0v = (unsigned)iy < (unsigned)ny, y1v = (unsigned)(iy + 1) < (unsigned)ny;
+      const bool z0v = NDIM == 2 || (unsigned)iz < (unsigned)nz;
+      const bool z1v = NDIM == 2 || (unsigned)(iz + 1) < (unsigned)nz;
+      const long long rb = (long long)iz * plane + (long long)iy * pitch;
+      masked5(fr + rb, y0v && z0v, ix, nx, v[0]);
+      masked5(fr + rb + pitch, y1v && z0v, ix, nx, v[1]);
+      if (NDIM == 3) {
+        masked5(fr + rb + plane, y0v && z1v, ix, nx, v[NDIM == 3 ? 2 : 0]);
+        masked5(fr + rb + plane + pitch, y1v && z1v, ix, nx, v[NDIM == 3 ? 3 : 1]);
+      }
+    }
+    const float wx0 = t0x - flx, wy0 = t0y - fly, wz0 = t0z - flz;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const float wx = fmaf((float)j, sx, wx0), wy = fmaf((float)j, sy, wy0);
+      const float c00 = fmaf(wx, v[0][j + 1] - v[0][j], v[0][j]);
+      const float c01 = fmaf(wx, v[1][j + 1] - v[1][j], v[1][j]);
+      float val = fmaf(wy, c01 - c00, c00);
+      if (NDIM == 3) {
+        const float wz = fmaf((float)j, sz, wz0);
+        const float c10 = fmaf(wx, v[NDIM == 3 ? 2 : 0][j + 1] - v[NDIM == 3 ? 2 : 0][j], v[NDIM == 3 ? 2 : 0][j]);
+        const float c11 = fmaf(wx, v[NDIM == 3 ? 3 : 1][j + 1] - v[NDIM == 3 ? 3 : 1][j], v[NDIM == 3 ? 3 : 1][j]);
+        const float c1 = fmaf(wy, c11 - c10, c10);
+        val = fmaf(wz, c1 - val, val);
+      }
+      const float e = (val > 0.0f) ? val - t4[j] : 0.0f;
+      af = fmaf(e, e, af);
+      const float fj = fmaf((float)j, fs, f0);
+      const float e1 = e * fj;
+      const float e0 = e - e1;
+#pragma unroll
+      for (int k = 0; k < NDIM; k++) {
+        acc0[k] = fmaf(g4[k][j], e0, acc0[k]);
+        acc1[k] = fmaf(g4[k][j], e1, acc1[k]);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int x = x0 + j;
+      const VoxelModel vm = voxel_model(rd, x, nx, flip, bidir, dq);
+      const int wi = min(max(vm.di - cw, 0), kWin - 2);
+      const float val = sample<NDIM, FT>(fr, plane, pitch, sD + wi * kDParamF4, vm.f, x, y, z, nx, ny, nz);
+      const float e = (val > 0.0f) ? val - t4[j] : 0.0f;
+      af = fmaf(e, e, af);
+      if (!vm.last) {
+        const float e1 = e * vm.f;
+        const float e0 = e * (1.0f - vm.f);
+        if (vm.r == r) {
+#pragma unroll
+          for (int k = 0; k < NDIM; k++) {
+            acc0[k] = fmaf(g4[k][j], e0, acc0[k]);
+            acc1[k] = fmaf(g4[k][j], e1, acc1[k]);
+          }
+        } else {
+          // voxel in the following range: controls r+1 and r+2
+          const int s2 = vm.r - c0;
+#pragma unroll
+          for (int k = 0; k < NDIM; k++) {
+            if (s2 == 1) {
+              ag[1][k] = fmaf(g4[k][j], e0, ag[1][k]);
+              ag[2][k] = fmaf(g4[k][j], e1, ag[2][k]);
+            } else {
+              ag[0][k] = fmaf(g4[k][j], e0, ag[0][k]);
+              ag[1][k] = fmaf(g4[k][j], e1, ag[1][k]);
+            }
+          }
+        }
+      }
+    }
+  }
+  if (r == c0) {
+#pragma unroll
+    for (int k = 0; k < NDIM; k++) {
+      ag[0][k] += acc0[k];
+      ag[1][k] += acc1[k];
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < NDIM; k++) {
+      ag[1][k] += acc0[k];
+      ag[2][k] += acc1[k];
+    }
+  }
+  return out;
+}
+
+// A row segment's parameters, computed by one lane for the whole warp (see eval4_tile).
+struct SegParams {
+  float w0x, w0y, w0z, f0;  // sample weights and control-point fraction of the segment's first voxel
+  float sx, sy, sz, fs;     // their change per voxel along the row
+  long long win;            // frame offset of lane 0's window (tap row y, plane z; multiple of 4 in x)
+  int p0;                   // reference / gradient offset of the segment's first voxel
+  int meta;                 // bit 0: uniform; bits 1-2: window alignment; bits 3..: storage range
+};
+constexpr int kSegBatch = 32;  // segments classified per round, one per lane
+
 // One tile of one frame, processed by one warp on its own: its control-point window sD (the warp's
 // slice of shared memory), its row segments, and its partial sums. No CTA barrier is involved, so
 // the warps of a CTA drift apart and hide each other's load latency.
+//
+// A row segment is 128 consecutive voxels of an image row, four per lane. Almost every segment is
+// uniform: its voxels share one displacement interval and one storage range, contain no range end,
+// and their sample positions x + d(x) share one integer offset per axis, because the displacement
+// changes by ~1e-5 px per voxel along a row. Whether it is, and its weights, slopes and window
+// offsets, follow from the row descriptor and the segment's two ends (the position is monotone in x
+// within an interval). The warp first classifies 32 segments at once, one per lane, into shared
+// memory, then walks them: a uniform segment needs no per-lane interval, range or offset logic, its
+// frame windows share one compile-time alignment, and its J^T e terms go to one pair of running sums
+// that are added to the tile's control points only when the range changes. Other segments take the
+// per-lane path (lane_item), which handles every case voxel by voxel where needed.
 template <int NDIM, typename FT, typename RT>
-__device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, const int tile, float4* sD) {
+__device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, const int tile, float4* sD,
+                                           SegParams* sp) {
   const int nx = R.nx, ny = R.ny, nz = R.nz;
   const int row_begin = tile * R.tile_rows;
   const int row_end = min(row_begin + R.tile_rows, R.n_rows);
@@ -112,7 +420,7 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
   const float dq = R.dq;
   const int lane = threadIdx.x & 31;
 
-  __syncwarp();  // the previous tile's readers of sD are done
+  __syncwarp();  // the previous tile's readers of sD and sp are done
   if (lane < kWin * kDParamF4) {
     const int k = cw + lane / kDParamF4;
     sD[lane] = (k < R.nD) ? job.dparams[k * kDParamF4 + lane % kDParamF4] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -120,19 +428,7 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
   __syncwarp();
 
   const FT* __restrict__ fr = static_cast<const FT*>(job.frame);
-  const RT* __restrict__ tref;
-  const RT* __restrict__ tg[3];
-  if constexpr (sizeof(RT) == 4) {
-    tref = reinterpret_cast<const RT*>(R.ref32);
-    tg[0] = reinterpret_cast<const RT*>(R.gx32);
-    tg[1] = reinterpret_cast<const RT*>(R.gy32);
-    tg[2] = reinterpret_cast<const RT*>(R.gz32);
-  } else {
-    tref = reinterpret_cast<const RT*>(R.ref16);
-    tg[0] = reinterpret_cast<const RT*>(R.gx16);
-    tg[1] = reinterpret_cast<const RT*>(R.gy16);
-    tg[2] = reinterpret_cast<const RT*>(R.gz16);
-  }
+  const RefGradSrc<RT> src(R);
 
   float af = 0.0f;
   float ag[3][NDIM];
@@ -140,182 +436,158 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
   for (int s = 0; s < 3; s++)
 #pragma unroll
     for (int k = 0; k < NDIM; k++) ag[s][k] = 0.0f;
+  // running J^T e sums of uniform segments, for controls ur and ur + 1 (ur: their storage range)
+  float ua0[NDIM], ua1[NDIM];
+#pragma unroll
+  for (int k = 0; k < NDIM; k++) ua0[k] = ua1[k] = 0.0f;
+  int ur = -1;
+  auto flush_uniform = [&]() {
+    if (ur == c0) {
+#pragma unroll
+      for (int k = 0; k < NDIM; k++) {
+        ag[0][k] += ua0[k];
+        ag[1][k] += ua1[k];
+      }
+    } else if (ur >= 0) {
+#pragma unroll
+      for (int k = 0; k < NDIM; k++) {
+        ag[1][k] += ua0[k];
+        ag[2][k] += ua1[k];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < NDIM; k++) ua0[k] = ua1[k] = 0.0f;
+  };
+  const float lane_u = (float)(lane * 4);  // x - (segment start) of the lane's first voxel
 
-  // 128-voxel segments of the tile's rows, one per step of the warp
+  // 128-voxel segments of the tile's rows
   const int segs = (nx + 127) >> 7;
   const int n_items = (row_end - row_begin) * segs;
   const long long plane = job.fplane;
   const int pitch = job.fpitch;
   const bool padded = job.fpad != 0;
-  int row = row_begin, seg = 0;
-  for (int item = 0; item < n_items; item++) {
-    const int x0 = seg * 128 + lane * 4;
-    const int row_here = row;
-    if (++seg == segs) {
-      seg = 0;
-      ++row;
-    }
-    if (x0 < nx) {
-      const RowDesc rd = R.rows[row_here];
-      const int z = rd.z;
-      const int y = rd.y;
-      const bool flip = bidir && (y & 1);
-      const long long p0 = (long long)row_here * nx + x0;
-      float t4[4], g4[NDIM][4];
-      load4(tref + p0, t4);
-#pragma unroll
-      for (int k = 0; k < NDIM; k++) load4(tg[k] + p0, g4[k]);
-
-      // Do the four voxels share interval, storage range and integer tap offsets, away from edges?
-      const int xs0 = flip ? nx - 1 - x0 : x0;
-      const int xs3 = flip ? xs0 - 3 : xs0 + 3;
-      const int di = rd.di0 + (xs0 >= rd.xdi ? 1 : 0);
-      const int di3 = rd.di0 + (xs3 >= rd.xdi ? 1 : 0);
-      const int r = bidir ? rd.r0 + (x0 >= rd.xr ? 1 : 0) : di;
-      const int r3 = bidir ? rd.r0 + (x0 + 3 >= rd.xr ? 1 : 0) : di3;
-      bool fast = (di == di3) && (r == r3) && (rd.xlast < x0 || rd.xlast > x0 + 3);
-      const float4* P = sD + min(max(di - cw, 0), kWin - 2) * kDParamF4;
-      const float f0 = fmaf((float)xs0, dq, rd.qbase) - (float)(di - rd.di0);
+  for (int base = 0; base < n_items; base += kSegBatch) {
+    // ---- classify segments base .. base + 31, segment base + lane by this lane ----
+    if (base + lane < n_items) {
+      const int it = base + lane;
+      const int row = row_begin + it / segs;
+      const int xa = (it - (row - row_begin) * segs) * 128;
+      const RowDesc rd = R.rows[row];
+      const bool flip = bidir && (rd.y & 1);
+      const int xb = min(xa + 127, nx - 1);
+      const int xsa = flip ? nx - 1 - xa : xa, xsb = flip ? nx - 1 - xb : xb;
+      const int dia = rd.di0 + (xsa >= rd.xdi ? 1 : 0);
+      const int dib = rd.di0 + (xsb >= rd.xdi ? 1 : 0);
+      const int ra = bidir ? rd.r0 + (xa >= rd.xr ? 1 : 0) : dia;
+      const int rb = bidir ? rd.r0 + (xb >= rd.xr ? 1 : 0) : dib;
+      bool uni = dia == dib && ra == rb && (rd.xlast < xa || rd.xlast > xb);
+      const float4* Pa = sD + min(max(dia - cw, 0), kWin - 2) * kDParamF4;
+      const float fsa = fmaf((float)xsa, dq, rd.qbase) - (float)(dia - rd.di0);
       const float fs = flip ? -dq : dq;
-      const float4 n = P[0], ph = P[1], dd = P[2];
-      const float t0x = fmaf(f0, dd.x, ph.x), t0y = fmaf(f0, dd.y, ph.y);
-      const float sx = fs * dd.x, sy = fs * dd.y;
-      const float flx = floorf(t0x), fly = floorf(t0y);
-      fast = fast && floorf(fmaf(3.0f, sx, t0x)) == flx && floorf(fmaf(3.0f, sy, t0y)) == fly;
-      const int ix = x0 + (int)n.x + (int)flx;
-      const int iy = y + (int)n.y + (int)fly;
-      bool inside = ix >= 0 && ix + 4 <= nx - 1 && iy >= 0 && iy + 1 <= ny - 1;
-      float t0z = 0.f, sz = 0.f, flz = 0.f;
-      int iz = 0;
+      const float span = (float)(xb - xa);
+      const float4 na = Pa[0], pha = Pa[1], dda = Pa[2];
+      const float sx = fs * dda.x, sy = fs * dda.y, sz = NDIM == 3 ? fs * dda.z : 0.0f;
+      const float tax = fmaf(fsa, dda.x, pha.x), tay = fmaf(fsa, dda.y, pha.y);
+      const float flx = floorf(tax), fly = floorf(tay);
+      uni = uni && floorf(fmaf(span, sx, tax)) == flx && floorf(fmaf(span, sy, tay)) == fly;
+      float taz = 0.f, flz = 0.f;
       if (NDIM == 3) {
-        t0z = fmaf(f0, dd.z, ph.z);
-        sz = fs * dd.z;
-        flz = floorf(t0z);
-        fast = fast && floorf(fmaf(3.0f, sz, t0z)) == flz;
-        iz = z + (int)n.z + (int)flz;
-        inside = inside && iz >= 0 && iz + 1 <= nz - 1;
+        taz = fmaf(fsa, dda.z, pha.z);
+        flz = floorf(taz);
+        uni = uni && floorf(fmaf(span, sz, taz)) == flz;
       }
-
-      float acc0[NDIM], acc1[NDIM];  // J^T e of controls r and r+1 for this lane's voxels
-#pragma unroll
-      for (int k = 0; k < NDIM; k++) acc0[k] = acc1[k] = 0.0f;
-
-      if (fast) {
-        float v[NDIM == 3 ? 4 : 2][5];
-        if (padded) {
-          // Clamp into the zero halo: a window that would lie wholly outside the volume along an
-          // axis reads halo zeros instead, exactly as the unclamped taps would read zero padding.
-          const int cx = min(max(ix, -kHaloX), nx + kHaloX - 5);
-          const int cy = min(max(iy, -kHaloY), ny + kHaloY - 2);
-          const int cz = NDIM == 3 ? min(max(iz, -kHaloZ), nz + kHaloZ - 2) : 0;
-          const int a = cx & ~3, s = cx - a;
-          const long long rb = (long long)cz * plane + (long long)cy * pitch + a;
-          window5(fr + rb, s, v[0]);
-          window5(fr + rb + pitch, s, v[1]);
-          if (NDIM == 3) {
-            window5(fr + rb + plane, s, v[NDIM == 3 ? 2 : 0]);
-            window5(fr + rb + plane + pitch, s, v[NDIM == 3 ? 3 : 1]);
-          }
-        } else if (inside) {
-          const int a = ix & ~3, s = ix & 3;
-          const long long rb = (long long)iz * plane + (long long)iy * pitch + a;
-          window5(fr + rb, s, v[0]);
-          window5(fr + rb + pitch, s, v[1]);
-          if (NDIM == 3) {
-            window5(fr + rb + plane, s, v[NDIM == 3 ? 2 : 0]);
-            window5(fr + rb + plane + pitch, s, v[NDIM == 3 ? 3 : 1]);
-          }
-        } else {
-          // tap rows (y, z), (y+1, z), (y, z+1), (y+1, z+1); rows outside the volume read zeros
-          const bool y0v = (unsigned)iy < (unsigned)ny, y1v = (unsigned)(iy + 1) < (unsigned)ny;
-          const bool z0v = NDIM == 2 || (unsigned)iz < (unsigned)nz;
-          const bool z1v = NDIM == 2 || (unsigned)(iz + 1) < (unsigned)nz;
-          const long long rb = (long long)iz * plane + (long long)iy * pitch;
-          masked5(fr + rb, y0v && z0v, ix, nx, v[0]);
-          masked5(fr + rb + pitch, y1v && z0v, ix, nx, v[1]);
-          if (NDIM == 3) {
-            masked5(fr + rb + plane, y0v && z1v, ix, nx, v[NDIM == 3 ? 2 : 0]);
-            masked5(fr + rb + plane + pitch, y1v && z1v, ix, nx, v[NDIM == 3 ? 3 : 1]);
-          }
-        }
-        const float wx0 = t0x - flx, wy0 = t0y - fly, wz0 = t0z - flz;
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-          const float wx = fmaf((float)j, sx, wx0), wy = fmaf((float)j, sy, wy0);
-          const float c00 = fmaf(wx, v[0][j + 1] - v[0][j], v[0][j]);
-          const float c01 = fmaf(wx, v[1][j + 1] - v[1][j], v[1][j]);
-          float val = fmaf(wy, c01 - c00, c00);
-          if (NDIM == 3) {
-            const float wz = fmaf((float)j, sz, wz0);
-            const float c10 = fmaf(wx, v[NDIM == 3 ? 2 : 0][j + 1] - v[NDIM == 3 ? 2 : 0][j], v[NDIM == 3 ? 2 : 0][j]);
-            const float c11 = fmaf(wx, v[NDIM == 3 ? 3 : 1][j + 1] - v[NDIM == 3 ? 3 : 1][j], v[NDIM == 3 ? 3 : 1][j]);
-            const float c1 = fmaf(wy, c11 - c10, c10);
-            val = fmaf(wz, c1 - val, val);
-          }
-          const float e = (val > 0.0f) ? val - t4[j] : 0.0f;
-          af = fmaf(e, e, af);
-          const float fj = fmaf((float)j, fs, f0);
-          const float e1 = e * fj;
-          const float e0 = e - e1;
-#pragma unroll
-          for (int k = 0; k < NDIM; k++) {
-            acc0[k] = fmaf(g4[k][j], e0, acc0[k]);
-            acc1[k] = fmaf(g4[k][j], e1, acc1[k]);
-          }
-        }
+      const int ox = (int)na.x + (int)flx;
+      const int iy = rd.y + (int)na.y + (int)fly;
+      const int iz = NDIM == 3 ? rd.z + (int)na.z + (int)flz : 0;
+      const int ab = ox & ~3;                   // window start relative to x0 (multiple of 4)
+      const int x_last = min(xa + 124, nx - 4);  // first voxel of the segment's last active lane
+      int cy, cz;
+      if (padded) {
+        // windows inside the row's zero halo; tap rows / planes wholly outside read halo zeros
+        uni = uni && xa + ab >= -kHaloX && x_last + ab + 7 <= nx - 1 + kHaloX;
+        cy = min(max(iy, -kHaloY), ny + kHaloY - 2);
+        cz = NDIM == 3 ? min(max(iz, -kHaloZ), nz + kHaloZ - 2) : 0;
       } else {
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-          const int x = x0 + j;
-          const VoxelModel vm = voxel_model(rd, x, nx, flip, bidir, dq);
-          const int wi = min(max(vm.di - cw, 0), kWin - 2);
-          const float val = sample<NDIM, FT>(fr, plane, pitch, sD + wi * kDParamF4, vm.f, x, y, z, nx, ny, nz);
-          const float e = (val > 0.0f) ? val - t4[j] : 0.0f;
-          af = fmaf(e, e, af);
-          if (!vm.last) {
-            const float e1 = e * vm.f;
-            const float e0 = e * (1.0f - vm.f);
-            if (vm.r == r) {
-#pragma unroll
-              for (int k = 0; k < NDIM; k++) {
-                acc0[k] = fmaf(g4[k][j], e0, acc0[k]);
-                acc1[k] = fmaf(g4[k][j], e1, acc1[k]);
-              }
-            } else {
-              // voxel in the following range: controls r+1 and r+2
-              const int s2 = vm.r - c0;
-#pragma unroll
-              for (int k = 0; k < NDIM; k++) {
-                if (s2 == 1) {
-                  ag[1][k] = fmaf(g4[k][j], e0, ag[1][k]);
-                  ag[2][k] = fmaf(g4[k][j], e1, ag[2][k]);
-                } else {
-                  ag[0][k] = fmaf(g4[k][j], e0, ag[0][k]);
-                  ag[1][k] = fmaf(g4[k][j], e1, ag[1][k]);
-                }
-              }
-            }
-          }
-        }
+        uni = uni && xa + ab >= 0 && x_last + ab + 7 <= nx - 1 && iy >= 0 && iy + 1 <= ny - 1 &&
+              (NDIM == 2 || (iz >= 0 && iz + 1 <= nz - 1));
+        cy = iy;
+        cz = iz;
       }
-      if (r == c0) {
-#pragma unroll
-        for (int k = 0; k < NDIM; k++) {
-          ag[0][k] += acc0[k];
-          ag[1][k] += acc1[k];
-        }
-      } else {
-#pragma unroll
-        for (int k = 0; k < NDIM; k++) {
-          ag[1][k] += acc0[k];
-          ag[2][k] += acc1[k];
-        }
-      }
+      SegParams q;
+      q.w0x = tax - flx;
+      q.w0y = tay - fly;
+      q.w0z = taz - flz;
+      q.f0 = fsa;
+      q.sx = sx;
+      q.sy = sy;
+      q.sz = sz;
+      q.fs = fs;
+      q.win = (long long)cz * plane + (long long)cy * pitch + xa + ab;
+      q.p0 = row * nx + xa;
+      q.meta = (uni ? 1 : 0) | ((ox & 3) << 1) | (ra << 3);
+      sp[lane] = q;
     }
-    // Explicit reconvergence point: the per-lane fast / per-voxel branches above must not leave
-    // the warp split into groups that then run the rest of the loop one after the other.
     __syncwarp();
+    // ---- walk them ----
+    const int cnt = min(kSegBatch, n_items - base);
+    for (int q = 0; q < cnt; q++) {
+      const SegParams P = sp[q];
+      const int xa = ((base + q) % segs) * 128;
+      const int x0 = xa + lane * 4;
+      if (P.meta & 1) {
+        const int ra = P.meta >> 3;
+        if (ra != ur) {
+          flush_uniform();
+          ur = ra;
+        }
+        if (x0 < nx) {
+          float t4[4], g4[NDIM][4];
+          src.template load<NDIM>(P.p0 + lane * 4, t4, g4);
+          const FT* wp = fr + (P.win + lane * 4);
+          const float wxl = fmaf(lane_u, P.sx, P.w0x);
+          const float wyl = fmaf(lane_u, P.sy, P.w0y);
+          const float wzl = NDIM == 3 ? fmaf(lane_u, P.sz, P.w0z) : 0.0f;
+          const float fl = fmaf(lane_u, P.fs, P.f0);
+          switch ((P.meta >> 1) & 3) {
+            case 0:
+              uniform4<NDIM, 0>(wp, plane, pitch, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
+              break;
+            case 1:
+              uniform4<NDIM, 1>(wp, plane, pitch, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
+              break;
+            case 2:
+              uniform4<NDIM, 2>(wp, plane, pitch, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
+              break;
+            default:
+              uniform4<NDIM, 3>(wp, plane, pitch, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
+              break;
+          }
+        }
+      }
+      __syncwarp();  // lanes past the row end rejoin here
+    }
+    // the batch's other segments, lane by lane (after the uniform walk, so that its registers are
+    // free for the per-lane path)
+    for (int q = 0; q < cnt; q++) {
+      if (sp[q].meta & 1) continue;
+      const int x0 = ((base + q) % segs) * 128 + lane * 4;
+      if (x0 < nx) {
+        const int row = row_begin + (base + q) / segs;
+        const LaneSums<NDIM> ls = lane_item<NDIM, FT, RT>(fr, plane, pitch, padded, src, R.rows[row], x0, row, nx,
+                                                         ny, nz, bidir, dq, sD, cw, c0);
+        af += ls.f;
+#pragma unroll
+        for (int s2 = 0; s2 < 3; s2++)
+#pragma unroll
+          for (int k = 0; k < NDIM; k++) ag[s2][k] += ls.g[s2][k];
+      }
+      // Explicit reconvergence point: the per-lane branches above must not leave the warp split
+      // into groups that then run the rest of the loop one after the other.
+      __syncwarp();
+    }
+    __syncwarp();  // every lane is done reading this batch's parameters
   }
+  flush_uniform();
 
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -341,13 +613,14 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
 template <int NDIM, typename FT, typename RT, int MB>
 __global__ void __launch_bounds__(kEvalThreads, MB) eval4_kernel(const Job* __restrict__ jobs) {
   __shared__ float4 sD[kEvalWarps][kWin * kDParamF4];
+  __shared__ SegParams sp[kEvalWarps][kSegBatch];
   const Job& job = jobs[blockIdx.y];
   if (job.state != nullptr && (job.state->phase == kPhaseDone || job.state->phase == kPhaseWaitWarm)) return;
   const RefDev& R = *job.ref;
   const int warp = threadIdx.x >> 5;
   const int tile = blockIdx.x * kEvalWarps + warp;
   if (tile >= R.n_tiles) return;
-  eval4_tile<NDIM, FT, RT>(job, R, tile, sD[warp]);
+  eval4_tile<NDIM, FT, RT>(job, R, tile, sD[warp], sp[warp]);
 }
 
 // Persistent form for batched solves: the grid's warps walk the (active frame, tile) items of the
@@ -360,6 +633,7 @@ __global__ void __launch_bounds__(kEvalThreads, MB) eval4_active_kernel(const Jo
                                                                      const int* __restrict__ n_active,
                                                                      const int* __restrict__ tile_prefix) {
   __shared__ float4 sD[kEvalWarps][kWin * kDParamF4];
+  __shared__ SegParams sp[kEvalWarps][kSegBatch];
   const int na = *n_active;
   const int n_items = tile_prefix[na];
   const int warp = threadIdx.x >> 5;
@@ -376,7 +650,7 @@ __global__ void __launch_bounds__(kEvalThreads, MB) eval4_active_kernel(const Jo
     }
     const int tile = item - tile_prefix[a];
     const Job& job = jobs[active[a]];
-    eval4_tile<NDIM, FT, RT>(job, *job.ref, tile, sD[warp]);
+    eval4_tile<NDIM, FT, RT>(job, *job.ref, tile, sD[warp], sp[warp]);
   }
 }
 

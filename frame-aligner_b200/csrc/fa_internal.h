@@ -97,10 +97,9 @@ struct RefDev {
   const float* gx32;
   const float* gy32;
   const float* gz32;
-  const __nv_bfloat16* ref16;
-  const __nv_bfloat16* gx16;
-  const __nv_bfloat16* gy16;
-  const __nv_bfloat16* gz16;
+  // Mixed precision: BF16 reference and gradient interleaved per group of four consecutive voxels
+  // (voxels 4g .. 4g+3: reference, gx, gy, gz, four values each; 32 bytes, two 16-byte loads).
+  const __nv_bfloat16* q16;
   const double* Hd;  // nD blocks of n_dim x n_dim (diagonal), row-major
   const double* Hl;  // nD blocks (block k couples k and k-1; block 0 unused)
   double h_inf;      // max_i sum_j |H_ij| (ascending j), the subproblem's bracket bound

@@ -80,6 +80,30 @@ cudaError_t launch_to_bf16(const float* in, __nv_bfloat16* out, long long n, cud
   return cudaGetLastError();
 }
 
+__global__ void to_quad16_kernel(const float* __restrict__ ref, const float* __restrict__ gx,
+                                 const float* __restrict__ gy, const float* __restrict__ gz, long long n,
+                                 __nv_bfloat16* __restrict__ q16) {
+  const long long groups = (n + 3) / 4;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < groups * 16;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long g = i >> 4;
+    const int k = (int)(i >> 2) & 3, j = (int)i & 3;
+    const long long p = 4 * g + j;
+    const float* src = k == 0 ? ref : (k == 1 ? gx : (k == 2 ? gy : gz));
+    q16[i] = __float2bfloat16_rn(p < n ? src[p] : 0.0f);
+  }
+}
+
+cudaError_t launch_to_quad16(const float* ref, const float* gx, const float* gy, const float* gz, long long n,
+                             __nv_bfloat16* q16, cudaStream_t s) {
+  const long long total = (n + 3) / 4 * 16;
+  int blocks = (int)((total + 255) / 256);
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  if (blocks < 1) blocks = 1;
+  to_quad16_kernel<<<blocks, 256, 0, s>>>(ref, gx, gy, gz, n, q16);
+  return cudaGetLastError();
+}
+
 __device__ __forceinline__ float load_any(const void* in, int t, long long i) {
   switch (t) {
     case FA_F32: return static_cast<const float*>(in)[i];
@@ -298,21 +322,15 @@ __global__ void __launch_bounds__(kEvalThreads) eval_kernel(const Job* __restric
   __syncthreads();
 
   const FT* __restrict__ fr = static_cast<const FT*>(job.frame);
-  const RT* __restrict__ tref;
-  const RT* __restrict__ tgx;
-  const RT* __restrict__ tgy;
-  const RT* __restrict__ tgz;
-  if constexpr (sizeof(RT) == 4) {
-    tref = reinterpret_cast<const RT*>(R.ref32);
-    tgx = reinterpret_cast<const RT*>(R.gx32);
-    tgy = reinterpret_cast<const RT*>(R.gy32);
-    tgz = reinterpret_cast<const RT*>(R.gz32);
-  } else {
-    tref = reinterpret_cast<const RT*>(R.ref16);
-    tgx = reinterpret_cast<const RT*>(R.gx16);
-    tgy = reinterpret_cast<const RT*>(R.gy16);
-    tgz = reinterpret_cast<const RT*>(R.gz16);
-  }
+  // reference / gradient value k (0: reference, 1..3: gx, gy, gz) of voxel p
+  auto refgrad = [&](int k, long long p) -> float {
+    if constexpr (sizeof(RT) == 4) {
+      const float* planes[4] = {R.ref32, R.gx32, R.gy32, R.gz32};
+      return __ldg(planes[k] + p);
+    } else {
+      return __bfloat162float(__ldg(R.q16 + (p >> 2) * 16 + k * 4 + (p & 3)));
+    }
+  };
 
   float af = 0.0f;
   float ag[3][NDIM];
@@ -335,7 +353,7 @@ __global__ void __launch_bounds__(kEvalThreads) eval_kernel(const Job* __restric
       const int wi = min(max(vm.di - cw, 0), kWin - 2);
       const float v = sample<NDIM, FT>(fr, job.fplane, job.fpitch, sD + wi * kDParamF4, vm.f, x, y, z, nx, ny, nz);
       const long long p = rowoff + x;
-      const float t = ldf(tref + p);
+      const float t = refgrad(0, p);
       // include iff the interpolated value is positive: CPU rule px == 0 -> -1, then wimg >= 0
       // (FrameWarper.cpp:67, 16-25)
       const float e = (v > 0.0f) ? v - t : 0.0f;
@@ -344,9 +362,9 @@ __global__ void __launch_bounds__(kEvalThreads) eval_kernel(const Job* __restric
         const float e1 = e * vm.f;           // weight of control r+1: Df
         const float e0 = e * (1.0f - vm.f);  // weight of control r:   1 - Df
         float gk[NDIM];
-        gk[0] = ldf(tgx + p);
-        gk[1] = ldf(tgy + p);
-        if (NDIM == 3) gk[NDIM - 1] = ldf(tgz + p);
+        gk[0] = refgrad(1, p);
+        gk[1] = refgrad(2, p);
+        if (NDIM == 3) gk[NDIM - 1] = refgrad(3, p);
         if (vm.r == c0) {
 #pragma unroll
           for (int k = 0; k < NDIM; k++) {

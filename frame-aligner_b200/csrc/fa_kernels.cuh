@@ -22,6 +22,10 @@ cudaError_t launch_hessian(const RefDev* ref_dev, const RefDev& ref_host, const 
 
 // FP32 -> BF16 copy.
 cudaError_t launch_to_bf16(const float* in, __nv_bfloat16* out, long long n, cudaStream_t s);
+// FP32 reference and gradient planes -> the interleaved BF16 groups of RefDev::q16 (ceil(n / 4) * 16
+// values; entries past the volume are zero).
+cudaError_t launch_to_quad16(const float* ref, const float* gx, const float* gy, const float* gz, long long n,
+                             __nv_bfloat16* q16, cudaStream_t s);
 // Any input dtype -> FP32 or FP16 frame storage.
 cudaError_t launch_convert(const void* in, fa_dtype in_type, void* out, fa_dtype out_type, long long n,
                            cudaStream_t s);
@@ -119,14 +123,23 @@ cudaError_t launch_phase_argmax_final(const double* block_val, const long long* 
 struct PlaneDims {
   int nz, ny, nx, rows;      // rows = nz * ny
   int log2M, log2ny, log2G;  // M = nx / 2; G rows per row CTA
-  int PP;                    // planes per plane CTA
+  int PP;                    // planes per plane CTA (one-kernel (z, y) pass); 0 when split
   int n_twx, tw_x_post;      // x twiddles: stage table of the nx/2-point DFT, then W_nx^k (k <= nx/2)
   int n_twy;                 // y twiddles: stage table of the ny-point DFT
   long long n_complex, n_el;
+  // Split (z, y) pass, for planes too large for one CTA (nz * ny > 8192 or nz > 16): a y-line pass,
+  // a z-column pass with the cross-power, and an inverse y-line pass.
+  bool split;
+  int log2nz;
+  int LY;                    // y lines per CTA of the y-line passes
+  int log2YB;                // y columns per CTA of the z-column pass
+  int n_twz;                 // z twiddles: stage table of the nz-point DFT
 };
 bool plane_dims(int nz, int ny, int nx, PlaneDims* d);
-// The twiddle tables the passes read (tw_x: d.n_twx entries, tw_y: d.n_twy), computed in long double.
-void plane_twiddles(const PlaneDims& d, std::vector<double2>* tw_x, std::vector<double2>* tw_y);
+// The twiddle tables the passes read (tw_x: d.n_twx entries, tw_y: d.n_twy, tw_z: d.n_twz when the
+// pass is split, else empty), computed in long double.
+void plane_twiddles(const PlaneDims& d, std::vector<double2>* tw_x, std::vector<double2>* tw_y,
+                    std::vector<double2>* tw_z);
 // CTAs (argmax partials) per frame of the last pass.
 int plane_blocks_per_frame(const PlaneDims& d);
 // Window + real DFT along x of each frame (dense FP32 or uint16, in_kind an fa_dtype) into spec
@@ -138,6 +151,12 @@ cudaError_t launch_plane_rows_fwd(const PlaneDims& d, const void* const* vols, i
 // out = inverse DFT of the normalised cross-power spectrum with ref_conj.
 cudaError_t launch_plane_yz(const PlaneDims& d, const double2* in, double2* out, const double2* ref_conj,
                             const double2* tw_y, int batch, bool reference, cudaStream_t s);
+// The same for split dimensions (d.split), in place in spec: forward DFT of every y line, then per
+// z column the forward z DFT and either conj (reference: written to ref_conj instead) or the
+// normalised cross-power with ref_conj and the inverse z DFT, then the inverse DFT of every y line
+// (not for the reference).
+cudaError_t launch_plane_yz_split(const PlaneDims& d, double2* spec, double2* ref_conj, const double2* tw_y,
+                                  const double2* tw_z, int batch, bool reference, cudaStream_t s);
 // One frame's half-spectrum from planes spec[kx][z][y] to cuFFT's order [z][y][kx].
 cudaError_t launch_plane_to_rows(const PlaneDims& d, const double2* in, double2* out, cudaStream_t s);
 // Inverse real DFT along x and the per-CTA first maximum (bval / bidx: batch * plane_blocks_per_frame);

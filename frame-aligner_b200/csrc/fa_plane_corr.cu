@@ -16,6 +16,11 @@
 //                           an nx/2-point complex inverse DFT) and the first maximum of the real
 //                           surface in flat (z, y, x) order, per CTA; then phase_argmax_final
 //
+// Planes too large for one CTA (nz * ny > 8192 or nz > 16, power-of-two nz >= 8) split the middle
+// pass in three: plane_y_kernel (DFT of y lines, in place), plane_z_kernel (per kx plane and block of
+// y columns: DFT along z, cross-power with the reference, inverse DFT along z) and plane_y_kernel
+// again (inverse), so every volume of these dimensions stays off cuFFT.
+//
 // DFTs along a row are Stockham radix-8/4/2 stages in shared memory (line l, element i at
 // l * (L + 1) + (i ^ ((i >> 3) & 7)): conflict-free for the stride-R writes of every stage and for
 // column reads across lines); the z DFT (<= 16 points) runs in registers, one (kx, y) column per
@@ -420,6 +425,162 @@ __global__ void __launch_bounds__(kPlaneThreads, 1) plane_yz_kernel(const double
   }
 }
 
+// The (z, y) pass for 16-plane volumes with twice the threads: 1024 threads of at most 64 registers
+// (32 warps per SM instead of 16; the plane still fills one CTA's shared memory), each y-line stage
+// one radix-8 butterfly per thread, and each 16-point z column split over a thread pair (lanes 2c,
+// 2c + 1): a radix-2 decimation-in-frequency step across the pair leaves the even bins on the first
+// thread and the odd bins on the second, each finished by an 8-point DFT in registers; the inverse
+// runs the same steps backwards (8-point inverse DFTs, then the radix-2 decimation-in-time step
+// across the pair). Same arithmetic contract as plane_yz_kernel<16, false>.
+constexpr int kPlane2Threads = 1024;
+constexpr int kPlane2EPT = 8;
+
+// W_16^n, n = 0..7 (forward)
+__device__ __forceinline__ double2 w16n(int n) {
+  switch (n) {
+    case 1: return make_double2(kC8, -kS8);
+    case 2: return make_double2(kS2, -kS2);
+    case 3: return make_double2(kS8, -kC8);
+    case 4: return make_double2(0.0, -1.0);
+    case 5: return make_double2(-kS8, -kC8);
+    case 6: return make_double2(-kS2, -kS2);
+    case 7: return make_double2(-kC8, -kS8);
+    default: return make_double2(1.0, 0.0);
+  }
+}
+
+__device__ __forceinline__ double2 shfl_xor1(double2 v) {
+  return make_double2(__shfl_xor_sync(0xffffffffu, v.x, 1), __shfl_xor_sync(0xffffffffu, v.y, 1));
+}
+
+__global__ void __launch_bounds__(kPlane2Threads, 1) plane_yz16_kernel(double2* spec,
+                                                                       const double2* __restrict__ ref_conj,
+                                                                       const double2* __restrict__ tw_y, PlaneDims d,
+                                                                       long long n_planes) {
+  constexpr int NZ = 16;
+  extern __shared__ double2 sm[];
+  const int ny = d.ny, S = ny + 1;
+  const int plane = NZ * ny;
+  const long long p0 = (long long)blockIdx.x * d.PP;
+  const int pp = (int)min((long long)d.PP, n_planes - p0);
+  double2* tws = sm + d.PP * NZ * S;
+  double2* base = spec + p0 * plane;
+  stage16<4>(
+      d.n_twy, [&](int i) { return reinterpret_cast<const uint4*>(tw_y) + i; },
+      [&](int i) { return reinterpret_cast<uint4*>(tws) + i; });
+  auto first = [&](int l, int i) -> double2 { return base[l * ny + i]; };
+  fft_rows<false, kPlane2EPT, kPlane2Threads, false, true>(sm, pp * NZ, d.log2ny, tws, first, NoIo{});
+  const int M1 = (d.nx >> 1) + 1;
+  const int h = threadIdx.x & 1;
+  // every thread pair takes columns (p, y) in turn; both threads of a pair always run together
+  for (int c = threadIdx.x >> 1; c < pp * ny; c += kPlane2Threads / 2) {
+    const int p = c >> d.log2ny, y = c & (ny - 1);
+    double2* col = sm + (p * NZ) * S + swz(y);
+    double2 a[8];
+#pragma unroll
+    for (int n = 0; n < 8; n++) a[n] = col[(8 * h + n) * S];
+    // forward: b[n] = x[n] + x[n+8] (even bins), c[n] = (x[n] - x[n+8]) W_16^n (odd bins)
+#pragma unroll
+    for (int n = 0; n < 8; n++) {
+      const double2 o = shfl_xor1(a[n]);
+      a[n] = h == 0 ? cadd(a[n], o) : cmul(csub(o, a[n]), w16n(n));
+    }
+    dft8<false>(a);  // a[k] = bin 2k + h
+    const int k = (int)((p0 + p) % M1);
+    const double2* rc = ref_conj + (long long)k * plane + y;
+#pragma unroll
+    for (int n = 0; n < 8; n++) a[n] = cross_power(a[n], __ldg(rc + (2 * n + h) * ny));
+    // inverse: e[n] = inverse 8-point DFT of the even bins, o[n] of the odd bins;
+    // x[n] = e[n] + W_16^-n o[n], x[n+8] = e[n] - W_16^-n o[n]
+    dft8<true>(a);
+#pragma unroll
+    for (int n = 0; n < 8; n++) {
+      const double2 other = shfl_xor1(a[n]);
+      const double2 e = h == 0 ? a[n] : other;
+      const double2 t = cmul_tw<true>(h == 0 ? other : a[n], w16n(n));
+      a[n] = h == 0 ? cadd(e, t) : csub(e, t);
+    }
+#pragma unroll
+    for (int n = 0; n < 8; n++) col[(8 * h + n) * S] = a[n];
+  }
+  __syncthreads();
+  // the last inverse stage writes the planes
+  auto last = [&](int l, int i, double2 v) { base[l * ny + i] = v; };
+  fft_rows<true, kPlane2EPT, kPlane2Threads, true, false>(sm, pp * NZ, d.log2ny, tws, NoIo{}, last);
+}
+
+// Split (z, y) pass. Lines of ny points along y, in place in the batch's plane array (line l = plane
+// p, plane z at offset l * ny of spec[kx][z][y]), d.LY lines per CTA; the first stage reads global
+// memory and the last writes it (ny >= 16: at least two stages, so a CTA reads all its lines before
+// it writes any). Shared memory: LY lines of S = ny + 1 points, then the ny twiddle slots.
+template <bool INV>
+__global__ void __launch_bounds__(kPlaneThreads, 1) plane_y_kernel(double2* spec, const double2* __restrict__ tw_y,
+                                                                   PlaneDims d, long long n_lines) {
+  extern __shared__ double2 sm[];
+  const int ny = d.ny, S = ny + 1;
+  const long long l0 = (long long)blockIdx.x * d.LY;
+  const int nl = (int)min((long long)d.LY, n_lines - l0);
+  double2* tws = sm + d.LY * S;
+  double2* base = spec + l0 * ny;
+  stage16<4>(
+      d.n_twy, [&](int i) { return reinterpret_cast<const uint4*>(tw_y) + i; },
+      [&](int i) { return reinterpret_cast<uint4*>(tws) + i; });
+  auto first = [&](int l, int i) -> double2 { return base[(long long)l * ny + i]; };
+  auto last = [&](int l, int i, double2 v) { base[(long long)l * ny + i] = v; };
+  fft_rows<INV, kPlaneEPT, kPlaneThreads, false, false>(sm, nl, d.log2ny, tws, first, last);
+}
+
+// Split (z, y) pass, z columns: CTA = plane p of the batch x YB = 2^log2YB consecutive y. The
+// columns are staged with loads along y (line yy = column y0 + yy, element z), transformed along z
+// in shared memory, then multiplied by the reference's conjugate spectrum and normalised (or, for
+// the reference, conjugated and written to ref_out), transformed back and stored along y.
+// Shared memory: YB lines of S = nz + 1 points, then the nz twiddle slots.
+template <bool REF>
+__global__ void __launch_bounds__(kPlaneThreads, 1) plane_z_kernel(double2* spec, double2* ref_out,
+                                                                   const double2* __restrict__ ref_conj,
+                                                                   const double2* __restrict__ tw_z, PlaneDims d) {
+  extern __shared__ double2 sm[];
+  const int nz = d.nz, ny = d.ny, S = nz + 1, YB = 1 << d.log2YB;
+  const int yblocks = ny >> d.log2YB;
+  const long long p = blockIdx.x / yblocks;
+  const int y0 = (int)(blockIdx.x - p * yblocks) << d.log2YB;
+  const long long plane = (long long)nz * ny;
+  double2* col = spec + p * plane + y0;
+  double2* tws = sm + YB * S;
+  const int E = nz << d.log2YB;
+  stage16<4>(
+      d.n_twz, [&](int i) { return reinterpret_cast<const uint4*>(tw_z) + i; },
+      [&](int i) { return reinterpret_cast<uint4*>(tws) + i; });
+  for (int idx = threadIdx.x; idx < E; idx += blockDim.x) {
+    const int z = idx >> d.log2YB, yy = idx & (YB - 1);
+    sm[yy * S + swz(z)] = col[(long long)z * ny + yy];
+  }
+  __syncthreads();
+  fft_rows<false, kPlaneEPT, kPlaneThreads, true, true>(sm, YB, d.log2nz, tws, NoIo{}, NoIo{});
+  if (REF) {
+    double2* dst = ref_out + p * plane + y0;
+    for (int idx = threadIdx.x; idx < E; idx += blockDim.x) {
+      const int z = idx >> d.log2YB, yy = idx & (YB - 1);
+      const double2 v = sm[yy * S + swz(z)];
+      dst[(long long)z * ny + yy] = make_double2(v.x, -v.y);
+    }
+    return;
+  }
+  const int M1 = (d.nx >> 1) + 1;
+  const double2* rc = ref_conj + (p % M1) * plane + y0;
+  for (int idx = threadIdx.x; idx < E; idx += blockDim.x) {
+    const int z = idx >> d.log2YB, yy = idx & (YB - 1);
+    double2* e = sm + yy * S + swz(z);
+    *e = cross_power(*e, __ldg(rc + (long long)z * ny + yy));
+  }
+  __syncthreads();
+  fft_rows<true, kPlaneEPT, kPlaneThreads, true, true>(sm, YB, d.log2nz, tws, NoIo{}, NoIo{});
+  for (int idx = threadIdx.x; idx < E; idx += blockDim.x) {
+    const int z = idx >> d.log2YB, yy = idx & (YB - 1);
+    col[(long long)z * ny + yy] = sm[yy * S + swz(z)];
+  }
+}
+
 // (value, index), greater value then smaller index; NaN never wins (phase_argmax_blocks' rule).
 __device__ __forceinline__ void better(double& v, long long& i, double v2, long long i2) {
   if (v2 > v || (v2 == v && i2 < i)) {
@@ -564,18 +725,27 @@ int stage_count(int L) {
 
 }  // namespace
 
-void plane_twiddles(const PlaneDims& d, std::vector<double2>* tw_x, std::vector<double2>* tw_y) {
+void plane_twiddles(const PlaneDims& d, std::vector<double2>* tw_x, std::vector<double2>* tw_y,
+                    std::vector<double2>* tw_z) {
   tw_x->clear();
   tw_y->clear();
+  tw_z->clear();
   stage_table(d.nx / 2, tw_x);
   for (int k = 0; k <= d.nx / 2; k++) tw_x->push_back(unit_root(k, d.nx));  // W_nx^k, k = 0..nx/2
   stage_table(d.ny, tw_y);
+  if (d.split) stage_table(d.nz, tw_z);
 }
 
 bool plane_dims(int nz, int ny, int nx, PlaneDims* d) {
-  if (!pow2(nz) || !pow2(ny) || !pow2(nx) || nz > 16 || ny < 8 || ny > 2048 || nx < 16 || nx > 4096 ||
-      (long long)nz * ny > kPlaneThreads * kPlaneEPT)
-    return false;
+  if (!pow2(nz) || !pow2(ny) || !pow2(nx) || ny < 8 || ny > 2048 || nx < 16 || nx > 4096) return false;
+  const bool fits = nz <= 16 && (long long)nz * ny <= kPlaneThreads * kPlaneEPT;
+  // split pass: z columns of 8 .. 1024 points (at least 8 columns per CTA), y lines of >= 16 points
+  if (!fits && (nz < 8 || nz > 1024 || ny < 16)) return false;
+  d->split = !fits;
+  d->log2nz = ilog2(nz);
+  d->LY = std::max(1, (kPlaneThreads * kPlaneEPT) / ny);
+  d->log2YB = ilog2(std::min<long long>(ny, (kPlaneThreads * kPlaneEPT) / nz));
+  d->n_twz = d->split ? stage_count(nz) : 0;
   d->nz = nz;
   d->ny = ny;
   d->nx = nx;
@@ -585,7 +755,7 @@ bool plane_dims(int nz, int ny, int nx, PlaneDims* d) {
   int G = 8;
   while (G > 1 && ((long long)G * (nx / 2) > (long long)kRowThreads * kRowEPT || G > d->rows)) G >>= 1;
   d->log2G = ilog2(G);
-  d->PP = std::max(1, (kPlaneThreads * kPlaneEPT) / (nz * ny));
+  d->PP = d->split ? 0 : std::max(1, (kPlaneThreads * kPlaneEPT) / (nz * ny));
   d->n_complex = (long long)(nx / 2 + 1) * d->rows;
   d->n_el = (long long)nx * d->rows;
   d->tw_x_post = stage_count(nx / 2);
@@ -642,8 +812,41 @@ cudaError_t launch_yz_nz(const PlaneDims& d, const double2* in, double2* out, co
 cudaError_t launch_plane_yz(const PlaneDims& d, const double2* in, double2* out, const double2* ref_conj,
                             const double2* tw_y, int batch, bool reference, cudaStream_t s) {
   const long long n_planes = (long long)batch * ((d.nx >> 1) + 1);
+  if (!reference && d.nz == 16 && in == out && (long long)d.PP * 16 * d.ny <= kPlane2Threads * kPlane2EPT &&
+      d.ny >= 64) {
+    const size_t smem = ((size_t)d.PP * 16 * (d.ny + 1) + d.ny) * sizeof(double2);
+    cudaError_t e = allow_smem(plane_yz16_kernel, smem);
+    if (e != cudaSuccess) return e;
+    const long long grid = (n_planes + d.PP - 1) / d.PP;
+    plane_yz16_kernel<<<(unsigned)grid, kPlane2Threads, smem, s>>>(out, ref_conj, tw_y, d, n_planes);
+    return cudaGetLastError();
+  }
   return reference ? launch_yz_nz<true>(d, in, out, nullptr, tw_y, n_planes, s)
                    : launch_yz_nz<false>(d, in, out, ref_conj, tw_y, n_planes, s);
+}
+
+cudaError_t launch_plane_yz_split(const PlaneDims& d, double2* spec, double2* ref_conj, const double2* tw_y,
+                                  const double2* tw_z, int batch, bool reference, cudaStream_t s) {
+  if (!d.split) return cudaErrorInvalidValue;
+  const long long n_planes = (long long)batch * ((d.nx >> 1) + 1);
+  const long long n_lines = n_planes * d.nz;
+  const size_t smem_y = ((size_t)d.LY * (d.ny + 1) + d.ny) * sizeof(double2);
+  const size_t smem_z = (((size_t)1 << d.log2YB) * (d.nz + 1) + d.nz) * sizeof(double2);
+  const long long grid_y = (n_lines + d.LY - 1) / d.LY;
+  const long long grid_z = n_planes * (d.ny >> d.log2YB);
+  cudaError_t e = allow_smem(plane_y_kernel<false>, smem_y);
+  if (e == cudaSuccess) e = allow_smem(plane_y_kernel<true>, smem_y);
+  if (e == cudaSuccess) e = allow_smem(plane_z_kernel<false>, smem_z);
+  if (e == cudaSuccess) e = allow_smem(plane_z_kernel<true>, smem_z);
+  if (e != cudaSuccess) return e;
+  plane_y_kernel<false><<<(unsigned)grid_y, kPlaneThreads, smem_y, s>>>(spec, tw_y, d, n_lines);
+  if (reference) {
+    plane_z_kernel<true><<<(unsigned)grid_z, kPlaneThreads, smem_z, s>>>(spec, ref_conj, nullptr, tw_z, d);
+    return cudaGetLastError();
+  }
+  plane_z_kernel<false><<<(unsigned)grid_z, kPlaneThreads, smem_z, s>>>(spec, nullptr, ref_conj, tw_z, d);
+  plane_y_kernel<true><<<(unsigned)grid_y, kPlaneThreads, smem_y, s>>>(spec, tw_y, d, n_lines);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_plane_to_rows(const PlaneDims& d, const double2* in, double2* out, cudaStream_t s) {

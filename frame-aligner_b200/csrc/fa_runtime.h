@@ -119,6 +119,7 @@ struct fa_correlator {
   fa::PlaneDims pd{};
   double2* tw_x = nullptr;              // W_nx^m, m < nx
   double2* tw_y = nullptr;              // W_ny^m, m < ny
+  double2* tw_z = nullptr;              // W_nz^m, m < nz (split (z, y) pass only)
   cudaStream_t stream = nullptr;
   double* wy = nullptr;                 // square-root Hann window along y
   double* wx = nullptr;                 // ... and along x (1 along z)

@@ -397,8 +397,10 @@ fa_status fa_test_correlation_surface(fa_correlator* c, const float* volume, int
    (interleaved re, im): the stage twiddles of the nx/2-point row DFT, then W_nx^k for k = 0..nx/2
    from index x_post; tw_y the stage twiddles of the ny-point DFT (n_y). For every stage after the
    first (Ns > 1, radix R: radix 8 while at least 3 octaves are left, then 4 or 2), the table holds
-   W_(Ns R)^(r k) at (r - 1) Ns + k, r = 1..R-1, k = 0..Ns-1. FA_ERR_UNSUPPORTED for dimensions that
-   take the cuFFT path. Lets CPU tests check the tables and the pass structure without a GPU. */
+   W_(Ns R)^(r k) at (r - 1) Ns + k, r = 1..R-1, k = 0..Ns-1. planes_per_cta is 0 when the (z, y)
+   pass is split into y-line and z-column passes (planes of more than 8192 points or nz > 16), whose
+   z DFT uses the same stage table for nz points. FA_ERR_UNSUPPORTED for dimensions that take the
+   cuFFT path. Lets CPU tests check the tables and the pass structure without a GPU. */
 fa_status fa_test_plane_tables(int nz, int ny, int nx, double* tw_x, int cap_x, int* n_x, int* x_post, double* tw_y,
                                int cap_y, int* n_y, int* rows_per_cta, int* planes_per_cta);
 

@@ -16,6 +16,8 @@ import fa_b200 as fa
 
 SHAPES = [(1, 8, 16), (2, 16, 16), (1, 64, 64), (4, 64, 128), (16, 32, 64), (8, 8, 32), (1, 256, 512),
           (2, 16, 1024), (4, 2048, 16), (1, 8, 4096)]
+# planes of more than 8192 points or nz > 16: the (z, y) pass split into y lines and z columns
+SPLIT_SHAPES = [(32, 16, 16), (64, 32, 32), (16, 1024, 32), (8, 2048, 16), (128, 16, 64)]
 
 
 def _stages(L):
@@ -89,14 +91,22 @@ def _model_surface(t, reference, volume):
         X = 0.5 * (zk + zm) - 0.5j * W[k] * (zk - zm)
         return X.T.reshape(M + 1, nz, ny)
 
+    split = t["planes_per_cta"] == 0
+    tw_z = _stage_table(nz)
+
+    def along_z(a, inverse):  # z by the stage tables (split pass) or any exact DFT (z in registers)
+        if split:
+            return np.swapaxes(_fft_rows(np.swapaxes(a, 1, 2), tw_z, inverse), 1, 2)
+        return np.fft.ifft(a, axis=1) * nz if inverse else np.fft.fft(a, axis=1)
+
     def pass_yz(spec, ref_conj):
-        F = np.fft.fft(_fft_rows(spec, t["tw_y"], False), axis=1)  # y by the tables, z in registers
+        F = along_z(_fft_rows(spec, t["tw_y"], False), False)  # y by the tables
         if ref_conj is None:
             return np.conj(F)
         c = F * ref_conj
         q = np.abs(c) ** 2
         c = np.where(q > 0, c / np.sqrt(np.where(q > 0, q, 1.0)), 0)
-        return _fft_rows(np.fft.ifft(c, axis=1) * nz, t["tw_y"], True)
+        return _fft_rows(along_z(c, True), t["tw_y"], True)
 
     def pass_rows_inv(spec):
         X = spec.reshape(M + 1, nz * ny).T
@@ -120,7 +130,7 @@ def _cpu_surface(reference, volume):
     return np.fft.ifftn(c).real * c.size
 
 
-@pytest.mark.parametrize("shape", SHAPES, ids=lambda s: "x".join(map(str, s)))
+@pytest.mark.parametrize("shape", SHAPES + SPLIT_SHAPES, ids=lambda s: "x".join(map(str, s)))
 def test_tables_and_launch_shape(shape):
     nz, ny, nx = shape
     t = fa.plane_tables(*shape)
@@ -132,10 +142,11 @@ def test_tables_and_launch_shape(shape):
     assert np.abs(t["tw_y"] - _stage_table(ny)).max(initial=0) <= 2.3e-16
     assert len(t["tw_x"]) <= nx and len(t["tw_y"]) < ny  # the kernels' twiddle slots
     assert t["rows_per_cta"] == min(8, nz * ny, 2048 // M)
-    assert t["planes_per_cta"] == max(1, 8192 // (nz * ny))
+    split = nz > 16 or nz * ny > 8192
+    assert t["planes_per_cta"] == (0 if split else max(1, 8192 // (nz * ny)))
 
 
-@pytest.mark.parametrize("shape", SHAPES[:8], ids=lambda s: "x".join(map(str, s)))
+@pytest.mark.parametrize("shape", SHAPES[:8] + SPLIT_SHAPES[:3], ids=lambda s: "x".join(map(str, s)))
 def test_pass_structure_matches_dft(shape):
     nz, ny, nx = shape
     rng = np.random.default_rng(nz * 7 + ny * 3 + nx)
@@ -147,7 +158,8 @@ def test_pass_structure_matches_dft(shape):
     assert int(np.argmax(got)) == int(np.argmax(want))
 
 
-@pytest.mark.parametrize("shape", [(3, 20, 30), (32, 16, 16), (1, 4, 64), (1, 64, 12), (1, 4096, 16), (1, 8, 8192)],
+@pytest.mark.parametrize("shape", [(3, 20, 30), (2, 8, 8192), (1, 4, 64), (1, 64, 12), (1, 4096, 16), (1, 8, 8192),
+                                   (2048, 16, 16), (32, 8, 16)],
                          ids=lambda s: "x".join(map(str, s)))
 def test_other_dimensions_take_cufft(shape):
     with pytest.raises(fa.FaError):
