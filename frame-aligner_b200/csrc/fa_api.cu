@@ -560,6 +560,20 @@ fa_status reference_setup(fa_reference* R, const float* src, bool src_device) {
   FA_CU(cudaMemcpyAsync(R->hl.data(), Hl, R->hl.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
   FA_CU(cudaStreamSynchronize(s));
   fa::band_bounds(R->hd.data(), R->hl.data(), R->nD, R->n_dim, &h.h_inf, &h.h_mindiag);
+  {
+    double *L0, *inv0;
+    int* ok_dev;
+    FA_TRY(dalloc_t(ctx, (size_t)R->P * 2 * R->n_dim, &L0, R->allocs));
+    FA_TRY(dalloc_t(ctx, (size_t)R->P, &inv0, R->allocs));
+    FA_TRY(dalloc_t(ctx, 1, &ok_dev, tmp));
+    FA_CU(fa::launch_chol0(Hd, Hl, R->nD, R->n_dim, L0, inv0, ok_dev, s));
+    int ok = 0;
+    FA_CU(cudaMemcpyAsync(&ok, ok_dev, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FA_CU(cudaStreamSynchronize(s));
+    h.L0 = L0;
+    h.inv0 = inv0;
+    h.chol0_ok = ok;
+  }
   FA_CU(cudaMemcpyAsync(R->dev, &h, sizeof(RefDev), cudaMemcpyHostToDevice, s));
   FA_CU(cudaStreamSynchronize(s));
   dfree_all(ctx, tmp);

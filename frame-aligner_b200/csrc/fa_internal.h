@@ -104,6 +104,12 @@ struct RefDev {
   const double* Hl;  // nD blocks (block k couples k and k-1; block 0 unused)
   double h_inf;      // max_i sum_j |H_ij| (ascending j), the subproblem's bracket bound
   double h_mindiag;  // min_i H_ii
+  // The band Cholesky factor of H itself (lambda = 0), the same for every frame and iteration of the
+  // reference: P rows of 2 * n_dim entries and P reciprocal diagonals, or null; chol0_ok = 0 when H
+  // is not positive definite.
+  const double* L0;
+  const double* inv0;
+  int chol0_ok;
 };
 
 // h_inf and h_mindiag of a block-tridiagonal H from its blocks (host), summing |H_ij| over ascending

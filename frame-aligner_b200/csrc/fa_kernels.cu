@@ -1,6 +1,6 @@
 // fa_kernels.cu -- sm_100a kernels of the warper path.
 //
-//   sobel_kernel    Sobel3d (FrameAligner/Sobel3d.cpp:8-85), bit-exact float arithmetic
+//   sobel_tiled_kernel  Sobel3d (FrameAligner/Sobel3d.cpp:8-85), bit-exact float arithmetic
 //   hessian_*       computeSteepestDecentImages + computeHessian (FrameWarper.cpp:296-395)
 //   eval_kernel     fused warpImageInterpolated + computeErrorImage + computeJacobian
 //                   (FrameWarper.cpp:4-69,147-176): one HBM pass per frame evaluation
@@ -29,39 +29,79 @@ __device__ __forceinline__ float pass(int i, int n, bool copy_if_single, const f
   return __fadd_rn(__fadd_rn(__fmul_rn(f[0], get(i - 1)), __fmul_rn(f[1], get(i))), __fmul_rn(f[2], get(i + 1)));
 }
 
-__global__ void __launch_bounds__(256) sobel_kernel(const float* __restrict__ m, int nz, int ny, int nx,
-                                                    float* __restrict__ gx, float* __restrict__ gy,
-                                                    float* __restrict__ gz) {
+// Sobel3d (Sobel3d.cpp:60-85) with each separable pass computed once per voxel: a CTA takes a tile of
+// kSbZ x kSbY x kSbX outputs, loads the reference over the tile plus a one-voxel halo (clipped to the
+// volume) into shared memory and forms the intermediate images there -- a = Sx(m) and a' = Sy(m) on
+// the halo, then b = Sy(a), c = Sz(a), b' = Sz(a'), then gz = Dz(b), gy = Dy(c), gx = Dx(b'). Every
+// value is produced by `pass` with the global index along its axis, so the edge rules apply at the
+// volume's faces and every product and sum is rounded in the reference's order: gx = Dx(Sz(Sy(m))),
+// gy = Dy(Sz(Sx(m))), gz = Dz(Sy(Sx(m))) (Sobel3d.cpp:73-84), bit for bit.
+constexpr int kSbX = 32, kSbY = 8, kSbZ = 4;
+constexpr int kSbHX = kSbX + 2, kSbHY = kSbY + 2, kSbHZ = kSbZ + 2;
+constexpr int kSbVol = kSbHX * kSbHY * kSbHZ;
+
+__global__ void __launch_bounds__(256) sobel_tiled_kernel(const float* __restrict__ m, int nz, int ny, int nx,
+                                                          float* __restrict__ gx, float* __restrict__ gy,
+                                                          float* __restrict__ gz) {
+  __shared__ float sM[kSbVol];   // m, later b
+  __shared__ float sA[kSbVol];   // a = Sx(m)
+  __shared__ float sA2[kSbVol];  // a' = Sy(m)
+  __shared__ float sC[kSbVol];   // c = Sz(a)
+  __shared__ float sB2[kSbVol];  // b' = Sz(a')
   const float sm[3] = {1.0f / 4.0f, 2.0f / 4.0f, 1.0f / 4.0f};
   const float se[2] = {2.0f / 3.0f, 2.0f / 3.0f};
   const float dm[3] = {-0.5f, 0.0f, 0.5f};
   const float de1[2] = {-0.5f, 0.5f};
   const float de2[2] = {0.5f, -0.5f};
-  const long long N = (long long)nz * ny * nx;
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N; p += (long long)gridDim.x * blockDim.x) {
-    const int x = (int)(p % nx);
-    const long long row = p / nx;
-    const int y = (int)(row % ny);
-    const int z = (int)(row / ny);
-    auto M = [&](int zz, int yy, int xx) { return __ldg(m + ((long long)zz * ny + yy) * nx + xx); };
-    // a = Sx(m); b = Sy(a); c = Sz(a); gz = Dz(b); gy = Dy(c)  (Sobel3d.cpp:73-79)
-    auto A = [&](int zz, int yy, int xx) { return pass(xx, nx, false, sm, se, se, [&](int k) { return M(zz, yy, k); }); };
-    auto B = [&](int zz, int yy, int xx) { return pass(yy, ny, false, sm, se, se, [&](int k) { return A(zz, k, xx); }); };
-    auto Cc = [&](int zz, int yy, int xx) { return pass(zz, nz, true, sm, se, se, [&](int k) { return A(k, yy, xx); }); };
-    gz[p] = pass(z, nz, true, dm, de1, de2, [&](int k) { return B(k, y, x); });
-    gy[p] = pass(y, ny, false, dm, de1, de2, [&](int k) { return Cc(z, k, x); });
-    // a' = Sy(m); b' = Sz(a'); gx = Dx(b')  (Sobel3d.cpp:81-84)
-    auto A2 = [&](int zz, int yy, int xx) { return pass(yy, ny, false, sm, se, se, [&](int k) { return M(zz, k, xx); }); };
-    auto B2 = [&](int zz, int yy, int xx) { return pass(zz, nz, true, sm, se, se, [&](int k) { return A2(k, yy, xx); }); };
-    gx[p] = pass(x, nx, false, dm, de1, de2, [&](int k) { return B2(z, y, k); });
-  }
+  const int x0 = blockIdx.x * kSbX, y0 = blockIdx.y * kSbY, z0 = blockIdx.z * kSbZ;
+  // local index of global (z, y, x): origin at (z0 - 1, y0 - 1, x0 - 1)
+  auto L = [&](int z, int y, int x) { return ((z - z0 + 1) * kSbHY + (y - y0 + 1)) * kSbHX + (x - x0 + 1); };
+  // a range [lo, hi) of global positions along an axis, clipped to the volume
+  const int hz0 = max(z0 - 1, 0), hz1 = min(z0 + kSbZ + 1, nz), tz1 = min(z0 + kSbZ, nz);
+  const int hy0 = max(y0 - 1, 0), hy1 = min(y0 + kSbY + 1, ny), ty1 = min(y0 + kSbY, ny);
+  const int hx0 = max(x0 - 1, 0), hx1 = min(x0 + kSbX + 1, nx), tx1 = min(x0 + kSbX, nx);
+  // run f(z, y, x) over a box
+  auto box = [&](int za, int zb, int ya, int yb, int xa, int xb, auto f) {
+    const int wx = xb - xa, wy = yb - ya, n = (zb - za) * wy * wx;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const int x = xa + i % wx, r = i / wx;
+      f(za + r / wy, ya + r % wy, x);
+    }
+  };
+  box(hz0, hz1, hy0, hy1, hx0, hx1,
+      [&](int z, int y, int x) { sM[L(z, y, x)] = __ldg(m + ((long long)z * ny + y) * nx + x); });
+  __syncthreads();
+  // a = Sx(m) on (halo z, halo y, tile x); a' = Sy(m) on (halo z, tile y, halo x)
+  box(hz0, hz1, hy0, hy1, x0, tx1, [&](int z, int y, int x) {
+    sA[L(z, y, x)] = pass(x, nx, false, sm, se, se, [&](int k) { return sM[L(z, y, k)]; });
+  });
+  box(hz0, hz1, y0, ty1, hx0, hx1, [&](int z, int y, int x) {
+    sA2[L(z, y, x)] = pass(y, ny, false, sm, se, se, [&](int k) { return sM[L(z, k, x)]; });
+  });
+  __syncthreads();
+  // b = Sy(a) on (halo z, tile y, tile x) into sM; c = Sz(a) on (tile z, halo y, tile x);
+  // b' = Sz(a') on (tile z, tile y, halo x)
+  box(hz0, hz1, y0, ty1, x0, tx1, [&](int z, int y, int x) {
+    sM[L(z, y, x)] = pass(y, ny, false, sm, se, se, [&](int k) { return sA[L(z, k, x)]; });
+  });
+  box(z0, tz1, hy0, hy1, x0, tx1, [&](int z, int y, int x) {
+    sC[L(z, y, x)] = pass(z, nz, true, sm, se, se, [&](int k) { return sA[L(k, y, x)]; });
+  });
+  box(z0, tz1, y0, ty1, hx0, hx1, [&](int z, int y, int x) {
+    sB2[L(z, y, x)] = pass(z, nz, true, sm, se, se, [&](int k) { return sA2[L(k, y, x)]; });
+  });
+  __syncthreads();
+  box(z0, tz1, y0, ty1, x0, tx1, [&](int z, int y, int x) {
+    const long long p = ((long long)z * ny + y) * nx + x;
+    gz[p] = pass(z, nz, true, dm, de1, de2, [&](int k) { return sM[L(k, y, x)]; });
+    gy[p] = pass(y, ny, false, dm, de1, de2, [&](int k) { return sC[L(z, k, x)]; });
+    gx[p] = pass(x, nx, false, dm, de1, de2, [&](int k) { return sB2[L(z, y, k)]; });
+  });
 }
 
 cudaError_t launch_sobel(const float* m, int nz, int ny, int nx, float* gx, float* gy, float* gz, cudaStream_t s) {
-  long long N = (long long)nz * ny * nx;
-  int blocks = (int)((N + 255) / 256);
-  if (blocks > 148 * 16) blocks = 148 * 16;
-  sobel_kernel<<<blocks, 256, 0, s>>>(m, nz, ny, nx, gx, gy, gz);
+  const dim3 grid((nx + kSbX - 1) / kSbX, (ny + kSbY - 1) / kSbY, (nz + kSbZ - 1) / kSbZ);
+  sobel_tiled_kernel<<<grid, 256, 0, s>>>(m, nz, ny, nx, gx, gy, gz);
   return cudaGetLastError();
 }
 

@@ -86,6 +86,10 @@ cudaError_t launch_solve(const Job* jobs_dev, int n_jobs, int max_nD, int n_dim,
                          const int* active = nullptr, const int* n_active = nullptr);
 
 // Test hook: the device trust-region subproblem on given dense H (P x P) and g.
+// The band Cholesky factor of H (lambda = 0) into L0 (nD * nd rows of 2 * nd) and inv0 (nD * nd); *ok
+// = 0 when H is not positive definite. One thread: the same arithmetic as the solver's factorisations.
+cudaError_t launch_chol0(const double* Hd, const double* Hl, int nD, int nd, double* L0, double* inv0, int* ok,
+                         cudaStream_t s);
 cudaError_t launch_test_subproblem(const double* Hd, const double* Hl, int nD, int nd, double hinf, double mindiag,
                                    const double* g, double radius, double* p_out, int* boundary_out, double* work,
                                    cudaStream_t s);

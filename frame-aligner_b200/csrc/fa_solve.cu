@@ -31,6 +31,10 @@ struct Band {
   const double* Hl;
   int nD, P;
   double hinf, mindiag;  // band_bounds of H
+  // band_chol(lambda = 0) computed once per reference (RefDev::L0), or null
+  const double* L0 = nullptr;
+  const double* inv0 = nullptr;
+  int chol0_ok = 0;
 };
 
 // Band factor storage: row i of block b holds 2*n_dim entries, the columns of block b-1 then those of
@@ -168,14 +172,26 @@ __device__ int subproblem(const Band<ND>& B, const double* g, double radius, dou
   double lambda = 0.0;
   for (int i = 0; i < P; i++) rhs[i] = -g[i];
   for (int it = 0; it < max_iter; it++) {
-    if (band_chol(B, lambda, L, inv) != 0) {
+    // H + 0 I is the same matrix for every frame and step of the reference: its factor is computed
+    // once (by this same band_chol, so the values are identical) and reused
+    const double* Lc = L;
+    const double* ic = inv;
+    bool ok;
+    if (lambda == 0.0 && B.L0 != nullptr) {
+      ok = B.chol0_ok != 0;
+      Lc = B.L0;
+      ic = B.inv0;
+    } else {
+      ok = band_chol(B, lambda, L, inv) == 0;
+    }
+    if (!ok) {
       if (lambda > lam_lo) lam_lo = lambda;
       const double a = sqrt(lam_lo * lam_hi), b = lam_lo + 0.001 * (lam_hi - lam_lo);
       lambda = a > b ? a : b;
       continue;
     }
-    band_forward(B, L, inv, rhs, y);
-    band_backward(B, L, inv, y, p);
+    band_forward(B, Lc, ic, rhs, y);
+    band_backward(B, Lc, ic, y, p);
     have_p = 1;
     const double pn = norm2(P, p);
     if (lambda == 0.0 && pn <= radius) {
@@ -188,7 +204,7 @@ __device__ int subproblem(const Band<ND>& B, const double* g, double radius, dou
     } else {
       if (lambda > lam_lo) lam_lo = lambda;
     }
-    band_forward(B, L, inv, p, y);
+    band_forward(B, Lc, ic, p, y);
     const double qn = norm2(P, y);
     const double r = pn / qn;
     double next = lambda + r * r * (pn - radius) / radius;
@@ -270,7 +286,7 @@ template <int ND>
 __device__ void state_step(const Job& job, FrameState* S, const RefDev& R, const double* Hd, const double* Hl,
                            double* gv, double* pv, double* work, double ft) {
   const int P = R.P, nd = ND;
-  Band<ND> B{Hd, Hl, R.nD, P, R.h_inf, R.h_mindiag};
+  Band<ND> B{Hd, Hl, R.nD, P, R.h_inf, R.h_mindiag, R.L0, R.inv0, R.chol0_ok};
   double* x = job.x;
   double* g = gv;
   double* p = pv;
@@ -461,6 +477,23 @@ cudaError_t launch_solve(const Job* jobs_dev, int n_jobs, int max_nD, int n_dim,
     if (e != cudaSuccess) return e;
   }
   solve_kernel<<<n_jobs, kSolveThreads, smem, s>>>(jobs_dev, smem / (int)sizeof(double), active, n_active);
+  return cudaGetLastError();
+}
+
+__global__ void chol0_kernel(const double* Hd, const double* Hl, int nD, int nd, double* L0, double* inv0, int* ok) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (nd == 3) {
+    Band<3> B{Hd, Hl, nD, nD * 3, 0.0, 0.0};
+    *ok = band_chol(B, 0.0, L0, inv0) == 0;
+  } else {
+    Band<2> B{Hd, Hl, nD, nD * 2, 0.0, 0.0};
+    *ok = band_chol(B, 0.0, L0, inv0) == 0;
+  }
+}
+
+cudaError_t launch_chol0(const double* Hd, const double* Hl, int nD, int nd, double* L0, double* inv0, int* ok,
+                         cudaStream_t s) {
+  chol0_kernel<<<1, 32, 0, s>>>(Hd, Hl, nD, nd, L0, inv0, ok);
   return cudaGetLastError();
 }
 
