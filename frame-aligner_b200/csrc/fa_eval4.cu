@@ -393,15 +393,18 @@ struct SegParams {
   int meta;                 // bit 0: uniform; bits 1-2: window alignment; bits 3..: storage range
 };
 constexpr int kSegBatch = 32;  // segments classified per round, one per lane
+// A segment is kSegGroups groups of 128 voxels; each lane takes four voxels of every group.
+constexpr int kSegGroups = 1;
+constexpr int kSegLen = 128 * kSegGroups;
 
 // One tile of one frame, processed by one warp on its own: its control-point window sD (the warp's
 // slice of shared memory), its row segments, and its partial sums. No CTA barrier is involved, so
 // the warps of a CTA drift apart and hide each other's load latency.
 //
-// A row segment is 128 consecutive voxels of an image row, four per lane. Almost every segment is
-// uniform: its voxels share one displacement interval and one storage range, contain no range end,
-// and their sample positions x + d(x) share one integer offset per axis, because the displacement
-// changes by ~1e-5 px per voxel along a row. Whether it is, and its weights, slopes and window
+// A row segment is kSegLen consecutive voxels of an image row, four per lane and 128-voxel group.
+// Almost every segment is uniform: its voxels share one displacement interval and one storage range,
+// contain no range end, and their sample positions x + d(x) share one integer offset per axis,
+// because the displacement changes by ~1e-5 px per voxel along a row. Whether it is, and its weights, slopes and window
 // offsets, follow from the row descriptor and the segment's two ends (the position is monotone in x
 // within an interval). The warp first classifies 32 segments at once, one per lane, into shared
 // memory, then walks them: a uniform segment needs no per-lane interval, range or offset logic, its
@@ -460,8 +463,8 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
   };
   const float lane_u = (float)(lane * 4);  // x - (segment start) of the lane's first voxel
 
-  // 128-voxel segments of the tile's rows
-  const int segs = (nx + 127) >> 7;
+  // segments of the tile's rows
+  const int segs = (nx + kSegLen - 1) / kSegLen;
   const int n_items = (row_end - row_begin) * segs;
   const long long plane = job.fplane;
   const int pitch = job.fpitch;
@@ -471,10 +474,10 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
     if (base + lane < n_items) {
       const int it = base + lane;
       const int row = row_begin + it / segs;
-      const int xa = (it - (row - row_begin) * segs) * 128;
+      const int xa = (it - (row - row_begin) * segs) * kSegLen;
       const RowDesc rd = R.rows[row];
       const bool flip = bidir && (rd.y & 1);
-      const int xb = min(xa + 127, nx - 1);
+      const int xb = min(xa + kSegLen - 1, nx - 1);
       const int xsa = flip ? nx - 1 - xa : xa, xsb = flip ? nx - 1 - xb : xb;
       const int dia = rd.di0 + (xsa >= rd.xdi ? 1 : 0);
       const int dib = rd.di0 + (xsb >= rd.xdi ? 1 : 0);
@@ -500,7 +503,7 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
       const int iy = rd.y + (int)na.y + (int)fly;
       const int iz = NDIM == 3 ? rd.z + (int)na.z + (int)flz : 0;
       const int ab = ox & ~3;                   // window start relative to x0 (multiple of 4)
-      const int x_last = min(xa + 124, nx - 4);  // first voxel of the segment's last active lane
+      const int x_last = min(xa + kSegLen - 4, nx - 4);  // first voxel of the segment's last active lane
       int cy, cz;
       if (padded) {
         // windows inside the row's zero halo; tap rows / planes wholly outside read halo zeros
@@ -532,35 +535,39 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
     const int cnt = min(kSegBatch, n_items - base);
     for (int q = 0; q < cnt; q++) {
       const SegParams P = sp[q];
-      const int xa = ((base + q) % segs) * 128;
-      const int x0 = xa + lane * 4;
+      const int xa = ((base + q) % segs) * kSegLen;
       if (P.meta & 1) {
         const int ra = P.meta >> 3;
         if (ra != ur) {
           flush_uniform();
           ur = ra;
         }
-        if (x0 < nx) {
-          float t4[4], g4[NDIM][4];
-          src.template load<NDIM>(P.p0 + lane * 4, t4, g4);
-          const FT* wp = fr + (P.win + lane * 4);
-          const float wxl = fmaf(lane_u, P.sx, P.w0x);
-          const float wyl = fmaf(lane_u, P.sy, P.w0y);
-          const float wzl = NDIM == 3 ? fmaf(lane_u, P.sz, P.w0z) : 0.0f;
-          const float fl = fmaf(lane_u, P.fs, P.f0);
-          switch ((P.meta >> 1) & 3) {
-            case 0:
-              uniform4<NDIM, 0>(wp, plane, pitch, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
-              break;
-            case 1:
-              uniform4<NDIM, 1>(wp, plane, pitch, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
-              break;
-            case 2:
-              uniform4<NDIM, 2>(wp, plane, pitch, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
-              break;
-            default:
-              uniform4<NDIM, 3>(wp, plane, pitch, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
-              break;
+#pragma unroll
+        for (int gi = 0; gi < kSegGroups; gi++) {
+          const int x0 = xa + gi * 128 + lane * 4;
+          if (x0 < nx) {
+            float t4[4], g4[NDIM][4];
+            src.template load<NDIM>(P.p0 + gi * 128 + lane * 4, t4, g4);
+            const FT* wp = fr + (P.win + gi * 128 + lane * 4);
+            const float u = lane_u + (float)(gi * 128);
+            const float wxl = fmaf(u, P.sx, P.w0x);
+            const float wyl = fmaf(u, P.sy, P.w0y);
+            const float wzl = NDIM == 3 ? fmaf(u, P.sz, P.w0z) : 0.0f;
+            const float fl = fmaf(u, P.fs, P.f0);
+            switch ((P.meta >> 1) & 3) {
+              case 0:
+                uniform4<NDIM, 0>(wp, plane, pitch, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
+                break;
+              case 1:
+                uniform4<NDIM, 1>(wp, plane, pitch, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
+                break;
+              case 2:
+                uniform4<NDIM, 2>(wp, plane, pitch, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
+                break;
+              default:
+                uniform4<NDIM, 3>(wp, plane, pitch, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
+                break;
+            }
           }
         }
       }
@@ -570,16 +577,18 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
     // free for the per-lane path)
     for (int q = 0; q < cnt; q++) {
       if (sp[q].meta & 1) continue;
-      const int x0 = ((base + q) % segs) * 128 + lane * 4;
-      if (x0 < nx) {
-        const int row = row_begin + (base + q) / segs;
-        const LaneSums<NDIM> ls = lane_item<NDIM, FT, RT>(fr, plane, pitch, padded, src, R.rows[row], x0, row, nx,
-                                                         ny, nz, bidir, dq, sD, cw, c0);
-        af += ls.f;
+      for (int gi = 0; gi < kSegGroups; gi++) {
+        const int x0 = ((base + q) % segs) * kSegLen + gi * 128 + lane * 4;
+        if (x0 < nx) {
+          const int row = row_begin + (base + q) / segs;
+          const LaneSums<NDIM> ls = lane_item<NDIM, FT, RT>(fr, plane, pitch, padded, src, R.rows[row], x0, row, nx,
+                                                           ny, nz, bidir, dq, sD, cw, c0);
+          af += ls.f;
 #pragma unroll
-        for (int s2 = 0; s2 < 3; s2++)
+          for (int s2 = 0; s2 < 3; s2++)
 #pragma unroll
-          for (int k = 0; k < NDIM; k++) ag[s2][k] += ls.g[s2][k];
+            for (int k = 0; k < NDIM; k++) ag[s2][k] += ls.g[s2][k];
+        }
       }
       // Explicit reconvergence point: the per-lane branches above must not leave the warp split
       // into groups that then run the rest of the loop one after the other.
