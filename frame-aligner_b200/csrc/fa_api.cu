@@ -1676,6 +1676,16 @@ fa_status aligner_grow(fa_aligner* A, int n, int kind, size_t staging_need) {
   return FA_OK;
 }
 
+// Solve groups of one call, as frame boundaries {0, ..., n}. Host batches of 2 * chunk frames or
+// more are solved in two groups: the first group's solve runs while the second group uploads and
+// correlates. Frames are independent, so the results do not depend on the grouping. The first group
+// takes about 45% of the frames (whole upload chunks), which balances its solve against the second
+// group's uploads. Frames already on the device are solved in one group.
+std::vector<int> solve_groups(int n, bool device_src, int chunk) {
+  if (device_src || n < 2 * chunk) return {0, n};
+  return {0, std::min(n - chunk, ((9 * n / 20 + chunk - 1) / chunk) * chunk), n};
+}
+
 fa_status aligner_run(fa_aligner* A, const void* const* frames, fa_dtype dtype, int n, bool device_src,
                       double* D_out, fa_align_stats* stats) {
   if (!A->ref) return fail(FA_ERR_STATE, "Reference imaging not yet set");  // FrameWarpAligner.cpp:119
@@ -1702,7 +1712,8 @@ fa_status aligner_run(fa_aligner* A, const void* const* frames, fa_dtype dtype, 
   const int chunk = device_src ? n : kChunk;
   if (!device_src) {
     if (!A->copy_stream) FA_CU(cudaStreamCreateWithFlags(&A->copy_stream, cudaStreamNonBlocking));
-    while ((int)A->copy_ev.size() < (n + chunk - 1) / chunk) {
+    // one event per upload chunk: chunks never straddle a solve group, so a group adds at most one
+    while ((int)A->copy_ev.size() < (n + chunk - 1) / chunk + (int)solve_groups(n, device_src, chunk).size()) {
       cudaEvent_t e;
       FA_CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
       A->copy_ev.push_back(e);
@@ -1721,12 +1732,9 @@ fa_status aligner_run(fa_aligner* A, const void* const* frames, fa_dtype dtype, 
     }
   } drain{device_src ? nullptr : A->copy_stream};
   FA_TRY(correlator_reserve(A->corr, n));
-  // Host batches of 2 * kChunk frames or more are solved in two groups: the first group's solve
-  // runs while the second group uploads and correlates. Frames are independent, so the results do
-  // not depend on the grouping. The first group takes about 45% of the frames: uploads run at about
-  // two thirds of the solve's rate, which balances its solve against the second group's uploads.
-  const int n_groups = (!device_src && n >= 2 * kChunk) ? 2 : 1;
-  const int g_split = n_groups == 2 ? std::min(n - kChunk, ((9 * n / 20 + kChunk - 1) / kChunk) * kChunk) : n;
+  const std::vector<int> gb = solve_groups(n, device_src, kChunk);  // group g: frames [gb[g], gb[g + 1])
+  const int n_groups = (int)gb.size() - 1;
+  while ((int)A->batch_cache.size() < n_groups) A->batch_cache.emplace_back();
   while ((int)A->group_ev.size() < n_groups) {
     cudaEvent_t e;
     FA_CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -1735,8 +1743,9 @@ fa_status aligner_run(fa_aligner* A, const void* const* frames, fa_dtype dtype, 
   fa_correlator* C = A->corr;
   std::vector<const void*> raw((size_t)n), cin((size_t)n);
   int cin_kind = dtype;
-  for (int c0 = 0, ci = 0; c0 < n; c0 += chunk, ci++) {
-    const int m = std::min({chunk, n - c0, c0 < g_split ? g_split - c0 : n - c0});
+  for (int c0 = 0, ci = 0, g = 0; c0 < n; ci++) {
+    while (gb[g + 1] <= c0) g++;
+    const int m = std::min(chunk, gb[g + 1] - c0);
     if (!device_src) {
       for (int i = c0; i < c0 + m; i++) {
         void* dst = static_cast<char*>(A->staging) + (size_t)i * raw_bytes;
@@ -1769,16 +1778,16 @@ fa_status aligner_run(fa_aligner* A, const void* const* frames, fa_dtype dtype, 
       }
     }
     FA_TRY(correlator_enqueue(C, cin.data() + c0, cin_kind, m, nullptr, true, c0));
-    if (c0 + m == g_split || c0 + m == n) {  // a group's peaks, read back without waiting for the rest
-      const int g0 = c0 + m == g_split ? 0 : g_split;
-      FA_CU(cudaMemcpyAsync(C->h_idx + g0, C->d_idx + g0, (size_t)(c0 + m - g0) * sizeof(long long),
+    c0 += m;
+    if (c0 == gb[g + 1]) {  // a group's peaks, read back without waiting for the rest
+      FA_CU(cudaMemcpyAsync(C->h_idx + gb[g], C->d_idx + gb[g], (size_t)(c0 - gb[g]) * sizeof(long long),
                             cudaMemcpyDeviceToHost, s));
-      FA_CU(cudaEventRecord(A->group_ev[g0 == 0 ? 0 : 1], s));
+      FA_CU(cudaEventRecord(A->group_ev[g], s));
     }
   }
   std::vector<fa_frame*> batch(A->slots.begin(), A->slots.begin() + n);
   for (int g = 0; g < n_groups; g++) {
-    const int g0 = g == 0 ? 0 : g_split, g1 = g == 0 ? g_split : n;
+    const int g0 = gb[g], g1 = gb[g + 1];
     FA_CU(cudaEventSynchronize(A->group_ev[g]));
     std::vector<double> rigid((size_t)3 * (g1 - g0));
     for (int i = g0; i < g1; i++) {

@@ -6,6 +6,7 @@
 #include <cufft.h>
 
 #include <atomic>
+#include <deque>
 #include <map>
 #include <mutex>
 #include <string>
@@ -182,7 +183,7 @@ struct fa_aligner {
   cudaStream_t copy_stream = nullptr;
   std::vector<cudaEvent_t> copy_ev;
   std::vector<cudaEvent_t> group_ev;  // peaks of a group of frames read back
-  fa_rt::BatchCache batch_cache[2];   // the batched solve's buffers and graph per solve group
+  std::deque<fa_rt::BatchCache> batch_cache;  // the batched solve's buffers and graph per solve group
   // smoothStack (smoothing > 0): Gaussian weights along x and y, and two frame-sized work buffers
   // used one frame at a time in stream order
   float* smooth_kx = nullptr;
