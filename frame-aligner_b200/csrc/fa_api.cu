@@ -745,9 +745,11 @@ fa_status frame_alloc(fa_reference* R, int kind, fa_frame** out) {
   j.fplane = plane;
   j.fpitch = pitch;
   j.fpad = 1;
-  if ((st = dalloc_t(ctx, (size_t)R->nD * fa::kDParamF4, &j.dparams, F->allocs)) != FA_OK) return cleanup(st);
-  if ((st = dalloc_t(ctx, (size_t)R->G.n_tiles * fa::kPartialDoubles, &j.partials, F->allocs)) != FA_OK)
+  if ((st = dalloc_t(ctx, (size_t)R->nD * fa::kDParamF4 * 2, &j.dparams, F->allocs)) != FA_OK) return cleanup(st);
+  j.dparams2 = j.dparams + (size_t)R->nD * fa::kDParamF4;
+  if ((st = dalloc_t(ctx, (size_t)R->G.n_tiles * fa::kPartialDoubles * 2, &j.partials, F->allocs)) != FA_OK)
     return cleanup(st);
+  j.partials2 = j.partials + (size_t)R->G.n_tiles * fa::kPartialDoubles;
   if ((st = dalloc_t(ctx, 1, &F->state, F->allocs)) != FA_OK) return cleanup(st);
   double* pool;
   size_t nd = 4 * P + work_doubles(R) + 1 + P;
@@ -924,7 +926,7 @@ extern "C" fa_status fa_warp(fa_frame* F, const double* D, float invalid_value, 
 
 namespace {
 
-fa_status init_solve(fa_frame* F, const double* rigid, int max_iterations) {
+fa_status init_solve(fa_frame* F, const double* rigid, int max_iterations, bool pair) {
   fa_reference* R = F->ref;
   fa::FrameState& S = *F->h_state;
   std::memset(&S, 0, sizeof(S));
@@ -932,8 +934,20 @@ fa_status init_solve(fa_frame* F, const double* rigid, int max_iterations) {
   S.max_iter = max_iterations > 0 ? max_iterations : 100;
   for (int c = 0; c < 3; c++) S.rigid[c] = rigid ? rigid[c] : 0.0;
   if (R->n_dim == 2) S.rigid[2] = 0.0;
+  bool nonzero = false;
+  for (int c = 0; c < R->n_dim; c++) nonzero = nonzero || S.rigid[c] != 0.0;
   Job j = F->job;
   j.state = F->state;
+  if (pair && nonzero) {
+    // both cold starting points in the first pass: the rigid shift's parameters go to dparams2
+    S.phase = fa::kPhaseStartPair;
+    std::vector<double> D((size_t)R->nD * 3);
+    for (int k = 0; k < R->nD; k++)
+      for (int c = 0; c < 3; c++) D[(size_t)3 * k + c] = S.rigid[c];
+    make_dparams(D.data(), R->nD, R->n_dim, F->h_dparams);
+    FA_CU(cudaMemcpyAsync(j.dparams2, F->h_dparams, (size_t)R->nD * fa::kDParamF4 * sizeof(float4),
+                          cudaMemcpyHostToDevice, F->stream));
+  }
   FA_CU(cudaMemcpyAsync(F->state, &S, sizeof(S), cudaMemcpyHostToDevice, F->stream));
   FA_CU(cudaMemsetAsync(j.x, 0, 4 * (size_t)R->P * sizeof(double), F->stream));
   FA_CU(cudaMemsetAsync(j.dparams, 0, (size_t)R->nD * fa::kDParamF4 * sizeof(float4), F->stream));
@@ -983,7 +997,7 @@ extern "C" fa_status fa_align_frame(fa_frame* F, const double* rigid_shift, int 
   std::lock_guard<std::mutex> lk(F->mu);
   fa_reference* R = F->ref;
   FA_CU(cudaSetDevice(R->ctx->device));
-  FA_TRY(init_solve(F, rigid_shift, max_iterations));
+  FA_TRY(init_solve(F, rigid_shift, max_iterations, false));
   Job j = F->job;
   j.state = F->state;
   FA_CU(cudaMemcpyAsync(F->job_dev, &j, sizeof(Job), cudaMemcpyHostToDevice, F->stream));
@@ -1030,23 +1044,26 @@ fa_status align_batch_impl(fa_frame* const* frames, int n, const double* rigid_s
   cudaStream_t s = frames[0]->stream;
   int max_tiles = 0, max_nD = 0;
   bool vec4 = true;
+  for (int i = 0; i < n; i++) vec4 = vec4 && (frames[i]->ref->nx % 4 == 0);
+  // the persistent pass evaluates both cold starting points of a frame in its first launch
+  const bool vec4_all = vec4;
   std::vector<Job> jobs(n);
   // initial states on every frame's stream, then one wait per stream (the copies are done by then)
   for (int i = 0; i < n; i++) {
     fa_frame* F = frames[i];
-    FA_TRY(init_solve(F, rigid_shifts ? rigid_shifts + 3 * i : nullptr, max_iterations));
+    FA_TRY(init_solve(F, rigid_shifts ? rigid_shifts + 3 * i : nullptr, max_iterations, vec4_all));
     jobs[i] = F->job;
     jobs[i].state = F->state;
     if (frame_data) jobs[i].frame = frame_data[i];
     max_tiles = std::max(max_tiles, F->ref->G.n_tiles);
-    vec4 = vec4 && (F->ref->nx % 4 == 0);
     max_nD = std::max(max_nD, F->ref->nD);
   }
   for (int i = 0; i < n; i++) FA_CU(cudaStreamSynchronize(frames[i]->stream));
   std::vector<int> all(n), prefix(n + 1, 0);
   for (int i = 0; i < n; i++) {
     all[i] = i;
-    prefix[i + 1] = prefix[i] + frames[i]->ref->G.n_tiles;
+    // a frame in the paired start phase has two items per tile
+    prefix[i + 1] = prefix[i] + frames[i]->ref->G.n_tiles * (frames[i]->h_state->phase == fa::kPhaseStartPair ? 2 : 1);
   }
   BatchCache local;
   BatchCache* bc = cache ? cache : &local;

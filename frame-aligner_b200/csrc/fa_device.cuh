@@ -170,4 +170,17 @@ __device__ __forceinline__ void write_trial_dparams(const Job& job, const RefDev
   }
 }
 
+// Control-point parameters of the displacement D[k] = d for every control point (a rigid shift):
+// the values write_trial_dparams produces for x + p = d, computed the same way.
+__device__ __forceinline__ void write_const_dparams(float4* dp, int nD, int nd, const double* d3, int t0, int stride) {
+  double d[3];
+  for (int c = 0; c < 3; c++) d[c] = c < nd ? 0.0 + d3[c] : 0.0;
+  const double f0 = floor(d[0]), f1 = floor(d[1]), f2 = floor(d[2]);
+  for (int k = t0; k < nD; k += stride) {
+    dp[k * kDParamF4 + 0] = make_float4((float)f0, (float)f1, (float)f2, 0.f);
+    dp[k * kDParamF4 + 1] = make_float4((float)(d[0] - f0), (float)(d[1] - f1), (float)(d[2] - f2), 0.f);
+    dp[k * kDParamF4 + 2] = make_float4((float)(d[0] - d[0]), (float)(d[1] - d[1]), (float)(d[2] - d[2]), 0.f);
+  }
+}
+
 }  // namespace fa

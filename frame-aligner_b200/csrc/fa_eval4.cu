@@ -413,7 +413,8 @@ constexpr int kSegLen = 128 * kSegGroups;
 // per-lane path (lane_item), which handles every case voxel by voxel where needed.
 template <int NDIM, typename FT, typename RT>
 __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, const int tile, float4* sD,
-                                           SegParams* sp) {
+                                           SegParams* sp, const float4* __restrict__ dparams,
+                                           double* __restrict__ partials) {
   const int nx = R.nx, ny = R.ny, nz = R.nz;
   const int row_begin = tile * R.tile_rows;
   const int row_end = min(row_begin + R.tile_rows, R.n_rows);
@@ -426,7 +427,7 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
   __syncwarp();  // the previous tile's readers of sD and sp are done
   if (lane < kWin * kDParamF4) {
     const int k = cw + lane / kDParamF4;
-    sD[lane] = (k < R.nD) ? job.dparams[k * kDParamF4 + lane % kDParamF4] : make_float4(0.f, 0.f, 0.f, 0.f);
+    sD[lane] = (k < R.nD) ? dparams[k * kDParamF4 + lane % kDParamF4] : make_float4(0.f, 0.f, 0.f, 0.f);
   }
   __syncwarp();
 
@@ -613,7 +614,7 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
   for (int s = 0; s < 3; s++)
 #pragma unroll
     for (int k = 0; k < 3; k++) pick = (lane == 2 + s * 3 + k) ? (k < NDIM ? ag[s][k < NDIM ? k : 0] : 0.0f) : pick;
-  double* out = job.partials + (long long)tile * kPartialDoubles;
+  double* out = partials + (long long)tile * kPartialDoubles;
   if (lane < 11) out[lane] = lane == 1 ? (double)c0 : (double)pick;
   __syncwarp();
 }
@@ -629,7 +630,7 @@ __global__ void __launch_bounds__(kEvalThreads, MB) eval4_kernel(const Job* __re
   const int warp = threadIdx.x >> 5;
   const int tile = blockIdx.x * kEvalWarps + warp;
   if (tile >= R.n_tiles) return;
-  eval4_tile<NDIM, FT, RT>(job, R, tile, sD[warp], sp[warp]);
+  eval4_tile<NDIM, FT, RT>(job, R, tile, sD[warp], sp[warp], job.dparams, job.partials);
 }
 
 // Persistent form for batched solves: the grid's warps walk the (active frame, tile) items of the
@@ -657,9 +658,14 @@ __global__ void __launch_bounds__(kEvalThreads, MB) eval4_active_kernel(const Jo
       else
         hi = mid - 1;
     }
-    const int tile = item - tile_prefix[a];
+    int tile = item - tile_prefix[a];
     const Job& job = jobs[active[a]];
-    eval4_tile<NDIM, FT, RT>(job, *job.ref, tile, sD[warp], sp[warp]);
+    const RefDev& R = *job.ref;
+    // a frame in the paired start phase has two items per tile: the zero start, then the rigid one
+    const bool second = tile >= R.n_tiles;
+    if (second) tile -= R.n_tiles;
+    eval4_tile<NDIM, FT, RT>(job, R, tile, sD[warp], sp[warp], second ? job.dparams2 : job.dparams,
+                             second ? job.partials2 : job.partials);
   }
 }
 

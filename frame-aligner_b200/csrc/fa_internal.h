@@ -47,8 +47,10 @@ enum Phase : int {
   kPhaseTrial = 2,       // trial = x + p
   kPhaseDone = 3,
   kPhaseStartLast = 4,   // trial = an earlier frame's solution (warm start)
-  kPhaseWaitWarm = 5     // cold starting points done; out of the passes until the warm-start vector
+  kPhaseWaitWarm = 5,    // cold starting points done; out of the passes until the warm-start vector
                          // has been written (resumed by the compact pass)
+  kPhaseStartPair = 6    // both cold starting points in one pass: zero (dparams, partials) and the
+                         // rigid shift (dparams2, partials2); persistent fused pass only
 };
 
 struct FrameState {
@@ -156,6 +158,8 @@ struct Job {
   int fpad;               // 1: the frame carries the kHalo* zero halo
   float4* dparams;        // nD * kDParamF4 (trial point of this job)
   double* partials;       // n_tiles * kPartialDoubles
+  float4* dparams2;       // the rigid starting point while the phase is kPhaseStartPair
+  double* partials2;      // its tile partial sums (n_tiles * kPartialDoubles)
   FrameState* state;      // solve state (may be null for a bare evaluation)
   double* x;              // P: accepted parameters
   double* g;              // P: gradient at x
@@ -171,7 +175,7 @@ struct Activation {
   int job;       // index in the job table
   int use_warm;  // 1: *warm is a starting point
   int max_iter;
-  int pad_;
+  int pair;      // 1: evaluate both cold starting points in one pass (kPhaseStartPair)
   double rigid[3];
   double* warm;          // FrameState::warm (null: none)
   long long* warm_seq;   // FrameState::warm_seq

@@ -693,7 +693,7 @@ __global__ void __launch_bounds__(1024) compact_kernel(const Job* __restrict__ j
     }
     const bool act = i < n && phase != kPhaseDone && phase != kPhaseWaitWarm;
     const bool fin = i < n && busy != nullptr && phase == kPhaseDone && busy[i] != 0;
-    const int tiles = act ? jobs[i].ref->n_tiles : 0;
+    const int tiles = act ? jobs[i].ref->n_tiles * (phase == kPhaseStartPair ? 2 : 1) : 0;
     int incl = tiles;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -765,9 +765,17 @@ __global__ void activate_kernel(const Job* __restrict__ jobs, const Activation* 
     j.gt[i] = 0.0;
   }
   for (int i = threadIdx.x; i < R.nD * kDParamF4; i += blockDim.x) j.dparams[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  double rigid[3];
+  bool nonzero = false;
+  for (int c = 0; c < 3; c++) {
+    rigid[c] = (c < R.n_dim) ? r.rigid[c] : 0.0;
+    nonzero = nonzero || rigid[c] != 0.0;
+  }
+  const bool pair = r.pair != 0 && nonzero;
+  if (pair) write_const_dparams(j.dparams2, R.nD, R.n_dim, rigid, threadIdx.x, blockDim.x);
   if (threadIdx.x == 0) {
     FrameState S{};
-    S.phase = kPhaseStartZero;
+    S.phase = pair ? kPhaseStartPair : kPhaseStartZero;
     S.max_iter = r.max_iter > 0 ? r.max_iter : 100;
     S.warm = r.warm;
     S.warm_seq = r.warm_seq;

@@ -302,7 +302,7 @@ fa_status class_capture(fa_server* S, SrvClass* C) {
       e = fa::launch_compact(C->jobs_dev, C->cap, C->list, n_active, C->prefix, C->busy, done_list, n_done, s);
       if (e == cudaSuccess) {
         if (C->vec4)
-          e = fa::launch_eval4_active(C->jobs_dev, C->list, n_active, C->prefix, (long long)C->cap * C->max_tiles,
+          e = fa::launch_eval4_active(C->jobs_dev, C->list, n_active, C->prefix, 2LL * C->cap * C->max_tiles,
                                       C->n_dim, C->kind, C->bf16, C->mb, C->grid_mult * S->sms, s);
         else
           e = fa::launch_eval(C->jobs_dev, C->cap, C->max_tiles, C->n_dim, C->kind, C->bf16, s, false);
@@ -545,7 +545,7 @@ fa_status class_launch(fa_server* S, SrvClass* C, bool* launched) {
       a.job = sl->index;
       a.use_warm = (lag > 0 && seq >= lag) ? 1 : 0;
       a.max_iter = q->A->prm.max_iterations;
-      a.pad_ = 0;
+      a.pair = C->vec4 ? 1 : 0;  // the persistent pass evaluates both cold starting points at once
       for (int c = 0; c < 3; c++) a.rigid[c] = sl->rigid[c];
       a.warm = lag > 0 ? q->warm + (size_t)(seq % lag) * q->A->ref->P : nullptr;
       a.warm_seq = lag > 0 ? q->warm_seq + seq % lag : nullptr;

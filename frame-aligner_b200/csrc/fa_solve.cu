@@ -284,7 +284,7 @@ __host__ __device__ inline long long solve_smem_doubles(int nD, int nd) {
 // The trust-region state machine for one frame after a fused pass at its trial point (thread 0).
 template <int ND>
 __device__ void state_step(const Job& job, FrameState* S, const RefDev& R, const double* Hd, const double* Hl,
-                           double* gv, double* pv, double* work, double ft) {
+                           double* gv, double* pv, double* work, double ft, double ft2) {
   const int P = R.P, nd = ND;
   Band<ND> B{Hd, Hl, R.nD, P, R.h_inf, R.h_mindiag, R.L0, R.inv0, R.chol0_ok};
   double* x = job.x;
@@ -311,6 +311,29 @@ __device__ void state_step(const Job& job, FrameState* S, const RefDev& R, const
         } else {
           go_top = true;
         }
+      }
+      break;
+    }
+    case kPhaseStartPair: {
+      // Both cold starting points from one pass: ft, gt at zero; ft2 and (in p) its gradient at the
+      // rigid shift. The same choice as kPhaseStartZero followed by kPhaseStartRigid.
+      S->evaluations++;
+      S->f_start = ft;
+      if (ft2 < ft) {
+        for (int k = 0; k < R.nD; k++)
+          for (int c = 0; c < nd; c++) {
+            x[k * nd + c] = S->rigid[c];
+            g[k * nd + c] = p[k * nd + c];
+          }
+        S->f = ft2;
+      } else {
+        for (int i = 0; i < P; i++) g[i] = gt[i];
+        S->f = ft;
+      }
+      if (S->use_warm && S->warm != nullptr) {
+        next = kPhaseWaitWarm;
+      } else {
+        go_top = true;
       }
       break;
     }
@@ -403,8 +426,11 @@ __global__ void __launch_bounds__(kSolveThreads, 1) solve_kernel(const Job* __re
   FrameState* S = job.state;
   if (S->phase == kPhaseDone || S->phase == kPhaseWaitWarm) return;
   const RefDev& R = *job.ref;
-  __shared__ double s_f;
+  __shared__ double s_f, s_f2;
   reduce_partials(R, job.partials, &s_f, job.gt);
+  // paired start: the rigid point's sums, its gradient into p (free until the first step)
+  const bool pair = S->phase == kPhaseStartPair;
+  if (pair) reduce_partials(R, job.partials2, &s_f2, job.p);
   __syncthreads();
   // Stage the Hessian blocks, g and p in shared memory when they fit; otherwise work in global.
   const int nn = R.n_dim * R.n_dim;
@@ -437,9 +463,9 @@ __global__ void __launch_bounds__(kSolveThreads, 1) solve_kernel(const Job* __re
   const int P = R.P;
   if (threadIdx.x == 0) {
     if (R.n_dim == 3)
-      state_step<3>(job, S, R, Hd, Hl, gv, pv, work, s_f);
+      state_step<3>(job, S, R, Hd, Hl, gv, pv, work, s_f, pair ? s_f2 : 0.0);
     else
-      state_step<2>(job, S, R, Hd, Hl, gv, pv, work, s_f);
+      state_step<2>(job, S, R, Hd, Hl, gv, pv, work, s_f, pair ? s_f2 : 0.0);
   }
   __syncthreads();
   if (staged) {
