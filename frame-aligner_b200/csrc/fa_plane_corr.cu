@@ -425,90 +425,6 @@ __global__ void __launch_bounds__(kPlaneThreads, 1) plane_yz_kernel(const double
   }
 }
 
-// The (z, y) pass for 16-plane volumes with twice the threads: 1024 threads of at most 64 registers
-// (32 warps per SM instead of 16; the plane still fills one CTA's shared memory), each y-line stage
-// one radix-8 butterfly per thread, and each 16-point z column split over a thread pair (lanes 2c,
-// 2c + 1): a radix-2 decimation-in-frequency step across the pair leaves the even bins on the first
-// thread and the odd bins on the second, each finished by an 8-point DFT in registers; the inverse
-// runs the same steps backwards (8-point inverse DFTs, then the radix-2 decimation-in-time step
-// across the pair). Same arithmetic contract as plane_yz_kernel<16, false>.
-constexpr int kPlane2Threads = 1024;
-constexpr int kPlane2EPT = 8;
-
-// W_16^n, n = 0..7 (forward)
-__device__ __forceinline__ double2 w16n(int n) {
-  switch (n) {
-    case 1: return make_double2(kC8, -kS8);
-    case 2: return make_double2(kS2, -kS2);
-    case 3: return make_double2(kS8, -kC8);
-    case 4: return make_double2(0.0, -1.0);
-    case 5: return make_double2(-kS8, -kC8);
-    case 6: return make_double2(-kS2, -kS2);
-    case 7: return make_double2(-kC8, -kS8);
-    default: return make_double2(1.0, 0.0);
-  }
-}
-
-__device__ __forceinline__ double2 shfl_xor1(double2 v) {
-  return make_double2(__shfl_xor_sync(0xffffffffu, v.x, 1), __shfl_xor_sync(0xffffffffu, v.y, 1));
-}
-
-__global__ void __launch_bounds__(kPlane2Threads, 1) plane_yz16_kernel(double2* spec,
-                                                                       const double2* __restrict__ ref_conj,
-                                                                       const double2* __restrict__ tw_y, PlaneDims d,
-                                                                       long long n_planes) {
-  constexpr int NZ = 16;
-  extern __shared__ double2 sm[];
-  const int ny = d.ny, S = ny + 1;
-  const int plane = NZ * ny;
-  const long long p0 = (long long)blockIdx.x * d.PP;
-  const int pp = (int)min((long long)d.PP, n_planes - p0);
-  double2* tws = sm + d.PP * NZ * S;
-  double2* base = spec + p0 * plane;
-  stage16<4>(
-      d.n_twy, [&](int i) { return reinterpret_cast<const uint4*>(tw_y) + i; },
-      [&](int i) { return reinterpret_cast<uint4*>(tws) + i; });
-  auto first = [&](int l, int i) -> double2 { return base[l * ny + i]; };
-  fft_rows<false, kPlane2EPT, kPlane2Threads, false, true>(sm, pp * NZ, d.log2ny, tws, first, NoIo{});
-  const int M1 = (d.nx >> 1) + 1;
-  const int h = threadIdx.x & 1;
-  // every thread pair takes columns (p, y) in turn; both threads of a pair always run together
-  for (int c = threadIdx.x >> 1; c < pp * ny; c += kPlane2Threads / 2) {
-    const int p = c >> d.log2ny, y = c & (ny - 1);
-    double2* col = sm + (p * NZ) * S + swz(y);
-    double2 a[8];
-#pragma unroll
-    for (int n = 0; n < 8; n++) a[n] = col[(8 * h + n) * S];
-    // forward: b[n] = x[n] + x[n+8] (even bins), c[n] = (x[n] - x[n+8]) W_16^n (odd bins)
-#pragma unroll
-    for (int n = 0; n < 8; n++) {
-      const double2 o = shfl_xor1(a[n]);
-      a[n] = h == 0 ? cadd(a[n], o) : cmul(csub(o, a[n]), w16n(n));
-    }
-    dft8<false>(a);  // a[k] = bin 2k + h
-    const int k = (int)((p0 + p) % M1);
-    const double2* rc = ref_conj + (long long)k * plane + y;
-#pragma unroll
-    for (int n = 0; n < 8; n++) a[n] = cross_power(a[n], __ldg(rc + (2 * n + h) * ny));
-    // inverse: e[n] = inverse 8-point DFT of the even bins, o[n] of the odd bins;
-    // x[n] = e[n] + W_16^-n o[n], x[n+8] = e[n] - W_16^-n o[n]
-    dft8<true>(a);
-#pragma unroll
-    for (int n = 0; n < 8; n++) {
-      const double2 other = shfl_xor1(a[n]);
-      const double2 e = h == 0 ? a[n] : other;
-      const double2 t = cmul_tw<true>(h == 0 ? other : a[n], w16n(n));
-      a[n] = h == 0 ? cadd(e, t) : csub(e, t);
-    }
-#pragma unroll
-    for (int n = 0; n < 8; n++) col[(8 * h + n) * S] = a[n];
-  }
-  __syncthreads();
-  // the last inverse stage writes the planes
-  auto last = [&](int l, int i, double2 v) { base[l * ny + i] = v; };
-  fft_rows<true, kPlane2EPT, kPlane2Threads, true, false>(sm, pp * NZ, d.log2ny, tws, NoIo{}, last);
-}
-
 // Split (z, y) pass. Lines of ny points along y, in place in the batch's plane array (line l = plane
 // p, plane z at offset l * ny of spec[kx][z][y]), d.LY lines per CTA; the first stage reads global
 // memory and the last writes it (ny >= 16: at least two stages, so a CTA reads all its lines before
@@ -812,15 +728,6 @@ cudaError_t launch_yz_nz(const PlaneDims& d, const double2* in, double2* out, co
 cudaError_t launch_plane_yz(const PlaneDims& d, const double2* in, double2* out, const double2* ref_conj,
                             const double2* tw_y, int batch, bool reference, cudaStream_t s) {
   const long long n_planes = (long long)batch * ((d.nx >> 1) + 1);
-  if (!reference && d.nz == 16 && in == out && (long long)d.PP * 16 * d.ny <= kPlane2Threads * kPlane2EPT &&
-      d.ny >= 64) {
-    const size_t smem = ((size_t)d.PP * 16 * (d.ny + 1) + d.ny) * sizeof(double2);
-    cudaError_t e = allow_smem(plane_yz16_kernel, smem);
-    if (e != cudaSuccess) return e;
-    const long long grid = (n_planes + d.PP - 1) / d.PP;
-    plane_yz16_kernel<<<(unsigned)grid, kPlane2Threads, smem, s>>>(out, ref_conj, tw_y, d, n_planes);
-    return cudaGetLastError();
-  }
   return reference ? launch_yz_nz<true>(d, in, out, nullptr, tw_y, n_planes, s)
                    : launch_yz_nz<false>(d, in, out, ref_conj, tw_y, n_planes, s);
 }
