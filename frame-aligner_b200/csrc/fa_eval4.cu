@@ -71,9 +71,9 @@ struct RefGradSrc<__nv_bfloat16> {
 //
 // A uniform segment's data -- its tap rows of the frame (two, or four for a stack) and the
 // reference / gradient values of its voxels -- is brought into the warp's shared memory by 1-D bulk
-// copies (cp.async.bulk, the TMA unit's untiled form) that complete on an mbarrier, one segment ahead
-// of the compute: while the warp works on segment i from one buffer, segment i+1's copies land in the
-// other. Each copy starts on a 16-byte boundary and moves a multiple of 16 bytes (frame rows of a
+// copies (cp.async.bulk, the TMA unit's untiled form), one per lane, that complete on an mbarrier: a
+// ring of kStageSlots buffers per warp keeps up to three segments in flight ahead of the one being
+// computed, so the compute finds its data in shared memory. Each copy starts on a 16-byte boundary and moves a multiple of 16 bytes (frame rows of a
 // padded slot start on 16-byte boundaries when nx is a multiple of 16 / element size; a row's staged
 // span is rounded to whole 16-byte chunks inside the row). The source is always this GPU's own memory
 // and no copy is multicast.
@@ -95,6 +95,13 @@ __host__ __device__ constexpr int stage_buffer_bytes() {
 // by the host after the launch), stops using its staging buffers and skips the rest of its work.
 __device__ unsigned int g_stage_timeouts;
 constexpr int kStageWaitLimit = 1 << 22;
+// Staging ring per warp: kStageSlots buffers (segments in flight ahead of the one in use: one fewer)
+// for 2-byte frames; FP32 frames, whose buffers are twice as large, use two.
+constexpr int kStageSlots = 4;
+template <typename FT>
+__host__ __device__ constexpr int stage_slots() {
+  return sizeof(FT) == 2 ? kStageSlots : 2;
+}
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -584,6 +591,7 @@ __device__ __forceinline__ bool eval4_tile(const Job& job, const RefDev& R, cons
   constexpr int RE = StageCfg<FT>::row_elems;
   constexpr int NR = NDIM == 3 ? 4 : 2;
   constexpr int SB = stage_buffer_bytes<NDIM, FT, RT>();
+  constexpr int NS = stage_slots<FT>();
   // padded slots whose rows start on 16-byte boundaries stage their segments (see above)
   const bool staged = stage != nullptr && padded && nx % C == 0 &&
                       (reinterpret_cast<uintptr_t>(fr) & 15u) == 0;
@@ -662,57 +670,65 @@ __device__ __forceinline__ bool eval4_tile(const Job& job, const RefDev& R, cons
     // ---- walk them ----
     const int cnt = min(kSegBatch, n_items - base);
     if (staged) {
-      // lane 0 issues segment q's copies into buffer bf; they complete on bars[bf]
-      auto issue = [&](int q, int bf) {
+      // segment q's copies into ring slot sl, one copy per lane (lanes 0 .. NR + n_rg - 1); they
+      // complete on bars[sl]
+      auto issue = [&](int q, int sl) {
         const SegParams P = sp[q];
         const int xa = ((base + q) % segs) * kSegLen;
         const int nv = min(kSegLen, nx - xa);  // voxels of the segment
         const int d = (int)(P.win & (long long)(C - 1));
-        const long long a0 = P.win - d;       // 16-byte aligned start of the tap rows' span
         const unsigned rb = (unsigned)(((d + nv + 4 + C - 1) & ~(C - 1)) * (int)sizeof(FT));
-        unsigned char* buf = stage + bf * SB;
         const unsigned rgb = sizeof(RT) == 2 ? (unsigned)(nv / 4) * 32u : (unsigned)nv * 4u;
-        const unsigned n_rg = sizeof(RT) == 2 ? 1u : (unsigned)(NDIM + 1);
-        fence_proxy_async_smem();
-        mbar_expect_tx(&bars[bf], NR * rb + n_rg * rgb);
-        const FT* src = fr + a0;
-        bulk_to_smem(buf, src, rb, &bars[bf]);
-        bulk_to_smem(buf + RE * sizeof(FT), src + pitch, rb, &bars[bf]);
-        if (NDIM == 3) {
-          bulk_to_smem(buf + 2 * RE * sizeof(FT), src + plane, rb, &bars[bf]);
-          bulk_to_smem(buf + 3 * RE * sizeof(FT), src + plane + pitch, rb, &bars[bf]);
-        }
-        unsigned char* rg = buf + NR * RE * sizeof(FT);
-        if constexpr (sizeof(RT) == 2) {
-          bulk_to_smem(rg, R.q16 + (long long)(P.p0 >> 2) * 16, rgb, &bars[bf]);
-        } else {
-          const float* planes[4] = {R.ref32, R.gx32, R.gy32, R.gz32};
-#pragma unroll
-          for (int k = 0; k <= NDIM; k++) bulk_to_smem(rg + k * 512, planes[k] + P.p0, rgb, &bars[bf]);
+        constexpr int n_rg = sizeof(RT) == 2 ? 1 : NDIM + 1;
+        unsigned char* buf = stage + sl * SB;
+        fence_proxy_async_smem();  // this lane's reads of the slot come before the refill
+        __syncwarp();
+        if (lane == 0) mbar_expect_tx(&bars[sl], NR * rb + n_rg * rgb);
+        __syncwarp();
+        if (lane < NR) {
+          // tap rows (y, z), (y + 1, z), (y, z + 1), (y + 1, z + 1) from the 16-byte aligned span start
+          const long long off = P.win - d + ((lane & 1) ? pitch : 0) + ((lane & 2) ? plane : 0);
+          bulk_to_smem(buf + lane * RE * sizeof(FT), fr + off, rb, &bars[sl]);
+        } else if (lane < NR + n_rg) {
+          unsigned char* rg = buf + NR * RE * sizeof(FT);
+          if constexpr (sizeof(RT) == 2) {
+            bulk_to_smem(rg, R.q16 + (long long)(P.p0 >> 2) * 16, rgb, &bars[sl]);
+          } else {
+            const int k = lane - NR;
+            const float* plane_k = k == 0 ? R.ref32 : (k == 1 ? R.gx32 : (k == 2 ? R.gy32 : R.gz32));
+            bulk_to_smem(rg + k * 512, plane_k + P.p0, rgb, &bars[sl]);
+          }
         }
       };
       auto next_uniform = [&](int q) {
         while (q < cnt && !(sp[q].meta & 1)) q++;
         return q;
       };
-      int q = next_uniform(0);
-      int bf = 0;
-      if (q < cnt && lane == 0) issue(q, bf);
-      while (q < cnt) {
-        const int qn = next_uniform(q + 1);
-        // the other buffer's last readers finished at the previous step's __syncwarp
-        if (qn < cnt && lane == 0) issue(qn, bf ^ 1);
-        if (!mbar_wait_bounded(&bars[bf], (phases >> bf) & 1u)) {
+      // ring of NS buffers: up to NS - 1 segments in flight ahead of the one in use
+      int qi = next_uniform(0), qc = qi;
+      int ki = 0, kc = 0;
+      while (qi < cnt && ki - kc < NS - 1) {
+        issue(qi, ki % NS);
+        ki++;
+        qi = next_uniform(qi + 1);
+      }
+      while (qc < cnt) {
+        if (qi < cnt && ki - kc < NS) {  // the slot it takes was released by an earlier step
+          issue(qi, ki % NS);
+          ki++;
+          qi = next_uniform(qi + 1);
+        }
+        const int sl = kc % NS;
+        if (!mbar_wait_bounded(&bars[sl], (phases >> sl) & 1u)) {
           // never expected: count it, let the copies in flight land (bounded), and give up on the
           // tile; the host fails the call
           if (lane == 0) atomicAdd(&g_stage_timeouts, 1u);
-          mbar_wait_bounded(&bars[bf], (phases >> bf) & 1u);
-          if (qn < cnt) mbar_wait_bounded(&bars[bf ^ 1], (phases >> (bf ^ 1)) & 1u);
+          for (int k = kc; k < ki; k++) mbar_wait_bounded(&bars[k % NS], (phases >> (k % NS)) & 1u);
           return false;
         }
-        phases ^= 1u << bf;
-        const SegParams P = sp[q];
-        const int xa = ((base + q) % segs) * kSegLen;
+        phases ^= 1u << sl;
+        const SegParams P = sp[qc];
+        const int xa = ((base + qc) % segs) * kSegLen;
         const int x0 = xa + lane * 4;
         const int ra = P.meta >> 3;
         if (ra != ur) {
@@ -720,7 +736,7 @@ __device__ __forceinline__ bool eval4_tile(const Job& job, const RefDev& R, cons
           ur = ra;
         }
         if (x0 < nx) {
-          const unsigned char* buf = stage + bf * SB;
+          const unsigned char* buf = stage + sl * SB;
           float t4[4], g4[NDIM][4];
           StagedRG<RT>::template load<NDIM>(buf + NR * RE * sizeof(FT), lane, t4, g4);
           const FT* wp = reinterpret_cast<const FT*>(buf) + (int)(P.win & (long long)(C - 1)) + lane * 4;
@@ -747,9 +763,9 @@ __device__ __forceinline__ bool eval4_tile(const Job& job, const RefDev& R, cons
               break;
           }
         }
-        __syncwarp();  // every lane is done with this buffer (and lanes past the row end rejoin)
-        q = qn;
-        bf ^= 1;
+        __syncwarp();  // every lane is done with this slot (and lanes past the row end rejoin)
+        kc++;
+        qc = next_uniform(qc + 1);
       }
     } else {
       for (int q = 0; q < cnt; q++) {
@@ -840,17 +856,16 @@ __device__ __forceinline__ bool eval4_tile(const Job& job, const RefDev& R, cons
 }
 
 // One grid per launch: CTA x of job y covers tiles 8x .. 8x+7, one per warp.
-// Dynamic shared memory of both kernels: two staging buffers per warp (stage_buffer_bytes each).
+// Dynamic shared memory of both kernels: kStageSlots staging buffers per warp.
 template <int NDIM, typename FT, typename RT>
 constexpr int eval4_dyn_smem() {
-  return kEvalWarps * 2 * stage_buffer_bytes<NDIM, FT, RT>();
+  return kEvalWarps * stage_slots<FT>() * stage_buffer_bytes<NDIM, FT, RT>();
 }
 
-// Per-warp staging state: two mbarriers (initialised by lane 0), their phase bits in a register.
+// Per-warp staging state: kStageSlots mbarriers (initialised by lane 0), their phase bits in a register.
 __device__ __forceinline__ void stage_init(unsigned long long* bars) {
   if ((threadIdx.x & 31) == 0) {
-    mbar_init(&bars[0]);
-    mbar_init(&bars[1]);
+    for (int i = 0; i < kStageSlots; i++) mbar_init(&bars[i]);
     mbar_init_fence();
   }
   __syncwarp();
@@ -860,7 +875,7 @@ template <int NDIM, typename FT, typename RT, int MB>
 __global__ void __launch_bounds__(kEvalThreads, MB) eval4_kernel(const Job* __restrict__ jobs) {
   __shared__ float4 sD[kEvalWarps][kWin * kDParamF4];
   __shared__ SegParams sp[kEvalWarps][kSegBatch];
-  __shared__ unsigned long long bars[kEvalWarps][2];
+  __shared__ unsigned long long bars[kEvalWarps][kStageSlots];
   extern __shared__ __align__(128) unsigned char dyn_stage[];
   const Job& job = jobs[blockIdx.y];
   if (job.state != nullptr && (job.state->phase == kPhaseDone || job.state->phase == kPhaseWaitWarm)) return;
@@ -871,7 +886,7 @@ __global__ void __launch_bounds__(kEvalThreads, MB) eval4_kernel(const Job* __re
   stage_init(bars[warp]);
   unsigned phases = 0;
   eval4_tile<NDIM, FT, RT>(job, R, tile, sD[warp], sp[warp], job.dparams, job.partials,
-                           dyn_stage + warp * 2 * stage_buffer_bytes<NDIM, FT, RT>(), bars[warp], phases);
+                           dyn_stage + warp * stage_slots<FT>() * stage_buffer_bytes<NDIM, FT, RT>(), bars[warp], phases);
 }
 
 // Persistent form for batched solves: the grid's warps walk the (active frame, tile) items of the
@@ -885,7 +900,7 @@ __global__ void __launch_bounds__(kEvalThreads, MB) eval4_active_kernel(const Jo
                                                                      const int* __restrict__ tile_prefix) {
   __shared__ float4 sD[kEvalWarps][kWin * kDParamF4];
   __shared__ SegParams sp[kEvalWarps][kSegBatch];
-  __shared__ unsigned long long bars[kEvalWarps][2];
+  __shared__ unsigned long long bars[kEvalWarps][kStageSlots];
   extern __shared__ __align__(128) unsigned char dyn_stage[];
   const int na = *n_active;
   const int n_items = tile_prefix[na];
@@ -893,7 +908,7 @@ __global__ void __launch_bounds__(kEvalThreads, MB) eval4_active_kernel(const Jo
   const int stride = gridDim.x * kEvalWarps;
   stage_init(bars[warp]);
   unsigned phases = 0;
-  unsigned char* stage = dyn_stage + warp * 2 * stage_buffer_bytes<NDIM, FT, RT>();
+  unsigned char* stage = dyn_stage + warp * stage_slots<FT>() * stage_buffer_bytes<NDIM, FT, RT>();
   int a = 0;
   for (int item = blockIdx.x * kEvalWarps + warp; item < n_items; item += stride) {
     int hi = na - 1;
