@@ -507,6 +507,8 @@ struct SegParams {
   long long win;            // frame offset of lane 0's window (tap row y, plane z; multiple of 4 in x)
   int p0;                   // reference / gradient offset of the segment's first voxel
   int meta;                 // bit 0: uniform; bits 1-2: window alignment; bits 3..: storage range
+  int xa;                   // x of the segment's first voxel
+  int row;                  // image row (z * ny + y)
 };
 constexpr int kSegBatch = 32;  // segments classified per round, one per lane
 // A segment is kSegGroups groups of 128 voxels; each lane takes four voxels of every group.
@@ -663,6 +665,8 @@ __device__ __forceinline__ bool eval4_tile(const Job& job, const RefDev& R, cons
       q.fs = fs;
       q.win = (long long)cz * plane + (long long)cy * pitch + xa + ab;
       q.p0 = row * nx + xa;
+      q.xa = xa;
+      q.row = row;
       q.meta = (uni ? 1 : 0) | ((ox & 3) << 1) | (ra << 3);
       sp[lane] = q;
     }
@@ -674,7 +678,7 @@ __device__ __forceinline__ bool eval4_tile(const Job& job, const RefDev& R, cons
       // complete on bars[sl]
       auto issue = [&](int q, int sl) {
         const SegParams P = sp[q];
-        const int xa = ((base + q) % segs) * kSegLen;
+        const int xa = P.xa;
         const int nv = min(kSegLen, nx - xa);  // voxels of the segment
         const int d = (int)(P.win & (long long)(C - 1));
         const unsigned rb = (unsigned)(((d + nv + 4 + C - 1) & ~(C - 1)) * (int)sizeof(FT));
@@ -728,7 +732,7 @@ __device__ __forceinline__ bool eval4_tile(const Job& job, const RefDev& R, cons
         }
         phases ^= 1u << sl;
         const SegParams P = sp[qc];
-        const int xa = ((base + qc) % segs) * kSegLen;
+        const int xa = P.xa;
         const int x0 = xa + lane * 4;
         const int ra = P.meta >> 3;
         if (ra != ur) {
@@ -770,7 +774,7 @@ __device__ __forceinline__ bool eval4_tile(const Job& job, const RefDev& R, cons
     } else {
       for (int q = 0; q < cnt; q++) {
         const SegParams P = sp[q];
-        const int xa = ((base + q) % segs) * kSegLen;
+        const int xa = P.xa;
         if (P.meta & 1) {
           const int ra = P.meta >> 3;
           if (ra != ur) {
@@ -814,9 +818,9 @@ __device__ __forceinline__ bool eval4_tile(const Job& job, const RefDev& R, cons
     for (int q = 0; q < cnt; q++) {
       if (sp[q].meta & 1) continue;
       for (int gi = 0; gi < kSegGroups; gi++) {
-        const int x0 = ((base + q) % segs) * kSegLen + gi * 128 + lane * 4;
+        const int x0 = sp[q].xa + gi * 128 + lane * 4;
         if (x0 < nx) {
-          const int row = row_begin + (base + q) / segs;
+          const int row = sp[q].row;
           const LaneSums<NDIM> ls = lane_item<NDIM, FT, RT>(fr, plane, pitch, padded, src, R.rows[row], x0, row, nx,
                                                            ny, nz, bidir, dq, sD, cw, c0);
           af += ls.f;
