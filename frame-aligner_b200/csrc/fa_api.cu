@@ -225,12 +225,6 @@ namespace {
 
 namespace fa_rt {
 
-// FA_ERR_TIMEOUT when a staging wait of the fused pass gave up (never in correct operation).
-fa_status stage_check() {
-  if (fa::take_stage_timeouts() != 0) return fail(FA_ERR_TIMEOUT, "fused pass: a staging copy did not complete");
-  return FA_OK;
-}
-
 bool finite_all(const double* v, size_t n) {
   for (size_t i = 0; i < n; i++)
     if (!std::isfinite(v[i])) return false;
@@ -1019,7 +1013,6 @@ extern "C" fa_status fa_align_frame(fa_frame* F, const double* rigid_shift, int 
     phase = F->h_state->phase;
   }
   F->have_last = false;
-  FA_TRY(stage_check());
   FA_TRY(finish_solve(F, D_out, stats));
   Job j0 = F->job;
   FA_CU(cudaMemcpyAsync(F->job_dev, &j0, sizeof(Job), cudaMemcpyHostToDevice, F->stream));
@@ -1151,10 +1144,6 @@ fa_status align_batch_impl(fa_frame* const* frames, int n, const double* rigid_s
     if (*bc->h_active == 0) break;
   }
   if (e != cudaSuccess) return done(fail(FA_ERR_CUDA, std::string("batch solve: ") + cudaGetErrorString(e)));
-  {
-    const fa_status sc = stage_check();
-    if (sc != FA_OK) return done(sc);
-  }
   // every frame's x and state in one batch of copies on the solve's stream
   for (int i = 0; i < n; i++) {
     fa_status r = finish_solve_enqueue(frames[i], s);
@@ -2033,7 +2022,6 @@ extern "C" fa_status fa_profile_eval(fa_frame* const* frames, int n, const doubl
   cudaEventDestroy(e1);
   dfree_all(R->ctx, tmp);
   if (e != cudaSuccess) return fail(FA_ERR_CUDA, std::string("profile: ") + cudaGetErrorString(e));
-  FA_TRY(stage_check());
   *ms_per_launch = ms / launches;
   return FA_OK;
 }

@@ -67,114 +67,6 @@ struct RefGradSrc<__nv_bfloat16> {
   }
 };
 
-// ------------------------------------------------------------------ segment staging ----------------
-//
-// A uniform segment's data -- its tap rows of the frame (two, or four for a stack) and the
-// reference / gradient values of its voxels -- is brought into the warp's shared memory by 1-D bulk
-// copies (cp.async.bulk, the TMA unit's untiled form), one per lane, that complete on an mbarrier: a
-// ring of kStageSlots buffers per warp keeps up to three segments in flight ahead of the one being
-// computed, so the compute finds its data in shared memory. Each copy starts on a 16-byte boundary and moves a multiple of 16 bytes (frame rows of a
-// padded slot start on 16-byte boundaries when nx is a multiple of 16 / element size; a row's staged
-// span is rounded to whole 16-byte chunks inside the row). The source is always this GPU's own memory
-// and no copy is multicast.
-
-// Frame elements staged per tap row (covers the 128 voxels' windows for any alignment) and the
-// bytes of one buffer: the tap rows, then the reference / gradient values of 128 voxels.
-template <typename FT>
-struct StageCfg {
-  static constexpr int esz = (int)sizeof(FT);
-  static constexpr int chunk = 16 / esz;  // elements per 16 bytes
-  static constexpr int row_elems = esz == 2 ? 136 : 132;
-};
-template <int NDIM, typename FT, typename RT>
-__host__ __device__ constexpr int stage_buffer_bytes() {
-  return (NDIM == 3 ? 4 : 2) * StageCfg<FT>::row_elems * (int)sizeof(FT) + ((int)sizeof(RT) == 2 ? 1024 : 2048);
-}
-
-// Waits that never end are bounded: after kStageWaitLimit polls the warp counts a timeout here (read
-// by the host after the launch), stops using its staging buffers and skips the rest of its work.
-__device__ unsigned int g_stage_timeouts;
-constexpr int kStageWaitLimit = 1 << 22;
-// Staging ring per warp: kStageSlots buffers (segments in flight ahead of the one in use: one fewer)
-// for 2-byte frames; FP32 frames, whose buffers are twice as large, use two.
-constexpr int kStageSlots = 4;
-template <typename FT>
-__host__ __device__ constexpr int stage_slots() {
-  return sizeof(FT) == 2 ? kStageSlots : 2;
-}
-
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(unsigned long long* bar) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ void mbar_init_fence() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void bulk_to_smem(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-               ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
-  unsigned done;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(done)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return done != 0;
-}
-// generic-proxy reads of a buffer before the async proxy refills it
-__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
-  for (int i = 0; i < kStageWaitLimit; i++)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
-}
-
-// The staged reference / gradient values of a lane's four voxels (group `lane` of the segment).
-template <typename RT>
-struct StagedRG;
-template <>
-struct StagedRG<__nv_bfloat16> {
-  template <int NDIM>
-  static __device__ __forceinline__ void load(const unsigned char* rg, int lane, float* t4, float (*g4)[4]) {
-    const uint4* b = reinterpret_cast<const uint4*>(rg) + 2 * lane;
-    const uint4 a = b[0], c = b[1];
-    auto unpack = [](unsigned lo, unsigned hi, float* v) {
-      v[0] = __uint_as_float(lo << 16);
-      v[1] = __uint_as_float(lo & 0xffff0000u);
-      v[2] = __uint_as_float(hi << 16);
-      v[3] = __uint_as_float(hi & 0xffff0000u);
-    };
-    unpack(a.x, a.y, t4);
-    unpack(a.z, a.w, g4[0]);
-    unpack(c.x, c.y, g4[1]);
-    if (NDIM == 3) unpack(c.z, c.w, g4[NDIM == 3 ? 2 : 0]);
-  }
-};
-template <>
-struct StagedRG<float> {
-  template <int NDIM>
-  static __device__ __forceinline__ void load(const unsigned char* rg, int lane, float* t4, float (*g4)[4]) {
-    const float4* b = reinterpret_cast<const float4*>(rg) + lane;  // plane k at + 32 k float4
-    auto put = [](float4 v, float* o) {
-      o[0] = v.x;
-      o[1] = v.y;
-      o[2] = v.z;
-      o[3] = v.w;
-    };
-    put(b[0], t4);
-#pragma unroll
-    for (int k = 0; k < NDIM; k++) put(b[32 * (k + 1)], g4[k]);
-  }
-};
-
 // Five consecutive frame values v[k] = p[s + k], k = 0..4, from the aligned 8-element window at p
 // (p is 8-element aligned in FP16 units or 4-element aligned in FP32 units; s in [0, 3]).
 __device__ __forceinline__ void window5(const __half* p, int s, float* v) {
@@ -237,19 +129,11 @@ __device__ __forceinline__ void masked5(const FT* row, bool row_valid, int ix, i
 }  // namespace
 
 // Frame values v[k] = p[S + k], k = 0..4, from the aligned 8-element window at p, for an alignment
-// S that is the same for every lane of the warp (known at compile time: no shifts or selects). SM:
-// p is in shared memory (a staged row), else global memory.
-template <bool SM, typename T>
-__device__ __forceinline__ T ld_win(const T* p) {
-  if constexpr (SM)
-    return *p;
-  else
-    return __ldg(p);
-}
-template <int S, bool SM = false>
+// S that is the same for every lane of the warp (known at compile time: no shifts or selects).
+template <int S>
 __device__ __forceinline__ void window5s(const RawU16* p, float* v) {
-  const uint2 lo = ld_win<SM>(reinterpret_cast<const uint2*>(p));
-  const uint2 hi = ld_win<SM>(reinterpret_cast<const uint2*>(p + 4));
+  const uint2 lo = __ldg(reinterpret_cast<const uint2*>(p));
+  const uint2 hi = __ldg(reinterpret_cast<const uint2*>(p + 4));
   const unsigned w[4] = {lo.x, lo.y, hi.x, hi.y};
 #pragma unroll
   for (int k = 0; k < 5; k++) {
@@ -257,10 +141,10 @@ __device__ __forceinline__ void window5s(const RawU16* p, float* v) {
     v[k] = __uint_as_float(__byte_perm(w[e >> 1], 0x4B000000u, (e & 1) ? 0x7632 : 0x7610)) - 8388608.0f;
   }
 }
-template <int S, bool SM = false>
+template <int S>
 __device__ __forceinline__ void window5s(const __half* p, float* v) {
-  const uint2 lo = ld_win<SM>(reinterpret_cast<const uint2*>(p));
-  const uint2 hi = ld_win<SM>(reinterpret_cast<const uint2*>(p + 4));
+  const uint2 lo = __ldg(reinterpret_cast<const uint2*>(p));
+  const uint2 hi = __ldg(reinterpret_cast<const uint2*>(p + 4));
   const unsigned w[4] = {lo.x, lo.y, hi.x, hi.y};
 #pragma unroll
   for (int k = 0; k < 5; k++) {
@@ -269,10 +153,10 @@ __device__ __forceinline__ void window5s(const __half* p, float* v) {
     v[k] = __half2float(__ushort_as_half(h));
   }
 }
-template <int S, bool SM = false>
+template <int S>
 __device__ __forceinline__ void window5s(const float* p, float* v) {
-  const float4 a = ld_win<SM>(reinterpret_cast<const float4*>(p));
-  const float4 b = ld_win<SM>(reinterpret_cast<const float4*>(p + 4));
+  const float4 a = __ldg(reinterpret_cast<const float4*>(p));
+  const float4 b = __ldg(reinterpret_cast<const float4*>(p + 4));
   const float w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
 #pragma unroll
   for (int k = 0; k < 5; k++) v[k] = w[S + k];
@@ -281,16 +165,16 @@ __device__ __forceinline__ void window5s(const float* p, float* v) {
 // Four voxels of a lane in a uniform row segment (see eval4_tile): the lane's window of each tap row
 // starts at wp (+ pitch for row y+1, + plane for plane z+1); weights of voxel j are w + j * s per
 // axis, its control-point fraction fl + j * fs.
-template <int NDIM, int S, typename FT, bool SM = false>
+template <int NDIM, int S, typename FT>
 __device__ __forceinline__ void uniform4(const FT* __restrict__ wp, long long plane, int pitch, const float* t4,
                                          const float (*g4)[4], float wxl, float sx, float wyl, float sy, float wzl,
                                          float sz, float fl, float fs, float& af, float* acc0, float* acc1) {
   float v[NDIM == 3 ? 4 : 2][5];
-  window5s<S, SM>(wp, v[0]);
-  window5s<S, SM>(wp + pitch, v[1]);
+  window5s<S>(wp, v[0]);
+  window5s<S>(wp + pitch, v[1]);
   if (NDIM == 3) {
-    window5s<S, SM>(wp + plane, v[NDIM == 3 ? 2 : 0]);
-    window5s<S, SM>(wp + plane + pitch, v[NDIM == 3 ? 3 : 1]);
+    window5s<S>(wp + plane, v[NDIM == 3 ? 2 : 0]);
+    window5s<S>(wp + plane + pitch, v[NDIM == 3 ? 3 : 1]);
   }
 #pragma unroll
   for (int j = 0; j < 4; j++) {
@@ -530,10 +414,9 @@ constexpr int kSegLen = 128 * kSegGroups;
 // that are added to the tile's control points only when the range changes. Other segments take the
 // per-lane path (lane_item), which handles every case voxel by voxel where needed.
 template <int NDIM, typename FT, typename RT>
-__device__ __forceinline__ bool eval4_tile(const Job& job, const RefDev& R, const int tile, float4* sD,
+__device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, const int tile, float4* sD,
                                            SegParams* sp, const float4* __restrict__ dparams,
-                                           double* __restrict__ partials, unsigned char* stage,
-                                           unsigned long long* bars, unsigned& phases) {
+                                           double* __restrict__ partials) {
   const int nx = R.nx, ny = R.ny, nz = R.nz;
   const int row_begin = tile * R.tile_rows;
   const int row_end = min(row_begin + R.tile_rows, R.n_rows);
@@ -589,14 +472,6 @@ __device__ __forceinline__ bool eval4_tile(const Job& job, const RefDev& R, cons
   const long long plane = job.fplane;
   const int pitch = job.fpitch;
   const bool padded = job.fpad != 0;
-  constexpr int C = StageCfg<FT>::chunk;
-  constexpr int RE = StageCfg<FT>::row_elems;
-  constexpr int NR = NDIM == 3 ? 4 : 2;
-  constexpr int SB = stage_buffer_bytes<NDIM, FT, RT>();
-  constexpr int NS = stage_slots<FT>();
-  // padded slots whose rows start on 16-byte boundaries stage their segments (see above)
-  const bool staged = stage != nullptr && padded && nx % C == 0 &&
-                      (reinterpret_cast<uintptr_t>(fr) & 15u) == 0;
   for (int base = 0; base < n_items; base += kSegBatch) {
     // ---- classify segments base .. base + 31, segment base + lane by this lane ----
     if (base + lane < n_items) {
@@ -644,16 +519,6 @@ __device__ __forceinline__ bool eval4_tile(const Job& job, const RefDev& R, cons
         cy = iy;
         cz = iz;
       }
-      if (staged && uni) {
-        // the staged span of the tap rows (see issue below) lies inside each row of the slot, starts
-        // on a 16-byte boundary and fits a buffer row; otherwise the segment takes the per-lane path
-        const int nv = min(kSegLen, nx - xa);
-        const int d = (xa + ab) & (C - 1);
-        const int span = (d + nv + 4 + C - 1) & ~(C - 1);
-        const long long a0 = (long long)cz * plane + (long long)cy * pitch + xa + ab - d;
-        uni = xa + ab - d >= -kHaloX && xa + ab - d + span <= nx + kHaloX && span <= RE &&
-              (reinterpret_cast<uintptr_t>(fr + a0) & 15u) == 0;
-      }
       SegParams q;
       q.w0x = tax - flx;
       q.w0y = tay - fly;
@@ -673,145 +538,45 @@ __device__ __forceinline__ bool eval4_tile(const Job& job, const RefDev& R, cons
     __syncwarp();
     // ---- walk them ----
     const int cnt = min(kSegBatch, n_items - base);
-    if (staged) {
-      // segment q's copies into ring slot sl, one copy per lane (lanes 0 .. NR + n_rg - 1); they
-      // complete on bars[sl]
-      auto issue = [&](int q, int sl) {
-        const SegParams P = sp[q];
-        const int xa = P.xa;
-        const int nv = min(kSegLen, nx - xa);  // voxels of the segment
-        const int d = (int)(P.win & (long long)(C - 1));
-        const unsigned rb = (unsigned)(((d + nv + 4 + C - 1) & ~(C - 1)) * (int)sizeof(FT));
-        const unsigned rgb = sizeof(RT) == 2 ? (unsigned)(nv / 4) * 32u : (unsigned)nv * 4u;
-        constexpr int n_rg = sizeof(RT) == 2 ? 1 : NDIM + 1;
-        unsigned char* buf = stage + sl * SB;
-        fence_proxy_async_smem();  // this lane's reads of the slot come before the refill
-        __syncwarp();
-        if (lane == 0) mbar_expect_tx(&bars[sl], NR * rb + n_rg * rgb);
-        __syncwarp();
-        if (lane < NR) {
-          // tap rows (y, z), (y + 1, z), (y, z + 1), (y + 1, z + 1) from the 16-byte aligned span start
-          const long long off = P.win - d + ((lane & 1) ? pitch : 0) + ((lane & 2) ? plane : 0);
-          bulk_to_smem(buf + lane * RE * sizeof(FT), fr + off, rb, &bars[sl]);
-        } else if (lane < NR + n_rg) {
-          unsigned char* rg = buf + NR * RE * sizeof(FT);
-          if constexpr (sizeof(RT) == 2) {
-            bulk_to_smem(rg, R.q16 + (long long)(P.p0 >> 2) * 16, rgb, &bars[sl]);
-          } else {
-            const int k = lane - NR;
-            const float* plane_k = k == 0 ? R.ref32 : (k == 1 ? R.gx32 : (k == 2 ? R.gy32 : R.gz32));
-            bulk_to_smem(rg + k * 512, plane_k + P.p0, rgb, &bars[sl]);
-          }
-        }
-      };
-      auto next_uniform = [&](int q) {
-        while (q < cnt && !(sp[q].meta & 1)) q++;
-        return q;
-      };
-      // ring of NS buffers: up to NS - 1 segments in flight ahead of the one in use
-      int qi = next_uniform(0), qc = qi;
-      int ki = 0, kc = 0;
-      while (qi < cnt && ki - kc < NS - 1) {
-        issue(qi, ki % NS);
-        ki++;
-        qi = next_uniform(qi + 1);
-      }
-      while (qc < cnt) {
-        if (qi < cnt && ki - kc < NS) {  // the slot it takes was released by an earlier step
-          issue(qi, ki % NS);
-          ki++;
-          qi = next_uniform(qi + 1);
-        }
-        const int sl = kc % NS;
-        if (!mbar_wait_bounded(&bars[sl], (phases >> sl) & 1u)) {
-          // never expected: count it, let the copies in flight land (bounded), and give up on the
-          // tile; the host fails the call
-          if (lane == 0) atomicAdd(&g_stage_timeouts, 1u);
-          for (int k = kc; k < ki; k++) mbar_wait_bounded(&bars[k % NS], (phases >> (k % NS)) & 1u);
-          return false;
-        }
-        phases ^= 1u << sl;
-        const SegParams P = sp[qc];
-        const int xa = P.xa;
-        const int x0 = xa + lane * 4;
+    for (int q = 0; q < cnt; q++) {
+      const SegParams P = sp[q];
+      const int xa = P.xa;
+      if (P.meta & 1) {
         const int ra = P.meta >> 3;
         if (ra != ur) {
           flush_uniform();
           ur = ra;
         }
-        if (x0 < nx) {
-          const unsigned char* buf = stage + sl * SB;
-          float t4[4], g4[NDIM][4];
-          StagedRG<RT>::template load<NDIM>(buf + NR * RE * sizeof(FT), lane, t4, g4);
-          const FT* wp = reinterpret_cast<const FT*>(buf) + (int)(P.win & (long long)(C - 1)) + lane * 4;
-          const float wxl = fmaf(lane_u, P.sx, P.w0x);
-          const float wyl = fmaf(lane_u, P.sy, P.w0y);
-          const float wzl = NDIM == 3 ? fmaf(lane_u, P.sz, P.w0z) : 0.0f;
-          const float fl = fmaf(lane_u, P.fs, P.f0);
-          switch ((P.meta >> 1) & 3) {
-            case 0:
-              uniform4<NDIM, 0, FT, true>(wp, 2 * RE, RE, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0,
-                                          ua1);
-              break;
-            case 1:
-              uniform4<NDIM, 1, FT, true>(wp, 2 * RE, RE, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0,
-                                          ua1);
-              break;
-            case 2:
-              uniform4<NDIM, 2, FT, true>(wp, 2 * RE, RE, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0,
-                                          ua1);
-              break;
-            default:
-              uniform4<NDIM, 3, FT, true>(wp, 2 * RE, RE, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0,
-                                          ua1);
-              break;
-          }
-        }
-        __syncwarp();  // every lane is done with this slot (and lanes past the row end rejoin)
-        kc++;
-        qc = next_uniform(qc + 1);
-      }
-    } else {
-      for (int q = 0; q < cnt; q++) {
-        const SegParams P = sp[q];
-        const int xa = P.xa;
-        if (P.meta & 1) {
-          const int ra = P.meta >> 3;
-          if (ra != ur) {
-            flush_uniform();
-            ur = ra;
-          }
 #pragma unroll
-          for (int gi = 0; gi < kSegGroups; gi++) {
-            const int x0 = xa + gi * 128 + lane * 4;
-            if (x0 < nx) {
-              float t4[4], g4[NDIM][4];
-              src.template load<NDIM>(P.p0 + gi * 128 + lane * 4, t4, g4);
-              const FT* wp = fr + (P.win + gi * 128 + lane * 4);
-              const float u = lane_u + (float)(gi * 128);
-              const float wxl = fmaf(u, P.sx, P.w0x);
-              const float wyl = fmaf(u, P.sy, P.w0y);
-              const float wzl = NDIM == 3 ? fmaf(u, P.sz, P.w0z) : 0.0f;
-              const float fl = fmaf(u, P.fs, P.f0);
-              switch ((P.meta >> 1) & 3) {
-                case 0:
-                  uniform4<NDIM, 0>(wp, plane, pitch, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
-                  break;
-                case 1:
-                  uniform4<NDIM, 1>(wp, plane, pitch, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
-                  break;
-                case 2:
-                  uniform4<NDIM, 2>(wp, plane, pitch, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
-                  break;
-                default:
-                  uniform4<NDIM, 3>(wp, plane, pitch, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
-                  break;
-              }
+        for (int gi = 0; gi < kSegGroups; gi++) {
+          const int x0 = xa + gi * 128 + lane * 4;
+          if (x0 < nx) {
+            float t4[4], g4[NDIM][4];
+            src.template load<NDIM>(P.p0 + gi * 128 + lane * 4, t4, g4);
+            const FT* wp = fr + (P.win + gi * 128 + lane * 4);
+            const float u = lane_u + (float)(gi * 128);
+            const float wxl = fmaf(u, P.sx, P.w0x);
+            const float wyl = fmaf(u, P.sy, P.w0y);
+            const float wzl = NDIM == 3 ? fmaf(u, P.sz, P.w0z) : 0.0f;
+            const float fl = fmaf(u, P.fs, P.f0);
+            switch ((P.meta >> 1) & 3) {
+              case 0:
+                uniform4<NDIM, 0>(wp, plane, pitch, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
+                break;
+              case 1:
+                uniform4<NDIM, 1>(wp, plane, pitch, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
+                break;
+              case 2:
+                uniform4<NDIM, 2>(wp, plane, pitch, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
+                break;
+              default:
+                uniform4<NDIM, 3>(wp, plane, pitch, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
+                break;
             }
           }
         }
-        __syncwarp();  // lanes past the row end rejoin here
       }
+      __syncwarp();  // lanes past the row end rejoin here
     }
     // the batch's other segments, lane by lane (after the uniform walk, so that its registers are
     // free for the per-lane path)
@@ -856,41 +621,20 @@ __device__ __forceinline__ bool eval4_tile(const Job& job, const RefDev& R, cons
   double* out = partials + (long long)tile * kPartialDoubles;
   if (lane < 11) out[lane] = lane == 1 ? (double)c0 : (double)pick;
   __syncwarp();
-  return true;
 }
 
 // One grid per launch: CTA x of job y covers tiles 8x .. 8x+7, one per warp.
-// Dynamic shared memory of both kernels: kStageSlots staging buffers per warp.
-template <int NDIM, typename FT, typename RT>
-constexpr int eval4_dyn_smem() {
-  return kEvalWarps * stage_slots<FT>() * stage_buffer_bytes<NDIM, FT, RT>();
-}
-
-// Per-warp staging state: kStageSlots mbarriers (initialised by lane 0), their phase bits in a register.
-__device__ __forceinline__ void stage_init(unsigned long long* bars) {
-  if ((threadIdx.x & 31) == 0) {
-    for (int i = 0; i < kStageSlots; i++) mbar_init(&bars[i]);
-    mbar_init_fence();
-  }
-  __syncwarp();
-}
-
 template <int NDIM, typename FT, typename RT, int MB>
 __global__ void __launch_bounds__(kEvalThreads, MB) eval4_kernel(const Job* __restrict__ jobs) {
   __shared__ float4 sD[kEvalWarps][kWin * kDParamF4];
   __shared__ SegParams sp[kEvalWarps][kSegBatch];
-  __shared__ unsigned long long bars[kEvalWarps][kStageSlots];
-  extern __shared__ __align__(128) unsigned char dyn_stage[];
   const Job& job = jobs[blockIdx.y];
   if (job.state != nullptr && (job.state->phase == kPhaseDone || job.state->phase == kPhaseWaitWarm)) return;
   const RefDev& R = *job.ref;
   const int warp = threadIdx.x >> 5;
   const int tile = blockIdx.x * kEvalWarps + warp;
   if (tile >= R.n_tiles) return;
-  stage_init(bars[warp]);
-  unsigned phases = 0;
-  eval4_tile<NDIM, FT, RT>(job, R, tile, sD[warp], sp[warp], job.dparams, job.partials,
-                           dyn_stage + warp * stage_slots<FT>() * stage_buffer_bytes<NDIM, FT, RT>(), bars[warp], phases);
+  eval4_tile<NDIM, FT, RT>(job, R, tile, sD[warp], sp[warp], job.dparams, job.partials);
 }
 
 // Persistent form for batched solves: the grid's warps walk the (active frame, tile) items of the
@@ -904,15 +648,10 @@ __global__ void __launch_bounds__(kEvalThreads, MB) eval4_active_kernel(const Jo
                                                                      const int* __restrict__ tile_prefix) {
   __shared__ float4 sD[kEvalWarps][kWin * kDParamF4];
   __shared__ SegParams sp[kEvalWarps][kSegBatch];
-  __shared__ unsigned long long bars[kEvalWarps][kStageSlots];
-  extern __shared__ __align__(128) unsigned char dyn_stage[];
   const int na = *n_active;
   const int n_items = tile_prefix[na];
   const int warp = threadIdx.x >> 5;
   const int stride = gridDim.x * kEvalWarps;
-  stage_init(bars[warp]);
-  unsigned phases = 0;
-  unsigned char* stage = dyn_stage + warp * stage_slots<FT>() * stage_buffer_bytes<NDIM, FT, RT>();
   int a = 0;
   for (int item = blockIdx.x * kEvalWarps + warp; item < n_items; item += stride) {
     int hi = na - 1;
@@ -929,17 +668,9 @@ __global__ void __launch_bounds__(kEvalThreads, MB) eval4_active_kernel(const Jo
     // a frame in the paired start phase has two items per tile: the zero start, then the rigid one
     const bool second = tile >= R.n_tiles;
     if (second) tile -= R.n_tiles;
-    if (!eval4_tile<NDIM, FT, RT>(job, R, tile, sD[warp], sp[warp], second ? job.dparams2 : job.dparams,
-                                  second ? job.partials2 : job.partials, stage, bars[warp], phases))
-      return;
+    eval4_tile<NDIM, FT, RT>(job, R, tile, sD[warp], sp[warp], second ? job.dparams2 : job.dparams,
+                             second ? job.partials2 : job.partials);
   }
-}
-
-// Opts a kernel into its dynamic shared memory once (above the 48 KB default when needed).
-template <typename K>
-cudaError_t allow_dyn_smem(K kernel, int bytes) {
-  if (bytes <= 48 * 1024) return cudaSuccess;
-  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
 template <typename Fn>
@@ -955,11 +686,7 @@ cudaError_t launch_eval4(const Job* jobs_dev, int n_jobs, int max_tiles, int n_d
   return dispatch_cfg(n_dim, frame_kind, ref_bf16, [&](auto c) {
     using C = decltype(c);
     return dispatch_mb(mb, [&](auto m) {
-      constexpr int smem = eval4_dyn_smem<C::nd, typename C::F, typename C::R>();
-      auto k = eval4_kernel<C::nd, typename C::F, typename C::R, decltype(m)::value>;
-      const cudaError_t e = allow_dyn_smem(k, smem);
-      if (e != cudaSuccess) return e;
-      k<<<grid, kEvalThreads, smem, s>>>(jobs_dev);
+      eval4_kernel<C::nd, typename C::F, typename C::R, decltype(m)::value><<<grid, kEvalThreads, 0, s>>>(jobs_dev);
       return cudaGetLastError();
     });
   });
@@ -988,25 +715,11 @@ cudaError_t launch_eval4_active(const Job* jobs_dev, const int* active, const in
   return dispatch_cfg(n_dim, frame_kind, ref_bf16, [&](auto c) {
     using C = decltype(c);
     return dispatch_mb(mb, [&](auto m) {
-      constexpr int smem = eval4_dyn_smem<C::nd, typename C::F, typename C::R>();
-      auto k = eval4_active_kernel<C::nd, typename C::F, typename C::R, decltype(m)::value>;
-      const cudaError_t e = allow_dyn_smem(k, smem);
-      if (e != cudaSuccess) return e;
-      k<<<g, kEvalThreads, smem, s>>>(jobs_dev, active, n_active, tile_prefix);
+      eval4_active_kernel<C::nd, typename C::F, typename C::R, decltype(m)::value>
+          <<<g, kEvalThreads, 0, s>>>(jobs_dev, active, n_active, tile_prefix);
       return cudaGetLastError();
     });
   });
-}
-
-// Staging waits that gave up since the last call (and clears the count); 0 in correct operation.
-unsigned take_stage_timeouts() {
-  unsigned n = 0;
-  if (cudaMemcpyFromSymbol(&n, g_stage_timeouts, sizeof(n)) != cudaSuccess) return 0;
-  if (n != 0) {
-    const unsigned zero = 0;
-    cudaMemcpyToSymbol(g_stage_timeouts, &zero, sizeof(zero));
-  }
-  return n;
 }
 
 }  // namespace fa

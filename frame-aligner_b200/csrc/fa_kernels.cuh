@@ -61,11 +61,6 @@ cudaError_t launch_eval4_active(const Job* jobs_dev, const int* active, const in
 // Thread-local (spill) bytes of that kernel's instantiation for a register budget of mb CTAs per SM.
 size_t eval4_active_local_bytes(int n_dim, int frame_kind, bool ref_bf16, int mb);
 
-// Staging waits of the fused pass that gave up since the last call (clears the count). A bounded
-// wait only gives up if a bulk copy never completes; the calls that run the pass then fail with
-// FA_ERR_TIMEOUT.
-unsigned take_stage_timeouts();
-
 // Rebuilds the active list of a job table (frames not done, ascending index), the exclusive prefix
 // sum of their tile counts (tile_prefix[*n_active] = items of the next fused pass), and, when busy is
 // non-null, appends frames that are done and still busy to done_list[*n_done...] and clears busy.

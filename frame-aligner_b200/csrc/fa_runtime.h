@@ -245,7 +245,6 @@ fa_status correlator_plans(fa_correlator* C, int batch, cufftHandle* fwd, cufftH
 // surfaces; planes selects the fused kx-plane passes (when C->planes) or cuFFT. Calls with
 // first > 0 use pointer and result slots reserved before (correlator_reserve(C, first + n)), so
 // that consecutive calls queue on the stream without waiting for one another.
-fa_status stage_check();
 fa_status correlator_enqueue(fa_correlator* C, const void* const* vols, int in_kind, int n,
                              double* surface = nullptr, bool planes = true, int first = 0);
 // Pointer staging and peak slots for n volumes (grows with a stream synchronisation).

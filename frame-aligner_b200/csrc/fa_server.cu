@@ -582,7 +582,6 @@ fa_status worker_pass(fa_server* S, bool* progress) {
     cudaError_t e = cudaEventQuery(C->ev);
     if (e == cudaErrorNotReady) continue;
     if (e != cudaSuccess) return fail(FA_ERR_CUDA, std::string("server solve: ") + cudaGetErrorString(e));
-    FA_TRY(stage_check());
     C->running = false;
     *progress = true;
     const double t = now_s();
