@@ -1022,12 +1022,28 @@ extern "C" fa_status fa_align_frame(fa_frame* F, const double* rigid_shift, int 
 
 namespace {
 
-// Batched solve; frame_data (optional) replaces each frame's own device data pointer for this call;
-// cache (optional) keeps the buffers and the graph for the next call on the same frames.
-fa_status align_batch_impl(fa_frame* const* frames, int n, const double* rigid_shifts, int max_iterations,
-                           double* D_out, fa_align_stats* stats, const void* const* frame_data,
-                           BatchCache* cache = nullptr) {
-  if (!frames || n <= 0 || !D_out) return fail(FA_ERR_BAD_ARG, "bad arguments");
+// Rigid starts of a batched solve taken on the device from phase-correlation peaks: frame i starts
+// from peaks[i] (flat index into a cnz x cny x cnx correlation surface, x and y scaled by binning),
+// once `ready` (recorded after the peaks were written) has completed.
+struct PeakStart {
+  const long long* peaks;
+  int cnx, cny, cnz, binning;
+  cudaEvent_t ready;
+};
+
+// Queues a batched solve of n frames on frames[0]'s stream: the starting states, one launch of the
+// cached solve graph, and the copies of every frame's x and state into its pinned buffers; the
+// caller's align_batch_finish waits for them. frame_data (optional) replaces each frame's own device
+// data pointer for this call. bc keeps the buffers and the graph for the next call on the same
+// frames. With `peak_start` the rigid starts come from device peaks (rigid_shifts is ignored) and the
+// states are set up on the device, so the host neither waits for the peaks nor copies a state.
+//
+// The graph holds one while-conditional node whose body is kGraphIters x (fused pass, solve step,
+// active-list compaction) and a loop-control kernel: the body repeats on the device until no frame is
+// active or the iteration limit is reached, with no host round trip between rounds.
+fa_status align_batch_enqueue(fa_frame* const* frames, int n, const double* rigid_shifts, int max_iterations,
+                              const void* const* frame_data, BatchCache* bc, const PeakStart* peak_start) {
+  if (!frames || n <= 0 || !bc) return fail(FA_ERR_BAD_ARG, "bad arguments");
   for (int i = 0; i < n; i++)
     if (!frames[i]) return fail(FA_ERR_BAD_ARG, "NULL frame");
   fa_reference* R0 = frames[0]->ref;
@@ -1039,8 +1055,6 @@ fa_status align_batch_impl(fa_frame* const* frames, int n, const double* rigid_s
   if (rigid_shifts && !finite_all(rigid_shifts, (size_t)3 * n)) return fail(FA_ERR_BAD_ARG, "rigid shift not finite");
   fa_context* ctx = R0->ctx;
   FA_CU(cudaSetDevice(ctx->device));
-  std::vector<std::unique_lock<std::mutex>> locks;
-  for (int i = 0; i < n; i++) locks.emplace_back(frames[i]->mu);
   cudaStream_t s = frames[0]->stream;
   int max_tiles = 0, max_nD = 0;
   bool vec4 = true;
@@ -1048,71 +1062,83 @@ fa_status align_batch_impl(fa_frame* const* frames, int n, const double* rigid_s
   // the persistent pass evaluates both cold starting points of a frame in its first launch
   const bool vec4_all = vec4;
   std::vector<Job> jobs(n);
-  // initial states on every frame's stream, then one wait per stream (the copies are done by then)
+  // most work items of one pass: a frame in the paired start phase has two items per tile
+  long long most_items = 0;
   for (int i = 0; i < n; i++) {
     fa_frame* F = frames[i];
-    FA_TRY(init_solve(F, rigid_shifts ? rigid_shifts + 3 * i : nullptr, max_iterations, vec4_all));
+    if (!peak_start) FA_TRY(init_solve(F, rigid_shifts ? rigid_shifts + 3 * i : nullptr, max_iterations, vec4_all));
     jobs[i] = F->job;
     jobs[i].state = F->state;
     if (frame_data) jobs[i].frame = frame_data[i];
     max_tiles = std::max(max_tiles, F->ref->G.n_tiles);
     max_nD = std::max(max_nD, F->ref->nD);
+    most_items += (long long)F->ref->G.n_tiles * (vec4_all ? 2 : 1);
   }
-  for (int i = 0; i < n; i++) FA_CU(cudaStreamSynchronize(frames[i]->stream));
-  std::vector<int> all(n), prefix(n + 1, 0);
-  for (int i = 0; i < n; i++) {
-    all[i] = i;
-    // a frame in the paired start phase has two items per tile
-    prefix[i + 1] = prefix[i] + frames[i]->ref->G.n_tiles * (frames[i]->h_state->phase == fa::kPhaseStartPair ? 2 : 1);
-  }
-  BatchCache local;
-  BatchCache* bc = cache ? cache : &local;
-  auto done = [&](fa_status r) {
-    std::string keep = g_err;
-    cudaStreamSynchronize(s);
-    if (bc == &local) batch_cache_release(ctx, &local);
-    g_err = keep;
-    return r;
-  };
+  // host-made initial states went on every frame's stream: one wait per stream (the copies are done then)
+  if (!peak_start)
+    for (int i = 0; i < n; i++) FA_CU(cudaStreamSynchronize(frames[i]->stream));
   if (bc->cap < n) {
     FA_CU(cudaStreamSynchronize(s));
     batch_cache_release(ctx, bc);
-    fa_status st = dalloc_t(ctx, (size_t)n, &bc->jobs_dev, bc->allocs);
-    if (st == FA_OK) st = dalloc_t(ctx, 1, &bc->d_active, bc->allocs);
-    if (st == FA_OK) st = dalloc_t(ctx, (size_t)n, &bc->d_list, bc->allocs);
-    if (st == FA_OK) st = dalloc_t(ctx, (size_t)n + 1, &bc->d_prefix, bc->allocs);
-    if (st == FA_OK && cudaMallocHost(&bc->h_active, sizeof(int)) != cudaSuccess) {
-      bc->h_active = nullptr;
-      st = fail(FA_ERR_OOM, "cudaMallocHost failed");
+    FA_TRY(dalloc_t(ctx, (size_t)n, &bc->jobs_dev, bc->allocs));
+    FA_TRY(dalloc_t(ctx, 2, &bc->d_active, bc->allocs));  // [0] active frames, [1] rounds of the loop
+    FA_TRY(dalloc_t(ctx, (size_t)n, &bc->d_list, bc->allocs));
+    FA_TRY(dalloc_t(ctx, (size_t)n + 1, &bc->d_prefix, bc->allocs));
+    if (cudaMallocHost(&bc->h_rounds, sizeof(int)) != cudaSuccess) {
+      bc->h_rounds = nullptr;
+      return fail(FA_ERR_OOM, "cudaMallocHost failed");
     }
-    if (st != FA_OK) return done(st);
     bc->cap = n;
   }
-  *bc->h_active = n;
-  if (cudaMemcpyAsync(bc->jobs_dev, jobs.data(), n * sizeof(Job), cudaMemcpyHostToDevice, s) != cudaSuccess ||
-      cudaMemcpyAsync(bc->d_list, all.data(), n * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess ||
-      cudaMemcpyAsync(bc->d_prefix, prefix.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess ||
-      cudaMemcpyAsync(bc->d_active, bc->h_active, sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess)
-    return done(fail(FA_ERR_CUDA, "active list upload failed"));
+  // The job table goes up before any wait on the peaks (a copy from pageable memory may wait for the
+  // stream); then the device-side start when the peaks are on the device, and the first active list
+  // from the states.
+  cudaError_t e = cudaMemcpyAsync(bc->jobs_dev, jobs.data(), n * sizeof(Job), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && peak_start) {
+    e = cudaStreamWaitEvent(s, peak_start->ready, 0);
+    if (e == cudaSuccess)
+      e = fa::launch_activate_peaks(bc->jobs_dev, n, peak_start->peaks, peak_start->cnx, peak_start->cny,
+                                    peak_start->cnz, peak_start->binning, max_iterations, vec4_all, s);
+    g_launches += 1;
+  }
+  if (e == cudaSuccess)
+    e = fa::launch_compact(bc->jobs_dev, n, bc->d_list, bc->d_active, bc->d_prefix, nullptr, nullptr, nullptr, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(bc->d_active + 1, 0, sizeof(int), s);
+  g_launches += 1;
+  if (e != cudaSuccess) return fail(FA_ERR_CUDA, std::string("batch start: ") + cudaGetErrorString(e));
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-  // Iterations run as a CUDA graph of kGraphIters x (fused pass, solve), then one active count.
   constexpr int kGraphIters = 4;
-  const long long key[6] = {n, prefix[n], max_nD, (vec4 ? 1 : 0) + 2 * frames[0]->kind, R0->host.tune_mb,
-                            R0->host.tune_grid_mult};
+  // each round runs kGraphIters iterations; the host loop this replaces stopped after max + 4 steps
+  const int max_steps = (max_iterations > 0 ? max_iterations : 100) + 4;
+  const int max_rounds = (max_steps + kGraphIters - 1) / kGraphIters;
+  const long long key[7] = {n, most_items, max_nD, (vec4 ? 1 : 0) + 2 * frames[0]->kind, R0->host.tune_mb,
+                            R0->host.tune_grid_mult, max_rounds};
   const bool reuse = bc->exec && bc->frames.size() == (size_t)n &&
-                     std::equal(bc->frames.begin(), bc->frames.end(), frames) && std::equal(key, key + 6, bc->key);
-  cudaError_t e = cudaSuccess;
+                     std::equal(bc->frames.begin(), bc->frames.end(), frames) && std::equal(key, key + 7, bc->key);
   if (!reuse) {
     if (bc->exec) cudaGraphExecDestroy(bc->exec);
     bc->exec = nullptr;
     bc->frames.clear();
-    cudaGraph_t graph = nullptr;
-    e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    cudaGraph_t graph = nullptr, body = nullptr;
+    cudaGraphConditionalHandle loop{};
+    e = cudaGraphCreate(&graph, 0);
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&loop, graph, 1, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) {
+      cudaGraphNodeParams cp{};
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = loop;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      cudaGraphNode_t node;
+      e = cudaGraphAddNode(&node, graph, nullptr, 0, &cp);
+      if (e == cudaSuccess) body = cp.conditional.phGraph_out[0];
+    }
+    if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
       for (int it = 0; it < kGraphIters && e == cudaSuccess; it++) {
         if (vec4)
-          e = fa::launch_eval4_active(bc->jobs_dev, bc->d_list, bc->d_active, bc->d_prefix, prefix[n], R0->n_dim,
+          e = fa::launch_eval4_active(bc->jobs_dev, bc->d_list, bc->d_active, bc->d_prefix, most_items, R0->n_dim,
                                       frames[0]->kind, R0->prec == FA_PREC_MIXED, R0->host.tune_mb,
                                       R0->host.tune_grid_mult * sms, s);
         else
@@ -1122,40 +1148,63 @@ fa_status align_batch_impl(fa_frame* const* frames, int n, const double* rigid_s
         if (e == cudaSuccess)
           e = fa::launch_compact(bc->jobs_dev, n, bc->d_list, bc->d_active, bc->d_prefix, nullptr, nullptr, nullptr, s);
       }
-      if (e == cudaSuccess) e = cudaMemcpyAsync(bc->h_active, bc->d_active, sizeof(int), cudaMemcpyDeviceToHost, s);
-      cudaError_t e2 = cudaStreamEndCapture(s, &graph);
+      if (e == cudaSuccess) e = fa::launch_loop_control(loop, bc->d_active, bc->d_active + 1, max_rounds, s);
+      cudaGraph_t captured = nullptr;
+      const cudaError_t e2 = cudaStreamEndCapture(s, &captured);
       if (e == cudaSuccess) e = e2;
     }
     if (e == cudaSuccess) e = cudaGraphInstantiate(&bc->exec, graph, 0);
     if (graph) cudaGraphDestroy(graph);
     if (e != cudaSuccess) {
       bc->exec = nullptr;
-      return done(fail(FA_ERR_CUDA, std::string("batch graph: ") + cudaGetErrorString(e)));
+      return fail(FA_ERR_CUDA, std::string("batch graph: ") + cudaGetErrorString(e));
     }
     bc->frames.assign(frames, frames + n);
-    std::copy(key, key + 6, bc->key);
+    std::copy(key, key + 7, bc->key);
   }
-  const int max_steps = (max_iterations > 0 ? max_iterations : 100) + 4;
-  for (int step = 0; step < max_steps; step += kGraphIters) {
-    e = cudaGraphLaunch(bc->exec, s);
-    g_launches += 3 * kGraphIters;
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) break;
-    if (*bc->h_active == 0) break;
-  }
-  if (e != cudaSuccess) return done(fail(FA_ERR_CUDA, std::string("batch solve: ") + cudaGetErrorString(e)));
+  e = cudaGraphLaunch(bc->exec, s);
+  // the rounds that ran, for the launch count
+  if (e == cudaSuccess) e = cudaMemcpyAsync(bc->h_rounds, bc->d_active + 1, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e != cudaSuccess) return fail(FA_ERR_CUDA, std::string("batch solve: ") + cudaGetErrorString(e));
+  bc->per_round = 3 * kGraphIters + 1;
   // every frame's x and state in one batch of copies on the solve's stream
-  for (int i = 0; i < n; i++) {
-    fa_status r = finish_solve_enqueue(frames[i], s);
-    if (r != FA_OK) return done(r);
-  }
-  if (cudaStreamSynchronize(s) != cudaSuccess) return done(fail(FA_ERR_CUDA, "result read failed"));
+  for (int i = 0; i < n; i++) FA_TRY(finish_solve_enqueue(frames[i], s));
+  return FA_OK;
+}
+
+// Waits for a batched solve queued with bc and writes D (and the statistics) of its frames.
+fa_status align_batch_finish(fa_frame* const* frames, int n, const BatchCache* bc, double* D_out,
+                             fa_align_stats* stats) {
+  if (cudaStreamSynchronize(frames[0]->stream) != cudaSuccess) return fail(FA_ERR_CUDA, "batch solve failed");
+  g_launches += (long long)*bc->h_rounds * bc->per_round;
   for (int i = 0; i < n; i++) {
     fa_frame* F = frames[i];
     finish_solve_read(F, D_out + (size_t)i * 3 * F->ref->nD, stats ? stats + i : nullptr);
     F->have_last = false;
   }
-  return done(FA_OK);
+  return FA_OK;
+}
+
+// Synchronous batched solve under the frames' locks; cache (optional) keeps the buffers and the
+// graph for the next call on the same frames.
+fa_status align_batch_impl(fa_frame* const* frames, int n, const double* rigid_shifts, int max_iterations,
+                           double* D_out, fa_align_stats* stats, const void* const* frame_data,
+                           BatchCache* cache = nullptr) {
+  if (!frames || n <= 0 || !D_out) return fail(FA_ERR_BAD_ARG, "bad arguments");
+  for (int i = 0; i < n; i++)
+    if (!frames[i]) return fail(FA_ERR_BAD_ARG, "NULL frame");
+  std::vector<std::unique_lock<std::mutex>> locks;
+  for (int i = 0; i < n; i++) locks.emplace_back(frames[i]->mu);
+  BatchCache local;
+  BatchCache* bc = cache ? cache : &local;
+  fa_status r = align_batch_enqueue(frames, n, rigid_shifts, max_iterations, frame_data, bc, nullptr);
+  if (r == FA_OK) r = align_batch_finish(frames, n, bc, D_out, stats);
+  std::string keep = g_err;
+  cudaSetDevice(frames[0]->ref->ctx->device);
+  cudaStreamSynchronize(frames[0]->stream);
+  if (bc == &local) batch_cache_release(frames[0]->ref->ctx, &local);
+  g_err = keep;
+  return r;
 }
 
 }  // namespace
@@ -1166,8 +1215,8 @@ void batch_cache_release(fa_context* ctx, BatchCache* c) {
   if (c->exec) cudaGraphExecDestroy(c->exec);
   c->exec = nullptr;
   c->frames.clear();
-  if (c->h_active) cudaFreeHost(c->h_active);
-  c->h_active = nullptr;
+  if (c->h_rounds) cudaFreeHost(c->h_rounds);
+  c->h_rounds = nullptr;
   dfree_all(ctx, c->allocs);
   c->jobs_dev = nullptr;
   c->d_active = c->d_list = c->d_prefix = nullptr;
@@ -1796,27 +1845,39 @@ fa_status aligner_run(fa_aligner* A, const void* const* frames, fa_dtype dtype, 
     }
     FA_TRY(correlator_enqueue(C, cin.data() + c0, cin_kind, m, nullptr, true, c0));
     c0 += m;
-    if (c0 == gb[g + 1]) {  // a group's peaks, read back without waiting for the rest
-      FA_CU(cudaMemcpyAsync(C->h_idx + gb[g], C->d_idx + gb[g], (size_t)(c0 - gb[g]) * sizeof(long long),
-                            cudaMemcpyDeviceToHost, s));
-      FA_CU(cudaEventRecord(A->group_ev[g], s));
-    }
+    if (c0 == gb[g + 1]) FA_CU(cudaEventRecord(A->group_ev[g], s));  // a group's frames and peaks are ready
   }
+  // Every group's solve is queued at once, each on its first slot's stream behind its own frames and
+  // peaks: the first group's solve runs while the later groups upload and correlate, and a later
+  // group starts as soon as its peaks are there. The rigid starts are unravelled and scaled by the
+  // binning on the device (FrameWarpAligner.cpp:181-190).
   std::vector<fa_frame*> batch(A->slots.begin(), A->slots.begin() + n);
-  for (int g = 0; g < n_groups; g++) {
+  fa_status r = FA_OK;
+  int queued = 0;
+  for (int g = 0; g < n_groups && r == FA_OK; g++) {
     const int g0 = gb[g], g1 = gb[g + 1];
-    FA_CU(cudaEventSynchronize(A->group_ev[g]));
-    std::vector<double> rigid((size_t)3 * (g1 - g0));
-    for (int i = g0; i < g1; i++) {
-      unravel_shift(C, C->h_idx[i], rigid.data() + (size_t)3 * (i - g0));
-      // FrameWarpAligner.cpp:186-188: x and y scaled by the phase-correlation downsampling
-      rigid[(size_t)3 * (i - g0)] *= A->prm.spatial_binning;
-      rigid[(size_t)3 * (i - g0) + 1] *= A->prm.spatial_binning;
-      A->slots[i]->have_last = false;
+    const PeakStart ps{C->d_idx + g0, C->nx, C->ny, C->nz, A->prm.spatial_binning, A->group_ev[g]};
+    r = align_batch_enqueue(batch.data() + g0, g1 - g0, nullptr, A->prm.max_iterations, nullptr, &A->batch_cache[g],
+                            &ps);
+    // the last group's stream also holds whatever its failed enqueue left queued
+    queued = g + 1;
+  }
+  for (int g = 0; g < queued; g++) {
+    const int g0 = gb[g], g1 = gb[g + 1];
+    if (r != FA_OK) {  // drain without reading, keeping the first error
+      std::string keep = g_err;
+      cudaStreamSynchronize(batch[g0]->stream);
+      g_err = keep;
+      continue;
     }
-    FA_TRY(align_batch_impl(batch.data() + g0, g1 - g0, rigid.data(), A->prm.max_iterations,
-                            D_out + (size_t)g0 * 3 * A->ref->nD, stats ? stats + g0 : nullptr, nullptr,
-                            &A->batch_cache[g]));
+    r = align_batch_finish(batch.data() + g0, g1 - g0, &A->batch_cache[g], D_out + (size_t)g0 * 3 * A->ref->nD,
+                           stats ? stats + g0 : nullptr);
+  }
+  if (r != FA_OK) return r;
+  // the end of the call: after every group's solve
+  for (int g = 1; g < n_groups; g++) {
+    FA_CU(cudaEventRecord(A->group_ev[g], batch[gb[g]]->stream));
+    FA_CU(cudaStreamWaitEvent(batch[0]->stream, A->group_ev[g], 0));
   }
   FA_CU(cudaEventRecord(A->ev1, batch[0]->stream));
   FA_CU(cudaEventSynchronize(A->ev1));

@@ -753,6 +753,21 @@ cudaError_t launch_compact(const Job* jobs_dev, int n_jobs, int* active, int* n_
   return cudaGetLastError();
 }
 
+// Last node of the body of a batched solve's device-side loop: counts the rounds and repeats the body
+// while a frame is still active and fewer than max_rounds rounds ran.
+__global__ void loop_control_kernel(cudaGraphConditionalHandle h, const int* __restrict__ n_active,
+                                    int* __restrict__ rounds, int max_rounds) {
+  const int r = *rounds + 1;
+  *rounds = r;
+  cudaGraphSetConditional(h, *n_active > 0 && r < max_rounds ? 1u : 0u);
+}
+
+cudaError_t launch_loop_control(cudaGraphConditionalHandle h, const int* n_active, int* rounds, int max_rounds,
+                                cudaStream_t s) {
+  loop_control_kernel<<<1, 1, 0, s>>>(h, n_active, rounds, max_rounds);
+  return cudaGetLastError();
+}
+
 // Zero start of a batched solve (the host-side init of the single-frame driver, on the device).
 __global__ void activate_kernel(const Job* __restrict__ jobs, const Activation* __restrict__ recs, int* busy) {
   const Activation r = recs[blockIdx.x];
@@ -787,6 +802,48 @@ __global__ void activate_kernel(const Job* __restrict__ jobs, const Activation* 
     *j.state = S;
     busy[r.job] = 1;
   }
+}
+
+// Start of the aligner's batched solve straight from the phase-correlation peaks in device memory, so
+// that the host need not read them first: job i takes peak i (flat index of the correlation surface
+// of a cnz x cny x cnx volume), unravels and wraps it like unravel_shift (VolumePhaseCorrelator.cpp:
+// 94-103), scales x and y by the binning (FrameWarpAligner.cpp:186-188) and sets the zero start, or the
+// paired start when `pair` and the shift is not zero.
+__global__ void activate_peaks_kernel(const Job* __restrict__ jobs, const long long* __restrict__ peaks, int cnx,
+                                      int cny, int cnz, int binning, int max_iter, int pair) {
+  const Job& j = jobs[blockIdx.x];
+  const RefDev& R = *j.ref;
+  const long long idx = peaks[blockIdx.x];
+  long long x = idx % cnx, y = (idx / cnx) % cny, z = idx / ((long long)cnx * cny);
+  if (x > cnx / 2) x -= cnx;
+  if (y > cny / 2) y -= cny;
+  if (z > cnz / 2) z -= cnz;
+  double rigid[3] = {(double)x * binning, (double)y * binning, R.n_dim == 3 ? (double)z : 0.0};
+  bool nonzero = false;
+  for (int c = 0; c < R.n_dim; c++) nonzero = nonzero || rigid[c] != 0.0;
+  const bool paired = pair != 0 && nonzero;
+  for (int i = threadIdx.x; i < R.P; i += blockDim.x) {
+    j.x[i] = 0.0;
+    j.g[i] = 0.0;
+    j.p[i] = 0.0;
+    j.gt[i] = 0.0;
+  }
+  for (int i = threadIdx.x; i < R.nD * kDParamF4; i += blockDim.x) j.dparams[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (paired) write_const_dparams(j.dparams2, R.nD, R.n_dim, rigid, threadIdx.x, blockDim.x);
+  if (threadIdx.x == 0) {
+    FrameState S{};
+    S.phase = paired ? kPhaseStartPair : kPhaseStartZero;
+    S.max_iter = max_iter > 0 ? max_iter : 100;
+    for (int c = 0; c < 3; c++) S.rigid[c] = rigid[c];
+    *j.state = S;
+  }
+}
+
+cudaError_t launch_activate_peaks(const Job* jobs_dev, int n, const long long* peaks, int cnx, int cny, int cnz,
+                                  int binning, int max_iter, bool pair, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  activate_peaks_kernel<<<n, 128, 0, s>>>(jobs_dev, peaks, cnx, cny, cnz, binning, max_iter, pair ? 1 : 0);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_activate(const Job* jobs_dev, const Activation* recs, int n, int* busy, cudaStream_t s) {

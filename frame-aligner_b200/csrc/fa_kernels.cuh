@@ -68,6 +68,14 @@ cudaError_t launch_compact(const Job* jobs_dev, int n_jobs, int* active, int* n_
                            int* done_list, int* n_done, cudaStream_t s);
 
 // Initialises the solve state of n frames (zero start, optional rigid and warm starts) and marks them busy.
+// Loop control inside a while-conditional graph body: ++*rounds, and the body repeats while
+// *n_active > 0 and *rounds < max_rounds.
+cudaError_t launch_loop_control(cudaGraphConditionalHandle h, const int* n_active, int* rounds, int max_rounds,
+                                cudaStream_t s);
+// Zero / paired start of n jobs from phase-correlation peak indices in device memory (correlator
+// dims cnz x cny x cnx, x and y scaled by the binning).
+cudaError_t launch_activate_peaks(const Job* jobs_dev, int n, const long long* peaks, int cnx, int cny, int cnz,
+                                  int binning, int max_iter, bool pair, cudaStream_t s);
 cudaError_t launch_activate(const Job* jobs_dev, const Activation* recs, int n, int* busy, cudaStream_t s);
 
 // Reduces one job's tile partials into result = [f, g(P)] (deterministic order).

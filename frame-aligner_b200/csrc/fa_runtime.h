@@ -149,14 +149,15 @@ namespace fa_rt {
 struct BatchCache {
   std::vector<Alloc> allocs;
   fa::Job* jobs_dev = nullptr;
-  int* d_active = nullptr;
+  int* d_active = nullptr;  // [0] active frames, [1] rounds of the device-side loop
   int* d_list = nullptr;
   int* d_prefix = nullptr;
-  int* h_active = nullptr;  // pinned
+  int* h_rounds = nullptr;  // pinned: rounds the last solve ran
+  int per_round = 0;        // kernel launches per round
   int cap = 0;
   cudaGraphExec_t exec = nullptr;
   std::vector<fa_frame*> frames;  // the frames the graph was captured for
-  long long key[6] = {0, 0, 0, 0, 0, 0};
+  long long key[7] = {0, 0, 0, 0, 0, 0, 0};
 };
 // Frees the cache's buffers and graph (after the caller's streams are idle).
 void batch_cache_release(fa_context* ctx, BatchCache* c);
