@@ -340,19 +340,27 @@ fa_status retile(fa_reference* R, int target_tile_voxels) {
   return FA_OK;
 }
 
+// Launches of at least this many frames use the register budget tuned for many frames.
+constexpr int kManyFrames = 4;
+
 struct TuneResult {
-  int target, mb, grid_mult;
+  int target, mb, grid_mult, mb_small;
   double ms;
 };
 std::mutex g_tune_mu;
 std::map<std::string, TuneResult> g_tune_cache;
 
 // The project's autotuner for the fused pass: times each (tile size, CTAs per SM) candidate with the
-// persistent kernel the batched solver uses, on a launch of 8 synthetic frames (the reference itself,
-// slightly displaced) and on a launch of one, keeps the lowest sum of per-frame times, and caches the
-// choice per volume shape, control-point count and precision for the life of the process. Register
-// budgets under which the kernel spills more than 128 bytes are skipped (the largest budget is
-// always a candidate).
+// persistent kernel the batched solver uses, on a launch of K distinct synthetic frames (copies of the
+// reference, slightly displaced; K up to 16, as many as fit in 256 MB, so that the frames do not all
+// stay in L2 as a real batch's do not) and on a launch of one. The tile size is the one with the
+// lowest sum of the best per-frame time of the K-frame launch and the best one-frame launch time (so
+// that it serves both the batched aligner and the few-frame launches of serving and of a batch's late
+// iterations); at that tile size the budget for launches of many frames is the fastest K-frame one
+// and the budget for a few frames the fastest one-frame one. The choice is cached
+// per volume shape, control-point count and precision for the life of the process. Register budgets
+// under which the kernel spills more than 128 bytes are skipped (the largest budget is always a
+// candidate).
 fa_status autotune(fa_reference* R) {
   char keyb[128];
   std::snprintf(keyb, sizeof(keyb), "%d,%d,%d,%d,%d,%d", R->nz, R->ny, R->nx, R->nD, (int)R->prec,
@@ -364,11 +372,11 @@ fa_status autotune(fa_reference* R) {
     if (it != g_tune_cache.end()) {
       R->host.tune_mb = it->second.mb;
       R->host.tune_grid_mult = it->second.grid_mult;
+      R->host.tune_mb_small = it->second.mb_small;
       return retile(R, it->second.target);
     }
   }
   fa_context* ctx = R->ctx;
-  const int K = 8;
   const int kind = R->prec == FA_PREC_MIXED ? fa::kFrameF16 : fa::kFrameF32;
   std::vector<Alloc> tmp;
   auto done = [&](fa_status st) {
@@ -388,7 +396,8 @@ fa_status autotune(fa_reference* R) {
   const long long plane = (long long)pitch * (R->ny + 2 * fa::kHaloY);
   const size_t esz = kind == fa::kFrameF16 ? 2 : 4;
   const size_t elems = (size_t)plane * (R->nz + 2 * hz);
-  fa_status st = dalloc(ctx, elems * esz, &frame, tmp);
+  const int K = (int)std::max<size_t>(2, std::min<size_t>(16, ((size_t)256 << 20) / (elems * esz)));
+  fa_status st = dalloc(ctx, (size_t)K * elems * esz, &frame, tmp);
   if (st == FA_OK) st = dalloc_t(ctx, (size_t)R->nD * fa::kDParamF4, &dp, tmp);
   if (st == FA_OK) st = dalloc_t(ctx, (size_t)K * R->G.n_rows * fa::kPartialDoubles, &parts, tmp);
   if (st == FA_OK) st = dalloc_t(ctx, (size_t)K, &jobs_dev, tmp);
@@ -401,6 +410,9 @@ fa_status autotune(fa_reference* R) {
   cudaError_t e = cudaMemsetAsync(frame, 0, elems * esz, s);
   if (e == cudaSuccess)
     e = fa::launch_to_slot(R->host.ref32, FA_F32, interior, kind, R->nz, R->ny, R->nx, pitch, plane, false, s);
+  for (int i = 1; i < K && e == cudaSuccess; i++)
+    e = cudaMemcpyAsync(static_cast<char*>(frame) + (size_t)i * elems * esz, frame, elems * esz,
+                        cudaMemcpyDeviceToDevice, s);
   std::vector<double> D((size_t)R->nD * 3);
   for (int k = 0; k < R->nD; k++) {
     D[3 * k] = 0.3 + 0.01 * k;
@@ -414,7 +426,7 @@ fa_status autotune(fa_reference* R) {
   for (int i = 0; i < K; i++) {
     Job j{};
     j.ref = R->dev;
-    j.frame = interior;
+    j.frame = static_cast<char*>(interior) + (size_t)i * elems * esz;
     j.fplane = plane;
     j.fpitch = pitch;
     j.fpad = 1;
@@ -435,17 +447,24 @@ fa_status autotune(fa_reference* R) {
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  TuneResult best{4096, 2, 2, 1e30};
+  TuneResult best{4096, 2, 2, 2, 1e30};
   const int targets[] = {1024, 2048, 4096, 8192, 16384};
   const int mbs[] = {2, 3, 4};
+  // per-frame time of the K-frame launch and time of the one-frame launch per (tile size, budget);
+  // 0 = not a candidate
+  double many[5][3], one[5][3];
+  for (int ti = 0; ti < 5; ti++)
+    for (int mi = 0; mi < 3; mi++) many[ti][mi] = one[ti][mi] = 0.0;
   std::vector<int> hprefix(K + 1);
-  for (int target : targets) {
+  for (int ti = 0; ti < 5; ti++) {
+    const int target = targets[ti];
     if (retile(R, target) != FA_OK) break;
     for (int i = 0; i <= K; i++) hprefix[i] = i * R->G.n_tiles;
     e = cudaMemcpyAsync(prefix, hprefix.data(), (K + 1) * sizeof(int), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) break;
-    for (int mb : mbs) {
+    for (int mi = 0; mi < 3; mi++) {
+      const int mb = mbs[mi];
       const bool mixed = R->prec == FA_PREC_MIXED;
       // register budgets under which the kernel spills more than a few values are not candidates
       if (mb != mbs[0] && fa::eval4_active_local_bytes(R->n_dim, kind, mixed, mb) > 128) continue;
@@ -453,10 +472,9 @@ fa_status autotune(fa_reference* R) {
         return fa::launch_eval4_active(jobs_dev, list, cnt, prefix, (long long)K * R->G.n_tiles, R->n_dim, kind, mixed,
                                        mb, mb * sms, s);
       };
-      // Score: per-frame time of a K-frame launch plus that of a one-frame launch, so that the
-      // choice also serves the late iterations of a batch and the few-frame launches of serving.
-      double score = 0;
-      for (int count : {K, 1}) {
+      double per_frame[2] = {0.0, 0.0};  // K frames, one frame
+      for (int c = 0; c < 2; c++) {
+        const int count = c == 0 ? K : 1;
         e = cudaMemcpyAsync(cnt, count == K ? &kcount : &kone, sizeof(int), cudaMemcpyHostToDevice, s);
         if (e == cudaSuccess) e = launch();
         if (e == cudaSuccess) e = cudaEventRecord(e0, s);
@@ -467,18 +485,35 @@ fa_status autotune(fa_reference* R) {
         if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
         g_launches += 4;
         if (e != cudaSuccess) break;
-        score += ms / count;
+        per_frame[c] = ms / count;
       }
       if (e != cudaSuccess) break;
-      if (score < best.ms) best = TuneResult{target, mb, mb, score};
+      many[ti][mi] = per_frame[0];
+      one[ti][mi] = per_frame[1];
     }
     if (e != cudaSuccess) break;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (e != cudaSuccess) return done(fail(FA_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e)));
+  for (int ti = 0; ti < 5; ti++) {
+    double tk = 1e30, t1 = 1e30;
+    int mb_k = 2, mb_1 = 2;
+    for (int mi = 0; mi < 3; mi++) {
+      if (many[ti][mi] > 0.0 && many[ti][mi] < tk) {
+        tk = many[ti][mi];
+        mb_k = mbs[mi];
+      }
+      if (one[ti][mi] > 0.0 && one[ti][mi] < t1) {
+        t1 = one[ti][mi];
+        mb_1 = mbs[mi];
+      }
+    }
+    if (tk < 1e30 && t1 < 1e30 && tk + t1 < best.ms) best = TuneResult{targets[ti], mb_k, mb_k, mb_1, tk + t1};
+  }
   R->host.tune_mb = best.mb;
   R->host.tune_grid_mult = best.grid_mult;
+  R->host.tune_mb_small = best.mb_small;
   fa_status r = retile(R, best.target);
   if (r == FA_OK) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -507,6 +542,7 @@ fa_status reference_setup(fa_reference* R, const float* src, bool src_device) {
   h.P = R->P;
   h.tune_mb = 2;
   h.tune_grid_mult = 2;
+  h.tune_mb_small = 2;
   RowDesc* rows;
   int* tile_c0;
   int2* ctrl;
@@ -647,6 +683,7 @@ extern "C" fa_status fa_reference_retune(fa_reference* R, int tile_voxels, int c
   FA_CU(cudaSetDevice(R->ctx->device));
   R->host.tune_mb = ctas_per_sm;
   R->host.tune_grid_mult = ctas_per_sm;
+  R->host.tune_mb_small = ctas_per_sm;
   return retile(R, tile_voxels);
 }
 
@@ -868,7 +905,7 @@ fa_status evaluate(fa_frame* F, const double* D) {
   const size_t np = (size_t)R->nD * fa::kDParamF4 * sizeof(float4);
   FA_CU(cudaMemcpyAsync(F->job.dparams, F->h_dparams, np, cudaMemcpyHostToDevice, F->stream));
   FA_CU(fa::launch_eval(F->job_dev, 1, R->G.n_tiles, R->n_dim, F->kind, R->prec == FA_PREC_MIXED, F->stream,
-                          R->nx % 4 == 0, R->host.tune_mb));
+                          R->nx % 4 == 0, R->host.tune_mb_small));
   FA_CU(fa::launch_reduce(F->job_dev, R->host, F->stream));
   g_launches += 2;
   FA_CU(cudaMemcpyAsync(F->h_result, F->job.result, (1 + R->P) * sizeof(double), cudaMemcpyDeviceToHost, F->stream));
@@ -1005,7 +1042,7 @@ extern "C" fa_status fa_align_frame(fa_frame* F, const double* rigid_shift, int 
   int phase = fa::kPhaseStartZero;
   for (int step = 0; step < max_steps && phase != fa::kPhaseDone; step++) {
     FA_CU(fa::launch_eval(F->job_dev, 1, R->G.n_tiles, R->n_dim, F->kind, R->prec == FA_PREC_MIXED, F->stream,
-                          R->nx % 4 == 0, R->host.tune_mb));
+                          R->nx % 4 == 0, R->host.tune_mb_small));
     FA_CU(fa::launch_solve(F->job_dev, 1, R->nD, R->n_dim, F->stream));
     g_launches += 2;
     FA_CU(cudaMemcpyAsync(&F->h_state->phase, &F->state->phase, sizeof(int), cudaMemcpyDeviceToHost, F->stream));
@@ -1112,8 +1149,9 @@ fa_status align_batch_enqueue(fa_frame* const* frames, int n, const double* rigi
   // each round runs kGraphIters iterations; the host loop this replaces stopped after max + 4 steps
   const int max_steps = (max_iterations > 0 ? max_iterations : 100) + 4;
   const int max_rounds = (max_steps + kGraphIters - 1) / kGraphIters;
-  const long long key[7] = {n, most_items, max_nD, (vec4 ? 1 : 0) + 2 * frames[0]->kind, R0->host.tune_mb,
-                            R0->host.tune_grid_mult, max_rounds};
+  // the register budget tuned for launches of many frames, or of a few
+  const int mb = n >= kManyFrames ? R0->host.tune_mb : R0->host.tune_mb_small;
+  const long long key[7] = {n, most_items, max_nD, (vec4 ? 1 : 0) + 2 * frames[0]->kind, mb, 0, max_rounds};
   const bool reuse = bc->exec && bc->frames.size() == (size_t)n &&
                      std::equal(bc->frames.begin(), bc->frames.end(), frames) && std::equal(key, key + 7, bc->key);
   if (!reuse) {
@@ -1139,8 +1177,7 @@ fa_status align_batch_enqueue(fa_frame* const* frames, int n, const double* rigi
       for (int it = 0; it < kGraphIters && e == cudaSuccess; it++) {
         if (vec4)
           e = fa::launch_eval4_active(bc->jobs_dev, bc->d_list, bc->d_active, bc->d_prefix, most_items, R0->n_dim,
-                                      frames[0]->kind, R0->prec == FA_PREC_MIXED, R0->host.tune_mb,
-                                      R0->host.tune_grid_mult * sms, s);
+                                      frames[0]->kind, R0->prec == FA_PREC_MIXED, mb, mb * sms, s);
         else
           e = fa::launch_eval(bc->jobs_dev, n, max_tiles, R0->n_dim, frames[0]->kind, R0->prec == FA_PREC_MIXED, s,
                               false);
@@ -1742,13 +1779,14 @@ fa_status aligner_grow(fa_aligner* A, int n, int kind, size_t staging_need) {
   return FA_OK;
 }
 
-// Solve groups of one call, as frame boundaries {0, ..., n}. Host batches of 2 * chunk frames or
-// more are solved in two groups: the first group's solve runs while the second group uploads and
-// correlates. Frames are independent, so the results do not depend on the grouping. The first group
-// takes about 45% of the frames (whole upload chunks), which balances its solve against the second
-// group's uploads. Frames already on the device are solved in one group.
-std::vector<int> solve_groups(int n, bool device_src, int chunk) {
-  if (device_src || n < 2 * chunk) return {0, n};
+// Solve groups of one call, as frame boundaries {0, ..., n}. Batches of 2 * chunk frames or more
+// are solved in two groups: the first group's solve runs while the second group uploads (host
+// frames) and correlates, and the correlation kernels fill the SMs that the first group's one-CTA-
+// per-frame solve steps leave idle. Frames are independent, so the results do not depend on the
+// grouping. The first group takes about 45% of the frames (whole chunks of `chunk` frames), which
+// balances its solve against the second group's uploads.
+std::vector<int> solve_groups(int n, int chunk) {
+  if (n < 2 * chunk) return {0, n};
   return {0, std::min(n - chunk, ((9 * n / 20 + chunk - 1) / chunk) * chunk), n};
 }
 
@@ -1770,6 +1808,7 @@ fa_status aligner_run(fa_aligner* A, const void* const* frames, fa_dtype dtype, 
   if (!A->ev0) {
     FA_CU(cudaEventCreate(&A->ev0));
     FA_CU(cudaEventCreate(&A->ev1));
+    FA_CU(cudaEventCreate(&A->ev_corr));
   }
   FA_CU(cudaEventRecord(A->ev0, s));
   // Host frames upload on a copy stream in chunks of kChunk; each chunk's conversion and phase
@@ -1779,7 +1818,7 @@ fa_status aligner_run(fa_aligner* A, const void* const* frames, fa_dtype dtype, 
   if (!device_src) {
     if (!A->copy_stream) FA_CU(cudaStreamCreateWithFlags(&A->copy_stream, cudaStreamNonBlocking));
     // one event per upload chunk: chunks never straddle a solve group, so a group adds at most one
-    while ((int)A->copy_ev.size() < (n + chunk - 1) / chunk + (int)solve_groups(n, device_src, chunk).size()) {
+    while ((int)A->copy_ev.size() < (n + chunk - 1) / chunk + (int)solve_groups(n, kChunk).size()) {
       cudaEvent_t e;
       FA_CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
       A->copy_ev.push_back(e);
@@ -1798,7 +1837,7 @@ fa_status aligner_run(fa_aligner* A, const void* const* frames, fa_dtype dtype, 
     }
   } drain{device_src ? nullptr : A->copy_stream};
   FA_TRY(correlator_reserve(A->corr, n));
-  const std::vector<int> gb = solve_groups(n, device_src, kChunk);  // group g: frames [gb[g], gb[g + 1])
+  const std::vector<int> gb = solve_groups(n, kChunk);  // group g: frames [gb[g], gb[g + 1])
   const int n_groups = (int)gb.size() - 1;
   while ((int)A->batch_cache.size() < n_groups) A->batch_cache.emplace_back();
   while ((int)A->group_ev.size() < n_groups) {
@@ -1847,6 +1886,7 @@ fa_status aligner_run(fa_aligner* A, const void* const* frames, fa_dtype dtype, 
     c0 += m;
     if (c0 == gb[g + 1]) FA_CU(cudaEventRecord(A->group_ev[g], s));  // a group's frames and peaks are ready
   }
+  FA_CU(cudaEventRecord(A->ev_corr, s));
   // Every group's solve is queued at once, each on its first slot's stream behind its own frames and
   // peaks: the first group's solve runs while the later groups upload and correlate, and a later
   // group starts as soon as its peaks are there. The rigid starts are unravelled and scaled by the
@@ -1884,6 +1924,8 @@ fa_status aligner_run(fa_aligner* A, const void* const* frames, fa_dtype dtype, 
   float ms = 0;
   FA_CU(cudaEventElapsedTime(&ms, A->ev0, A->ev1));
   A->last_ms = ms;
+  FA_CU(cudaEventElapsedTime(&ms, A->ev0, A->ev_corr));
+  A->last_corr_ms = ms;
   return FA_OK;
 }
 
@@ -1953,6 +1995,7 @@ extern "C" fa_status fa_aligner_destroy(fa_aligner* A) {
   if (A->stream) cudaStreamDestroy(A->stream);
   if (A->ev0) cudaEventDestroy(A->ev0);
   if (A->ev1) cudaEventDestroy(A->ev1);
+  if (A->ev_corr) cudaEventDestroy(A->ev_corr);
   for (cudaEvent_t e : A->copy_ev) cudaEventDestroy(e);
   for (cudaEvent_t e : A->group_ev) cudaEventDestroy(e);
   if (A->copy_stream) cudaStreamDestroy(A->copy_stream);
@@ -2044,6 +2087,13 @@ extern "C" fa_status fa_aligner_last_device_ms(const fa_aligner* A, double* ms) 
   return FA_OK;
 }
 
+extern "C" fa_status fa_aligner_last_phase_ms(const fa_aligner* A, double* correlate_ms, double* total_ms) {
+  if (!A || !correlate_ms || !total_ms) return fail(FA_ERR_BAD_ARG, "NULL argument");
+  *correlate_ms = A->last_corr_ms;
+  *total_ms = A->last_ms;
+  return FA_OK;
+}
+
 extern "C" fa_status fa_profile_eval(fa_frame* const* frames, int n, const double* D, int launches,
                                      double* ms_per_launch) {
   if (!frames || n <= 0 || !D || launches <= 0 || !ms_per_launch) return fail(FA_ERR_BAD_ARG, "bad arguments");
@@ -2069,11 +2119,12 @@ extern "C" fa_status fa_profile_eval(fa_frame* const* frames, int n, const doubl
   if (e == cudaSuccess) e = cudaEventCreate(&e1);
   // one untimed launch, then the timed ones
   const bool v4 = R->nx % 4 == 0;
+  const int mb = n >= kManyFrames ? R->host.tune_mb : R->host.tune_mb_small;
   if (e == cudaSuccess)
-    e = fa::launch_eval(jd, n, R->G.n_tiles, R->n_dim, frames[0]->kind, R->prec == FA_PREC_MIXED, s, v4, R->host.tune_mb);
+    e = fa::launch_eval(jd, n, R->G.n_tiles, R->n_dim, frames[0]->kind, R->prec == FA_PREC_MIXED, s, v4, mb);
   if (e == cudaSuccess) e = cudaEventRecord(e0, s);
   for (int l = 0; l < launches && e == cudaSuccess; l++)
-    e = fa::launch_eval(jd, n, R->G.n_tiles, R->n_dim, frames[0]->kind, R->prec == FA_PREC_MIXED, s, v4, R->host.tune_mb);
+    e = fa::launch_eval(jd, n, R->G.n_tiles, R->n_dim, frames[0]->kind, R->prec == FA_PREC_MIXED, s, v4, mb);
   if (e == cudaSuccess) e = cudaEventRecord(e1, s);
   if (e == cudaSuccess) e = cudaEventSynchronize(e1);
   float ms = 0;

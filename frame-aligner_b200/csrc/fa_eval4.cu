@@ -10,9 +10,9 @@
 // displacement that changes by ~1e-5 px per voxel, so four neighbours almost always share the
 // integer tap offset. They then need only five frame values per tap row, fetched as one aligned
 // 8-element window (two 64-bit loads for FP16, two 128-bit loads for FP32) and shifted into place,
-// instead of eight gathers per voxel; the reference and gradient planes are read with one vector
-// load per plane. Lanes whose four voxels straddle an interval boundary, a range end, a change of
-// the integer offset or the volume edge take the per-voxel path.
+// instead of eight gathers per voxel; the reference and gradient values come with two 128-bit
+// loads (BF16 groups) or one per plane (FP32). Row segments of 128 voxels that straddle an interval
+// boundary, a range end, a change of the integer offset or the volume edge take the per-voxel path.
 #include <type_traits>
 
 #include "fa_device.cuh"
@@ -45,6 +45,13 @@ struct RefGradSrc<float> {
 #pragma unroll
     for (int k = 0; k < NDIM; k++) load4(g[k] + p0, g4[k]);
   }
+  // one voxel's reference and gradient values
+  template <int NDIM>
+  __device__ __forceinline__ void load1(long long p, float& t, float* g1) const {
+    t = __ldg(r + p);
+#pragma unroll
+    for (int k = 0; k < NDIM; k++) g1[k] = __ldg(g[k] + p);
+  }
 };
 template <>
 struct RefGradSrc<__nv_bfloat16> {
@@ -65,66 +72,15 @@ struct RefGradSrc<__nv_bfloat16> {
     unpack(c.x, c.y, g4[1]);
     if (NDIM == 3) unpack(c.z, c.w, g4[NDIM == 3 ? 2 : 0]);
   }
-};
-
-// Five consecutive frame values v[k] = p[s + k], k = 0..4, from the aligned 8-element window at p
-// (p is 8-element aligned in FP16 units or 4-element aligned in FP32 units; s in [0, 3]).
-__device__ __forceinline__ void window5(const __half* p, int s, float* v) {
-  const uint2 lo = __ldg(reinterpret_cast<const uint2*>(p));
-  const uint2 hi = __ldg(reinterpret_cast<const uint2*>(p + 4));
-  const bool e = (s >> 1) != 0;
-  const unsigned sh = (unsigned)(s & 1) * 16u;
-  const unsigned A = e ? lo.y : lo.x;
-  const unsigned B = e ? hi.x : lo.y;
-  const unsigned C = e ? hi.y : hi.x;
-  const unsigned p0 = __funnelshift_r(A, B, sh);
-  const unsigned p1 = __funnelshift_r(B, C, sh);
-  const unsigned p2 = __funnelshift_r(C, hi.y, sh);
-  const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&p0));
-  const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&p1));
-  v[0] = a.x;
-  v[1] = a.y;
-  v[2] = b.x;
-  v[3] = b.y;
-  v[4] = __half2float(__ushort_as_half((unsigned short)(p2 & 0xffffu)));
-}
-__device__ __forceinline__ void window5(const RawU16* p, int s, float* v) {
-  const uint2 lo = __ldg(reinterpret_cast<const uint2*>(p));
-  const uint2 hi = __ldg(reinterpret_cast<const uint2*>(p + 4));
-  const bool e = (s >> 1) != 0;
-  const unsigned sh = (unsigned)(s & 1) * 16u;
-  const unsigned A = e ? lo.y : lo.x;
-  const unsigned B = e ? hi.x : lo.y;
-  const unsigned C = e ? hi.y : hi.x;
-  const unsigned p0 = __funnelshift_r(A, B, sh);
-  const unsigned p1 = __funnelshift_r(B, C, sh);
-  const unsigned p2 = __funnelshift_r(C, hi.y, sh);
-  v[0] = __uint_as_float(__byte_perm(p0, 0x4B000000u, 0x7610)) - 8388608.0f;
-  v[1] = __uint_as_float(__byte_perm(p0, 0x4B000000u, 0x7632)) - 8388608.0f;
-  v[2] = __uint_as_float(__byte_perm(p1, 0x4B000000u, 0x7610)) - 8388608.0f;
-  v[3] = __uint_as_float(__byte_perm(p1, 0x4B000000u, 0x7632)) - 8388608.0f;
-  v[4] = __uint_as_float(__byte_perm(p2, 0x4B000000u, 0x7610)) - 8388608.0f;
-}
-__device__ __forceinline__ void window5(const float* p, int s, float* v) {
-  const float4 a = __ldg(reinterpret_cast<const float4*>(p));
-  const float4 b = __ldg(reinterpret_cast<const float4*>(p + 4));
-  const bool e = (s >> 1) != 0, o = (s & 1) != 0;
-  const float r0 = e ? a.z : a.x, r1 = e ? a.w : a.y, r2 = e ? b.x : a.z, r3 = e ? b.y : a.w, r4 = e ? b.z : b.x,
-              r5 = e ? b.w : b.y;
-  v[0] = o ? r1 : r0;
-  v[1] = o ? r2 : r1;
-  v[2] = o ? r3 : r2;
-  v[3] = o ? r4 : r3;
-  v[4] = o ? r5 : r4;
-}
-
-// Edge version: v[k] = frame value at column ix + k of the row starting at `row`, zero outside the
-// row or when the whole tap row lies outside the volume (getZeroPadded, FrameWarper.h:39-47).
-template <typename FT>
-__device__ __forceinline__ void masked5(const FT* row, bool row_valid, int ix, int nx, float* v) {
+  // one voxel's reference and gradient values (element p & 3 of each quantity's four in the group)
+  template <int NDIM>
+  __device__ __forceinline__ void load1(long long p, float& t, float* g1) const {
+    const __nv_bfloat16* b = q + (p >> 2) * 16 + (p & 3);
+    t = __bfloat162float(__ldg(b));
 #pragma unroll
-  for (int k = 0; k < 5; k++) v[k] = (row_valid && (unsigned)(ix + k) < (unsigned)nx) ? ldf(row + ix + k) : 0.0f;
-}
+    for (int k = 0; k < NDIM; k++) g1[k] = __bfloat162float(__ldg(b + 4 * (k + 1)));
+  }
+};
 
 }  // namespace
 
@@ -203,185 +159,41 @@ __device__ __forceinline__ void uniform4(const FT* __restrict__ wp, long long pl
   }
 }
 
-// The sums one lane adds for its four voxels on the per-lane path.
-template <int NDIM>
-struct LaneSums {
-  float f;
-  float g[3][NDIM];
-};
-
-// Per-lane path of eval4_tile for the four voxels x0 .. x0+3 of one image row (row descriptor rd):
-// the lane decides for itself whether they share interval, range and tap offsets (then one window
-// per tap row), else samples voxel by voxel. Kept out of line: it runs for a small share of the
-// segments, and inlined its registers would be reserved for the whole tile loop.
+// Per-lane path of eval4_tile for the four voxels x0 .. x0+3 of one image row (row descriptor rd),
+// voxel by voxel: interval, fraction and range per voxel, eight zero-padded taps, and the J^T e
+// terms added straight into the tile's control-point sums ag (controls c0 .. c0+2). It runs for the
+// few segments that are not uniform, so it is written for few live registers rather than speed: the
+// whole pass is compiled to the register budget of its busiest point.
 template <int NDIM, typename FT, typename RT>
-__device__ __forceinline__ LaneSums<NDIM> lane_item(const FT* __restrict__ fr, long long plane, int pitch, bool padded,
-                                                    const RefGradSrc<RT> src, const RowDesc rd,
-                                                 int x0, int row_here, int nx, int ny, int nz, bool bidir, float dq,
-                                                 const float4* sD, int cw, int c0) {
-  LaneSums<NDIM> out;
-  float& af = out.f;
-  auto& ag = out.g;
-  af = 0.0f;
-#pragma unroll
-  for (int s = 0; s < 3; s++)
-#pragma unroll
-    for (int k = 0; k < NDIM; k++) ag[s][k] = 0.0f;
-  const int z = rd.z;
-  const int y = rd.y;
-  const bool flip = bidir && (y & 1);
-  const float fs = flip ? -dq : dq;
-  // ---- per-lane path: each lane classifies its own four voxels ----
+__device__ __forceinline__ void lane_item(const FT* __restrict__ fr, long long plane, int pitch,
+                                          const RefGradSrc<RT> src, const RowDesc rd, int x0, int row_here, int nx,
+                                          int ny, int nz, bool bidir, float dq, const float4* sD, int cw, int c0,
+                                          float& af, float* ag) {
+  const bool flip = bidir && (rd.y & 1);
   const long long p0 = (long long)row_here * nx + x0;
-  float t4[4], g4[NDIM][4];
-  src.template load<NDIM>(p0, t4, g4);
-
-  // Do the four voxels share interval, storage range and integer tap offsets, away from edges?
-  const int xs0 = flip ? nx - 1 - x0 : x0;
-  const int xs3 = flip ? xs0 - 3 : xs0 + 3;
-  const int di = rd.di0 + (xs0 >= rd.xdi ? 1 : 0);
-  const int di3 = rd.di0 + (xs3 >= rd.xdi ? 1 : 0);
-  const int r = bidir ? rd.r0 + (x0 >= rd.xr ? 1 : 0) : di;
-  const int r3 = bidir ? rd.r0 + (x0 + 3 >= rd.xr ? 1 : 0) : di3;
-  bool fast = (di == di3) && (r == r3) && (rd.xlast < x0 || rd.xlast > x0 + 3);
-  const float4* P = sD + min(max(di - cw, 0), kWin - 2) * kDParamF4;
-  const float f0 = fmaf((float)xs0, dq, rd.qbase) - (float)(di - rd.di0);
-  const float4 n = P[0], ph = P[1], dd = P[2];
-  const float t0x = fmaf(f0, dd.x, ph.x), t0y = fmaf(f0, dd.y, ph.y);
-  const float sx = fs * dd.x, sy = fs * dd.y;
-  const float flx = floorf(t0x), fly = floorf(t0y);
-  fast = fast && floorf(fmaf(3.0f, sx, t0x)) == flx && floorf(fmaf(3.0f, sy, t0y)) == fly;
-  const int ix = x0 + (int)n.x + (int)flx;
-  const int iy = y + (int)n.y + (int)fly;
-  // the whole aligned 8-element window of each tap row inside the row
-  bool inside = ix >= 0 && (ix & ~3) + 7 <= nx - 1 && iy >= 0 && iy + 1 <= ny - 1;
-  float t0z = 0.f, sz = 0.f, flz = 0.f;
-  int iz = 0;
-  if (NDIM == 3) {
-    t0z = fmaf(f0, dd.z, ph.z);
-    sz = fs * dd.z;
-    flz = floorf(t0z);
-    fast = fast && floorf(fmaf(3.0f, sz, t0z)) == flz;
-    iz = z + (int)n.z + (int)flz;
-    inside = inside && iz >= 0 && iz + 1 <= nz - 1;
-  }
-
-  float acc0[NDIM], acc1[NDIM];  // J^T e of controls r and r+1 for this lane's voxels
-#pragma unroll
-  for (int k = 0; k < NDIM; k++) acc0[k] = acc1[k] = 0.0f;
-
-  if (fast) {
-    float v[NDIM == 3 ? 4 : 2][5];
-    if (padded) {
-      // Clamp into the zero halo: a window that would lie wholly outside the volume along an
-      // axis reads halo zeros instead, exactly as the unclamped taps would read zero padding.
-      const int cx = min(max(ix, -kHaloX), nx + kHaloX - 5);
-      const int cy = min(max(iy, -kHaloY), ny + kHaloY - 2);
-      const int cz = NDIM == 3 ? min(max(iz, -kHaloZ), nz + kHaloZ - 2) : 0;
-      const int a = cx & ~3, s = cx - a;
-      const long long rb = (long long)cz * plane + (long long)cy * pitch + a;
-      window5(fr + rb, s, v[0]);
-      window5(fr + rb + pitch, s, v[1]);
-      if (NDIM == 3) {
-        window5(fr + rb + plane, s, v[NDIM == 3 ? 2 : 0]);
-        window5(fr + rb + plane + pitch, s, v[NDIM == 3 ? 3 : 1]);
-      }
-    } else if (inside) {
-      const int a = ix & ~3, s = ix & 3;
-      const long long rb = (long long)iz * plane + (long long)iy * pitch + a;
-      window5(fr + rb, s, v[0]);
-      window5(fr + rb + pitch, s, v[1]);
-      if (NDIM == 3) {
-        window5(fr + rb + plane, s, v[NDIM == 3 ? 2 : 0]);
-        window5(fr + rb + plane + pitch, s, v[NDIM == 3 ? 3 : 1]);
-      }
-    } else {
-      // tap rows (y, z), (y+1, z), (y, z+1), (y+1, z+1); rows outside the volume read zeros
-      const bool y0v = (unsigned)iy < (unsigned)ny, y1v = (unsigned)(iy + 1) < (unsigned)ny;
-      const bool z0v = NDIM == 2 || (unsigned)iz < (unsigned)nz;
-      const bool z1v = NDIM == 2 || (unsigned)(iz + 1) < (unsigned)nz;
-      const long long rb = (long long)iz * plane + (long long)iy * pitch;
-      masked5(fr + rb, y0v && z0v, ix, nx, v[0]);
-      masked5(fr + rb + pitch, y1v && z0v, ix, nx, v[1]);
-      if (NDIM == 3) {
-        masked5(fr + rb + plane, y0v && z1v, ix, nx, v[NDIM == 3 ? 2 : 0]);
-        masked5(fr + rb + plane + pitch, y1v && z1v, ix, nx, v[NDIM == 3 ? 3 : 1]);
-      }
-    }
-    const float wx0 = t0x - flx, wy0 = t0y - fly, wz0 = t0z - flz;
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const float wx = fmaf((float)j, sx, wx0), wy = fmaf((float)j, sy, wy0);
-      const float c00 = fmaf(wx, v[0][j + 1] - v[0][j], v[0][j]);
-      const float c01 = fmaf(wx, v[1][j + 1] - v[1][j], v[1][j]);
-      float val = fmaf(wy, c01 - c00, c00);
-      if (NDIM == 3) {
-        const float wz = fmaf((float)j, sz, wz0);
-        const float c10 = fmaf(wx, v[NDIM == 3 ? 2 : 0][j + 1] - v[NDIM == 3 ? 2 : 0][j], v[NDIM == 3 ? 2 : 0][j]);
-        const float c11 = fmaf(wx, v[NDIM == 3 ? 3 : 1][j + 1] - v[NDIM == 3 ? 3 : 1][j], v[NDIM == 3 ? 3 : 1][j]);
-        const float c1 = fmaf(wy, c11 - c10, c10);
-        val = fmaf(wz, c1 - val, val);
-      }
-      const float e = (val > 0.0f) ? val - t4[j] : 0.0f;
-      af = fmaf(e, e, af);
-      const float fj = fmaf((float)j, fs, f0);
-      const float e1 = e * fj;
-      const float e0 = e - e1;
+#pragma unroll 1
+  for (int j = 0; j < 4; j++) {
+    const int x = x0 + j;
+    const VoxelModel vm = voxel_model(rd, x, nx, flip, bidir, dq);
+    const int wi = min(max(vm.di - cw, 0), kWin - 2);
+    const float val = sample<NDIM, FT>(fr, plane, pitch, sD + wi * kDParamF4, vm.f, x, rd.y, rd.z, nx, ny, nz);
+    float t, g[NDIM];
+    src.template load1<NDIM>(p0 + j, t, g);
+    const float e = (val > 0.0f) ? val - t : 0.0f;
+    af = fmaf(e, e, af);
+    if (!vm.last) {
+      const float e1 = e * vm.f;
+      const float e0 = e * (1.0f - vm.f);
+      const bool first = vm.r == c0;  // controls c0, c0+1; else c0+1, c0+2
 #pragma unroll
       for (int k = 0; k < NDIM; k++) {
-        acc0[k] = fmaf(g4[k][j], e0, acc0[k]);
-        acc1[k] = fmaf(g4[k][j], e1, acc1[k]);
-      }
-    }
-  } else {
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const int x = x0 + j;
-      const VoxelModel vm = voxel_model(rd, x, nx, flip, bidir, dq);
-      const int wi = min(max(vm.di - cw, 0), kWin - 2);
-      const float val = sample<NDIM, FT>(fr, plane, pitch, sD + wi * kDParamF4, vm.f, x, y, z, nx, ny, nz);
-      const float e = (val > 0.0f) ? val - t4[j] : 0.0f;
-      af = fmaf(e, e, af);
-      if (!vm.last) {
-        const float e1 = e * vm.f;
-        const float e0 = e * (1.0f - vm.f);
-        if (vm.r == r) {
-#pragma unroll
-          for (int k = 0; k < NDIM; k++) {
-            acc0[k] = fmaf(g4[k][j], e0, acc0[k]);
-            acc1[k] = fmaf(g4[k][j], e1, acc1[k]);
-          }
-        } else {
-          // voxel in the following range: controls r+1 and r+2
-          const int s2 = vm.r - c0;
-#pragma unroll
-          for (int k = 0; k < NDIM; k++) {
-            if (s2 == 1) {
-              ag[1][k] = fmaf(g4[k][j], e0, ag[1][k]);
-              ag[2][k] = fmaf(g4[k][j], e1, ag[2][k]);
-            } else {
-              ag[0][k] = fmaf(g4[k][j], e0, ag[0][k]);
-              ag[1][k] = fmaf(g4[k][j], e1, ag[1][k]);
-            }
-          }
-        }
+        const float a0 = g[k] * e0, a1 = g[k] * e1;
+        ag[(0 * 3 + k) * 32] += first ? a0 : 0.0f;
+        ag[(1 * 3 + k) * 32] += first ? a1 : a0;
+        ag[(2 * 3 + k) * 32] += first ? 0.0f : a1;
       }
     }
   }
-  if (r == c0) {
-#pragma unroll
-    for (int k = 0; k < NDIM; k++) {
-      ag[0][k] += acc0[k];
-      ag[1][k] += acc1[k];
-    }
-  } else {
-#pragma unroll
-    for (int k = 0; k < NDIM; k++) {
-      ag[1][k] += acc0[k];
-      ag[2][k] += acc1[k];
-    }
-  }
-  return out;
 }
 
 // A row segment's parameters, computed by one lane for the whole warp (see eval4_tile).
@@ -415,7 +227,7 @@ constexpr int kSegLen = 128 * kSegGroups;
 // per-lane path (lane_item), which handles every case voxel by voxel where needed.
 template <int NDIM, typename FT, typename RT>
 __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, const int tile, float4* sD,
-                                           SegParams* sp, const float4* __restrict__ dparams,
+                                           SegParams* sp, float* sg, const float4* __restrict__ dparams,
                                            double* __restrict__ partials) {
   const int nx = R.nx, ny = R.ny, nz = R.nz;
   const int row_begin = tile * R.tile_rows;
@@ -437,11 +249,11 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
   const RefGradSrc<RT> src(R);
 
   float af = 0.0f;
-  float ag[3][NDIM];
+  // the lane's J^T e sums of controls c0 .. c0+2, entry (s * 3 + k) * 32 (shared memory: they change
+  // only when a range ends and on the per-lane path)
+  float* ag = sg + lane;
 #pragma unroll
-  for (int s = 0; s < 3; s++)
-#pragma unroll
-    for (int k = 0; k < NDIM; k++) ag[s][k] = 0.0f;
+  for (int i = 0; i < 9; i++) ag[i * 32] = 0.0f;
   // running J^T e sums of uniform segments, for controls ur and ur + 1 (ur: their storage range)
   float ua0[NDIM], ua1[NDIM];
 #pragma unroll
@@ -451,14 +263,14 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
     if (ur == c0) {
 #pragma unroll
       for (int k = 0; k < NDIM; k++) {
-        ag[0][k] += ua0[k];
-        ag[1][k] += ua1[k];
+        ag[(0 * 3 + k) * 32] += ua0[k];
+        ag[(1 * 3 + k) * 32] += ua1[k];
       }
     } else if (ur >= 0) {
 #pragma unroll
       for (int k = 0; k < NDIM; k++) {
-        ag[1][k] += ua0[k];
-        ag[2][k] += ua1[k];
+        ag[(1 * 3 + k) * 32] += ua0[k];
+        ag[(2 * 3 + k) * 32] += ua1[k];
       }
     }
 #pragma unroll
@@ -586,13 +398,8 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
         const int x0 = sp[q].xa + gi * 128 + lane * 4;
         if (x0 < nx) {
           const int row = sp[q].row;
-          const LaneSums<NDIM> ls = lane_item<NDIM, FT, RT>(fr, plane, pitch, padded, src, R.rows[row], x0, row, nx,
-                                                           ny, nz, bidir, dq, sD, cw, c0);
-          af += ls.f;
-#pragma unroll
-          for (int s2 = 0; s2 < 3; s2++)
-#pragma unroll
-            for (int k = 0; k < NDIM; k++) ag[s2][k] += ls.g[s2][k];
+          lane_item<NDIM, FT, RT>(fr, plane, pitch, src, R.rows[row], x0, row, nx, ny, nz, bidir, dq, sD, cw, c0, af,
+                                  ag);
         }
       }
       // Explicit reconvergence point: the per-lane branches above must not leave the warp split
@@ -602,14 +409,19 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
     __syncwarp();  // every lane is done reading this batch's parameters
   }
   flush_uniform();
-
+  float g9[3][NDIM];
+#pragma unroll
+  for (int s = 0; s < 3; s++)
+#pragma unroll
+    for (int k = 0; k < NDIM; k++) g9[s][k] = ag[(s * 3 + k) * 32];
+  __syncwarp();  // sg is free for the next tile
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     af += __shfl_xor_sync(0xffffffffu, af, o);
 #pragma unroll
     for (int s = 0; s < 3; s++)
 #pragma unroll
-      for (int k = 0; k < NDIM; k++) ag[s][k] += __shfl_xor_sync(0xffffffffu, ag[s][k], o);
+      for (int k = 0; k < NDIM; k++) g9[s][k] += __shfl_xor_sync(0xffffffffu, g9[s][k], o);
   }
   // Lane i < 11 writes entry i of the tile's partial sums [f, c0, g(3 x 3)] (every lane holds the
   // totals; the value is picked with selects so that the warp does not branch).
@@ -617,7 +429,7 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
 #pragma unroll
   for (int s = 0; s < 3; s++)
 #pragma unroll
-    for (int k = 0; k < 3; k++) pick = (lane == 2 + s * 3 + k) ? (k < NDIM ? ag[s][k < NDIM ? k : 0] : 0.0f) : pick;
+    for (int k = 0; k < 3; k++) pick = (lane == 2 + s * 3 + k) ? (k < NDIM ? g9[s][k < NDIM ? k : 0] : 0.0f) : pick;
   double* out = partials + (long long)tile * kPartialDoubles;
   if (lane < 11) out[lane] = lane == 1 ? (double)c0 : (double)pick;
   __syncwarp();
@@ -628,13 +440,14 @@ template <int NDIM, typename FT, typename RT, int MB>
 __global__ void __launch_bounds__(kEvalThreads, MB) eval4_kernel(const Job* __restrict__ jobs) {
   __shared__ float4 sD[kEvalWarps][kWin * kDParamF4];
   __shared__ SegParams sp[kEvalWarps][kSegBatch];
+  __shared__ float sg[kEvalWarps][9 * 32];
   const Job& job = jobs[blockIdx.y];
   if (job.state != nullptr && (job.state->phase == kPhaseDone || job.state->phase == kPhaseWaitWarm)) return;
   const RefDev& R = *job.ref;
   const int warp = threadIdx.x >> 5;
   const int tile = blockIdx.x * kEvalWarps + warp;
   if (tile >= R.n_tiles) return;
-  eval4_tile<NDIM, FT, RT>(job, R, tile, sD[warp], sp[warp], job.dparams, job.partials);
+  eval4_tile<NDIM, FT, RT>(job, R, tile, sD[warp], sp[warp], sg[warp], job.dparams, job.partials);
 }
 
 // Persistent form for batched solves: the grid's warps walk the (active frame, tile) items of the
@@ -648,6 +461,7 @@ __global__ void __launch_bounds__(kEvalThreads, MB) eval4_active_kernel(const Jo
                                                                      const int* __restrict__ tile_prefix) {
   __shared__ float4 sD[kEvalWarps][kWin * kDParamF4];
   __shared__ SegParams sp[kEvalWarps][kSegBatch];
+  __shared__ float sg[kEvalWarps][9 * 32];
   const int na = *n_active;
   const int n_items = tile_prefix[na];
   const int warp = threadIdx.x >> 5;
@@ -668,7 +482,7 @@ __global__ void __launch_bounds__(kEvalThreads, MB) eval4_active_kernel(const Jo
     // a frame in the paired start phase has two items per tile: the zero start, then the rigid one
     const bool second = tile >= R.n_tiles;
     if (second) tile -= R.n_tiles;
-    eval4_tile<NDIM, FT, RT>(job, R, tile, sD[warp], sp[warp], second ? job.dparams2 : job.dparams,
+    eval4_tile<NDIM, FT, RT>(job, R, tile, sD[warp], sp[warp], sg[warp], second ? job.dparams2 : job.dparams,
                              second ? job.partials2 : job.partials);
   }
 }

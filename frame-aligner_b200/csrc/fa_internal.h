@@ -90,8 +90,9 @@ struct RefDev {
   int tile_rows;
   int n_tiles;
   int P;
-  int tune_mb;         // fused pass: CTAs per SM the register budget is sized for (2, 3 or 4)
+  int tune_mb;         // fused pass: CTAs per SM the register budget is sized for (2, 3 or 4), launches of many frames
   int tune_grid_mult;  // persistent fused pass: CTAs per SM launched
+  int tune_mb_small;   // the same for launches of one or a few frames (single-frame, static-scratch, serving)
   const RowDesc* rows;
   const int* tile_c0;      // per tile: storage range index of its first voxel
   const int2* ctrl_tiles;  // per control point: tiles [x, y) whose partial slots may hold it

@@ -127,7 +127,7 @@ extern "C" fa_status fa_get_error_jacobian_static(const fa_reference* ref, const
   const bool vec4 = host->nx % 4 == 0 && (reinterpret_cast<uintptr_t>(frame_device) & 15u) == 0;
   if (e == cudaSuccess)
     e = fa::launch_eval(jd, 1, host->n_tiles, n_dim, dtype == FA_F16 ? fa::kFrameF16 : fa::kFrameF32, mixed, 0, vec4,
-                        host->tune_mb);
+                        host->tune_mb_small);
   if (e == cudaSuccess) e = fa::launch_reduce(jd, *host, 0);
   if (e == cudaSuccess) e = cudaMemcpy(f, job.result, sizeof(double), cudaMemcpyDeviceToHost);
   if (e == cudaSuccess) e = cudaMemcpy(jac, job.result + 1, (size_t)P * sizeof(double), cudaMemcpyDeviceToHost);

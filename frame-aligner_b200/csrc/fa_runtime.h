@@ -178,8 +178,9 @@ struct fa_aligner {
   size_t staging_bytes = 0;
   float* vols = nullptr;       // downsampled frames for the correlator (spatial_binning > 1)
   size_t vols_count = 0;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_corr = nullptr;
   double last_ms = 0;
+  double last_corr_ms = 0;  // of last_ms: until the last frame's conversion and phase correlation
   // host frames: uploads on their own stream, one event per chunk of frames
   cudaStream_t copy_stream = nullptr;
   std::vector<cudaEvent_t> copy_ev;

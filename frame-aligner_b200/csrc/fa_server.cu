@@ -275,10 +275,10 @@ fa_status attach(fa_server* S, SrvAcq* q) {
   C->acqs.push_back(q);
   C->max_nD = std::max(C->max_nD, R->nD);
   C->max_tiles = std::max(C->max_tiles, R->G.n_tiles);
-  if (R->N > C->tuned_for) {  // the largest volume's autotuned register budget and grid
+  if (R->N > C->tuned_for) {  // the largest volume's register budget tuned for launches of a few frames
     C->tuned_for = R->N;
-    C->mb = R->host.tune_mb;
-    C->grid_mult = R->host.tune_grid_mult;
+    C->mb = R->host.tune_mb_small;
+    C->grid_mult = R->host.tune_mb_small;
   }
   C->dirty = true;
   return FA_OK;

@@ -177,6 +177,7 @@ SIGNATURES = {
     "fa_get_error_jacobian_static": [_vp, _vp, C.c_int, _f64p, C.POINTER(C.c_double), _f64p],
     "fa_kernel_launches": [],
     "fa_aligner_last_device_ms": [_vp, C.POINTER(C.c_double)],
+    "fa_aligner_last_phase_ms": [_vp, C.POINTER(C.c_double), C.POINTER(C.c_double)],
     "fa_profile_eval": [_vp, C.c_int, _f64p, C.c_int, C.POINTER(C.c_double)],
     "fa_test_tr_subproblem": [_vp, C.c_int, C.c_int, _f64p, _f64p, C.c_double, _f64p, C.POINTER(C.c_int)],
     "fa_test_correlation_surface": [_vp, _f32p, C.c_int, _f64p],
@@ -473,6 +474,12 @@ class Aligner:
         ms = C.c_double()
         check(lib().fa_aligner_last_device_ms(self._h, C.byref(ms)))
         return ms.value
+
+    def last_phase_ms(self):
+        """(correlation ms, total ms) of the last add_frames call (fa_aligner_last_phase_ms)."""
+        c, t = C.c_double(), C.c_double()
+        check(lib().fa_aligner_last_phase_ms(self._h, C.byref(c), C.byref(t)))
+        return c.value, t.value
 
     def reference_gradient(self):
         """The Sobel gradient of the aligner's warper reference (its smoothed reference + 1)."""

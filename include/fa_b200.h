@@ -361,6 +361,10 @@ fa_status fa_get_error_jacobian_static(const fa_reference* ref, const void* fram
 long long fa_kernel_launches(void);
 /* Device time (CUDA events on the library's streams) of the last fa_aligner_add_frames* call, ms. */
 fa_status fa_aligner_last_device_ms(const fa_aligner* a, double* ms);
+/* The same call split: correlate_ms = device time from the call's start until every frame was
+   converted and phase-correlated (uploads, conversion, window, transforms, peak), total_ms = all of
+   it (the solve of the first frames overlaps the correlation of the later ones). */
+fa_status fa_aligner_last_phase_ms(const fa_aligner* a, double* correlate_ms, double* total_ms);
 /* Times the fused warp + error + J^T e pass alone: `launches` back-to-back launches over n
    registered frames (of one reference) at displacement D (nD*3 doubles, host memory), bracketed by
    CUDA events on the launching stream. ms_per_launch receives the average duration. */
