@@ -60,8 +60,9 @@ def parse():
     ap.add_argument("--large-pool", type=int, default=2)
     ap.add_argument("--large-cpu", type=int, default=1, help="frames of the large volume solved on the CPU")
     ap.add_argument("--uneven-pool", type=int, default=4, help="distinct frames per size in the uneven batch")
-    ap.add_argument("--only", choices=["roofline"], default=None,
-                    help="roofline: only the fused-pass probe on --frames FP16 frames (for ncu captures)")
+    ap.add_argument("--only", choices=["roofline", "aligner"], default=None,
+                    help="roofline: only the fused-pass probe on --frames FP16 frames; aligner: one aligner call "
+                         "on --frames raw uint16 frames in HBM (both for ncu captures)")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="length of the Poisson arrival stream")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="total arrivals per second")
     ap.add_argument("--serve-pool", type=int, default=6, help="distinct frames per served acquisition")
@@ -516,11 +517,37 @@ def run_roofline_probe(args, local):
     return 0
 
 
+def run_aligner_probe(args, local):
+    """One aligner call alone: the mixed-precision aligner of the headline workload on args.frames raw
+    uint16 frames already in HBM (phase correlation, conversion and batched solve), after one
+    untimed call (the command the correlator captures in profiles/ run)."""
+    import torch
+
+    import fa_b200 as fa
+
+    acq = make_data(args.frames, 0)
+    nz, ny, nx = acq.reference.shape
+    line, il, ifr = acq.scan
+    ctx = fa.Context(device=local, autotune=True)
+    al = fa.Aligner(ctx, nD=acq.nD, precision=fa.PREC_MIXED, max_iterations=100)
+    al.set_reference(acq.reference, fa.scan_params(line, il, ifr, nx, ny, nz))
+    dev = torch.from_numpy(np.ascontiguousarray(acq.frames.astype(np.uint16)).view(np.int16)).to(f"cuda:{local}")
+    ptrs = [dev[k].data_ptr() for k in range(args.frames)]
+    al.add_frames_device(ptrs, fa.U16, args.frames)
+    al.add_frames_device(ptrs, fa.U16, args.frames)
+    corr_ms, total_ms = al.last_phase_ms()
+    print(json.dumps({"probe": "aligner", "frames": args.frames, "ms": total_ms, "ms_until_last_peak": corr_ms}))
+    al.close()
+    return 0
+
+
 def run_ours(args, rank, world, local):
     import fa_b200 as fa
 
     if args.only == "roofline":
         return run_roofline_probe(args, local)
+    if args.only == "aligner":
+        return run_aligner_probe(args, local)
 
     pg = None
     if world > 1:
