@@ -21,15 +21,6 @@ namespace fa {
 
 namespace {
 
-// Four consecutive FP32 reference / gradient values starting at a multiple of 4.
-__device__ __forceinline__ void load4(const float* p, float* v) {
-  const float4 a = __ldg(reinterpret_cast<const float4*>(p));
-  v[0] = a.x;
-  v[1] = a.y;
-  v[2] = a.z;
-  v[3] = a.w;
-}
-
 // The reference and gradient values of four consecutive voxels starting at a multiple of 4: four
 // FP32 planes, or the BF16 groups of RefDev::q16 (two 16-byte loads for all four quantities).
 template <typename RT>
@@ -39,11 +30,29 @@ struct RefGradSrc<float> {
   const float* r;
   const float* g[3];
   __device__ explicit RefGradSrc(const RefDev& R) : r(R.ref32), g{R.gx32, R.gy32, R.gz32} {}
+  // the loads (issued early), then the values
+  struct Raw {
+    float4 t, g[3];
+  };
   template <int NDIM>
-  __device__ __forceinline__ void load(long long p0, float* t4, float (*g4)[4]) const {
-    load4(r + p0, t4);
+  __device__ __forceinline__ Raw load_raw(long long p0) const {
+    Raw w;
+    w.t = __ldg(reinterpret_cast<const float4*>(r + p0));
 #pragma unroll
-    for (int k = 0; k < NDIM; k++) load4(g[k] + p0, g4[k]);
+    for (int k = 0; k < NDIM; k++) w.g[k] = __ldg(reinterpret_cast<const float4*>(g[k] + p0));
+    return w;
+  }
+  template <int NDIM>
+  __device__ __forceinline__ static void unpack(const Raw& w, float* t4, float (*g4)[4]) {
+    auto put = [](float4 a, float* v) {
+      v[0] = a.x;
+      v[1] = a.y;
+      v[2] = a.z;
+      v[3] = a.w;
+    };
+    put(w.t, t4);
+#pragma unroll
+    for (int k = 0; k < NDIM; k++) put(w.g[k], g4[k]);
   }
   // one voxel's reference and gradient values
   template <int NDIM>
@@ -57,20 +66,27 @@ template <>
 struct RefGradSrc<__nv_bfloat16> {
   const __nv_bfloat16* q;
   __device__ explicit RefGradSrc(const RefDev& R) : q(R.q16) {}
+  // the loads (issued early), then the values
+  struct Raw {
+    uint4 a, c;
+  };
   template <int NDIM>
-  __device__ __forceinline__ void load(long long p0, float* t4, float (*g4)[4]) const {
+  __device__ __forceinline__ Raw load_raw(long long p0) const {
     const uint4* b = reinterpret_cast<const uint4*>(q + (p0 >> 2) * 16);
-    const uint4 a = __ldg(b), c = __ldg(b + 1);
-    auto unpack = [](unsigned lo, unsigned hi, float* v) {
+    return Raw{__ldg(b), __ldg(b + 1)};
+  }
+  template <int NDIM>
+  __device__ __forceinline__ static void unpack(const Raw& w, float* t4, float (*g4)[4]) {
+    auto put = [](unsigned lo, unsigned hi, float* v) {
       v[0] = __uint_as_float(lo << 16);
       v[1] = __uint_as_float(lo & 0xffff0000u);
       v[2] = __uint_as_float(hi << 16);
       v[3] = __uint_as_float(hi & 0xffff0000u);
     };
-    unpack(a.x, a.y, t4);
-    unpack(a.z, a.w, g4[0]);
-    unpack(c.x, c.y, g4[1]);
-    if (NDIM == 3) unpack(c.z, c.w, g4[NDIM == 3 ? 2 : 0]);
+    put(w.a.x, w.a.y, t4);
+    put(w.a.z, w.a.w, g4[0]);
+    put(w.c.x, w.c.y, g4[1]);
+    if (NDIM == 3) put(w.c.z, w.c.w, g4[NDIM == 3 ? 2 : 0]);
   }
   // one voxel's reference and gradient values (element p & 3 of each quantity's four in the group)
   template <int NDIM>
@@ -84,13 +100,30 @@ struct RefGradSrc<__nv_bfloat16> {
 
 }  // namespace
 
-// Frame values v[k] = p[S + k], k = 0..4, from the aligned 8-element window at p, for an alignment
-// S that is the same for every lane of the warp (known at compile time: no shifts or selects).
+// The raw words of one lane's aligned 8-element frame window of one tap row (16 bytes for 16-bit
+// samples, 32 for FP32), loaded before they are decoded so that a segment's loads can be issued
+// while the previous segment is computed.
+template <typename FT>
+struct WinRaw {
+  uint2 lo, hi;
+};
+template <>
+struct WinRaw<float> {
+  float4 lo, hi;
+};
+template <typename FT>
+__device__ __forceinline__ WinRaw<FT> load_win(const FT* p) {
+  if constexpr (std::is_same<FT, float>::value)
+    return WinRaw<FT>{__ldg(reinterpret_cast<const float4*>(p)), __ldg(reinterpret_cast<const float4*>(p + 4))};
+  else
+    return WinRaw<FT>{__ldg(reinterpret_cast<const uint2*>(p)), __ldg(reinterpret_cast<const uint2*>(p + 4))};
+}
+
+// Frame values v[k] = window[S + k], k = 0..4, for an alignment S that is the same for every lane of
+// the warp (known at compile time: no shifts or selects).
 template <int S>
-__device__ __forceinline__ void window5s(const RawU16* p, float* v) {
-  const uint2 lo = __ldg(reinterpret_cast<const uint2*>(p));
-  const uint2 hi = __ldg(reinterpret_cast<const uint2*>(p + 4));
-  const unsigned w[4] = {lo.x, lo.y, hi.x, hi.y};
+__device__ __forceinline__ void window5s(const WinRaw<RawU16>& r, float* v) {
+  const unsigned w[4] = {r.lo.x, r.lo.y, r.hi.x, r.hi.y};
 #pragma unroll
   for (int k = 0; k < 5; k++) {
     const int e = S + k;
@@ -98,10 +131,8 @@ __device__ __forceinline__ void window5s(const RawU16* p, float* v) {
   }
 }
 template <int S>
-__device__ __forceinline__ void window5s(const __half* p, float* v) {
-  const uint2 lo = __ldg(reinterpret_cast<const uint2*>(p));
-  const uint2 hi = __ldg(reinterpret_cast<const uint2*>(p + 4));
-  const unsigned w[4] = {lo.x, lo.y, hi.x, hi.y};
+__device__ __forceinline__ void window5s(const WinRaw<__half>& r, float* v) {
+  const unsigned w[4] = {r.lo.x, r.lo.y, r.hi.x, r.hi.y};
 #pragma unroll
   for (int k = 0; k < 5; k++) {
     const int e = S + k;
@@ -110,28 +141,30 @@ __device__ __forceinline__ void window5s(const __half* p, float* v) {
   }
 }
 template <int S>
-__device__ __forceinline__ void window5s(const float* p, float* v) {
-  const float4 a = __ldg(reinterpret_cast<const float4*>(p));
-  const float4 b = __ldg(reinterpret_cast<const float4*>(p + 4));
-  const float w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+__device__ __forceinline__ void window5s(const WinRaw<float>& r, float* v) {
+  const float w[8] = {r.lo.x, r.lo.y, r.lo.z, r.lo.w, r.hi.x, r.hi.y, r.hi.z, r.hi.w};
 #pragma unroll
   for (int k = 0; k < 5; k++) v[k] = w[S + k];
 }
 
-// Four voxels of a lane in a uniform row segment (see eval4_tile): the lane's window of each tap row
-// starts at wp (+ pitch for row y+1, + plane for plane z+1); weights of voxel j are w + j * s per
-// axis, its control-point fraction fl + j * fs.
+// Everything one lane loads for its four voxels of a uniform segment: the reference / gradient
+// group and the windows of the tap rows (y, z), (y+1, z), (y, z+1), (y+1, z+1).
+template <int NDIM, typename FT, typename RT>
+struct SegLoad {
+  typename RefGradSrc<RT>::Raw rg;
+  WinRaw<FT> w[NDIM == 3 ? 4 : 2];
+};
+
+// Four voxels of a lane in a uniform row segment (see eval4_tile), from the raw windows of its tap
+// rows (y, z), (y+1, z), (y, z+1), (y+1, z+1); weights of voxel j are w + j * s per axis, its
+// control-point fraction fl + j * fs.
 template <int NDIM, int S, typename FT>
-__device__ __forceinline__ void uniform4(const FT* __restrict__ wp, long long plane, int pitch, const float* t4,
-                                         const float (*g4)[4], float wxl, float sx, float wyl, float sy, float wzl,
-                                         float sz, float fl, float fs, float& af, float* acc0, float* acc1) {
+__device__ __forceinline__ void uniform4(const WinRaw<FT>* win, const float* t4, const float (*g4)[4], float wxl,
+                                         float sx, float wyl, float sy, float wzl, float sz, float fl, float fs,
+                                         float& af, float* acc0, float* acc1) {
   float v[NDIM == 3 ? 4 : 2][5];
-  window5s<S>(wp, v[0]);
-  window5s<S>(wp + pitch, v[1]);
-  if (NDIM == 3) {
-    window5s<S>(wp + plane, v[NDIM == 3 ? 2 : 0]);
-    window5s<S>(wp + plane + pitch, v[NDIM == 3 ? 3 : 1]);
-  }
+#pragma unroll
+  for (int r = 0; r < (NDIM == 3 ? 4 : 2); r++) window5s<S>(win[r], v[r]);
 #pragma unroll
   for (int j = 0; j < 4; j++) {
     const float wx = j ? fmaf((float)j, sx, wxl) : wxl;
@@ -207,15 +240,13 @@ struct SegParams {
   int row;                  // image row (z * ny + y)
 };
 constexpr int kSegBatch = 32;  // segments classified per round, one per lane
-// A segment is kSegGroups groups of 128 voxels; each lane takes four voxels of every group.
-constexpr int kSegGroups = 1;
-constexpr int kSegLen = 128 * kSegGroups;
+constexpr int kSegLen = 128;   // voxels per segment: four per lane
 
 // One tile of one frame, processed by one warp on its own: its control-point window sD (the warp's
 // slice of shared memory), its row segments, and its partial sums. No CTA barrier is involved, so
 // the warps of a CTA drift apart and hide each other's load latency.
 //
-// A row segment is kSegLen consecutive voxels of an image row, four per lane and 128-voxel group.
+// A row segment is kSegLen consecutive voxels of an image row, four per lane.
 // Almost every segment is uniform: its voxels share one displacement interval and one storage range,
 // contain no range end, and their sample positions x + d(x) share one integer offset per axis,
 // because the displacement changes by ~1e-5 px per voxel along a row. Whether it is, and its weights, slopes and window
@@ -225,7 +256,12 @@ constexpr int kSegLen = 128 * kSegGroups;
 // frame windows share one compile-time alignment, and its J^T e terms go to one pair of running sums
 // that are added to the tile's control points only when the range changes. Other segments take the
 // per-lane path (lane_item), which handles every case voxel by voxel where needed.
-template <int NDIM, typename FT, typename RT>
+//
+// PIPE: the uniform walk is software-pipelined, the loads of the next uniform segment issued before
+// the current one is computed (two segments' loads live at once: only with 16-bit storage and the
+// largest register budget, 2 CTAs per SM); without it each segment's loads are followed by its
+// arithmetic.
+template <int NDIM, typename FT, typename RT, bool PIPE>
 __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, const int tile, float4* sD,
                                            SegParams* sp, float* sg, const float4* __restrict__ dparams,
                                            double* __restrict__ partials) {
@@ -348,59 +384,104 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
       sp[lane] = q;
     }
     __syncwarp();
-    // ---- walk them ----
+    // ---- walk the uniform ones, in order ----
     const int cnt = min(kSegBatch, n_items - base);
-    for (int q = 0; q < cnt; q++) {
-      const SegParams P = sp[q];
-      const int xa = P.xa;
-      if (P.meta & 1) {
-        const int ra = P.meta >> 3;
-        if (ra != ur) {
-          flush_uniform();
-          ur = ra;
-        }
-#pragma unroll
-        for (int gi = 0; gi < kSegGroups; gi++) {
-          const int x0 = xa + gi * 128 + lane * 4;
-          if (x0 < nx) {
-            float t4[4], g4[NDIM][4];
-            src.template load<NDIM>(P.p0 + gi * 128 + lane * 4, t4, g4);
-            const FT* wp = fr + (P.win + gi * 128 + lane * 4);
-            const float u = lane_u + (float)(gi * 128);
-            const float wxl = fmaf(u, P.sx, P.w0x);
-            const float wyl = fmaf(u, P.sy, P.w0y);
-            const float wzl = NDIM == 3 ? fmaf(u, P.sz, P.w0z) : 0.0f;
-            const float fl = fmaf(u, P.fs, P.f0);
-            switch ((P.meta >> 1) & 3) {
-              case 0:
-                uniform4<NDIM, 0>(wp, plane, pitch, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
-                break;
-              case 1:
-                uniform4<NDIM, 1>(wp, plane, pitch, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
-                break;
-              case 2:
-                uniform4<NDIM, 2>(wp, plane, pitch, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
-                break;
-              default:
-                uniform4<NDIM, 3>(wp, plane, pitch, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
-                break;
-            }
-          }
+    unsigned umask = __ballot_sync(0xffffffffu, lane < cnt && (sp[lane].meta & 1) != 0);
+    // the loads of one lane for segment P (lanes past the row end load nothing)
+    auto seg_load = [&](const SegParams& P, SegLoad<NDIM, FT, RT>& L) {
+      if (P.xa + lane * 4 < nx) {
+        L.rg = src.template load_raw<NDIM>(P.p0 + lane * 4);
+        const FT* wp = fr + (P.win + lane * 4);
+        L.w[0] = load_win(wp);
+        L.w[1] = load_win(wp + pitch);
+        if (NDIM == 3) {
+          L.w[NDIM == 3 ? 2 : 0] = load_win(wp + plane);
+          L.w[NDIM == 3 ? 3 : 1] = load_win(wp + plane + pitch);
         }
       }
+    };
+    // a segment's range: the running sums are flushed when it changes
+    auto seg_range = [&](const SegParams& P) {
+      const int ra = P.meta >> 3;
+      if (ra != ur) {
+        flush_uniform();
+        ur = ra;
+      }
+    };
+    // the arithmetic of segment P on loaded values (lanes inside the row)
+    auto seg_math = [&](const SegParams& P, const SegLoad<NDIM, FT, RT>& L) {
+      {
+        float t4[4], g4[NDIM][4];
+        RefGradSrc<RT>::template unpack<NDIM>(L.rg, t4, g4);
+        const float wxl = fmaf(lane_u, P.sx, P.w0x);
+        const float wyl = fmaf(lane_u, P.sy, P.w0y);
+        const float wzl = NDIM == 3 ? fmaf(lane_u, P.sz, P.w0z) : 0.0f;
+        const float fl = fmaf(lane_u, P.fs, P.f0);
+        switch ((P.meta >> 1) & 3) {
+          case 0:
+            uniform4<NDIM, 0, FT>(L.w, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
+            break;
+          case 1:
+            uniform4<NDIM, 1, FT>(L.w, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
+            break;
+          case 2:
+            uniform4<NDIM, 2, FT>(L.w, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
+            break;
+          default:
+            uniform4<NDIM, 3, FT>(L.w, t4, g4, wxl, P.sx, wyl, P.sy, wzl, P.sz, fl, P.fs, af, ua0, ua1);
+            break;
+        }
+      }
+    };
+    auto seg_compute = [&](const SegParams& P, const SegLoad<NDIM, FT, RT>& L) {
+      seg_range(P);
+      if (P.xa + lane * 4 < nx) seg_math(P, L);
       __syncwarp();  // lanes past the row end rejoin here
+    };
+    // next uniform segment of the batch (-1: none), taken off the mask
+    auto next_uniform = [&]() {
+      if (umask == 0u) return -1;
+      const int q = __ffs(umask) - 1;
+      umask &= umask - 1u;
+      return q;
+    };
+    if constexpr (PIPE) {
+      // two load buffers, alternating: A holds segment q while B receives the one after it
+      SegLoad<NDIM, FT, RT> A, B;
+      int q = next_uniform();
+      if (q >= 0) seg_load(sp[q], A);
+      while (q >= 0) {
+        int qn = next_uniform();
+        if (qn >= 0) seg_load(sp[qn], B);
+        seg_compute(sp[q], A);
+        q = qn;
+        if (q < 0) break;
+        qn = next_uniform();
+        if (qn >= 0) seg_load(sp[qn], A);
+        seg_compute(sp[q], B);
+        q = qn;
+      }
+    } else {
+      for (int q = next_uniform(); q >= 0; q = next_uniform()) {
+        const SegParams& P = sp[q];
+        seg_range(P);
+        if (P.xa + lane * 4 < nx) {
+          SegLoad<NDIM, FT, RT> L;
+          seg_load(P, L);
+          seg_math(P, L);
+        }
+        __syncwarp();  // lanes past the row end rejoin here
+      }
     }
     // the batch's other segments, lane by lane (after the uniform walk, so that its registers are
     // free for the per-lane path)
     for (int q = 0; q < cnt; q++) {
       if (sp[q].meta & 1) continue;
-      for (int gi = 0; gi < kSegGroups; gi++) {
-        const int x0 = sp[q].xa + gi * 128 + lane * 4;
-        if (x0 < nx) {
-          const int row = sp[q].row;
-          lane_item<NDIM, FT, RT>(fr, plane, pitch, src, R.rows[row], x0, row, nx, ny, nz, bidir, dq, sD, cw, c0, af,
-                                  ag);
-        }
+      const int x0 = sp[q].xa + lane * 4;
+      if (x0 < nx) {
+        const int row = sp[q].row;
+        lane_item<NDIM, FT, RT>(fr, plane, pitch, src, R.rows[row], x0, row, nx, ny, nz, bidir, dq, sD, cw, c0, af,
+                                ag);
       }
       // Explicit reconvergence point: the per-lane branches above must not leave the warp split
       // into groups that then run the rest of the loop one after the other.
@@ -435,6 +516,10 @@ __device__ __forceinline__ void eval4_tile(const Job& job, const RefDev& R, cons
   __syncwarp();
 }
 
+// Whether eval4_tile pipelines its uniform walk for this storage and register budget.
+template <typename FT, typename RT, int MB>
+constexpr bool kPipe = MB == 2 && sizeof(FT) == 2 && sizeof(RT) == 2;
+
 // One grid per launch: CTA x of job y covers tiles 8x .. 8x+7, one per warp.
 template <int NDIM, typename FT, typename RT, int MB>
 __global__ void __launch_bounds__(kEvalThreads, MB) eval4_kernel(const Job* __restrict__ jobs) {
@@ -447,7 +532,7 @@ __global__ void __launch_bounds__(kEvalThreads, MB) eval4_kernel(const Job* __re
   const int warp = threadIdx.x >> 5;
   const int tile = blockIdx.x * kEvalWarps + warp;
   if (tile >= R.n_tiles) return;
-  eval4_tile<NDIM, FT, RT>(job, R, tile, sD[warp], sp[warp], sg[warp], job.dparams, job.partials);
+  eval4_tile<NDIM, FT, RT, kPipe<FT, RT, MB>>(job, R, tile, sD[warp], sp[warp], sg[warp], job.dparams, job.partials);
 }
 
 // Persistent form for batched solves: the grid's warps walk the (active frame, tile) items of the
@@ -482,7 +567,7 @@ __global__ void __launch_bounds__(kEvalThreads, MB) eval4_active_kernel(const Jo
     // a frame in the paired start phase has two items per tile: the zero start, then the rigid one
     const bool second = tile >= R.n_tiles;
     if (second) tile -= R.n_tiles;
-    eval4_tile<NDIM, FT, RT>(job, R, tile, sD[warp], sp[warp], sg[warp], second ? job.dparams2 : job.dparams,
+    eval4_tile<NDIM, FT, RT, kPipe<FT, RT, MB>>(job, R, tile, sD[warp], sp[warp], sg[warp], second ? job.dparams2 : job.dparams,
                              second ? job.partials2 : job.partials);
   }
 }
