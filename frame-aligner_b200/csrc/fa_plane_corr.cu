@@ -26,6 +26,7 @@
 // column reads across lines); the z DFT (<= 16 points) runs in registers, one (kx, y) column per
 // thread. Twiddles W_L^m = exp(-2 pi i m / L) come from tables rounded from long double on the host.
 // The inverse transforms are unnormalised (a positive scale does not move the maximum).
+#include <cooperative_groups.h>
 #include <float.h>
 
 #include <algorithm>
@@ -425,6 +426,91 @@ __global__ void __launch_bounds__(kPlaneThreads, 1) plane_yz_kernel(const double
   }
 }
 
+// The same pass for planes of exactly 8192 points (nz in {4, 8, 16}), one plane per pair of CTAs
+// (a 2-CTA cluster), so that each CTA needs half the shared memory and two fit per SM. CTA r holds
+// the z lines [r NZ/2, (r + 1) NZ/2) and runs their y DFTs; after a cluster barrier it takes the z
+// columns y in [r ny/2, (r + 1) ny/2), reading the other CTA's half of each column from that CTA's
+// shared memory (distributed shared memory) and writing it back there; after a second barrier each
+// CTA runs its own lines' inverse y DFTs. The arithmetic is plane_yz_kernel's, in the same order.
+constexpr int kPairThreads = 256;
+constexpr int kPairEPT = 16;  // NZ/2 * ny = 4096 points per CTA
+
+template <int NZ, bool REF>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPairThreads, 2)
+    plane_yz_pair_kernel(const double2* in, double2* out, const double2* __restrict__ ref_conj,
+                         const double2* __restrict__ tw_y, PlaneDims d) {
+  namespace cg = cooperative_groups;
+  extern __shared__ double2 sm[];
+  constexpr int H = NZ / 2;  // z lines per CTA
+  cg::cluster_group cluster = cg::this_cluster();
+  const int r = (int)cluster.block_rank();
+  const int ny = d.ny, S = ny + 1;
+  const int plane = NZ * ny;
+  const long long p = blockIdx.x >> 1;
+  double2* tws = sm + H * S;
+  stage16<4>(
+      d.n_twy, [&](int i) { return reinterpret_cast<const uint4*>(tw_y) + i; },
+      [&](int i) { return reinterpret_cast<uint4*>(tws) + i; });
+  // this CTA's lines (in may be out: each CTA reads its own lines before it writes them)
+  const double2* src = in + p * plane + (long long)r * H * ny;
+  auto first = [&](int l, int i) -> double2 { return src[l * ny + i]; };
+  fft_rows<false, kPairEPT, kPairThreads, false, true>(sm, H, d.log2ny, tws, first, NoIo{});
+  cluster.sync();  // both halves transformed along y, visible to the other CTA
+  // lines 0 .. H-1 live in CTA 0, lines H .. NZ-1 in CTA 1
+  double2* lo = r == 0 ? sm : cluster.map_shared_rank(sm, 0);
+  double2* hi = r == 1 ? sm : cluster.map_shared_rank(sm, 1);
+  const int M1 = (d.nx >> 1) + 1;
+  const int half = ny >> 1;
+  for (int c = threadIdx.x; c < half; c += blockDim.x) {
+    const int y = r * half + c;
+    const int o = swz(y);
+    double2 a[NZ];
+#pragma unroll
+    for (int z = 0; z < H; z++) {
+      a[z] = lo[z * S + o];
+      a[H + z] = hi[z * S + o];
+    }
+    if (REF) {
+      dft<NZ, false>(a);
+#pragma unroll
+      for (int z = 0; z < NZ; z++) a[z].y = -a[z].y;
+    } else {
+      constexpr int kH = (NZ + 1) / 2;
+      const int k = (int)(p % M1);
+      const double2* rc = ref_conj + (long long)k * plane + y;
+      double2 b[kH];
+#pragma unroll
+      for (int z = 0; z < kH; z++) b[z] = __ldg(rc + z * ny);
+      dft<NZ, false>(a);
+#pragma unroll
+      for (int z = 0; z < kH; z++) a[z] = cross_power(a[z], b[z]);
+#pragma unroll
+      for (int z = kH; z < NZ; z++) b[z - kH] = __ldg(rc + z * ny);
+#pragma unroll
+      for (int z = kH; z < NZ; z++) a[z] = cross_power(a[z], b[z - kH]);
+      dft<NZ, true>(a);
+    }
+#pragma unroll
+    for (int z = 0; z < H; z++) {
+      lo[z * S + o] = a[z];
+      hi[z * S + o] = a[H + z];
+    }
+  }
+  cluster.sync();  // every column written back; no shared-memory access crosses CTAs after this
+  double2* dst = out + p * plane + (long long)r * H * ny;
+  if (!REF) {
+    auto last = [&](int l, int i, double2 v) { dst[l * ny + i] = v; };
+    fft_rows<true, kPairEPT, kPairThreads, true, false>(sm, H, d.log2ny, tws, NoIo{}, last);
+  } else {
+    const int E = H * ny;
+#pragma unroll
+    for (int u = 0; u < kPairEPT; u++) {
+      const int idx = threadIdx.x + u * kPairThreads;
+      if (idx < E) dst[idx] = sm[(idx >> d.log2ny) * S + swz(idx & (ny - 1))];
+    }
+  }
+}
+
 // Split (z, y) pass. Lines of ny points along y, in place in the batch's plane array (line l = plane
 // p, plane z at offset l * ny of spec[kx][z][y]), d.LY lines per CTA; the first stage reads global
 // memory and the last writes it (ny >= 16: at least two stages, so a CTA reads all its lines before
@@ -703,6 +789,15 @@ namespace {
 template <int NZ, bool REF>
 cudaError_t launch_yz(const PlaneDims& d, const double2* in, double2* out, const double2* ref_conj,
                       const double2* tw_y, long long n_planes, cudaStream_t s) {
+  if constexpr (NZ >= 4) {
+    if ((long long)NZ * d.ny == 2LL * kPairThreads * kPairEPT) {  // one plane per pair of CTAs
+      const size_t smem = ((size_t)(NZ / 2) * (d.ny + 1) + d.ny) * sizeof(double2);
+      cudaError_t e = allow_smem(plane_yz_pair_kernel<NZ, REF>, smem);
+      if (e != cudaSuccess) return e;
+      plane_yz_pair_kernel<NZ, REF><<<(unsigned)(2 * n_planes), kPairThreads, smem, s>>>(in, out, ref_conj, tw_y, d);
+      return cudaGetLastError();
+    }
+  }
   const size_t smem = ((size_t)d.PP * NZ * (d.ny + 1) + d.ny) * sizeof(double2);
   cudaError_t e = allow_smem(plane_yz_kernel<NZ, REF>, smem);
   if (e != cudaSuccess) return e;

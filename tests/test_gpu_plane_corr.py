@@ -46,6 +46,8 @@ def _pair(shape, shift, seed):
 
 PLANE_SHAPES = [(1, 8, 16), (2, 16, 16), (1, 64, 64), (4, 64, 128), (8, 32, 64), (16, 8, 32), (1, 256, 256),
                 (2, 16, 512), (16, 64, 64), (1, 8, 4096), (16, 512, 512),
+                # planes of 8192 points, one per pair of CTAs (a 2-CTA cluster)
+                (16, 512, 64), (8, 1024, 32), (4, 2048, 16),
                 # split (z, y) pass: y-line, z-column and inverse y-line kernels
                 (32, 16, 16), (64, 32, 32), (16, 1024, 32), (8, 2048, 16), (64, 128, 128), (128, 16, 64)]
 
