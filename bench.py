@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--only", choices=["roofline", "aligner"], default=None,
                     help="roofline: only the fused-pass probe on --frames FP16 frames; aligner: one aligner call "
                          "on --frames raw uint16 frames in HBM (both for ncu captures)")
+    ap.add_argument("--tuning", default=None,
+                    help="TILE_VOXELS,CTAS_PER_SM: the roofline probe's fused-pass tuning instead of the autotuner's "
+                         "(under ncu the autotuner's timings do not represent a plain run; pass the plain run's choice)")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="length of the Poisson arrival stream")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="total arrivals per second")
     ap.add_argument("--serve-pool", type=int, default=6, help="distinct frames per served acquisition")
@@ -510,6 +513,9 @@ def run_roofline_probe(args, local):
     line, il, ifr = acq.scan
     ctx = fa.Context(device=local, autotune=True)
     ref = fa.Reference(ctx, acq.reference + 1, acq.nD, fa.scan_params(line, il, ifr, nx, ny, nz), fa.PREC_MIXED)
+    if args.tuning:
+        tile_voxels, ctas_per_sm = (int(v) for v in args.tuning.split(","))
+        ref.retune(tile_voxels, ctas_per_sm)
     frs = [fa.Frame(ref, (acq.frames[k] + 1).astype(np.float16)) for k in range(args.frames)]
     ms = fa.profile_eval(frs, acq.D_true[0], 2)
     print(json.dumps({"probe": "eval4_kernel<3, half, bf16>", "frames": args.frames, "ms_per_launch": ms,
