@@ -353,11 +353,10 @@ std::map<std::string, TuneResult> g_tune_cache;
 // The project's autotuner for the fused pass: times each (tile size, CTAs per SM) candidate with the
 // persistent kernel the batched solver uses, on a launch of K distinct synthetic frames (copies of the
 // reference, slightly displaced; K up to 16, as many as fit in 256 MB, so that the frames do not all
-// stay in L2 as a real batch's do not) and on a launch of one. The tile size is the one with the
-// lowest sum of the best per-frame time of the K-frame launch and the best one-frame launch time (so
-// that it serves both the batched aligner and the few-frame launches of serving and of a batch's late
-// iterations); at that tile size the budget for launches of many frames is the fastest K-frame one
-// and the budget for a few frames the fastest one-frame one. The choice is cached
+// stay in L2 as a real batch's do not) and on a launch of one. The tile size and the budget for
+// launches of many frames are those of the lowest per-frame time of the K-frame launch; at that tile
+// size the budget for launches of a few frames (single-frame path, static-scratch entry, serving loop)
+// is the fastest one-frame one. The choice is cached
 // per volume shape, control-point count and precision for the life of the process. Register budgets
 // under which the kernel spills more than 128 bytes are skipped (the largest budget is always a
 // candidate).
@@ -509,7 +508,7 @@ fa_status autotune(fa_reference* R) {
         mb_1 = mbs[mi];
       }
     }
-    if (tk < 1e30 && t1 < 1e30 && tk + t1 < best.ms) best = TuneResult{targets[ti], mb_k, mb_k, mb_1, tk + t1};
+    if (tk < 1e30 && t1 < 1e30 && tk < best.ms) best = TuneResult{targets[ti], mb_k, mb_k, mb_1, tk};
   }
   R->host.tune_mb = best.mb;
   R->host.tune_grid_mult = best.grid_mult;
@@ -1281,9 +1280,9 @@ fa_status correlator_reserve(fa_correlator* C, int n) {
   C->h_ptrs = nullptr;
   C->h_idx = nullptr;
   C->ptr_cap = 0;
-  FA_TRY(dalloc_t(C->ctx, (size_t)n, &C->d_ptrs, C->ptr_allocs));
+  FA_TRY(dalloc_t(C->ctx, 2 * (size_t)n, &C->d_ptrs, C->ptr_allocs));
   FA_TRY(dalloc_t(C->ctx, (size_t)n, &C->d_idx, C->ptr_allocs));
-  if (cudaMallocHost(&C->h_ptrs, (size_t)n * sizeof(void*)) != cudaSuccess ||
+  if (cudaMallocHost(&C->h_ptrs, 2 * (size_t)n * sizeof(void*)) != cudaSuccess ||
       cudaMallocHost(&C->h_idx, (size_t)n * sizeof(long long)) != cudaSuccess)
     return fail(FA_ERR_OOM, "cudaMallocHost failed");
   C->ptr_cap = n;
@@ -1293,7 +1292,9 @@ fa_status correlator_reserve(fa_correlator* C, int n) {
 // Window, forward DFT, cross-power normalisation, inverse DFT and first-maximum argmax for n volumes
 // (device pointers, FP32 or raw uint16) in batches of C->cap; peak indices to C->d_idx[first ..].
 fa_status correlator_enqueue(fa_correlator* C, const void* const* vols, int in_kind, int n, double* surface,
-                             bool planes, int first) {
+                             bool planes, int first, void* const* slots, int slot_kind, int slot_pitch,
+                             long long slot_plane, bool* slots_written) {
+  if (slots_written) *slots_written = false;
   if (first > 0 && first + n > C->ptr_cap) return fail(FA_ERR_STATE, "correlator slots not reserved");
   FA_TRY(correlator_reserve(C, first + n));
   // the fused passes stage frames in 16-byte chunks: 16-byte aligned frames only
@@ -1305,6 +1306,24 @@ fa_status correlator_enqueue(fa_correlator* C, const void* const* vols, int in_k
   FA_CU(cudaMemcpyAsync(C->d_ptrs + first, C->h_ptrs + first, (size_t)n * sizeof(void*), cudaMemcpyHostToDevice,
                         C->stream));
   const void* const* d_ptrs = C->d_ptrs + first;
+  // slots filled by the first pass: 16-byte aligned rows, and a raw uint16 slot only from uint16 frames
+  const size_t slot_esz = slot_kind == fa::kFrameF32 ? 4 : 2;
+  const bool fill = planes && slots && (slot_kind != fa::kFrameRawU16 || in_kind == FA_U16) &&
+                    ((size_t)slot_pitch * slot_esz) % 16 == 0 && ((size_t)slot_plane * slot_esz) % 16 == 0 &&
+                    C->nx % 8 == 0;
+  bool fill_ok = fill;
+  if (fill) {
+    for (int i = 0; i < n; i++) {
+      C->h_ptrs[C->ptr_cap + first + i] = slots[i];
+      if (reinterpret_cast<uintptr_t>(slots[i]) % 16) fill_ok = false;
+    }
+  }
+  fa::SlotOut slot_out{};
+  if (fill_ok) {
+    FA_CU(cudaMemcpyAsync(C->d_ptrs + C->ptr_cap + first, C->h_ptrs + C->ptr_cap + first, (size_t)n * sizeof(void*),
+                          cudaMemcpyHostToDevice, C->stream));
+    slot_out = fa::SlotOut{C->d_ptrs + C->ptr_cap + first, slot_kind, slot_pitch, slot_plane};
+  }
   long long* d_idx = C->d_idx + first;
   if (!planes && C->planes && !C->ref_conj_rows) {  // a plane-path correlator falling back to cuFFT
     FA_CU(cudaStreamSynchronize(C->stream));
@@ -1319,7 +1338,10 @@ fa_status correlator_enqueue(fa_correlator* C, const void* const* vols, int in_k
     double* surf = surface ? surface + (size_t)c0 * C->n_el : nullptr;
     if (planes) {
       const int nb = fa::plane_blocks_per_frame(C->pd);
-      FA_CU(fa::launch_plane_rows_fwd(C->pd, d_ptrs + c0, in_kind, m, C->wy, C->wx, C->tw_x, C->spec, C->stream));
+      fa::SlotOut so = slot_out;
+      if (fill_ok) so.ptrs += c0;
+      FA_CU(fa::launch_plane_rows_fwd(C->pd, d_ptrs + c0, in_kind, m, C->wy, C->wx, C->tw_x, C->spec, C->stream,
+                                      fill_ok ? &so : nullptr));
       if (C->pd.split)
         FA_CU(fa::launch_plane_yz_split(C->pd, C->spec, C->ref_conj, C->tw_y, C->tw_z, m, false, C->stream));
       else
@@ -1345,6 +1367,7 @@ fa_status correlator_enqueue(fa_correlator* C, const void* const* vols, int in_k
     }
     c0 += m;
   }
+  if (slots_written) *slots_written = fill_ok;
   return FA_OK;
 }
 
@@ -1852,7 +1875,11 @@ fa_status aligner_run(fa_aligner* A, const void* const* frames, fa_dtype dtype, 
   }
   fa_correlator* C = A->corr;
   std::vector<const void*> raw((size_t)n), cin((size_t)n);
+  std::vector<void*> slot_ptrs((size_t)n);
   int cin_kind = dtype;
+  // Without smoothing or binning the correlator's first pass reads the raw frames anyway: it also
+  // writes their slots (count + 1), in place of a separate conversion pass.
+  const bool fuse_slots = A->prm.smoothing <= 0 && A->prm.spatial_binning <= 1;
   for (int c0 = 0, ci = 0, g = 0; c0 < n; ci++) {
     while (gb[g + 1] <= c0) g++;
     const int m = std::min(chunk, gb[g + 1] - c0);
@@ -1871,11 +1898,12 @@ fa_status aligner_run(fa_aligner* A, const void* const* frames, fa_dtype dtype, 
         FA_TRY(aligner_smooth(A, raw[i], dtype, s));
         FA_CU(fa::launch_to_slot(A->smooth_out, FA_F32, F->data, kind, A->nz, A->ny, A->nx, F->job.fpitch,
                                  F->job.fplane, true, s));
-      } else {
+      } else if (!fuse_slots) {
         FA_CU(fa::launch_to_slot(raw[i], dtype, F->data, kind, A->nz, A->ny, A->nx, F->job.fpitch, F->job.fplane,
                                  true, s));
       }
-      g_launches += 1;
+      slot_ptrs[i] = F->data;
+      if (!fuse_slots) g_launches += 1;
       // Phase correlation on the raw frames (FrameWarpAligner.cpp:181-190), downsampled when binning.
       if (A->prm.spatial_binning > 1) {
         float* vol = A->vols + (size_t)i * A->dz * A->dy * A->dx;
@@ -1887,7 +1915,17 @@ fa_status aligner_run(fa_aligner* A, const void* const* frames, fa_dtype dtype, 
         cin[i] = raw[i];
       }
     }
-    FA_TRY(correlator_enqueue(C, cin.data() + c0, cin_kind, m, nullptr, true, c0));
+    bool written = false;
+    FA_TRY(correlator_enqueue(C, cin.data() + c0, cin_kind, m, nullptr, true, c0, fuse_slots ? slot_ptrs.data() + c0 : nullptr,
+                              kind, A->slots[c0]->job.fpitch, A->slots[c0]->job.fplane, &written));
+    if (fuse_slots && !written) {  // the correlator took the cuFFT path: a separate conversion
+      for (int i = c0; i < c0 + m; i++) {
+        fa_frame* F = A->slots[i];
+        FA_CU(fa::launch_to_slot(raw[i], dtype, F->data, kind, A->nz, A->ny, A->nx, F->job.fpitch, F->job.fplane,
+                                 true, s));
+        g_launches += 1;
+      }
+    }
     c0 += m;
     if (c0 == gb[g + 1]) FA_CU(cudaEventRecord(A->group_ev[g], s));  // a group's frames and peaks are ready
   }

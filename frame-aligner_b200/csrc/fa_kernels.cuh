@@ -154,11 +154,20 @@ void plane_twiddles(const PlaneDims& d, std::vector<double2>* tw_x, std::vector<
                     std::vector<double2>* tw_z);
 // CTAs (argmax partials) per frame of the last pass.
 int plane_blocks_per_frame(const PlaneDims& d);
+// Frame slots the first pass may fill while it reads the frames: frame i's value + 1 (the slot
+// conversion, stored as `kind`: raw uint16 saturated, FP16 or FP32) at ptrs[i] + z * plane +
+// y * pitch + x (16-byte aligned rows).
+struct SlotOut {
+  const void* const* ptrs;  // device array, one interior pointer per frame of the batch (writable slots)
+  int kind;           // FrameKind
+  int pitch;
+  long long plane;
+};
 // Window + real DFT along x of each frame (dense FP32 or uint16, in_kind an fa_dtype) into spec
-// (batch * n_complex).
+// (batch * n_complex); with `slot` (optional) also the frames' slots.
 cudaError_t launch_plane_rows_fwd(const PlaneDims& d, const void* const* vols, int in_kind, int batch,
                                   const double* wy, const double* wx, const double2* tw_x, double2* spec,
-                                  cudaStream_t s);
+                                  cudaStream_t s, const SlotOut* slot = nullptr);
 // Per plane: forward DFT over (z, y), then either out = conj (reference) or, in place,
 // out = inverse DFT of the normalised cross-power spectrum with ref_conj.
 cudaError_t launch_plane_yz(const PlaneDims& d, const double2* in, double2* out, const double2* ref_conj,

@@ -296,12 +296,13 @@ __host__ __device__ inline size_t rows_smem_bytes(const PlaneDims& d) {
   return (G * ((d.nx >> 1) + 1) + d.nx) * 16;
 }
 
-template <bool U16>
+// SLOT: -1, or the FrameKind of the slots written from the same loads (SlotOut).
+template <bool U16, int SLOT>
 __global__ void __launch_bounds__(kRowThreads) plane_rows_fwd_kernel(const void* const* __restrict__ vols,
                                                                      const double* __restrict__ wy,
                                                                      const double* __restrict__ wx,
                                                                      const double2* __restrict__ tw_x, PlaneDims d,
-                                                                     double2* __restrict__ spec) {
+                                                                     double2* __restrict__ spec, SlotOut slot) {
   extern __shared__ double2 sm[];
   const int M = d.nx >> 1, S = M + 1, G = 1 << d.log2G;
   double2* tws = sm + G * S;
@@ -317,14 +318,32 @@ __global__ void __launch_bounds__(kRowThreads) plane_rows_fwd_kernel(const void*
     const int r = r0 + g;
     const long long off = (long long)r * d.nx + 2 * m;
     float v0, v1;
+    unsigned q0 = 0, q1 = 0;
     if (U16) {
       const ushort2 q = __ldg(reinterpret_cast<const ushort2*>(static_cast<const unsigned short*>(vol) + off));
       v0 = (float)q.x;
       v1 = (float)q.y;
+      q0 = q.x;
+      q1 = q.y;
     } else {
       const float2 f = __ldg(reinterpret_cast<const float2*>(static_cast<const float*>(vol) + off));
       v0 = f.x;
       v1 = f.y;
+    }
+    if constexpr (SLOT >= 0) {
+      // the slot conversion of these two values (count + 1 saturated, or value + 1 rounded to the
+      // slot's type), at (z, y, 2m) of this frame's slot
+      const long long so = (long long)(r >> d.log2ny) * slot.plane + (long long)(r & (d.ny - 1)) * slot.pitch + 2 * m;
+      void* dst = const_cast<void*>(slot.ptrs[blockIdx.y]);
+      if constexpr (SLOT == kFrameRawU16) {
+        const unsigned lo = min(q0 + 1u, 65535u), hi = min(q1 + 1u, 65535u);
+        *reinterpret_cast<unsigned*>(static_cast<unsigned short*>(dst) + so) = lo | (hi << 16);
+      } else if constexpr (SLOT == kFrameF16) {
+        *reinterpret_cast<__half2*>(static_cast<__half*>(dst) + so) =
+            __halves2half2(__float2half_rn(v0 + 1.0f), __float2half_rn(v1 + 1.0f));
+      } else {
+        *reinterpret_cast<float2*>(static_cast<float*>(dst) + so) = make_float2(v0 + 1.0f, v1 + 1.0f);
+      }
     }
     const double wrow = __dmul_rn(1.0, __ldg(wy + (r & (d.ny - 1))));
     const double2 w = __ldg(reinterpret_cast<const double2*>(wx) + m);
@@ -768,21 +787,33 @@ bool plane_dims(int nz, int ny, int nx, PlaneDims* d) {
 
 int plane_blocks_per_frame(const PlaneDims& d) { return d.rows >> d.log2G; }
 
+namespace {
+template <bool U16, int SLOT>
+cudaError_t launch_rows_fwd(const PlaneDims& d, const void* const* vols, int batch, const double* wy,
+                            const double* wx, const double2* tw_x, double2* spec, cudaStream_t s, const SlotOut& so) {
+  const size_t smem = rows_smem_bytes(d);
+  cudaError_t e = allow_smem(plane_rows_fwd_kernel<U16, SLOT>, smem);
+  if (e != cudaSuccess) return e;
+  plane_rows_fwd_kernel<U16, SLOT><<<dim3(d.rows >> d.log2G, batch), kRowThreads, smem, s>>>(vols, wy, wx, tw_x, d,
+                                                                                             spec, so);
+  return cudaGetLastError();
+}
+}  // namespace
+
 cudaError_t launch_plane_rows_fwd(const PlaneDims& d, const void* const* vols, int in_kind, int batch,
                                   const double* wy, const double* wx, const double2* tw_x, double2* spec,
-                                  cudaStream_t s) {
-  const size_t smem = rows_smem_bytes(d);
-  const dim3 grid(d.rows >> d.log2G, batch);
+                                  cudaStream_t s, const SlotOut* slot) {
+  const SlotOut so = slot ? *slot : SlotOut{nullptr, -1, 0, 0};
+  const int k = slot ? slot->kind : -1;
   if (in_kind == FA_U16) {
-    cudaError_t e = allow_smem(plane_rows_fwd_kernel<true>, smem);
-    if (e != cudaSuccess) return e;
-    plane_rows_fwd_kernel<true><<<grid, kRowThreads, smem, s>>>(vols, wy, wx, tw_x, d, spec);
-  } else {
-    cudaError_t e = allow_smem(plane_rows_fwd_kernel<false>, smem);
-    if (e != cudaSuccess) return e;
-    plane_rows_fwd_kernel<false><<<grid, kRowThreads, smem, s>>>(vols, wy, wx, tw_x, d, spec);
+    if (k == kFrameRawU16) return launch_rows_fwd<true, kFrameRawU16>(d, vols, batch, wy, wx, tw_x, spec, s, so);
+    if (k == kFrameF16) return launch_rows_fwd<true, kFrameF16>(d, vols, batch, wy, wx, tw_x, spec, s, so);
+    if (k == kFrameF32) return launch_rows_fwd<true, kFrameF32>(d, vols, batch, wy, wx, tw_x, spec, s, so);
+    return launch_rows_fwd<true, -1>(d, vols, batch, wy, wx, tw_x, spec, s, so);
   }
-  return cudaGetLastError();
+  if (k == kFrameF16) return launch_rows_fwd<false, kFrameF16>(d, vols, batch, wy, wx, tw_x, spec, s, so);
+  if (k == kFrameF32) return launch_rows_fwd<false, kFrameF32>(d, vols, batch, wy, wx, tw_x, spec, s, so);
+  return launch_rows_fwd<false, -1>(d, vols, batch, wy, wx, tw_x, spec, s, so);
 }
 
 namespace {

@@ -129,7 +129,7 @@ struct fa_correlator {
   double2* ref_conj = nullptr;          // n_complex (planes [kx][z][y] when `planes`, else cuFFT's order)
   double2* ref_conj_rows = nullptr;     // cuFFT's order, made when a plane-path correlator falls back
   float* vol = nullptr;                 // one host-uploaded volume
-  const void** d_ptrs = nullptr;        // device array of input pointers
+  const void** d_ptrs = nullptr;        // device array of input pointers, then (from ptr_cap) slot pointers
   const void** h_ptrs = nullptr;        // pinned staging of the same
   int ptr_cap = 0;
   double* bval = nullptr;
@@ -247,8 +247,13 @@ fa_status correlator_plans(fa_correlator* C, int batch, cufftHandle* fwd, cufftH
 // surfaces; planes selects the fused kx-plane passes (when C->planes) or cuFFT. Calls with
 // first > 0 use pointer and result slots reserved before (correlator_reserve(C, first + n)), so
 // that consecutive calls queue on the stream without waiting for one another.
+// With `slots` (n interior pointers of frame slots of `slot_kind` with the given pitch and plane),
+// the plane path also writes each frame + 1 into its slot as it reads it (*slots_written = true);
+// on the cuFFT path it does not, and the caller converts the frames itself.
 fa_status correlator_enqueue(fa_correlator* C, const void* const* vols, int in_kind, int n,
-                             double* surface = nullptr, bool planes = true, int first = 0);
+                             double* surface = nullptr, bool planes = true, int first = 0,
+                             void* const* slots = nullptr, int slot_kind = 0, int slot_pitch = 0,
+                             long long slot_plane = 0, bool* slots_written = nullptr);
 // Pointer staging and peak slots for n volumes (grows with a stream synchronisation).
 fa_status correlator_reserve(fa_correlator* C, int n);
 // Peak index -> signed integer shift (x, y, z).

@@ -232,11 +232,28 @@ def _c64(a):
 class Context:
     def __init__(self, device=0, memory_budget=0, autotune=False):
         self._h = _vp()
+        # Handles made from this context, closed before it (frames, then aligners, servers and
+        # correlators, then references): a handle must not outlive the context whose memory it uses,
+        # also when the garbage collector finalises both in one cycle.
+        self._children = set()
         cfg = Config(device, memory_budget, int(autotune))
         check(lib().fa_create(C.byref(cfg), C.byref(self._h)))
 
+    def _adopt(self, obj, rank):
+        obj._close_rank = rank
+        obj._owner = self
+        self._children.add(obj)
+
+    def _release(self, obj):
+        self._children.discard(obj)
+
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
+            for obj in sorted(list(getattr(self, "_children", ())), key=lambda o: o._close_rank):
+                try:
+                    obj.close()
+                except Exception:
+                    pass
             lib().fa_destroy(self._h)
             self._h = _vp()
 
@@ -245,6 +262,14 @@ class Context:
             self.close()
         except Exception:
             pass
+
+
+def _released(obj):
+    """Takes obj off its context's list of live handles (after obj closed its handle)."""
+    owner = getattr(obj, "_owner", None)
+    if owner is not None:
+        owner._release(obj)
+        obj._owner = None
 
 
 class Reference:
@@ -265,6 +290,7 @@ class Reference:
             nz, ny, nx = ref.shape
             check(lib().fa_set_reference(ctx._h, ref, nz, ny, nx, int(nD), C.byref(scan), precision,
                                          C.byref(self._h)))
+        ctx._adopt(self, 2)
         self.dims = (nz, ny, nx)
         self.nD = int(nD)
         self.precision = precision
@@ -316,6 +342,7 @@ class Reference:
         if getattr(self, "_h", None) and self._h.value:
             check(lib().fa_reference_destroy(self._h))
             self._h = _vp()
+            _released(self)
 
     def __del__(self):
         try:
@@ -339,6 +366,7 @@ class Frame:
             self._keep = arr
             check(lib().fa_register_frame(ref._h, arr.ctypes.data, _DTYPES[arr.dtype], C.byref(self._h)))
             self._keep = None
+        ref.ctx._adopt(self, 0)
 
     def update(self, data):
         arr = np.ascontiguousarray(data)
@@ -373,6 +401,7 @@ class Frame:
         if getattr(self, "_h", None) and self._h.value:
             check(lib().fa_deregister_frame(self._h))
             self._h = _vp()
+            _released(self)
 
     def __del__(self):
         try:
@@ -403,6 +432,7 @@ class Correlator:
         self.dims = ref.shape
         self._h = _vp()
         check(lib().fa_correlator_create(ctx._h, ref, *ref.shape, C.byref(self._h)))
+        ctx._adopt(self, 1)
 
     def compute_shift(self, volume):
         s = np.empty(3, np.float64)
@@ -426,6 +456,7 @@ class Correlator:
         if getattr(self, "_h", None) and self._h.value:
             lib().fa_correlator_destroy(self._h)
             self._h = _vp()
+            _released(self)
 
     def __del__(self):
         try:
@@ -443,6 +474,7 @@ class Aligner:
         self._h = _vp()
         prm = AlignerParams(spatial_binning, n_resampling_points, nD, smoothing, precision, max_iterations)
         check(lib().fa_aligner_create(ctx._h, C.byref(prm), C.byref(self._h)))
+        ctx._adopt(self, 1)
 
     def set_reference(self, reference, scan: ScanParams):
         ref = np.ascontiguousarray(reference)
@@ -524,6 +556,7 @@ class Aligner:
         if getattr(self, "_h", None) and self._h.value:
             lib().fa_aligner_destroy(self._h)
             self._h = _vp()
+            _released(self)
 
     def __del__(self):
         try:
@@ -543,6 +576,7 @@ class Server:
         lag = int(warm_start)  # True -> 1 (the previous frame), False -> 0, d -> frame k - d
         cfg = ServerConfig(memory_budget, max_in_flight, iterations_per_launch, lag, 1 if shared_launches else 0)
         check(lib().fa_server_create(ctx._h, C.byref(cfg), C.byref(self._h)))
+        ctx._adopt(self, 1)
         self.acqs = {}
         self._keep = {}  # host frames referenced by outstanding tickets
 
@@ -609,6 +643,7 @@ class Server:
             lib().fa_server_destroy(self._h)
             self._h = _vp()
             self._keep.clear()
+            _released(self)
 
     def __del__(self):
         try:

@@ -129,3 +129,39 @@ def test_device_peak_start_wraps_and_scales(ctx, factor):
         r = _rms(D[k], D_cpu, 2)
         assert r <= 0.01, (k, shifts[k], r)
     al.close()
+
+
+@pytest.mark.parametrize("precision", [fa.PREC_MIXED, fa.PREC_F32], ids=["mixed", "f32"])
+def test_slots_written_by_the_correlator(ctx, precision):
+    """Without smoothing or binning the phase correlator's first pass writes each frame + 1 into its
+    slot as it reads the frame: raw uint16 counts (saturated) from uint16 frames and FP16 values from
+    FP32 frames in mixed precision, FP32 values in FP32 precision. The same counts given as uint16 and
+    as FP32 frames fill slots with the same values (counts below 2048 are exact in FP16), so D is
+    identical; host and device inputs give identical D; and D is within 0.01 px of the CPU solve
+    (the reference's 256 x 256 single-plane case, nD = 10)."""
+    import torch
+
+    n = 3
+    acq = S.make_config(S.CONFIG0, n_frames=n)
+    assert acq.frames.max() + 1 < 2048
+    nz, ny, nx = acq.reference.shape
+    line, il, ifr = acq.scan
+    al = fa.Aligner(ctx, nD=acq.nD, precision=precision)
+    al.set_reference(acq.reference, _scan(acq))
+    Ds = []
+    for dtype, view, kind in ((np.uint16, np.int16, fa.U16), (np.float32, np.float32, fa.F32)):
+        host = np.ascontiguousarray(acq.frames.astype(dtype))
+        D, _ = al.add_frames([host[k] for k in range(n)])
+        dev = torch.from_numpy(host.view(view)).to("cuda:0")
+        torch.cuda.synchronize()
+        D_dev, _ = al.add_frames_device([dev[k].data_ptr() for k in range(n)], kind, n)
+        assert np.array_equal(D, D_dev)
+        Ds.append(D)
+    assert np.array_equal(Ds[0], Ds[1])
+    ow = O.OracleWarper(acq.reference + 1, acq.nD, O.scan_init(line, il, ifr, nx, ny, nz))
+    for k in range(n):
+        shift = O.phase_shift(acq.reference, acq.frames[k])
+        D_cpu, _ = ow.align_frame(acq.frames[k] + 1, shift, 100)
+        r = _rms(Ds[0][k], D_cpu, 2)
+        assert r <= 0.01, (k, r)
+    al.close()
