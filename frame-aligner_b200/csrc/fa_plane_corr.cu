@@ -308,6 +308,7 @@ __global__ void __launch_bounds__(kRowThreads) plane_rows_fwd_kernel(const void*
   double2* tws = sm + G * S;
   const int r0 = blockIdx.x << d.log2G;
   const void* vol = vols[blockIdx.y];
+  void* const slot_base = SLOT >= 0 ? const_cast<void*>(slot.ptrs[blockIdx.y]) : nullptr;
   // the twiddles (published by the first stage's closing barrier; the first stage needs none)
   stage16<4>(
       d.n_twx, [&](int i) { return reinterpret_cast<const uint4*>(tw_x) + i; },
@@ -334,7 +335,7 @@ __global__ void __launch_bounds__(kRowThreads) plane_rows_fwd_kernel(const void*
       // the slot conversion of these two values (count + 1 saturated, or value + 1 rounded to the
       // slot's type), at (z, y, 2m) of this frame's slot
       const long long so = (long long)(r >> d.log2ny) * slot.plane + (long long)(r & (d.ny - 1)) * slot.pitch + 2 * m;
-      void* dst = const_cast<void*>(slot.ptrs[blockIdx.y]);
+      void* dst = slot_base;
       if constexpr (SLOT == kFrameRawU16) {
         const unsigned lo = min(q0 + 1u, 65535u), hi = min(q1 + 1u, 65535u);
         *reinterpret_cast<unsigned*>(static_cast<unsigned short*>(dst) + so) = lo | (hi << 16);
@@ -630,28 +631,37 @@ __global__ void __launch_bounds__(kRowThreads) plane_rows_inv_argmax_kernel(cons
   double2* tws = sm + G * S;
   const int r0 = blockIdx.x << d.log2G;
   const double2* in = spec + (long long)blockIdx.y * d.n_complex;
+  stage16<4>(
+      d.n_twx, [&](int i) { return reinterpret_cast<const uint4*>(tw_x) + i; },
+      [&](int i) { return reinterpret_cast<uint4*>(tws) + i; });
+  // Bins k and M - k of each row, folded as they arrive (the fold's twiddles from global memory, so
+  // that it need not wait for the staged table): four pairs per thread in flight.
   {
-    const int n_bins = (M + 1) << d.log2G;
-    stage16<8>(
-        n_bins + d.n_twx,
-        [&](int i) {
-          return reinterpret_cast<const uint4*>(
-              i < n_bins ? in + (long long)(i >> d.log2G) * d.rows + r0 + (i & (G - 1)) : tw_x + (i - n_bins));
-        },
-        [&](int i) {
-          const int k = i >> d.log2G;
-          return reinterpret_cast<uint4*>(i < n_bins ? sm + (i & (G - 1)) * S + (k < M ? swz(k) : M)
-                                                     : tws + (i - n_bins));
-        });
-  }
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < ((H + 1) << d.log2G); idx += blockDim.x) {
-    const int k = idx >> d.log2G, g = idx & (G - 1);
-    double2* line = sm + g * S;
-    const int ik = swz(k), im = k == 0 ? M : swz(M - k);
-    const double2 xk = line[ik], xm = line[im];
-    line[ik] = fold(xk, xm, tws[d.tw_x_post + k]);
-    if (k > 0 && k < H) line[im] = fold(xm, xk, tws[d.tw_x_post + M - k]);
+    constexpr int K = 4;
+    const int n_pairs = (H + 1) << d.log2G;
+    for (int base = 0; base < n_pairs; base += K * (int)blockDim.x) {
+      double2 xk[K], xm[K];
+#pragma unroll
+      for (int u = 0; u < K; u++) {
+        const int idx = base + (int)threadIdx.x + u * (int)blockDim.x;
+        if (idx < n_pairs) {
+          const int k = idx >> d.log2G, g = idx & (G - 1);
+          xk[u] = in[(long long)k * d.rows + r0 + g];
+          xm[u] = in[(long long)(M - k) * d.rows + r0 + g];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < K; u++) {
+        const int idx = base + (int)threadIdx.x + u * (int)blockDim.x;
+        if (idx < n_pairs) {
+          const int k = idx >> d.log2G, g = idx & (G - 1);
+          double2* line = sm + g * S;
+          const int ik = swz(k), im = k == 0 ? M : swz(M - k);
+          line[ik] = fold(xk[u], xm[u], __ldg(tw_x + d.tw_x_post + k));
+          if (k > 0 && k < H) line[im] = fold(xm[u], xk[u], __ldg(tw_x + d.tw_x_post + M - k));
+        }
+      }
+    }
   }
   __syncthreads();
   // the last inverse stage feeds the first-maximum search (and the optional surface)
