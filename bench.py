@@ -70,9 +70,7 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="length of the Poisson arrival stream")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="total arrivals per second")
     ap.add_argument("--serve-pool", type=int, default=6, help="distinct frames per served acquisition")
-    ap.add_argument("--serve-slots", type=int, default=48,
-                    help="frame slots reserved per served acquisition (a slot made during the stream costs "
-                         "device and pinned-memory allocations on the worker thread)")
+    ap.add_argument("--serve-slots", type=int, default=24, help="frame slots reserved per served acquisition")
     ap.add_argument("--serve-iters", type=int, default=4, help="trust-region iterations per serving graph launch")
     ap.add_argument("--serve-lags", type=int, nargs="+", default=[1, 4],
                     help="warm-start lags to serve with (1 = the previous frame's solution)")
