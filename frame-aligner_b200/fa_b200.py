@@ -17,6 +17,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import weakref
 
 import numpy as np
 
@@ -232,10 +233,16 @@ def _c64(a):
 class Context:
     def __init__(self, device=0, memory_budget=0, autotune=False):
         self._h = _vp()
-        # Handles made from this context, closed before it (frames, then aligners, servers and
-        # correlators, then references): a handle must not outlive the context whose memory it uses,
-        # also when the garbage collector finalises both in one cycle.
-        self._children = set()
+        # Handles made from this context (frames, references, correlators, aligners, servers) must
+        # not outlive it: the context counts its live handles and destroys itself only when the
+        # count is zero, when asked to close or after the last handle closed. close() first closes
+        # the handles still reachable (frames, then aligners, servers and correlators, then
+        # references); handles the garbage collector finalises in the same cycle as the context are
+        # unreachable for it, and the last of them to close destroys the context. Handles no longer
+        # referenced are collected as usual.
+        self._children = weakref.WeakSet()
+        self._live = 0
+        self._closing = False
         cfg = Config(device, memory_budget, int(autotune))
         check(lib().fa_create(C.byref(cfg), C.byref(self._h)))
 
@@ -243,19 +250,30 @@ class Context:
         obj._close_rank = rank
         obj._owner = self
         self._children.add(obj)
+        self._live += 1
 
     def _release(self, obj):
         self._children.discard(obj)
+        self._live -= 1
+        if self._closing and self._live == 0:
+            self._destroy()
 
-    def close(self):
+    def _destroy(self):
         if getattr(self, "_h", None) and self._h.value:
-            for obj in sorted(list(getattr(self, "_children", ())), key=lambda o: o._close_rank):
-                try:
-                    obj.close()
-                except Exception:
-                    pass
             lib().fa_destroy(self._h)
             self._h = _vp()
+
+    def close(self):
+        if not (getattr(self, "_h", None) and self._h.value) or getattr(self, "_closing", False):
+            return
+        self._closing = True
+        for obj in sorted(list(getattr(self, "_children", ())), key=lambda o: o._close_rank):
+            try:
+                obj.close()
+            except Exception:
+                pass
+        if getattr(self, "_live", 0) == 0:
+            self._destroy()
 
     def __del__(self):
         try:
