@@ -667,14 +667,6 @@ def run_ours(args, rank, world, local):
             f.close()
         ref_m.close()
         plain = measure_plain(fa, ctx, acq, scan, min(args.plain_frames, n), local)
-        cb = None
-        D_cpu = None
-        if not args.no_cpu:
-            try:
-                nt = os.cpu_count() or 1
-                cb, D_cpu, _ = cpu_baseline(acq, nt, args.cpu_frames or min(nt, n))
-            except Exception as ex:  # the baseline is reported, never required
-                cb = {"value": None, "unit": UNIT, "cores": 0, "kind": "unavailable", "sample": str(ex)[:200]}
         serving = None
         if not args.no_serve:
             sacqs, spools = serving_data(args)
@@ -690,6 +682,16 @@ def run_ours(args, rank, world, local):
         uneven = None
         if not args.no_uneven:
             uneven = measure_uneven(fa, ctx, args)
+        # The CPU baseline last: its 16 host threads and their multi-GB warpers change the host's
+        # memory state, after which the latency-bound lag-1 served stream showed 30-50 ms stalls.
+        cb = None
+        D_cpu = None
+        if not args.no_cpu:
+            try:
+                nt = os.cpu_count() or 1
+                cb, D_cpu, _ = cpu_baseline(acq, nt, args.cpu_frames or min(nt, n))
+            except Exception as ex:  # the baseline is reported, never required
+                cb = {"value": None, "unit": UNIT, "cores": 0, "kind": "unavailable", "sample": str(ex)[:200]}
         rms_vs_cpu = None
         if D_cpu is not None:
             k = D_cpu.shape[0]
