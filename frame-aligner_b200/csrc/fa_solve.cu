@@ -275,18 +275,20 @@ __device__ bool loop_top(FrameState* S, const Band<ND>& B, const double* g, doub
 }  // namespace
 
 // Doubles of shared memory one frame's solve uses when staged: Hessian blocks, band factor,
-// 1/L_ii, two work vectors, g and p.
+// 1/L_ii, two work vectors, g and p, and a copy of the reference's cached factor of H (and its 1/L_ii),
+// which the serial chain of every interior step reads.
 __host__ __device__ inline long long solve_smem_doubles(int nD, int nd) {
   const long long P = (long long)nD * nd;
-  return 2LL * nD * nd * nd + P * 2 * nd + 5 * P;
+  return 2LL * nD * nd * nd + 2 * (P * 2 * nd) + 6 * P;
 }
 
 // The trust-region state machine for one frame after a fused pass at its trial point (thread 0).
 template <int ND>
 __device__ void state_step(const Job& job, FrameState* S, const RefDev& R, const double* Hd, const double* Hl,
-                           double* gv, double* pv, double* work, double ft, double ft2) {
+                           const double* L0, const double* inv0, double* gv, double* pv, double* work, double ft,
+                           double ft2) {
   const int P = R.P, nd = ND;
-  Band<ND> B{Hd, Hl, R.nD, P, R.h_inf, R.h_mindiag, R.L0, R.inv0, R.chol0_ok};
+  Band<ND> B{Hd, Hl, R.nD, P, R.h_inf, R.h_mindiag, L0, inv0, R.chol0_ok};
   double* x = job.x;
   double* g = gv;
   double* p = pv;
@@ -440,6 +442,8 @@ __global__ void __launch_bounds__(kSolveThreads, 1) solve_kernel(const Job* __re
   double* work = job.work;
   double* gv = job.g;
   double* pv = job.p;
+  const double* L0 = R.L0;
+  const double* inv0 = R.inv0;
   if (staged) {
     double* sHd = s_dyn;
     double* sHl = sHd + R.nD * nn;
@@ -458,14 +462,22 @@ __global__ void __launch_bounds__(kSolveThreads, 1) solve_kernel(const Job* __re
     gv = sg;
     pv = sp;
     work = sp + R.P;
+    if (R.L0 != nullptr) {  // after the subproblem's work area (factor, 1/L_ii, two vectors)
+      double* sL0 = work + R.P * 2 * R.n_dim + 3 * R.P;
+      double* sinv0 = sL0 + R.P * 2 * R.n_dim;
+      for (int i = threadIdx.x; i < R.P * 2 * R.n_dim; i += blockDim.x) sL0[i] = R.L0[i];
+      for (int i = threadIdx.x; i < R.P; i += blockDim.x) sinv0[i] = R.inv0[i];
+      L0 = sL0;
+      inv0 = sinv0;
+    }
     __syncthreads();
   }
   const int P = R.P;
   if (threadIdx.x == 0) {
     if (R.n_dim == 3)
-      state_step<3>(job, S, R, Hd, Hl, gv, pv, work, s_f, pair ? s_f2 : 0.0);
+      state_step<3>(job, S, R, Hd, Hl, L0, inv0, gv, pv, work, s_f, pair ? s_f2 : 0.0);
     else
-      state_step<2>(job, S, R, Hd, Hl, gv, pv, work, s_f, pair ? s_f2 : 0.0);
+      state_step<2>(job, S, R, Hd, Hl, L0, inv0, gv, pv, work, s_f, pair ? s_f2 : 0.0);
   }
   __syncthreads();
   if (staged) {
